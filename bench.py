@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Throughput of the keldy QMC hot path on B200: integrand evaluations per second at
+perturbation order 8.
+
+Workload (the batched flat-band configuration): single-level dot, flat-band leads
+Gamma = 1, eps_d = 0, V = 0, beta = 50; g0^<, g0^> tabulated on 40,001 points over
+[-20, 20]; charge observable G^<_{up,up}(t, t) at t = 20; warper chain
+[plasma_uv(20), product-1D exponential(20, 1/Gamma)]; unshifted Sobol points. One step
+= 2^20 Sobol points per GPU through Sobol -> warpers -> Wick-determinant integrand ->
+QMC sum. Synthetic g0 tables built on the host from the model's closed form.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Under torchrun each rank takes its own contiguous block of Sobol indices (weak
+scaling); the per-rank sums are combined with one all_reduce, as keldy's
+integrator::reduce_result does.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
+
+
+def flop_lu(m):
+    """FLOPs of an m x m complex LU with determinant (complex FMA = 8, multiply = 6)."""
+    return 8 * (m - 1) * m * (2 * m - 1) // 6 + 6 * m * (m - 1) // 2 + 6 * (m - 1)
+
+
+def reference_flops(n):
+    """keldy's algorithm: 2^n configurations x (LU(n+1) + LU(n) + product)."""
+    return (1 << n) * (flop_lu(n + 1) + flop_lu(n) + 8)
+
+
+def tree_flops(n):
+    """FLOPs the Schur-complement tree executes per point: per child of a level-k node
+    of size m = 2(n-k)+1, one reciprocal (~8), the prefix product (6), (m-2) scaled
+    pivot entries (6 each) and (m-2)^2 complex FMAs (8 each); per leaf ~34."""
+    total = 0
+    for k in range(n - 1):
+        m = 2 * (n - k) + 1
+        total += (1 << (k + 1)) * (8 + 6 + 6 * (m - 2) + 8 * (m - 2) ** 2)
+    return total + (1 << n) * 34
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = max(mx, float(parts[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[4:8]):
+                if flag.lower() in ("active", "1", "yes"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class CpuReference:
+    """keldy's own integrand (oracle/_ref: wick_direct.cpp, digitalseq_b2g.hpp and the
+    warper headers) on the host cores, on bounded samples of the workload. It picks the
+    faster of keldy's two parallel modes: OpenMP over the Keldysh configurations inside
+    one integrand call (as shipped), or one worker per core keeping every P-th Sobol point
+    (its MPI round robin). Without a built oracle/_ref it times the C restatement."""
+
+    def __init__(self, order, threads=None):
+        import numpy as np  # noqa: F401
+        from keldy_b200.g0_tables import flatband
+        from oracle import pyoracle as po
+        self.order = order
+        self.threads = threads or os.cpu_count() or 1
+        _, le, gr = flatband(GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS)
+        self.A, self.B = (T_MAX, 0, 0, 0, 0), (T_MAX, 0, 1, 0, 0)
+        self.chain = [(po.W_PLASMA_UV, T_MAX, 0.0), (po.W_EXPONENTIAL, T_MAX, 1.0 / GAMMA)]
+        if po.reference_available():
+            self.ref = po.Reference(timed=True)
+            self.model = self.ref.model(T_MAX, le, gr)
+            self.kind = "reference"
+            best = None
+            for mode in (0, 1):
+                n = max(self.threads, 64)
+                dt = self._run(n, mode)
+                if best is None or n / dt > best[1]:
+                    best = (mode, n / dt)
+            self.mode, self.rate = best
+            self.desc = ("keldy wick_direct.cpp + digitalseq_b2g.hpp + warper headers, g++ -O3 -march=x86-64-v3, "
+                         + ("OpenMP over Keldysh configurations" if self.mode == 0
+                            else f"{self.threads} round-robin workers"))
+        else:
+            self.ref = None
+            self.oracle = po.Oracle()
+            self.model = self.oracle.model(T_MAX, le, gr)
+            self.kind = "port"
+            self.threads = 1
+            self.mode = None
+            self.rate = 200 / self._run(200, None)
+            self.desc = "C restatement, 1 thread"
+
+    def _run(self, n, mode):
+        t0 = time.perf_counter()
+        if self.ref is not None:
+            self.ref.integrate(self.model, self.A, self.B, self.chain, self.order, n, mode=mode, threads=self.threads)
+        else:
+            self.oracle.integrate(self.model, self.A, self.B, self.chain, self.order, n)
+        return time.perf_counter() - t0
+
+    def sample_size(self, seconds):
+        return int(max(self.threads * 4, min(1 << 20, self.rate * seconds)))
+
+    def measure(self, n):
+        dt = self._run(n, self.mode)
+        return {"value": n / dt, "unit": "evals/s", "cores": self.threads, "kind": self.kind, "n": n, "seconds": dt,
+                "sample": f"{n} Sobol points of the order-{self.order} workload ({self.desc})"}
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    order = args.order
+    cpu = CpuReference(order)
+    n = cpu.sample_size(args.ref_seconds)
+    for _ in range(args.warmup):
+        cpu.measure(max(cpu.threads, n // 8))
+    res = [cpu.measure(n) for _ in range(args.steps)]
+    pts = sum(r["n"] for r in res)
+    secs = sum(r["seconds"] for r in res)
+    value = pts / secs
+    line = {"metric": f"integrand evals/s at order {order}", "value": value, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": workload_config(order, args.points),
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": res[0]["cores"], "kind": res[0]["kind"],
+                             "sample": res[0]["sample"]},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(order, points):
+    return {"workload": f"flat-band dot Gamma=1 eps_d=0 V=0 beta=50, charge G^<(t=20), g0 {NPTS} points on "
+                        f"[-20,20], chain [plasma_uv(20), exponential(20, 1/Gamma)], order {order}, "
+                        f"{points} Sobol points per GPU per step",
+            "order": order, "points_per_gpu_per_step": points, "g0_points": NPTS, "t": T_MAX, "beta": BETA,
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    from keldy_b200 import capi
+    from keldy_b200.g0_tables import flatband
+
+    order, N = args.order, args.points
+    ctx = capi.Context(local_rank)
+    _, le, gr = flatband(GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS)
+    # pinned host copies of the per-step inputs (end-to-end leg)
+    le_pin = torch.empty(2 * NPTS, dtype=torch.float64, pin_memory=True).numpy()
+    gr_pin = torch.empty(2 * NPTS, dtype=torch.float64, pin_memory=True).numpy()
+    le_pin[:] = le.view(np.float64)
+    gr_pin[:] = gr.view(np.float64)
+    model = ctx.model(T_MAX, le, gr)
+    rng = ctx.sobol(order)
+    chain = [(capi.WARPER_PLASMA_UV, T_MAX, 0.0), (capi.WARPER_EXPONENTIAL, T_MAX, 1.0 / GAMMA)]
+    A, B = (T_MAX, 0, 0, 0, 0), (T_MAX, 0, 1, 0, 0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    peak = ctx.fp64_peak()
+
+    def item(step, mdl=model):
+        k_first = 1 + ((step * world + rank) * N) % ((1 << 31) - N - 1)
+        return dict(model=mdl, rng=rng, chain=chain, A=A, B=B, order=order, k_first=k_first, n_points=N)
+
+    def allreduce(res):
+        if world == 1:
+            return res
+        import torch.distributed as dist
+        t = torch.tensor([res[0][0].real, res[0][0].imag, res[0][1], res[0][2]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t)
+        return [(complex(t[0].item(), t[1].item()), int(t[2].item()), int(t[3].item()), res[0][3])]
+
+    ctx.set_timing(True)
+    for s in range(args.warmup):
+        allreduce(capi.integrate(ctx, [item(s)]))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    barrier()
+    dev_ms, integ_ms, launches, in_domain, fallback = 0.0, 0.0, 0, 0, 0
+    for s in range(args.steps):
+        flush.fill_(s & 0xFF)
+        torch.cuda.synchronize()
+        res = allreduce(capi.integrate(ctx, [item(args.warmup + s)]))
+        a, b, c, n = ctx.last_timing()
+        dev_ms += a + b + c
+        integ_ms += a
+        launches += n
+        in_domain += res[0][2]
+        fallback += res[0][3]
+    barrier()
+    clocks = sampler.stop()
+    # end to end through the public API with host buffers: per step, upload the g0
+    # tables from pinned memory, integrate, read the sums back
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        m2 = capi.Model(ctx, T_MAX, le_pin.view(np.complex128), gr_pin.view(np.complex128))
+        allreduce(capi.integrate(ctx, [item(args.warmup + args.steps + s, m2)]))
+        del m2
+    barrier()
+    e2e_s = time.perf_counter() - t0
+
+    t_max_ms = dev_ms
+    e2e_max = e2e_s
+    integ_max = integ_ms
+    if world > 1:
+        import torch.distributed as dist
+        v = torch.tensor([dev_ms, e2e_s, integ_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(v, op=dist.ReduceOp.MAX)
+        t_max_ms, e2e_max, integ_max = v.tolist()
+
+    total_points = world * N * args.steps
+    value = total_points / (t_max_ms * 1e-3)
+    line = None
+    if rank == 0:
+        # batched launch: orders 1..10, 2^20 points each, one kb_integrate call
+        rngs = {n: ctx.sobol(n) for n in range(1, 11)}
+        batch = [dict(model=model, rng=rngs[n], chain=chain, A=A, B=B, order=n, k_first=1, n_points=1 << 20)
+                 for n in range(1, 11)]
+        capi.integrate(ctx, batch)
+        torch.cuda.synchronize()
+        bt = []
+        for _ in range(2):
+            capi.integrate(ctx, batch)
+            bt.append(sum(ctx.last_timing()[:3]))
+        b_ms = min(bt)
+        b_ref_flop = sum(reference_flops(n) << 20 for n in range(1, 11))
+        ref_flop_launch = N * reference_flops(order)
+        achieved = ref_flop_launch / (integ_max * 1e-3 / args.steps)
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cref = CpuReference(order)
+            cpu = cref.measure(cref.sample_size(10.0))
+        h2d = 2 * NPTS * 16 + 8 * 1024
+        line = {
+            "metric": f"integrand evals/s at order {order}", "value": value, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(order, N),
+            "e2e": {"value": total_points / e2e_max, "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": 40},
+            "gpu_launches": launches,
+            "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "numerator": f"reference-equivalent: {reference_flops(order)} FLOP per evaluation "
+                                      f"(keldy's 2^n LU pairs); the tree executes ~{tree_flops(order)}",
+                         "peak_source": "FP64 FMA rate measured in this run (kb_fp64_peak, 8 independent "
+                                        "chains per thread); MEASURED_PEAKS.json has no FP64 figure",
+                         "executed_tflops": N * tree_flops(order) / (integ_max * 1e-3 / args.steps) / 1e12,
+                         "kernel_ms": integ_max / args.steps},
+            "in_domain_evals_per_s": in_domain / (t_max_ms * 1e-3),
+            "fallback_points": fallback,
+            "batched_orders_1_10": {"ms": b_ms, "evals_per_s": 10 * (1 << 20) / (b_ms * 1e-3),
+                                    "reference_equivalent_tflops": b_ref_flop / (b_ms * 1e-3) / 1e12},
+            "clocks": clocks,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--order", type=int, default=8)
+    ap.add_argument("--points", type=int, default=1 << 20)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--ref-seconds", type=float, default=2.0, help="seconds of CPU work per reference-arm step")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

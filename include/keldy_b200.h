@@ -1,0 +1,193 @@
+/*
+ * keldy_b200 C ABI: the boundary between keldy's host classes and the sm_100a kernels.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes. Every function
+ * returns KB_OK (0) or a negative KB_E* code; kb_last_error() gives the message of the
+ * calling thread's last failure. Host-pointer entry points copy their inputs to the
+ * device, run on the context's CUDA stream and copy results back before returning;
+ * the *_dev entry points take device pointers and only enqueue work on the stream.
+ *
+ * Each entry point names the keldy interface it replaces (paths relative to keldy's
+ * c++/keldy/ source tree).
+ */
+#ifndef KELDY_B200_H
+#define KELDY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KB_OK 0
+#define KB_E_INVALID -1   /* bad argument (keldy raises TRIQS_RUNTIME_ERROR for these) */
+#define KB_E_CUDA -2      /* a CUDA call failed */
+#define KB_E_NOMEM -3     /* device or host allocation failed */
+#define KB_E_RANGE -4     /* g0 evaluated outside its tabulated window */
+#define KB_E_EXHAUSTED -5 /* Sobol generator past its last point */
+#define KB_E_NODEVICE -6  /* no CUDA device: the library has no CPU path */
+
+typedef struct kb_context kb_context;
+typedef struct kb_model kb_model;
+typedef struct kb_sobol kb_sobol;
+
+/* ---------------------------------------------------------------- context --- */
+const char *kb_last_error(void);
+int kb_version(void);
+/* One context per device: a CUDA stream plus reusable device buffers. */
+int kb_context_create(int device, kb_context **out);
+int kb_context_destroy(kb_context *ctx);
+int kb_context_synchronize(kb_context *ctx);
+/* The context's CUDA stream, as a cudaStream_t cast to void*. */
+void *kb_context_stream(kb_context *ctx);
+/* Kernel timing (measurement aid, off by default): when enabled, kb_integrate brackets
+ * its integrand, pivoted-LU and reduction launches with CUDA events on the context's
+ * stream; kb_context_last_timing returns the last call's times in milliseconds
+ * (summed over its launch groups). */
+int kb_context_set_timing(kb_context *ctx, int enable);
+int kb_context_last_timing(kb_context *ctx, double *integrand_ms, double *fallback_ms, double *reduce_ms,
+                           int *launches);
+
+/* ------------------------------------------------------------------ Sobol --- */
+/* keldy::sobol(dim, seed, do_shift, do_scramble, seed_shift, log_max_points)
+ * (qrng.hpp:77-109; the unshifted qrng.hpp:69-75 is do_shift = do_scramble = 0).
+ * Generating matrices of the Joe-Kuo 2008 sequence, optional random digital shift and
+ * linear scramble from std::mt19937_64(seed_shift). The generator state (the index of
+ * the last point drawn) stays with the caller: point number k (k >= 1) is the point
+ * digitalseq_b2g::next() returns when its counter becomes k. */
+int kb_sobol_create(kb_context *ctx, int dim, int log_max_points, int do_shift, int do_scramble, int seed_shift,
+                    kb_sobol **out);
+int kb_sobol_destroy(kb_sobol *s);
+/* Host only (no device needed): the generator's bit-reversed generating matrices
+ * Csr[dim * log_max_points] and shift vector shfr[dim], in digitalseq_b2g's Csr/shfr
+ * layout (digitalseq_b2g.hpp:307-312, 486-513; qmc::JK2008_sobol_matrices and
+ * qmc::scramble, digitalseq_b2g.hpp:178-186, 598-861). */
+int kb_sobol_matrices(int dim, int log_max_points, int do_shift, int do_scramble, int seed_shift, uint32_t *Csr,
+                      uint32_t *shfr);
+/* Points k_first .. k_first+count-1, row-major [count][dim] doubles
+ * (replaces digitalseq_b2g::next/set_state, digitalseq_b2g.hpp:415-471, and
+ * sobol::operator()/seed/discard, qrng.hpp:51-67). KB_E_EXHAUSTED past 2^log_max_points - 1. */
+int kb_sobol_points(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out);
+int kb_sobol_points_dev(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out_dev);
+
+/* ---------------------------------------------------------------- warpers --- */
+#define KB_WARPER_IDENTITY 0       /* warper_identity_t (warpers/identity.hpp:30-49) */
+#define KB_WARPER_PLASMA_UV 1      /* warper_plasma_uv_t(t_max) (warpers/plasma_uv.hpp:55-81) */
+#define KB_WARPER_EXPONENTIAL 2    /* make_product_1d_simple_exponential(u_max, w) (product_1d_simple.hpp:560-576) */
+#define KB_WARPER_INVERSE 3        /* make_product_1d_simple_inverse(u_max, w) (:578-592) */
+#define KB_WARPER_INVERSE_SQUARE 4 /* make_product_1d_simple_inverse_square(u_max, w) (:594-608) */
+#define KB_WARPER_INVERSE_POWER 5  /* make_product_1d_simple_inverse_power(power, u_max, w) (:610-630) */
+#define KB_WARPER_UNIFORM 6        /* warper_product_1d_simple_t with f1 = 1/u_max (product_1d_simple_test.cpp:10-23) */
+#define KB_MAX_CHAIN 8
+
+typedef struct {
+  int kind;
+  int power;    /* KB_WARPER_INVERSE_POWER only */
+  double u_max; /* domain_u_max, or t_max for the plasma warper */
+  double w;     /* w_scale of the product makers */
+} kb_warper;
+
+/* warper_train_t::map_reverse(li, start, end) (warpers.hpp:72-85; direction 0) or
+ * map_forward(ui, start, end) (warpers.hpp:88-101; direction 1) on count points of n
+ * coordinates each. Warpers are applied last-to-first in reverse, first-to-last
+ * forward. jac may be NULL (ui_from_li / li_from_ui). */
+#define KB_REVERSE 0
+#define KB_FORWARD 1
+int kb_warp(kb_context *ctx, const kb_warper *chain, int chain_len, int direction, int start, int end, int n,
+            int64_t count, const double *in, double *out, double *jac);
+
+/* ---------------------------------------------------------------- g0 model --- */
+/* g0 tables on the uniform mesh t_i = -time_max + i*2*time_max/(npts-1), i < npts
+ * (keldy's g0_model::g0_lesser / g0_greater, model.hpp:183-190): complex values as
+ * interleaved (re, im) doubles. One table pair per (spin, orbital a, orbital b); the
+ * Keldysh adaptor (model.hpp:244-265) picks lesser or greater by contour order. */
+int kb_model_create(kb_context *ctx, int npts, double time_max, double alpha, kb_model **out);
+int kb_model_destroy(kb_model *m);
+/* Upload the (spin, o1, o2) block; lesser/greater: npts interleaved complex values. */
+int kb_model_set_table(kb_model *m, int spin, int o1, int o2, const double *lesser, const double *greater);
+/* Same from device memory. */
+int kb_model_set_table_dev(kb_model *m, int spin, int o1, int o2, const double *lesser_dev,
+                           const double *greater_dev);
+
+/* A point of the Keldysh contour with spin and orbital: keldy's gf_index_t (model.hpp:55-78). */
+typedef struct {
+  double time;
+  int spin;      /* 0 = up, 1 = down */
+  int k_idx;     /* 0 = forward, 1 = backward */
+  int timesplit; /* orders equal-time points */
+  int orbital;
+} kb_gf_index;
+
+/* g0_keldysh_contour_t::operator()(a[i], b[i], internal[i]) (model.hpp:244-265);
+ * out: count interleaved complex values. internal may be NULL (all true). */
+int kb_g0_eval(kb_context *ctx, const kb_model *m, const kb_gf_index *a, const kb_gf_index *b, const int *internal,
+               int64_t count, double *out);
+
+/* ------------------------------------------------------------- integrand --- */
+/* integrand_g_direct(g0, external_A, external_B, cutoff) (wick_direct.hpp:34-65). */
+typedef struct {
+  kb_gf_index A;
+  kb_gf_index B;
+  double cutoff;
+} kb_integrand;
+
+#define KB_ALGO_AUTO 0   /* Schur-complement tree, pivoted per-configuration LU where the tree cannot run */
+#define KB_ALGO_TREE 1   /* Schur-complement tree over the Keldysh bits */
+#define KB_ALGO_DIRECT 2 /* one partial-pivot LU pair per Keldysh configuration (keldy's own algorithm) */
+
+/* integrand_g_direct::operator()(times, keep_u_hypercube) (wick_direct.cpp:43-158) on
+ * count time vectors of `order` entries. out: interleaved complex; in_domain: int per
+ * point; scale (optional, may be NULL): sum over Keldysh configurations of
+ * |det up * det down| (error scale of the alternating sum). */
+int kb_integrand_eval(kb_context *ctx, const kb_model *m, const kb_integrand *f, int order, int64_t count,
+                      const double *times, int keep_u_hypercube, int algo, double *out, int *in_domain,
+                      double *scale);
+/* integrand_g_direct::eval_no_det (wick_direct.cpp:161-228), orders 0..2. */
+int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integrand *f, int order, int64_t count,
+                             const double *times, int keep_u_hypercube, double *out, int *in_domain);
+
+/* integrator::evaluate_warped_integrand(li, start_domain_nr, keep_u_hypercube)
+ * (integrator.hpp:68-79): out = f(map_reverse(li, start, 0)) * J as interleaved
+ * complex; jac (optional): J; in_domain: int per point. */
+int kb_evaluate_warped(kb_context *ctx, const kb_model *m, const kb_integrand *f, const kb_warper *chain,
+                       int chain_len, int start_domain_nr, int order, int64_t count, const double *li,
+                       int keep_u_hypercube, int algo, double *out, double *jac, int *in_domain);
+
+/* ------------------------------------------------------------- integrator --- */
+/* Running sums of integrator::run (integrator.hpp:50-52). */
+typedef struct {
+  double sum_re;        /* sum of f*J */
+  double sum_im;
+  uint64_t n_points;    /* points run */
+  uint64_t n_in_domain; /* integrand evaluations in domain */
+  uint64_t n_fallback;  /* points the tree handed to the pivoted-LU kernel (guarded pivots) */
+} kb_accum;
+
+/* One unit of QMC work: `n_points` Sobol points k_first.. of `rng` through `chain` into
+ * the integrand of `order` on model `m`. */
+typedef struct {
+  const kb_model *m;
+  const kb_sobol *rng;
+  const kb_warper *chain;
+  int chain_len;
+  kb_integrand f;
+  int order;
+  uint32_t k_first;
+  int64_t n_points;
+} kb_work;
+
+/* integrator::run(nr_steps) (integrator.hpp:81-95) for every work item, summed into
+ * acc[i] (acc is added to, not overwritten). All items run in one batched launch
+ * sequence on the context's stream; sums are deterministic (fixed reduction order). */
+int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc);
+
+/* ----------------------------------------------------------------- peaks --- */
+/* Measures the FP64 FMA rate of this device (FLOP/s, 2 per FMA) with a dependent-chain
+ * kernel of `iters` FMAs per thread; used as the roofline denominator. */
+int kb_fp64_peak(kb_context *ctx, int iters, double *flops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KELDY_B200_H */

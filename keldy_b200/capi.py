@@ -1,0 +1,337 @@
+"""ctypes binding of the keldy_b200 C ABI (include/keldy_b200.h).
+
+This is the thinnest way into the library: plain pointers and sizes, numpy arrays on
+the Python side. Every call runs on the GPU; there is no CPU path, and loading the
+library or creating a context fails loudly when the shared library or a CUDA device is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libkeldy_b200.so")
+
+KB_OK = 0
+KB_E_INVALID, KB_E_CUDA, KB_E_NOMEM, KB_E_RANGE, KB_E_EXHAUSTED, KB_E_NODEVICE = -1, -2, -3, -4, -5, -6
+
+WARPER_IDENTITY, WARPER_PLASMA_UV, WARPER_EXPONENTIAL, WARPER_INVERSE = 0, 1, 2, 3
+WARPER_INVERSE_SQUARE, WARPER_INVERSE_POWER, WARPER_UNIFORM = 4, 5, 6
+MAX_CHAIN = 8
+REVERSE, FORWARD = 0, 1
+ALGO_AUTO, ALGO_TREE, ALGO_DIRECT = 0, 1, 2
+
+# every symbol include/keldy_b200.h declares
+EXPORTS = [
+    "kb_last_error", "kb_version", "kb_context_create", "kb_context_destroy", "kb_context_synchronize",
+    "kb_context_stream", "kb_context_set_timing", "kb_context_last_timing", "kb_sobol_create", "kb_sobol_destroy", "kb_sobol_matrices", "kb_sobol_points",
+    "kb_sobol_points_dev",
+    "kb_warp", "kb_model_create", "kb_model_destroy", "kb_model_set_table", "kb_model_set_table_dev",
+    "kb_g0_eval", "kb_integrand_eval", "kb_integrand_eval_no_det", "kb_evaluate_warped", "kb_integrate",
+    "kb_fp64_peak",
+]
+
+
+class KbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class Warper(C.Structure):
+    _fields_ = [("kind", C.c_int), ("power", C.c_int), ("u_max", C.c_double), ("w", C.c_double)]
+
+
+class GfIndex(C.Structure):
+    _fields_ = [("time", C.c_double), ("spin", C.c_int), ("k_idx", C.c_int), ("timesplit", C.c_int),
+                ("orbital", C.c_int)]
+
+
+class Integrand(C.Structure):
+    _fields_ = [("A", GfIndex), ("B", GfIndex), ("cutoff", C.c_double)]
+
+
+class Accum(C.Structure):
+    _fields_ = [("sum_re", C.c_double), ("sum_im", C.c_double), ("n_points", C.c_uint64),
+                ("n_in_domain", C.c_uint64), ("n_fallback", C.c_uint64)]
+
+
+class Work(C.Structure):
+    _fields_ = [("m", C.c_void_p), ("rng", C.c_void_p), ("chain", C.POINTER(Warper)), ("chain_len", C.c_int),
+                ("f", Integrand), ("order", C.c_int), ("k_first", C.c_uint32), ("n_points", C.c_int64)]
+
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_VP = C.c_void_p
+_lib = None
+
+
+def load():
+    """The library handle; raises if libkeldy_b200.so has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m keldy_b200.build` "
+                          "(keldy_b200 has no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    L.kb_last_error.restype = C.c_char_p
+    L.kb_context_create.argtypes = [C.c_int, C.POINTER(_VP)]
+    L.kb_context_destroy.argtypes = [_VP]
+    L.kb_context_synchronize.argtypes = [_VP]
+    L.kb_context_stream.argtypes = [_VP]
+    L.kb_context_stream.restype = _VP
+    L.kb_context_set_timing.argtypes = [_VP, C.c_int]
+    L.kb_context_last_timing.argtypes = [_VP, _D, _D, _D, _I]
+    L.kb_sobol_create.argtypes = [_VP, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_VP)]
+    L.kb_sobol_destroy.argtypes = [_VP]
+    L.kb_sobol_matrices.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]
+    L.kb_sobol_points.argtypes = [_VP, _VP, C.c_uint32, C.c_int64, _D]
+    L.kb_sobol_points_dev.argtypes = [_VP, _VP, C.c_uint32, C.c_int64, _VP]
+    L.kb_warp.argtypes = [_VP, C.POINTER(Warper), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64, _D, _D,
+                          _D]
+    L.kb_model_create.argtypes = [_VP, C.c_int, C.c_double, C.c_double, C.POINTER(_VP)]
+    L.kb_model_destroy.argtypes = [_VP]
+    L.kb_model_set_table.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D]
+    L.kb_model_set_table_dev.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _VP, _VP]
+    L.kb_g0_eval.argtypes = [_VP, _VP, C.POINTER(GfIndex), C.POINTER(GfIndex), _I, C.c_int64, _D]
+    L.kb_integrand_eval.argtypes = [_VP, _VP, C.POINTER(Integrand), C.c_int, C.c_int64, _D, C.c_int, C.c_int, _D,
+                                    _I, _D]
+    L.kb_integrand_eval_no_det.argtypes = [_VP, _VP, C.POINTER(Integrand), C.c_int, C.c_int64, _D, C.c_int, _D,
+                                           _I]
+    L.kb_evaluate_warped.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, C.c_int, C.c_int,
+                                     C.c_int64, _D, C.c_int, C.c_int, _D, _D, _I]
+    L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
+    L.kb_fp64_peak.argtypes = [_VP, C.c_int, _D]
+    _lib = L
+    return L
+
+
+def check(code):
+    if code != KB_OK:
+        raise KbError(code, load().kb_last_error().decode())
+
+
+def sobol_matrices(dim, log_max_points=31, do_shift=False, do_scramble=False, seed_shift=0):
+    """Host-only: (Csr[dim, m], shfr[dim]) as keldy::sobol would build them."""
+    L = load()
+    Csr = np.zeros(dim * log_max_points, dtype=np.uint32)
+    shfr = np.zeros(dim, dtype=np.uint32)
+    U = C.POINTER(C.c_uint32)
+    check(L.kb_sobol_matrices(dim, log_max_points, int(do_shift), int(do_scramble), int(seed_shift),
+                              Csr.ctypes.data_as(U), shfr.ctypes.data_as(U)))
+    return Csr.reshape(dim, log_max_points), shfr
+
+
+def _dp(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def _ip(a):
+    return None if a is None else a.ctypes.data_as(_I)
+
+
+def chain_array(chain):
+    """chain: list of (kind, u_max, w[, power]) -> (ctypes array, length)."""
+    arr = (Warper * MAX_CHAIN)()
+    for i, c in enumerate(chain):
+        arr[i] = Warper(int(c[0]), int(c[3]) if len(c) > 3 else 0, float(c[1]), float(c[2]))
+    return arr, len(chain)
+
+
+def gf_index(x):
+    if isinstance(x, GfIndex):
+        return x
+    t = tuple(x) + (0,) * (5 - len(x))
+    return GfIndex(float(t[0]), int(t[1]), int(t[2]), int(t[3]), int(t[4]))
+
+
+class Context:
+    """One CUDA device: a stream plus the library's bookkeeping."""
+
+    def __init__(self, device=0):
+        L = load()
+        h = _VP()
+        check(L.kb_context_create(device, C.byref(h)))
+        self.h = h
+        self.L = L
+
+    def close(self):
+        if self.h:
+            self.L.kb_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self):
+        return self.L.kb_context_stream(self.h)
+
+    def synchronize(self):
+        check(self.L.kb_context_synchronize(self.h))
+
+    def set_timing(self, enable=True):
+        check(self.L.kb_context_set_timing(self.h, int(enable)))
+
+    def last_timing(self):
+        """(integrand_ms, fallback_ms, reduce_ms, launches) of the last kb_integrate."""
+        a, b, c, n = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        check(self.L.kb_context_last_timing(self.h, C.byref(a), C.byref(b), C.byref(c), C.byref(n)))
+        return a.value, b.value, c.value, n.value
+
+    def fp64_peak(self, iters=1 << 16):
+        v = C.c_double()
+        check(self.L.kb_fp64_peak(self.h, iters, C.byref(v)))
+        return v.value
+
+    # --- Sobol -------------------------------------------------------------
+    def sobol(self, dim, log_max_points=31, do_shift=False, do_scramble=False, seed_shift=0):
+        return Sobol(self, dim, log_max_points, do_shift, do_scramble, seed_shift)
+
+    # --- warpers -----------------------------------------------------------
+    def warp(self, chain, x, direction=REVERSE, start=None, end=None, want_jac=True):
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        count, n = x.shape
+        arr, L = chain_array(chain)
+        if direction == REVERSE:
+            start = L if start is None else start
+            end = 0 if end is None else end
+        else:
+            start = 0 if start is None else start
+            end = L if end is None else end
+        out = np.empty_like(x)
+        jac = np.empty(count) if want_jac else None
+        check(self.L.kb_warp(self.h, arr, L, direction, start, end, n, count, _dp(x), _dp(out), _dp(jac)))
+        return out, jac
+
+    # --- model ---------------------------------------------------------------
+    def model(self, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None, blocks=None):
+        return Model(self, time_max, lesser, greater, alpha, lesser_down, greater_down, blocks)
+
+
+class Sobol:
+    def __init__(self, ctx, dim, log_max_points=31, do_shift=False, do_scramble=False, seed_shift=0):
+        self.ctx = ctx
+        self.dim = dim
+        self.m = log_max_points
+        h = _VP()
+        check(ctx.L.kb_sobol_create(ctx.h, dim, log_max_points, int(do_shift), int(do_scramble), int(seed_shift),
+                                    C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        try:
+            self.ctx.L.kb_sobol_destroy(self.h)
+        except Exception:
+            pass
+
+    def points(self, k_first, count):
+        out = np.empty((count, self.dim))
+        check(self.ctx.L.kb_sobol_points(self.ctx.h, self.h, k_first, count, _dp(out)))
+        return out
+
+
+class Model:
+    """g0 tables (complex arrays on [-time_max, time_max]) uploaded to the device."""
+
+    def __init__(self, ctx, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None, blocks=None):
+        self.ctx = ctx
+        lesser = np.ascontiguousarray(lesser, dtype=np.complex128)
+        greater = np.ascontiguousarray(greater, dtype=np.complex128)
+        self.npts = len(lesser)
+        self.time_max = time_max
+        h = _VP()
+        check(ctx.L.kb_model_create(ctx.h, self.npts, float(time_max), float(alpha), C.byref(h)))
+        self.h = h
+        self.set_table(0, 0, 0, lesser, greater)
+        if lesser_down is not None:
+            self.set_table(1, 0, 0, lesser_down, greater_down)
+        for (spin, o1, o2), (le, gr) in (blocks or {}).items():
+            self.set_table(spin, o1, o2, le, gr)
+
+    def set_table(self, spin, o1, o2, lesser, greater):
+        le = np.ascontiguousarray(lesser, dtype=np.complex128).view(np.float64)
+        gr = np.ascontiguousarray(greater, dtype=np.complex128).view(np.float64)
+        assert le.size == 2 * self.npts and gr.size == 2 * self.npts
+        check(self.ctx.L.kb_model_set_table(self.h, spin, o1, o2, _dp(le), _dp(gr)))
+
+    def __del__(self):
+        try:
+            self.ctx.L.kb_model_destroy(self.h)
+        except Exception:
+            pass
+
+    def g0(self, a, b, internal=None):
+        a = list(a)
+        b = list(b)
+        count = len(a)
+        A = (GfIndex * count)(*[gf_index(x) for x in a])
+        B = (GfIndex * count)(*[gf_index(x) for x in b])
+        inte = None if internal is None else np.ascontiguousarray(internal, dtype=np.int32)
+        out = np.empty(count, dtype=np.complex128)
+        check(self.ctx.L.kb_g0_eval(self.ctx.h, self.h, A, B, _ip(inte), count, _dp(out.view(np.float64))))
+        return out
+
+    def integrand(self, A, B, times, cutoff=0.0, keep_u_hypercube=True, algo=ALGO_AUTO, want_scale=False,
+                  order=None):
+        times = np.ascontiguousarray(times, dtype=np.float64)
+        if times.ndim == 1:
+            times = times[None, :] if order is None or order > 0 else times.reshape(-1, 0)
+        count, n = times.shape
+        f = Integrand(gf_index(A), gf_index(B), float(cutoff))
+        out = np.empty(count, dtype=np.complex128)
+        dom = np.empty(count, dtype=np.int32)
+        sc = np.empty(count) if want_scale else None
+        check(self.ctx.L.kb_integrand_eval(self.ctx.h, self.h, C.byref(f), n, count, _dp(times),
+                                           int(keep_u_hypercube), algo, _dp(out.view(np.float64)), _ip(dom),
+                                           _dp(sc)))
+        return (out, dom, sc) if want_scale else (out, dom)
+
+    def integrand_no_det(self, A, B, times, cutoff=0.0, keep_u_hypercube=True):
+        times = np.ascontiguousarray(np.atleast_2d(times), dtype=np.float64)
+        count, n = times.shape
+        f = Integrand(gf_index(A), gf_index(B), float(cutoff))
+        out = np.empty(count, dtype=np.complex128)
+        dom = np.empty(count, dtype=np.int32)
+        check(self.ctx.L.kb_integrand_eval_no_det(self.ctx.h, self.h, C.byref(f), n, count, _dp(times),
+                                                  int(keep_u_hypercube), _dp(out.view(np.float64)), _ip(dom)))
+        return out, dom
+
+    def evaluate_warped(self, A, B, chain, li, cutoff=0.0, start=None, keep_u_hypercube=True, algo=ALGO_AUTO):
+        li = np.ascontiguousarray(np.atleast_2d(li), dtype=np.float64)
+        count, n = li.shape
+        arr, L = chain_array(chain)
+        f = Integrand(gf_index(A), gf_index(B), float(cutoff))
+        out = np.empty(count, dtype=np.complex128)
+        jac = np.empty(count)
+        dom = np.empty(count, dtype=np.int32)
+        check(self.ctx.L.kb_evaluate_warped(self.ctx.h, self.h, C.byref(f), arr, L, L if start is None else start, n,
+                                            count, _dp(li), int(keep_u_hypercube), algo, _dp(out.view(np.float64)),
+                                            _dp(jac), _ip(dom)))
+        return out, jac, dom
+
+
+def integrate(ctx, items, algo=ALGO_AUTO):
+    """items: list of dicts {model, rng, chain, A, B, cutoff, order, k_first, n_points}.
+    Returns a list of (sum f*J, n_points, n_in_domain, n_fallback)."""
+    n = len(items)
+    works = (Work * n)()
+    keep = []
+    for i, it in enumerate(items):
+        arr, L = chain_array(it["chain"])
+        keep.append(arr)
+        works[i] = Work(it["model"].h.value, it["rng"].h.value, C.cast(arr, C.POINTER(Warper)), L,
+                        Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
+                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]))
+    acc = (Accum * n)()
+    check(ctx.L.kb_integrate(ctx.h, works, n, algo, acc))
+    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback) for a in acc]

@@ -1,0 +1,800 @@
+// C ABI of keldy_b200 (declared in include/keldy_b200.h): argument checks, device
+// memory, and the launch sequences of the kernels in tree.cu / misc_kernels.cu.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "kb_launch.h"
+#include "kb_types.h"
+
+namespace kb {
+void sobol_setup(int dim, int m, bool do_shift, bool do_scramble, int seed_shift, uint32_t *Csr, uint32_t *shfr);
+}
+
+using namespace kb;
+
+// ------------------------------------------------------------------ errors
+namespace {
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define KB_CUDA(call)                                                                                        \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess) return fail(KB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
+  } while (0)
+
+#define KB_CHECK(cond, msg)                                                                                  \
+  do {                                                                                                       \
+    if (!(cond)) return fail(KB_E_INVALID, msg);                                                            \
+  } while (0)
+
+// Stream-ordered device buffer released at scope exit (on the same stream).
+struct DevBuf {
+  void *p = nullptr;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  cudaError_t alloc(size_t bytes, cudaStream_t s) {
+    st = s;
+    return cudaMallocAsync(&p, bytes ? bytes : 16, s);
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+uint64_t fnv1a(const void *data, size_t n) {
+  const unsigned char *c = static_cast<const unsigned char *>(data);
+  uint64_t h = 1469598103934665603ULL;
+  for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ULL;
+  return h;
+}
+} // namespace
+
+struct kb_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  int tree_grid = 0;
+  int *d_err = nullptr; // error flags written by kernels
+  bool timing = false;
+  cudaEvent_t ev[4] = {};
+  double last_ms[3] = {0, 0, 0};
+  int last_launches = 0;
+  std::mutex mu;
+};
+
+struct kb_model {
+  kb_context *ctx = nullptr;
+  int npts = 0;
+  double tmax = 0, alpha = 0;
+  double2 *tab[2][2][2] = {};
+  uint64_t hash[2][2][2] = {}; // 0 = unknown (device upload)
+  double tabmax = 0;
+};
+
+struct kb_sobol {
+  kb_context *ctx = nullptr;
+  int dim = 0, m = 0;
+  uint32_t *d_Csr = nullptr;
+  uint32_t *d_shfr = nullptr;
+};
+
+extern "C" {
+
+const char *kb_last_error(void) { return g_last_error.c_str(); }
+
+int kb_version(void) { return 100; }
+
+int kb_context_create(int device, kb_context **out) {
+  KB_CHECK(out, "kb_context_create: out is NULL");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(KB_E_NODEVICE, "keldy_b200 needs a CUDA device and found none (" +
+                                   std::string(cudaGetErrorString(e)) + "); the library has no CPU path");
+  KB_CHECK(device >= 0 && device < n, "kb_context_create: device index out of range");
+  KB_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  KB_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return fail(KB_E_NODEVICE, std::string("keldy_b200 is built for sm_100a; device is ") + prop.name);
+  auto *ctx = new kb_context;
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return fail(KB_E_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  }
+  e = cudaMalloc(&ctx->d_err, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(int));
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return fail(KB_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  // Persistent tree kernel: as many CTAs as fit on the device at once.
+  int per_sm = 2;
+  ctx->tree_grid = ctx->sm_count * per_sm;
+  *out = ctx;
+  return KB_OK;
+}
+
+int kb_context_destroy(kb_context *ctx) {
+  if (!ctx) return KB_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  cudaFree(ctx->d_err);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return KB_OK;
+}
+
+int kb_context_synchronize(kb_context *ctx) {
+  KB_CHECK(ctx, "null context");
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return KB_OK;
+}
+
+void *kb_context_stream(kb_context *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int kb_context_set_timing(kb_context *ctx, int enable) {
+  KB_CHECK(ctx, "null context");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  if (enable && !ctx->ev[0])
+    for (auto &e : ctx->ev) KB_CUDA(cudaEventCreate(&e));
+  ctx->timing = enable != 0;
+  return KB_OK;
+}
+
+int kb_context_last_timing(kb_context *ctx, double *integrand_ms, double *fallback_ms, double *reduce_ms,
+                           int *launches) {
+  KB_CHECK(ctx, "null context");
+  if (integrand_ms) *integrand_ms = ctx->last_ms[0];
+  if (fallback_ms) *fallback_ms = ctx->last_ms[1];
+  if (reduce_ms) *reduce_ms = ctx->last_ms[2];
+  if (launches) *launches = ctx->last_launches;
+  return KB_OK;
+}
+
+// ------------------------------------------------------------------ Sobol
+int kb_sobol_create(kb_context *ctx, int dim, int log_max_points, int do_shift, int do_scramble, int seed_shift,
+                    kb_sobol **out) {
+  KB_CHECK(ctx && out, "kb_sobol_create: null argument");
+  KB_CHECK(dim >= 1 && dim <= 250, "Sobol dimension must be in [1, 250]");
+  if (log_max_points > 31) return fail(KB_E_INVALID, "To many points requested from Sobol generator.");
+  KB_CHECK(log_max_points >= 1, "log_max_points must be >= 1");
+  std::vector<uint32_t> Csr(static_cast<size_t>(dim) * log_max_points), shfr(static_cast<size_t>(dim));
+  sobol_setup(dim, log_max_points, do_shift != 0, do_scramble != 0, seed_shift, Csr.data(), shfr.data());
+  auto *s = new kb_sobol;
+  s->ctx = ctx;
+  s->dim = dim;
+  s->m = log_max_points;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaMalloc(&s->d_Csr, Csr.size() * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&s->d_shfr, shfr.size() * sizeof(uint32_t));
+  if (e == cudaSuccess) e = cudaMemcpy(s->d_Csr, Csr.data(), Csr.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->d_shfr, shfr.data(), shfr.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(s->d_Csr);
+    cudaFree(s->d_shfr);
+    delete s;
+    return fail(KB_E_CUDA, std::string("kb_sobol_create: ") + cudaGetErrorString(e));
+  }
+  *out = s;
+  return KB_OK;
+}
+
+int kb_sobol_matrices(int dim, int log_max_points, int do_shift, int do_scramble, int seed_shift, uint32_t *Csr,
+                      uint32_t *shfr) {
+  KB_CHECK(Csr && shfr, "kb_sobol_matrices: null argument");
+  KB_CHECK(dim >= 1 && dim <= 250, "Sobol dimension must be in [1, 250]");
+  if (log_max_points > 31) return fail(KB_E_INVALID, "To many points requested from Sobol generator.");
+  KB_CHECK(log_max_points >= 1, "log_max_points must be >= 1");
+  sobol_setup(dim, log_max_points, do_shift != 0, do_scramble != 0, seed_shift, Csr, shfr);
+  return KB_OK;
+}
+
+int kb_sobol_destroy(kb_sobol *s) {
+  if (!s) return KB_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaFree(s->d_Csr);
+  cudaFree(s->d_shfr);
+  delete s;
+  return KB_OK;
+}
+
+static SobolDev sobol_dev(const kb_sobol *s) {
+  SobolDev d;
+  d.Csr = s->d_Csr;
+  d.shfr = s->d_shfr;
+  d.dim = s->dim;
+  d.m = s->m;
+  return d;
+}
+
+static int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count) {
+  if (k_first < 1) return fail(KB_E_INVALID, "Sobol point index must be >= 1 (first draw of sobol(dim, seed) is seed+1)");
+  uint64_t last = (uint64_t)k_first + (uint64_t)(count > 0 ? count - 1 : 0);
+  if (count > 0 && last >= (1ull << s->m))
+    return fail(KB_E_EXHAUSTED, "More sample points requested then generator can hold.");
+  return KB_OK;
+}
+
+int kb_sobol_points_dev(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out_dev) {
+  KB_CHECK(ctx && s, "kb_sobol_points: null argument");
+  KB_CHECK(count >= 0, "count must be >= 0");
+  int st = check_sobol_range(s, k_first, count);
+  if (st) return st;
+  KB_CUDA(cudaSetDevice(ctx->device));
+  KB_CUDA(launch_sobol_points(sobol_dev(s), k_first, count, out_dev, ctx->stream));
+  return KB_OK;
+}
+
+int kb_sobol_points(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out) {
+  KB_CHECK(ctx && s && (out || count == 0), "kb_sobol_points: null argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  DevBuf d;
+  size_t bytes = (size_t)count * s->dim * sizeof(double);
+  KB_CUDA(d.alloc(bytes, ctx->stream));
+  int st = kb_sobol_points_dev(ctx, s, k_first, count, d.as<double>());
+  if (st) return st;
+  KB_CUDA(cudaMemcpyAsync(out, d.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return KB_OK;
+}
+
+// ---------------------------------------------------------------- warpers
+// Maker constants, evaluated as keldy's makers do (long double norms) and rounded.
+static int make_warper_dev(const kb_warper &w, WarperDev &d) {
+  memset(&d, 0, sizeof(d));
+  d.kind = w.kind;
+  d.power = w.power;
+  d.u_max = w.u_max;
+  d.w = w.w;
+  switch (w.kind) {
+  case KB_WARPER_IDENTITY:
+    return KB_OK;
+  case KB_WARPER_PLASMA_UV:
+    return KB_OK;
+  case KB_WARPER_UNIFORM:
+    if (!(w.u_max > 0.0)) return fail(KB_E_INVALID, "coord_domain_u coordinates must be ordered.");
+    return KB_OK;
+  case KB_WARPER_EXPONENTIAL: {
+    if (!(w.u_max > 0.0)) return fail(KB_E_INVALID, "coord_domain_u coordinates must be ordered.");
+    if (!(w.w > 0.0)) return fail(KB_E_INVALID, "w_scale must be > 0");
+    long double norm = -std::expm1(-static_cast<long double>(w.u_max) / w.w);
+    d.c[0] = std::expm1(w.u_max / w.w);
+    d.c[1] = static_cast<double>(static_cast<long double>(w.w) * norm);
+    return KB_OK;
+  }
+  case KB_WARPER_INVERSE: {
+    if (!(w.u_max > 0.0)) return fail(KB_E_INVALID, "coord_domain_u coordinates must be ordered.");
+    if (!(w.w > 0.0)) return fail(KB_E_INVALID, "w_scale must be > 0");
+    d.c[0] = static_cast<double>(std::log1p(static_cast<long double>(w.u_max) / w.w));
+    return KB_OK;
+  }
+  case KB_WARPER_INVERSE_SQUARE: {
+    if (!(w.u_max > 0.0)) return fail(KB_E_INVALID, "coord_domain_u coordinates must be ordered.");
+    if (!(w.w > 0.0)) return fail(KB_E_INVALID, "w_scale must be > 0");
+    d.c[0] = static_cast<double>(static_cast<long double>(w.u_max) / (w.w + w.u_max));
+    return KB_OK;
+  }
+  case KB_WARPER_INVERSE_POWER: {
+    if (!(w.u_max > 0.0)) return fail(KB_E_INVALID, "coord_domain_u coordinates must be ordered.");
+    if (!(w.w > 0.0)) return fail(KB_E_INVALID, "w_scale must be > 0");
+    if (w.power < 1) return fail(KB_E_INVALID, "inverse_power warper needs power >= 1");
+    if (w.power == 1) { // make_product_1d_simple_inverse_power(1, ...) is the inverse maker
+      kb_warper v = w;
+      v.kind = KB_WARPER_INVERSE;
+      return make_warper_dev(v, d);
+    }
+    long double u_max = w.u_max;
+    int p = w.power;
+    long double den = std::pow(u_max / w.w + 1, p - 1) - 1;
+    d.c[0] = static_cast<double>((p - 1) * std::pow(u_max + w.w, p - 1) / den);
+    d.c[1] = static_cast<double>(std::pow(u_max + w.w, p - 1) / den);
+    d.c[2] = static_cast<double>(std::pow(w.w / (u_max + w.w), p - 1) - 1);
+    return KB_OK;
+  }
+  default:
+    return fail(KB_E_INVALID, "unknown warper kind " + std::to_string(w.kind));
+  }
+}
+
+static int make_chain(const kb_warper *chain, int len, WarperDev *out) {
+  if (len < 0 || len > KB_MAX_CHAIN) return fail(KB_E_INVALID, "warper chain longer than KB_MAX_CHAIN");
+  if (len > 0 && !chain) return fail(KB_E_INVALID, "null warper chain");
+  for (int i = 0; i < KB_MAX_CHAIN; ++i) memset(&out[i], 0, sizeof(WarperDev));
+  for (int i = 0; i < len; ++i) {
+    int st = make_warper_dev(chain[i], out[i]);
+    if (st) return st;
+  }
+  return KB_OK;
+}
+
+int kb_warp(kb_context *ctx, const kb_warper *chain, int chain_len, int direction, int start, int end, int n,
+            int64_t count, const double *in, double *out, double *jac) {
+  KB_CHECK(ctx, "null context");
+  KB_CHECK(n >= 0 && n <= MAX_ORDER, "number of coordinates must be in [0, 16]");
+  KB_CHECK(count >= 0 && (count == 0 || (in && out)), "kb_warp: null buffer");
+  KB_CHECK(direction == KB_REVERSE || direction == KB_FORWARD, "direction must be KB_REVERSE or KB_FORWARD");
+  if (direction == KB_REVERSE)
+    KB_CHECK(0 <= end && end <= start && start <= chain_len, "map_reverse needs 0 <= end <= start <= size");
+  else
+    KB_CHECK(0 <= start && start <= end && end <= chain_len, "map_forward needs 0 <= start <= end <= size");
+  WarperDev w[KB_MAX_CHAIN];
+  int st = make_chain(chain, chain_len, w);
+  if (st) return st;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  size_t bytes = (size_t)count * n * sizeof(double);
+  DevBuf dw, din, dout, djac;
+  KB_CUDA(dw.alloc(sizeof(w), ctx->stream));
+  KB_CUDA(din.alloc(bytes, ctx->stream));
+  KB_CUDA(dout.alloc(bytes, ctx->stream));
+  KB_CUDA(djac.alloc((size_t)count * sizeof(double), ctx->stream));
+  KB_CUDA(cudaMemcpyAsync(dw.p, w, sizeof(w), cudaMemcpyHostToDevice, ctx->stream));
+  KB_CUDA(cudaMemcpyAsync(din.p, in, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  KB_CUDA(launch_warp(dw.as<WarperDev>(), start, end, direction, n, count, din.as<double>(), dout.as<double>(),
+                      djac.as<double>(), ctx->stream));
+  KB_CUDA(cudaMemcpyAsync(out, dout.p, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (jac) KB_CUDA(cudaMemcpyAsync(jac, djac.p, (size_t)count * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return KB_OK;
+}
+
+// ---------------------------------------------------------------- model
+int kb_model_create(kb_context *ctx, int npts, double time_max, double alpha, kb_model **out) {
+  KB_CHECK(ctx && out, "kb_model_create: null argument");
+  KB_CHECK(npts >= 2, "g0 tables need at least 2 mesh points");
+  KB_CHECK(time_max > 0.0 && std::isfinite(time_max), "time_max must be > 0");
+  auto *m = new kb_model;
+  m->ctx = ctx;
+  m->npts = npts;
+  m->tmax = time_max;
+  m->alpha = alpha;
+  *out = m;
+  return KB_OK;
+}
+
+int kb_model_destroy(kb_model *m) {
+  if (!m) return KB_OK;
+  cudaSetDevice(m->ctx->device);
+  cudaStreamSynchronize(m->ctx->stream);
+  for (int s = 0; s < 2; ++s)
+    for (int a = 0; a < 2; ++a)
+      for (int b = 0; b < 2; ++b) cudaFree(m->tab[s][a][b]);
+  delete m;
+  return KB_OK;
+}
+
+static int set_table(kb_model *m, int spin, int o1, int o2, const double *lesser, const double *greater,
+                     cudaMemcpyKind kind) {
+  KB_CHECK(m && lesser && greater, "kb_model_set_table: null argument");
+  KB_CHECK(spin >= 0 && spin < 2 && o1 >= 0 && o1 < 2 && o2 >= 0 && o2 < 2, "spin/orbital index out of range");
+  kb_context *ctx = m->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)m->npts;
+  if (!m->tab[spin][o1][o2]) KB_CUDA(cudaMalloc(&m->tab[spin][o1][o2], n * 2 * sizeof(double2)));
+  double2 *dst = m->tab[spin][o1][o2];
+  // interleave lesser/greater per mesh point
+  KB_CUDA(cudaMemcpy2DAsync(dst, 2 * sizeof(double2), lesser, sizeof(double2), sizeof(double2), n, kind,
+                            ctx->stream));
+  KB_CUDA(cudaMemcpy2DAsync(dst + 1, 2 * sizeof(double2), greater, sizeof(double2), sizeof(double2), n, kind,
+                            ctx->stream));
+  double tmax_tab = 0.0;
+  if (kind == cudaMemcpyHostToDevice) {
+    double mx = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+      mx = std::max(mx, fabs(lesser[2 * i]) + fabs(lesser[2 * i + 1]));
+      mx = std::max(mx, fabs(greater[2 * i]) + fabs(greater[2 * i + 1]));
+    }
+    tmax_tab = mx;
+    m->hash[spin][o1][o2] = fnv1a(lesser, n * 16) ^ (fnv1a(greater, n * 16) * 31ULL) ^ 1ULL;
+  } else {
+    DevBuf d;
+    KB_CUDA(d.alloc(sizeof(double), ctx->stream));
+    KB_CUDA(launch_table_max(dst, m->npts, d.as<double>(), ctx->stream));
+    KB_CUDA(cudaMemcpyAsync(&tmax_tab, d.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    m->hash[spin][o1][o2] = 0;
+  }
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (!std::isfinite(tmax_tab)) return fail(KB_E_INVALID, "g0 table contains non-finite values");
+  m->tabmax = std::max(m->tabmax, tmax_tab);
+  return KB_OK;
+}
+
+int kb_model_set_table(kb_model *m, int spin, int o1, int o2, const double *lesser, const double *greater) {
+  return set_table(m, spin, o1, o2, lesser, greater, cudaMemcpyHostToDevice);
+}
+
+int kb_model_set_table_dev(kb_model *m, int spin, int o1, int o2, const double *lesser_dev,
+                           const double *greater_dev) {
+  return set_table(m, spin, o1, o2, lesser_dev, greater_dev, cudaMemcpyDeviceToDevice);
+}
+
+// Device view of a model. A spin whose (o1,o2) block was never uploaded uses the
+// other spin's block (keldy's models are spin symmetric, model.cpp:209-211).
+static ModelDev model_dev(const kb_model *m, bool *spin_symmetric) {
+  ModelDev d;
+  memset(&d, 0, sizeof(d));
+  bool sym = true;
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      double2 *up = m->tab[0][a][b], *dn = m->tab[1][a][b];
+      d.tab[0][a][b] = up ? up : dn;
+      d.tab[1][a][b] = dn ? dn : up;
+      if (up && dn && !(m->hash[0][a][b] != 0 && m->hash[0][a][b] == m->hash[1][a][b])) sym = false;
+    }
+  d.npts = m->npts;
+  d.tmax = m->tmax;
+  d.xmin = -m->tmax;
+  d.delta = (m->tmax - d.xmin) / (double)(m->npts - 1);
+  d.alpha = m->alpha;
+  d.pivot_floor = 1e-8 * (m->tabmax > 0 ? m->tabmax : 1.0);
+  if (spin_symmetric) *spin_symmetric = sym;
+  return d;
+}
+
+int kb_g0_eval(kb_context *ctx, const kb_model *m, const kb_gf_index *a, const kb_gf_index *b, const int *internal,
+               int64_t count, double *out) {
+  KB_CHECK(ctx && m && (count == 0 || (a && b && out)), "kb_g0_eval: null argument");
+  for (int64_t i = 0; i < count; ++i) {
+    KB_CHECK(a[i].spin >= 0 && a[i].spin < 2 && b[i].spin >= 0 && b[i].spin < 2, "spin must be 0 or 1");
+    KB_CHECK(a[i].orbital >= 0 && a[i].orbital < 2 && b[i].orbital >= 0 && b[i].orbital < 2, "orbital must be 0 or 1");
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  DevBuf da, db, di, dout;
+  KB_CUDA(da.alloc(count * sizeof(kb_gf_index), ctx->stream));
+  KB_CUDA(db.alloc(count * sizeof(kb_gf_index), ctx->stream));
+  KB_CUDA(dout.alloc(count * sizeof(double2), ctx->stream));
+  KB_CUDA(cudaMemcpyAsync(da.p, a, count * sizeof(kb_gf_index), cudaMemcpyHostToDevice, ctx->stream));
+  KB_CUDA(cudaMemcpyAsync(db.p, b, count * sizeof(kb_gf_index), cudaMemcpyHostToDevice, ctx->stream));
+  if (internal) {
+    KB_CUDA(di.alloc(count * sizeof(int), ctx->stream));
+    KB_CUDA(cudaMemcpyAsync(di.p, internal, count * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+  KB_CUDA(launch_g0_eval(model_dev(m, nullptr), da.as<kb_gf_index>(), db.as<kb_gf_index>(),
+                         internal ? di.as<int>() : nullptr, count, dout.as<double2>(), ctx->d_err, ctx->stream));
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(out, dout.p, count * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  return KB_OK;
+}
+
+// ------------------------------------------------------------- integrand
+static int check_integrand(const kb_model *m, const kb_integrand *f, int order) {
+  KB_CHECK(m && f, "null model or integrand");
+  KB_CHECK(order >= 0 && order <= MAX_ORDER, "order must be in [0, 16]");
+  const kb_gf_index *e[2] = {&f->A, &f->B};
+  for (auto *x : e) {
+    KB_CHECK(x->spin >= 0 && x->spin < 2, "spin must be 0 or 1");
+    KB_CHECK(x->k_idx >= 0 && x->k_idx < 2, "keldysh index must be 0 or 1");
+    KB_CHECK(x->orbital >= 0 && x->orbital < 2, "orbital must be 0 or 1");
+    // integrand_g_direct's constructor checks (wick_direct.hpp:50-56)
+    if (x->time < 0.0) return fail(KB_E_INVALID, "An external point has negative time.");
+    if (x->time > m->tmax) return fail(KB_E_INVALID, "An external point is out of g0 time window.");
+  }
+  return KB_OK;
+}
+
+static ItemDev make_item(const kb_model *m, const kb_integrand *f, int order) {
+  ItemDev it;
+  memset(&it, 0, sizeof(it));
+  bool sym = true;
+  it.model = model_dev(m, &sym);
+  it.spin_symmetric = sym ? 1 : 0;
+  it.f = *f;
+  it.order = order;
+  return it;
+}
+
+// Runs the tree (or direct) kernel over `count` points of one item in an evaluation
+// mode, then re-evaluates points the tree flagged with the pivoted-LU kernel.
+static int run_eval(kb_context *ctx, ItemDev it, int mode, int64_t count, const double *in_host, int keep,
+                    int algo, double *out, double *jac, int *in_domain, double *scale) {
+  KB_CHECK(algo == KB_ALGO_AUTO || algo == KB_ALGO_TREE || algo == KB_ALGO_DIRECT, "unknown algorithm");
+  if (count == 0) return KB_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  it.n_points = count;
+  const int N = it.order;
+  const bool use_tree = (algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric);
+  if (algo == KB_ALGO_TREE && !it.spin_symmetric)
+    return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
+  long long nchunks = (count + CHUNK_POINTS - 1) / CHUNK_POINTS;
+  long long offs[2] = {0, nchunks};
+  DevBuf ditem, doff, dcnt, din, dval, djac, ddom, dscale, dflag;
+  KB_CUDA(ditem.alloc(sizeof(ItemDev), st));
+  KB_CUDA(doff.alloc(sizeof(offs), st));
+  KB_CUDA(dcnt.alloc(sizeof(int), st));
+  size_t inbytes = (size_t)count * N * sizeof(double);
+  KB_CUDA(din.alloc(inbytes, st));
+  KB_CUDA(dval.alloc(count * sizeof(double2), st));
+  KB_CUDA(djac.alloc(count * sizeof(double), st));
+  KB_CUDA(ddom.alloc(count * sizeof(int), st));
+  KB_CUDA(dflag.alloc(count * sizeof(int), st));
+  if (scale) KB_CUDA(dscale.alloc(count * sizeof(double), st));
+  KB_CUDA(cudaMemcpyAsync(ditem.p, &it, sizeof(ItemDev), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(doff.p, offs, sizeof(offs), cudaMemcpyHostToDevice, st));
+  if (inbytes) KB_CUDA(cudaMemcpyAsync(din.p, in_host, inbytes, cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(int), st));
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.items = ditem.as<ItemDev>();
+  L.n_items = 1;
+  L.chunk_offsets = doff.as<long long>();
+  L.n_chunks = (int)nchunks;
+  L.chunk_counter = dcnt.as<int>();
+  L.mode = mode;
+  L.keep_u_hypercube = keep;
+  L.in = din.as<double>();
+  L.out_val = dval.as<double2>();
+  L.out_jac = djac.as<double>();
+  L.out_dom = ddom.as<int>();
+  L.out_scale = scale ? dscale.as<double>() : nullptr;
+  L.out_flag = dflag.as<int>();
+  L.err = ctx->d_err;
+  int grid = (int)std::min<long long>(nchunks, use_tree ? ctx->tree_grid : ctx->sm_count * 4);
+  if (use_tree) {
+    KB_CUDA(launch_tree(L, grid, st));
+    std::vector<int> flags((size_t)count);
+    KB_CUDA(cudaMemcpyAsync(flags.data(), dflag.p, count * sizeof(int), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    std::vector<int> idx;
+    for (int64_t i = 0; i < count; ++i)
+      if (flags[(size_t)i]) idx.push_back((int)i);
+    if (!idx.empty()) {
+      DevBuf didx;
+      KB_CUDA(didx.alloc(idx.size() * sizeof(int), st));
+      KB_CUDA(cudaMemcpyAsync(didx.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+      long long nc2 = ((long long)idx.size() + CHUNK_POINTS - 1) / CHUNK_POINTS;
+      long long offs2[2] = {0, nc2};
+      KB_CUDA(cudaMemcpyAsync(doff.p, offs2, sizeof(offs2), cudaMemcpyHostToDevice, st));
+      KB_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(int), st));
+      Launch L2 = L;
+      L2.index = didx.as<int>();
+      L2.n_index = (int)idx.size();
+      L2.n_chunks = (int)nc2;
+      KB_CUDA(launch_direct(L2, (int)std::min<long long>(nc2, ctx->sm_count * 4), st));
+      KB_CUDA(cudaStreamSynchronize(st));
+    }
+  } else {
+    KB_CUDA(launch_direct(L, grid, st));
+  }
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(out, dval.p, count * sizeof(double2), cudaMemcpyDeviceToHost, st));
+  if (jac) KB_CUDA(cudaMemcpyAsync(jac, djac.p, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (in_domain) KB_CUDA(cudaMemcpyAsync(in_domain, ddom.p, count * sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (scale) KB_CUDA(cudaMemcpyAsync(scale, dscale.p, count * sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  return KB_OK;
+}
+
+int kb_integrand_eval(kb_context *ctx, const kb_model *m, const kb_integrand *f, int order, int64_t count,
+                      const double *times, int keep_u_hypercube, int algo, double *out, int *in_domain,
+                      double *scale) {
+  KB_CHECK(ctx, "null context");
+  int st = check_integrand(m, f, order);
+  if (st) return st;
+  KB_CHECK(count >= 0 && (count == 0 || (out && (times || order == 0))), "kb_integrand_eval: null buffer");
+  ItemDev it = make_item(m, f, order);
+  return run_eval(ctx, it, IN_TIMES, count, times, keep_u_hypercube, algo, out, nullptr, in_domain, scale);
+}
+
+int kb_evaluate_warped(kb_context *ctx, const kb_model *m, const kb_integrand *f, const kb_warper *chain,
+                       int chain_len, int start_domain_nr, int order, int64_t count, const double *li,
+                       int keep_u_hypercube, int algo, double *out, double *jac, int *in_domain) {
+  KB_CHECK(ctx, "null context");
+  int st = check_integrand(m, f, order);
+  if (st) return st;
+  KB_CHECK(count >= 0 && (count == 0 || (out && (li || order == 0))), "kb_evaluate_warped: null buffer");
+  KB_CHECK(0 <= start_domain_nr && start_domain_nr <= chain_len, "start_domain_nr must be in [0, chain size]");
+  ItemDev it = make_item(m, f, order);
+  st = make_chain(chain, chain_len, it.chain);
+  if (st) return st;
+  it.chain_len = chain_len;
+  it.chain_start = start_domain_nr;
+  return run_eval(ctx, it, IN_LI, count, li, keep_u_hypercube, algo, out, jac, in_domain, nullptr);
+}
+
+int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integrand *f, int order, int64_t count,
+                             const double *times, int keep_u_hypercube, double *out, int *in_domain) {
+  KB_CHECK(ctx, "null context");
+  int st = check_integrand(m, f, order);
+  if (st) return st;
+  if (order > 2) return fail(KB_E_INVALID, "Not supported for order > 2");
+  if (count == 0) return KB_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  DevBuf dt, dv, dd;
+  size_t tb = (size_t)count * order * sizeof(double);
+  KB_CUDA(dt.alloc(tb, s));
+  KB_CUDA(dv.alloc(count * sizeof(double2), s));
+  KB_CUDA(dd.alloc(count * sizeof(int), s));
+  if (tb) KB_CUDA(cudaMemcpyAsync(dt.p, times, tb, cudaMemcpyHostToDevice, s));
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+  KB_CUDA(launch_no_det(model_dev(m, nullptr), *f, order, count, dt.as<double>(), keep_u_hypercube,
+                        dv.as<double2>(), dd.as<int>(), ctx->d_err, s));
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(out, dv.p, count * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  if (in_domain) KB_CUDA(cudaMemcpyAsync(in_domain, dd.p, count * sizeof(int), cudaMemcpyDeviceToHost, s));
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  KB_CUDA(cudaStreamSynchronize(s));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  return KB_OK;
+}
+
+// ------------------------------------------------------------- integrator
+int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc) {
+  KB_CHECK(ctx && (n_work == 0 || (work && acc)), "kb_integrate: null argument");
+  KB_CHECK(algo == KB_ALGO_AUTO || algo == KB_ALGO_TREE || algo == KB_ALGO_DIRECT, "unknown algorithm");
+  if (n_work == 0) return KB_OK;
+  std::vector<ItemDev> items((size_t)n_work);
+  std::vector<int> use_tree((size_t)n_work);
+  for (int i = 0; i < n_work; ++i) {
+    const kb_work &w = work[i];
+    int st = check_integrand(w.m, &w.f, w.order);
+    if (st) return st;
+    KB_CHECK(w.rng, "work item without a Sobol generator");
+    KB_CHECK(w.n_points >= 0, "n_points must be >= 0");
+    KB_CHECK(w.order >= 1, "integrator dimension must be > 0 (Dimension of the integration space must be > 0.)");
+    if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
+    st = check_sobol_range(w.rng, w.k_first, w.n_points);
+    if (st) return st;
+    ItemDev &it = items[(size_t)i];
+    it = make_item(w.m, &w.f, w.order);
+    st = make_chain(w.chain, w.chain_len, it.chain);
+    if (st) return st;
+    it.chain_len = w.chain_len;
+    it.chain_start = w.chain_len;
+    it.rng = sobol_dev(w.rng);
+    it.k_first = w.k_first;
+    it.n_points = w.n_points;
+    if (algo == KB_ALGO_TREE && !it.spin_symmetric)
+      return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
+    use_tree[(size_t)i] = (algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric);
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  ctx->last_ms[0] = ctx->last_ms[1] = ctx->last_ms[2] = 0.0;
+  ctx->last_launches = 0;
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  DevBuf dacc;
+  KB_CUDA(dacc.alloc((size_t)n_work * sizeof(kb_accum), st));
+  KB_CUDA(cudaMemsetAsync(dacc.p, 0, (size_t)n_work * sizeof(kb_accum), st));
+  // Two groups (tree / pivoted LU), each one persistent launch over its items, heaviest
+  // orders first.
+  for (int group = 0; group < 2; ++group) {
+    std::vector<int> ids;
+    for (int i = 0; i < n_work; ++i)
+      if (use_tree[(size_t)i] == (group == 0) && items[(size_t)i].n_points > 0) ids.push_back(i);
+    if (ids.empty()) continue;
+    std::stable_sort(ids.begin(), ids.end(), [&](int a, int b) { return items[(size_t)a].order > items[(size_t)b].order; });
+    std::vector<ItemDev> sorted;
+    std::vector<long long> offs(1, 0);
+    for (int i : ids) {
+      sorted.push_back(items[(size_t)i]);
+      offs.push_back(offs.back() + (items[(size_t)i].n_points + CHUNK_POINTS - 1) / CHUNK_POINTS);
+    }
+    const long long nchunks = offs.back();
+    if (nchunks > INT32_MAX) return fail(KB_E_INVALID, "too many points in one kb_integrate call");
+    DevBuf ditems, doff, dcnt, dpart, dacc_s;
+    KB_CUDA(ditems.alloc(sorted.size() * sizeof(ItemDev), st));
+    KB_CUDA(doff.alloc(offs.size() * sizeof(long long), st));
+    KB_CUDA(dcnt.alloc(sizeof(int), st));
+    KB_CUDA(dpart.alloc((size_t)nchunks * sizeof(ChunkPartial), st));
+    KB_CUDA(dacc_s.alloc(sorted.size() * sizeof(kb_accum), st));
+    KB_CUDA(cudaMemcpyAsync(ditems.p, sorted.data(), sorted.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, st));
+    KB_CUDA(cudaMemcpyAsync(doff.p, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
+    KB_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(int), st));
+    KB_CUDA(cudaMemsetAsync(dacc_s.p, 0, sorted.size() * sizeof(kb_accum), st));
+    Launch L;
+    memset(&L, 0, sizeof(L));
+    L.items = ditems.as<ItemDev>();
+    L.n_items = (int)sorted.size();
+    L.chunk_offsets = doff.as<long long>();
+    L.n_chunks = (int)nchunks;
+    L.chunk_counter = dcnt.as<int>();
+    L.mode = IN_SOBOL;
+    L.partials = dpart.as<ChunkPartial>();
+    L.err = ctx->d_err;
+    if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
+    if (group == 0)
+      KB_CUDA(launch_tree(L, (int)std::min<long long>(nchunks, ctx->tree_grid), st));
+    else
+      KB_CUDA(launch_direct(L, (int)std::min<long long>(nchunks, ctx->sm_count * 4), st));
+    if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[1], st));
+    if (group == 0) {
+      KB_CUDA(launch_fallback(L, ctx->sm_count * 4, st));
+      ctx->last_launches++;
+    }
+    if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[2], st));
+    KB_CUDA(launch_reduce(L, dacc_s.as<kb_accum>(), st));
+    if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[3], st));
+    ctx->last_launches += 2;
+    std::vector<kb_accum> part(sorted.size());
+    KB_CUDA(cudaMemcpyAsync(part.data(), dacc_s.p, part.size() * sizeof(kb_accum), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    if (ctx->timing) {
+      float a = 0, b = 0, c = 0;
+      KB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
+      KB_CUDA(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
+      KB_CUDA(cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]));
+      ctx->last_ms[0] += a;
+      ctx->last_ms[1] += b;
+      ctx->last_ms[2] += c;
+    }
+    for (size_t j = 0; j < ids.size(); ++j) {
+      kb_accum &a = acc[ids[j]];
+      a.sum_re += part[j].sum_re;
+      a.sum_im += part[j].sum_im;
+      a.n_points += part[j].n_points;
+      a.n_in_domain += part[j].n_in_domain;
+      a.n_fallback += part[j].n_fallback;
+    }
+  }
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  return KB_OK;
+}
+
+// ------------------------------------------------------------------ peaks
+int kb_fp64_peak(kb_context *ctx, int iters, double *flops_per_s) {
+  KB_CHECK(ctx && flops_per_s && iters > 0, "kb_fp64_peak: bad argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  const int block = 256, grid = ctx->sm_count * 8;
+  DevBuf sink;
+  KB_CUDA(sink.alloc(grid * sizeof(double), ctx->stream));
+  cudaEvent_t e0, e1;
+  KB_CUDA(cudaEventCreate(&e0));
+  KB_CUDA(cudaEventCreate(&e1));
+  KB_CUDA(launch_fp64_peak(iters, sink.as<double>(), grid, block, ctx->stream)); // warm-up
+  KB_CUDA(cudaEventRecord(e0, ctx->stream));
+  KB_CUDA(launch_fp64_peak(iters, sink.as<double>(), grid, block, ctx->stream));
+  KB_CUDA(cudaEventRecord(e1, ctx->stream));
+  KB_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  KB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *flops_per_s = 2.0 * 8.0 * (double)iters * grid * block / (ms * 1e-3);
+  return KB_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,220 @@
+// Device building blocks of the QMC pipeline: complex arithmetic, g0 lookup on the
+// Keldysh contour, Sobol points and the warper chain.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "kb_types.h"
+
+namespace kb {
+
+// ------------------------------------------------------------------ complex
+__device__ __forceinline__ double2 c2(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return c2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return c2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+// c - a*b with four fused multiply-adds
+__device__ __forceinline__ double2 cfms(double2 c, double2 a, double2 b) {
+  return c2(fma(-a.x, b.x, fma(a.y, b.y, c.x)), fma(-a.x, b.y, fma(-a.y, b.x, c.y)));
+}
+__device__ __forceinline__ double2 crcp(double2 a) {
+  double r = 1.0 / fma(a.x, a.x, a.y * a.y);
+  return c2(a.x * r, -a.y * r);
+}
+__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
+__device__ __forceinline__ double cabs(double2 a) { return hypot(a.x, a.y); }
+
+// --------------------------------------------------------------- g0 lookup
+// Linear interpolation on the uniform mesh [xmin, xmin + (npts-1) delta], the last
+// interval closed at the right end. Every product and sum is rounded separately
+// (no contraction), so the values equal the CPU oracle's bit for bit.
+// Returns false outside the tabulated window.
+__device__ __forceinline__ bool interp_index(const ModelDev &m, double x, int &i, double &w) {
+  double a = __ddiv_rn(__dsub_rn(x, m.xmin), m.delta);
+  double fi = floor(a);
+  if (!(fi >= 0.0) || fi > (double)(m.npts - 1)) return false;
+  i = (int)fi;
+  if (i == m.npts - 1) i = m.npts - 2;
+  w = __dsub_rn(a, (double)i);
+  return true;
+}
+
+// g^<(x) and g^>(x) of one table (interleaved lesser/greater per mesh point).
+__device__ __forceinline__ void interp_pair(const double2 *tab, int i, double w, double2 &gl, double2 &gg) {
+  double2 l0 = __ldg(tab + 2 * i), g0 = __ldg(tab + 2 * i + 1);
+  double2 l1 = __ldg(tab + 2 * i + 2), g1 = __ldg(tab + 2 * i + 3);
+  double v = __dsub_rn(1.0, w);
+  gl = c2(__dadd_rn(__dmul_rn(v, l0.x), __dmul_rn(w, l1.x)), __dadd_rn(__dmul_rn(v, l0.y), __dmul_rn(w, l1.y)));
+  gg = c2(__dadd_rn(__dmul_rn(v, g0.x), __dmul_rn(w, g1.x)), __dadd_rn(__dmul_rn(v, g0.y), __dmul_rn(w, g1.y)));
+}
+
+// Both tables at x; zero when the block is absent. Sets *bad outside the window.
+__device__ __forceinline__ void g0_pair(const ModelDev &m, const double2 *tab, double x, double2 &gl, double2 &gg,
+                                        int *bad) {
+  if (!tab) {
+    gl = gg = c2(0.0, 0.0);
+    return;
+  }
+  int i;
+  double w;
+  if (!interp_index(m, x, i, w)) {
+    *bad = 1;
+    i = 0;
+    w = 0.0;
+  }
+  interp_pair(tab, i, w, gl, gg);
+}
+
+// keldy::compare_3way (common.cpp:47-57) on (time, keldysh index, timesplit).
+__device__ __forceinline__ int compare_3way(double ta, int ka, int sa, double tb, int kb, int sb) {
+  int k3 = ka - kb;
+  if (k3 != 0) return k3;
+  double d = ta - tb;
+  if (d != 0.0) return (1 - 2 * ka) * (2 * (!signbit(d)) - 1);
+  return (1 - 2 * ka) * (sa - sb);
+}
+
+// g0_keldysh_contour_t::operator() (model.hpp:244-265) for general indices.
+__device__ inline double2 g0_contour(const ModelDev &m, const kb_gf_index &a, const kb_gf_index &b, int internal,
+                                     int *bad) {
+  if (a.spin != b.spin) return c2(0.0, 0.0);
+  int ord = compare_3way(a.time, a.k_idx, a.timesplit, b.time, b.k_idx, b.timesplit);
+  double2 gl, gg;
+  if (ord != 0) {
+    g0_pair(m, m.tab[a.spin][a.orbital][b.orbital], a.time - b.time, gl, gg, bad);
+    return ord > 0 ? gg : gl;
+  }
+  if (a.orbital != b.orbital) {
+    g0_pair(m, m.tab[a.spin][a.orbital][b.orbital], 0.0, gl, gg, bad);
+    return gl;
+  }
+  g0_pair(m, m.tab[a.spin][a.orbital][a.orbital], 0.0, gl, gg, bad);
+  return c2(gl.x, gl.y - (double)internal * m.alpha);
+}
+
+// ------------------------------------------------------------------ Sobol
+// Point number k (k >= 1) of the digital sequence: the state digitalseq_b2g::set_state
+// builds for Gray code gray(k), x_j = 2^-32 (cur_j ^ shift_j) (digitalseq_b2g.hpp:455-471).
+__device__ __forceinline__ double sobol_coord(const SobolDev &s, uint32_t k, int j) {
+  uint32_t g = k ^ (k >> 1);
+  uint32_t cur = 0;
+  const uint32_t *C = s.Csr + j * s.m;
+  while (g) {
+    int b = __ffs(g) - 1;
+    cur ^= __ldg(C + b);
+    g &= g - 1;
+  }
+  return 2.3283064365386963e-10 * (double)(cur ^ __ldg(s.shfr + j));
+}
+
+// ---------------------------------------------------------------- warpers
+// f1, f1_integrated and f1_integrated_inverse of the analytic product makers
+// (product_1d_simple.hpp:560-630). The constants c[] are the makers' normalisations,
+// evaluated once on the host in long double and rounded to double.
+__device__ __forceinline__ double warper_f1(const WarperDev &w, double t) {
+  switch (w.kind) {
+  case KB_WARPER_EXPONENTIAL: return exp(-t / w.w) / w.c[1];
+  case KB_WARPER_INVERSE: return 1.0 / (w.c[0] * (w.w + t));
+  case KB_WARPER_INVERSE_SQUARE: return w.w / ((w.w + t) * (w.w + t) * w.c[0]);
+  case KB_WARPER_INVERSE_POWER: return w.c[0] / pow(w.w + t, (double)w.power);
+  case KB_WARPER_UNIFORM: return 1.0 / w.u_max;
+  default: return 1.0;
+  }
+}
+
+__device__ __forceinline__ double warper_F(const WarperDev &w, double t) {
+  switch (w.kind) {
+  case KB_WARPER_EXPONENTIAL: return expm1((w.u_max - t) / w.w) / w.c[0];
+  case KB_WARPER_INVERSE: return log1p(t / w.w) / w.c[0];
+  case KB_WARPER_INVERSE_SQUARE: return t / ((w.w + t) * w.c[0]);
+  case KB_WARPER_INVERSE_POWER:
+    return w.c[1] * (pow(t / w.w + 1.0, (double)(w.power - 1)) - 1.0) / pow(t + w.w, (double)(w.power - 1));
+  case KB_WARPER_UNIFORM: return t / w.u_max;
+  default: return t;
+  }
+}
+
+__device__ __forceinline__ double warper_Finv(const WarperDev &w, double l) {
+  switch (w.kind) {
+  case KB_WARPER_EXPONENTIAL: return w.u_max - w.w * log1p(w.c[0] * l);
+  case KB_WARPER_INVERSE: return w.w * expm1(l * w.c[0]);
+  case KB_WARPER_INVERSE_SQUARE: return w.c[0] * l * w.w / (1.0 - w.c[0] * l);
+  case KB_WARPER_INVERSE_POWER: {
+    double d = pow(1.0 + l * w.c[2], 1.0 / (w.power - 1.0));
+    return w.w * (1.0 - d) / d;
+  }
+  case KB_WARPER_UNIFORM: return w.u_max * l;
+  default: return l;
+  }
+}
+
+// One warper's map_reverse on x[0..n) (identity.hpp:34-48, plasma_uv.hpp:46-51,
+// product_1d_simple.hpp:109-117); returns its Jacobian.
+__device__ inline double warp_reverse_one(const WarperDev &w, int n, double *x, int stride) {
+  if (w.kind == KB_WARPER_IDENTITY) return 1.0;
+  if (w.kind == KB_WARPER_PLASMA_UV) {
+    if (n > 0) {
+      double u = w.u_max - x[0];
+      x[0] = u;
+      for (int i = 1; i < n; ++i) {
+        u = u - x[i * stride];
+        x[i * stride] = u;
+      }
+    }
+    return 1.0;
+  }
+  double jac = 1.0;
+  for (int i = 0; i < n; ++i) {
+    double u = warper_Finv(w, x[i * stride]);
+    x[i * stride] = u;
+    jac *= 1.0 / warper_f1(w, u);
+  }
+  return jac;
+}
+
+// One warper's map_forward (plasma_uv.hpp:35-44, product_1d_simple.hpp:119-127).
+__device__ inline double warp_forward_one(const WarperDev &w, int n, double *x, int stride) {
+  if (w.kind == KB_WARPER_IDENTITY) return 1.0;
+  if (w.kind == KB_WARPER_PLASMA_UV) {
+    if (n > 0) {
+      // sort descending (insertion sort; n <= MAX_ORDER), then consecutive differences
+      for (int i = 1; i < n; ++i) {
+        double v = x[i * stride];
+        int j = i - 1;
+        while (j >= 0 && x[j * stride] < v) {
+          x[(j + 1) * stride] = x[j * stride];
+          --j;
+        }
+        x[(j + 1) * stride] = v;
+      }
+      for (int i = n - 1; i > 0; --i) x[i * stride] = x[(i - 1) * stride] - x[i * stride];
+      x[0] = w.u_max - x[0];
+    }
+    return 1.0;
+  }
+  double jac = 1.0;
+  for (int i = 0; i < n; ++i) {
+    double u = x[i * stride];
+    jac *= warper_f1(w, u);
+    x[i * stride] = warper_F(w, u);
+  }
+  return jac;
+}
+
+// warper_train_t::map_reverse(li, start, end) (warpers.hpp:72-85): warpers start-1
+// down to end.
+__device__ inline double chain_reverse(const WarperDev *chain, int start, int end, int n, double *x, int stride) {
+  double jac = 1.0;
+  for (int i = start - 1; i >= end; --i) jac *= warp_reverse_one(chain[i], n, x, stride);
+  return jac;
+}
+
+__device__ inline double chain_forward(const WarperDev *chain, int start, int end, int n, double *x, int stride) {
+  double jac = 1.0;
+  for (int i = start; i < end; ++i) jac *= warp_forward_one(chain[i], n, x, stride);
+  return jac;
+}
+
+} // namespace kb

@@ -1,0 +1,68 @@
+// Host-side launch interface of the kernels (implemented in tree.cu and misc_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "kb_types.h"
+
+namespace kb {
+
+enum InputMode {
+  IN_TIMES = 0, // vertex times given: integrand_g_direct::operator()
+  IN_LI = 1,    // hypercube points given, warped: evaluate_warped_integrand
+  IN_SOBOL = 2, // Sobol points generated and warped, summed per chunk: integrator::run
+};
+
+// Per-chunk partial sums of the integrate mode. fb_mask marks the chunk's points whose
+// tree pivots were guarded; the pivoted-LU pass adds them to sum_re/sum_im.
+struct ChunkPartial {
+  double sum_re;
+  double sum_im;
+  unsigned long long n_in_domain;
+  unsigned long long n_fallback;
+  unsigned long long fb_mask[2];
+};
+
+constexpr int CHUNK_POINTS = 128; // points per scheduling chunk (<= 128: two 64-bit masks)
+
+struct Launch {
+  const ItemDev *items; // device
+  int n_items;
+  const long long *chunk_offsets; // device [n_items+1]: first chunk of each item (items sorted by cost)
+  int n_chunks;
+  int *chunk_counter; // device, zeroed before the launch (dynamic scheduling)
+  int mode;
+  int keep_u_hypercube;
+  // IN_TIMES / IN_LI
+  const double *in;     // [count][order]
+  const int *index;     // optional list of point indices to evaluate (direct kernel, fallback)
+  int n_index;
+  double2 *out_val;     // f*J (or f)
+  double *out_jac;
+  int *out_dom;
+  double *out_scale;
+  int *out_flag;        // tree: 1 = point needs the pivoted-LU kernel
+  // IN_SOBOL
+  ChunkPartial *partials; // [n_chunks]
+  // errors
+  int *err; // bit 0: g0 evaluated outside its window
+};
+
+size_t tree_smem_bytes();
+cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st);
+cudaError_t launch_direct(const Launch &L, int grid, cudaStream_t st);
+// pivoted-LU evaluation of the points marked in the chunk partials' fb_mask
+cudaError_t launch_fallback(const Launch &L, int grid, cudaStream_t st);
+// acc[item] += sum over the item's chunks in chunk order
+cudaError_t launch_reduce(const Launch &L, kb_accum *acc_dev, cudaStream_t st);
+
+cudaError_t launch_sobol_points(SobolDev s, uint32_t k_first, long long count, double *out, cudaStream_t st);
+cudaError_t launch_warp(const WarperDev *chain_dev, int start, int end, int direction, int n, long long count,
+                        const double *in, double *out, double *jac, cudaStream_t st);
+cudaError_t launch_g0_eval(ModelDev m, const kb_gf_index *a, const kb_gf_index *b, const int *internal,
+                           long long count, double2 *out, int *err, cudaStream_t st);
+cudaError_t launch_no_det(ModelDev m, kb_integrand f, int order, long long count, const double *times, int keep,
+                          double2 *out, int *dom, int *err, cudaStream_t st);
+cudaError_t launch_table_max(const double2 *tab, int npts, double *out, cudaStream_t st);
+cudaError_t launch_fp64_peak(int iters, double *sink, int grid, int block, cudaStream_t st);
+
+} // namespace kb

@@ -1,0 +1,100 @@
+// Descriptors shared by the host side of the library (capi.cu) and the kernels.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/keldy_b200.h"
+
+namespace kb {
+
+constexpr int MAX_ORDER = 16;      // 2^16 Keldysh configurations per point
+constexpr int SOBOL_COLS = 31;     // columns of the generating matrices (log_max_points <= 31)
+constexpr int CTA_THREADS = 128;   // threads per CTA of the tree kernel
+constexpr int TREE_MAX_SUB = 9;    // largest order solved breadth-first in one pass
+
+// g0 tables of one model on the device: per mesh point {lesser.re, lesser.im,
+// greater.re, greater.im} (32 bytes), one array per (spin, orbital a, orbital b); null
+// = zero block.
+struct ModelDev {
+  const double2 *tab[2][2][2]; // [spin][o1][o2] -> 2*npts double2 (lesser, greater interleaved)
+  int npts;
+  double tmax;
+  double xmin;
+  double delta;
+  double alpha;
+  double pivot_floor; // |re|+|im| below which a tree pivot hands the point to the pivoted-LU kernel
+};
+
+struct WarperDev {
+  int kind;
+  int power;
+  double u_max;
+  double w;
+  double c[3]; // constants of the product makers, computed on the host (see make_warper_dev)
+};
+
+struct SobolDev {
+  const uint32_t *Csr; // [dim][SOBOL_COLS] bit-reversed generating matrices
+  const uint32_t *shfr;
+  int dim;
+  int m; // log_max_points
+};
+
+// Everything a kernel needs to evaluate one integrand configuration.
+struct ItemDev {
+  ModelDev model;
+  SobolDev rng;
+  WarperDev chain[KB_MAX_CHAIN];
+  int chain_len;
+  int chain_start; // map_reverse(li, chain_start, 0)
+  kb_integrand f;
+  int order;
+  int spin_symmetric; // spin-down tables equal spin-up ones: det(s2) = det of s1's vertex block
+  uint32_t k_first;
+  int64_t n_points;
+};
+
+// One chunk of points of one item, processed by one CTA iteration.
+struct ChunkDev {
+  int item;
+  int order;
+  int64_t first; // offset of the first point within the item
+  int count;
+};
+
+// Per-chunk partial sums (deterministic reduction afterwards).
+struct PartialDev {
+  double sum_re;
+  double sum_im;
+  unsigned long long n_in_domain;
+  unsigned long long n_fallback;
+};
+
+// A point the tree handed to the pivoted-LU kernel.
+struct FallbackDev {
+  int item;
+  int pad;
+  int64_t index; // point offset within the item
+};
+
+// Points per CTA chunk of the tree kernel for each order (shared-memory budget of two
+// 51.2 KB frontier buffers; see tree_smem_bytes()).
+__host__ __device__ inline int tree_points_per_chunk(int n) {
+  switch (n) {
+  case 0: return 128;
+  case 1: return 128;
+  case 2: return 128;
+  case 3: return 64;
+  case 4: return 32;
+  case 5: return 16;
+  case 6: return 8;
+  case 7: return 4;
+  case 8: return 2;
+  default: return 1;
+  }
+}
+
+// Complex entries per frontier buffer: enough for the widest breadth-first level of
+// every order (P * max_k 2^k (2(R-k)+1)^2 = 3200 for every P, R pair above).
+constexpr int FRONTIER = 3200;
+
+} // namespace kb

@@ -1,0 +1,726 @@
+// Wick-determinant integrand kernels (sm_100a).
+//
+// keldy's integrand (impurity_oneband/wick_direct.cpp:43-158) sums, over the 2^n
+// Keldysh configurations a, (-1)^|a| det(s1_a) det(s2_a), where s1_a is the (n+1)^2
+// matrix of g0 between the chosen vertex copies and the two external points (corner
+// set to 0) and s2_a the n^2 matrix of the opposite spin. Every s1_a/s2_a is a
+// principal submatrix of one (2n+1)^2 matrix G (vertex j forward = row 2j, backward =
+// row 2j+1, external = row 2n).
+//
+// Tree kernel: Gaussian elimination of G with the pivot of vertex k taken on the
+// diagonal entry of the chosen copy (2k or 2k+1) visits all 2^n configurations as the
+// leaves of a binary tree; the Schur complement of a node is shared by its whole
+// subtree. At a leaf, det(s2_a) is the product of the pivots along the path (spin
+// symmetric models) and the remaining 1x1 Schur complement of the external corner is
+// det(s1_a)/det(s2_a). Cost O(2^n) complex FMAs per point instead of O(2^n n^3).
+// The top levels run breadth-first in shared memory (one 51.2 KB frontier buffer per
+// level, ping-pong), the last two levels per thread in registers. Orders above 9 walk
+// their first n-9 levels one root-to-subtree path at a time.
+//
+// Direct kernel: keldy's own algorithm, one partial-pivot LU pair per configuration
+// (pivot = first maximum of |re|+|im|, as LAPACK's zgetf2). It serves models whose
+// spin-down tables differ from spin-up ones, points whose tree pivots fall below the
+// guard, and cross-checks.
+#include <cuda_runtime.h>
+#include <stdio.h>
+
+#include "kb_device.cuh"
+#include "kb_launch.h"
+
+namespace kb {
+
+namespace {
+
+constexpr int NT = CTA_THREADS;
+
+struct TreeShared {
+  double2 buf[2][FRONTIER];
+  double2 D[2][NT];  // prefix determinant per node (ping-pong with the frontier)
+  double2 tmp[NT];   // pivot reciprocals during a level; per-node partial sums after the bottom
+  double u[256];     // vertex times, u[j * np + p]
+  double jac[NT];
+  double2 fval[NT];
+  double fscale[NT];
+  int flag[NT];      // bit 0: out of domain, bit 1: needs the pivoted-LU kernel
+};
+
+__device__ __forceinline__ int find_item(const long long *off, int n_items, long long c) {
+  int lo = 0, hi = n_items; // off[lo] <= c < off[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (off[mid] <= c)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Inputs of np points (thread p < np): vertex times into u[j*np+p], Jacobian and
+// domain flag. keep: drop points with a negative time (keep_u_hypercube).
+__device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, long long gp0, double *u,
+                            double *jac_out, int *flag_out, bool keep) {
+  int p = threadIdx.x;
+  if (p >= np) return;
+  long long gp = gp0 + p;
+  double *x = u + p;
+  double jac = 1.0;
+  if (L.mode == IN_SOBOL) {
+    uint32_t k = it.k_first + (uint32_t)gp;
+    for (int j = 0; j < N; ++j) x[j * np] = sobol_coord(it.rng, k, j);
+    jac = chain_reverse(it.chain, it.chain_len, 0, N, x, np);
+  } else {
+    long long src = L.index ? (long long)L.index[gp] : gp;
+    for (int j = 0; j < N; ++j) x[j * np] = L.in[src * N + j];
+    if (L.mode == IN_LI) jac = chain_reverse(it.chain, it.chain_start, 0, N, x, np);
+  }
+  int dom = 1;
+  if (it.f.A.spin != it.f.B.spin) dom = 0;
+  if (keep)
+    for (int j = 0; j < N; ++j)
+      if (x[j * np] < 0.0) dom = 0;
+  jac_out[p] = jac;
+  flag_out[p] = dom ? 0 : 1;
+}
+
+// G (row-major, M = 2N+1) of np points: G[p*M*M + r*M + c]. Out-of-domain points get
+// the identity (their values are discarded; this keeps every pivot finite).
+__device__ void build_G(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
+                        int spin, int *bad) {
+  const ModelDev &m = it.model;
+  const int M = 2 * N + 1;
+  const int per = N * N + N + 1;
+  const kb_gf_index &A = it.f.A, &B = it.f.B;
+  const double2 *t00 = m.tab[spin][0][0];
+  const double2 *trow = m.tab[spin][A.orbital][0];
+  const double2 *tcol = m.tab[spin][0][B.orbital];
+  for (int r = threadIdx.x; r < np * per; r += blockDim.x) {
+    int p = r / per, q = r - p * per;
+    double2 *G = buf + (size_t)p * M * M;
+    const double *x = u + p;
+    bool out = flag[p] & 1;
+    if (q < N * N) {
+      int i = q / N, j = q - i * N;
+      double2 *g = G + (2 * i) * M + 2 * j;
+      if (out) {
+        double2 z = c2(0.0, 0.0), one = c2(1.0, 0.0);
+        g[0] = (i == j) ? one : z;
+        g[M + 1] = (i == j) ? one : z;
+        g[1] = z;
+        g[M] = z;
+      } else if (i != j) {
+        double d = x[i * np] - x[j * np];
+        double2 gl, gg;
+        g0_pair(m, t00, d, gl, gg, bad);
+        bool later = (d != 0.0) ? (d > 0.0) : (i > j);
+        g[0] = later ? gg : gl;      // forward-forward
+        g[M + 1] = later ? gl : gg;  // backward-backward
+        g[1] = gl;                   // forward-backward
+        g[M] = gg;                   // backward-forward
+      } else {
+        double2 gl, gg;
+        g0_pair(m, t00, 0.0, gl, gg, bad);
+        double2 eq = c2(gl.x, gl.y - m.alpha); // equal contour points, internal
+        g[0] = eq;
+        g[M + 1] = eq;
+        g[1] = gl;
+        g[M] = gg;
+      }
+    } else if (q < N * N + N) {
+      int j = q - N * N;
+      double2 *row = G + (2 * N) * M + 2 * j;
+      double2 *col = G + (2 * j) * M + 2 * N;
+      if (out) {
+        row[0] = row[1] = col[0] = col[M] = c2(0.0, 0.0);
+      } else {
+        double uj = x[j * np];
+        double2 gl, gg;
+        g0_pair(m, trow, A.time - uj, gl, gg, bad);
+        row[0] = compare_3way(A.time, A.k_idx, N, uj, 0, j) > 0 ? gg : gl;
+        row[1] = compare_3way(A.time, A.k_idx, N, uj, 1, j) > 0 ? gg : gl;
+        g0_pair(m, tcol, uj - B.time, gl, gg, bad);
+        col[0] = compare_3way(uj, 0, j, B.time, B.k_idx, N) > 0 ? gg : gl;
+        col[M] = compare_3way(uj, 1, j, B.time, B.k_idx, N) > 0 ? gg : gl;
+      }
+    } else {
+      G[(2 * N) * M + 2 * N] = out ? c2(1.0, 0.0) : c2(0.0, 0.0);
+    }
+  }
+}
+
+// One breadth-first level: every node (size m) of the frontier spawns the children
+// that pivot on its rows 0 and 1 and drop both (size m-2).
+__device__ void tree_level(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *inv,
+                           int *flag, int nodes, int npp, int m, double floor_) {
+  const int mc = m - 2, nchild = 2 * nodes, mm = m * m;
+  for (int c = threadIdx.x; c < nchild; c += blockDim.x) {
+    int par = c >> 1, b = c & 1;
+    double2 piv = cur[par * mm + b * m + b];
+    if (!(cabs1(piv) >= floor_)) flag[par / npp] |= 2;
+    inv[c] = crcp(piv);
+    Dn[c] = cmul(Dc[par], piv);
+  }
+  __syncthreads();
+  const int rows = nchild * mc;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    int c = r / mc, i = r - c * mc;
+    int par = c >> 1, b = c & 1;
+    const double2 *S = cur + par * mm;
+    double2 Lf = cmul(S[(i + 2) * m + b], inv[c]);
+    const double2 *prow = S + b * m + 2;
+    const double2 *srow = S + (i + 2) * m + 2;
+    double2 *o = nxt + c * mc * mc + i * mc;
+    for (int j = 0; j < mc; ++j) o[j] = cfms(srow[j], Lf, prow[j]);
+  }
+  __syncthreads();
+}
+
+// One step down a fixed path (single point): pivot on row b, drop rows 0 and 1.
+__device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *tmp,
+                               int *flag, int m, int b, double floor_) {
+  const int mc = m - 2;
+  if (threadIdx.x == 0) {
+    double2 piv = cur[b * m + b];
+    if (!(cabs1(piv) >= floor_)) flag[0] |= 2;
+    tmp[0] = crcp(piv);
+    Dn[0] = cmul(Dc[0], piv);
+  }
+  __syncthreads();
+  const double2 inv = tmp[0];
+  for (int r = threadIdx.x; r < mc * mc; r += blockDim.x) {
+    int i = r / mc, j = r - i * mc;
+    double2 Lf = cmul(cur[(i + 2) * m + b], inv);
+    nxt[r] = cfms(cur[(i + 2) * m + j + 2], Lf, cur[b * m + j + 2]);
+  }
+  __syncthreads();
+}
+
+// Last two levels of a 5x5 node in registers: children on pivots 0/1, then the four
+// leaves, each leaf term (-1)^|a| det(s2)^2 * (1x1 Schur complement) written without
+// division as Db^2 T_cc (T_cc T_ee - T_ce T_ec).
+__device__ __forceinline__ void tree_bottom5(const double2 *R, double2 D, int parity, double floor_, bool want_scale,
+                                             double2 &sum, double &scale, bool &guard) {
+  double2 s[25];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) s[i] = R[i];
+  sum = c2(0.0, 0.0);
+  scale = 0.0;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    double2 piv = s[b * 6];
+    if (!(cabs1(piv) >= floor_)) guard = true;
+    double2 inv = crcp(piv);
+    double2 Db = cmul(D, piv);
+    double2 T[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      double2 Lf = cmul(s[(i + 2) * 5 + b], inv);
+#pragma unroll
+      for (int j = 0; j < 3; ++j) T[i * 3 + j] = cfms(s[(i + 2) * 5 + j + 2], Lf, s[b * 5 + j + 2]);
+    }
+    double2 Db2 = cmul(Db, Db);
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+      double2 q = cmul(T[c * 4], cfms(cmul(T[c * 4], T[8]), T[c * 3 + 2], T[6 + c]));
+      double2 term = cmul(Db2, q);
+      if ((b ^ c) & 1)
+        sum = c2(sum.x - term.x, sum.y - term.y);
+      else
+        sum = cadd(sum, term);
+      if (want_scale) scale += cabs(term);
+    }
+  }
+  if (parity & 1) sum = c2(-sum.x, -sum.y);
+}
+
+// Order 1: the 3x3 root's two leaves directly.
+__device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, double &scale, bool want_scale) {
+  sum = c2(0.0, 0.0);
+  scale = 0.0;
+#pragma unroll
+  for (int b = 0; b < 2; ++b) {
+    double2 piv = R[b * 4];
+    double2 term = cmul(piv, cfms(cmul(piv, R[8]), R[b * 3 + 2], R[6 + b]));
+    if (b)
+      sum = c2(sum.x - term.x, sum.y - term.y);
+    else
+      sum = cadd(sum, term);
+    if (want_scale) scale += cabs(term);
+  }
+}
+
+// Integrand of np points whose inputs are loaded (S.u, S.flag): S.fval, S.fscale, and
+// flag bit 1 where a pivot fell below the guard.
+__device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad) {
+  const int tid = threadIdx.x;
+  if (tid < np) {
+    S.fval[tid] = c2(0.0, 0.0);
+    S.fscale[tid] = 0.0;
+  }
+  if (N == 0) {
+    if (tid < np && !(S.flag[tid] & 1)) {
+      kb_gf_index a = it.f.A, b = it.f.B;
+      a.timesplit = 0;
+      b.timesplit = 0;
+      double2 v = g0_contour(it.model, a, b, 0, bad);
+      S.fval[tid] = v;
+      S.fscale[tid] = cabs(v);
+    }
+    __syncthreads();
+    return;
+  }
+  const int R = N < TREE_MAX_SUB ? N : TREE_MAX_SUB;
+  const int K0 = N - R;
+  const int LTOP = R >= 2 ? R - 2 : 0;
+  const double floor_ = it.model.pivot_floor;
+  const int spin = it.f.A.spin;
+  for (int sub = 0; sub < (1 << K0); ++sub) {
+    build_G(it, N, np, S.u, S.flag, S.buf[0], spin, bad);
+    if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
+    __syncthreads();
+    int m = 2 * N + 1, cur = 0;
+    for (int k = 0; k < K0; ++k) {
+      int b = (sub >> (K0 - 1 - k)) & 1;
+      tree_path_step(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, m, b, floor_);
+      m -= 2;
+      cur ^= 1;
+    }
+    int nodes = np;
+    for (int k = 0; k < LTOP; ++k) {
+      tree_level(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, nodes, nodes / np, m, floor_);
+      nodes *= 2;
+      m -= 2;
+      cur ^= 1;
+    }
+    // nodes == np << LTOP, each of size m (5, or 3 at order 1)
+    if (tid < nodes) {
+      double2 sum;
+      double sc;
+      bool guard = false;
+      int p = tid >> LTOP;
+      if (m == 5) {
+        int parity = __popc(tid & ((1 << LTOP) - 1)) + __popc(sub);
+        tree_bottom5(S.buf[cur] + tid * 25, S.D[cur][tid], parity, floor_, want_scale, sum, sc, guard);
+      } else {
+        tree_bottom3(S.buf[cur] + tid * 9, sum, sc, want_scale);
+      }
+      if (guard) S.flag[p] |= 2;
+      S.tmp[tid] = sum;
+      S.D[cur ^ 1][tid].x = sc;
+    }
+    __syncthreads();
+    if (tid < np) {
+      double2 f = S.fval[tid];
+      double sc = S.fscale[tid];
+      for (int g = tid << LTOP; g < ((tid + 1) << LTOP); ++g) {
+        f = cadd(f, S.tmp[g]);
+        sc += S.D[cur ^ 1][g].x;
+      }
+      S.fval[tid] = f;
+      S.fscale[tid] = sc;
+    }
+    __syncthreads();
+  }
+  if (tid < np) {
+    double2 f = S.fval[tid];
+    if (!isfinite(f.x) || !isfinite(f.y)) S.flag[tid] |= 2;
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ double2 apply_cutoff(double2 f, double cutoff) {
+  return (cabs(f) < cutoff) ? c2(0.0, 0.0) : f;
+}
+
+template <bool EVAL>
+__global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
+  __shared__ int s_chunk;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_bad = 0;
+  for (;;) {
+    if (tid == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
+    __syncthreads();
+    const int c = s_chunk;
+    if (c >= L.n_chunks) break;
+    const int item = find_item(L.chunk_offsets, L.n_items, c);
+    const ItemDev &it = L.items[item];
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * CHUNK_POINTS;
+    const long long total = EVAL ? (L.index ? (long long)L.n_index : it.n_points) : it.n_points;
+    const int ccount = (int)min((long long)CHUNK_POINTS, total - cfirst);
+    const int N = it.order;
+    const int P = tree_points_per_chunk(N);
+    const bool keep = (L.mode == IN_SOBOL) ? true : (L.keep_u_hypercube != 0);
+    double2 csum = c2(0.0, 0.0);
+    unsigned long long cdom = 0, cfb = 0, mask0 = 0, mask1 = 0;
+    for (int sb = 0; sb < ccount; sb += P) {
+      const int np = min(P, ccount - sb);
+      load_points(L, it, N, np, cfirst + sb, S.u, S.jac, S.flag, keep);
+      __syncthreads();
+      tree_points(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
+      if (EVAL) {
+        if (tid < np) {
+          long long o = cfirst + sb + tid;
+          int fl = S.flag[tid];
+          bool dom = !(fl & 1);
+          double2 f = dom ? apply_cutoff(S.fval[tid], it.f.cutoff) : c2(0.0, 0.0);
+          double j = S.jac[tid];
+          L.out_val[o] = c2(f.x * j, f.y * j);
+          if (L.out_jac) L.out_jac[o] = j;
+          if (L.out_dom) L.out_dom[o] = dom ? 1 : 0;
+          if (L.out_scale) L.out_scale[o] = dom ? S.fscale[tid] * fabs(j) : 0.0;
+          if (L.out_flag) L.out_flag[o] = (dom && (fl & 2)) ? 1 : 0;
+        }
+      } else if (tid == 0) {
+        for (int p = 0; p < np; ++p) {
+          int fl = S.flag[p];
+          if (fl & 1) continue;
+          cdom++;
+          if (fl & 2) {
+            int bit = sb + p;
+            if (bit < 64)
+              mask0 |= 1ull << bit;
+            else
+              mask1 |= 1ull << (bit - 64);
+            cfb++;
+            continue;
+          }
+          double2 f = apply_cutoff(S.fval[p], it.f.cutoff);
+          double j = S.jac[p];
+          csum.x += f.x * j;
+          csum.y += f.y * j;
+        }
+      }
+      __syncthreads();
+    }
+    if (!EVAL && tid == 0) {
+      ChunkPartial pr;
+      pr.sum_re = csum.x;
+      pr.sum_im = csum.y;
+      pr.n_in_domain = cdom;
+      pr.n_fallback = cfb;
+      pr.fb_mask[0] = mask0;
+      pr.fb_mask[1] = mask1;
+      L.partials[c] = pr;
+    }
+  }
+  if (tid == 0 && s_bad) atomicOr(L.err, 1);
+}
+
+// ---------------------------------------------------------------- direct kernel
+
+struct DirectShared {
+  double2 G1[(2 * MAX_ORDER + 1) * (2 * MAX_ORDER + 1)];
+  double2 G2[(2 * MAX_ORDER + 1) * (2 * MAX_ORDER + 1)];
+  double u[MAX_ORDER];
+  double jac[1];
+  int flag[1];
+  double2 red[NT];
+  double reds[NT];
+};
+
+// det of the n x n row-major matrix a (destroyed): partial pivoting on the first
+// maximum of |re|+|im| in the column, multipliers with the pivot's reciprocal.
+__device__ double2 lu_det(double2 *a, int n) {
+  double2 det = c2(1.0, 0.0);
+  bool neg = false;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double best = cabs1(a[k * n + k]);
+    for (int i = k + 1; i < n; ++i) {
+      double v = cabs1(a[i * n + k]);
+      if (v > best) {
+        best = v;
+        p = i;
+      }
+    }
+    if (best == 0.0) return c2(0.0, 0.0);
+    if (p != k) {
+      for (int j = 0; j < n; ++j) {
+        double2 t = a[k * n + j];
+        a[k * n + j] = a[p * n + j];
+        a[p * n + j] = t;
+      }
+      neg = !neg;
+    }
+    double2 piv = a[k * n + k];
+    det = cmul(det, piv);
+    double2 inv = crcp(piv);
+    for (int i = k + 1; i < n; ++i) {
+      double2 l = cmul(a[i * n + k], inv);
+      for (int j = k + 1; j < n; ++j) a[i * n + j] = cfms(a[i * n + j], l, a[k * n + j]);
+    }
+  }
+  return neg ? c2(-det.x, -det.y) : det;
+}
+
+// The integrand of one point (inputs in D.u / D.flag): keldy's algorithm.
+__device__ __forceinline__ void direct_point(DirectShared &D, const ItemDev &it, int N, bool want_scale, double2 &f_out,
+                             double &scale_out, int *bad) {
+  const int tid = threadIdx.x;
+  if (D.flag[0] & 1) {
+    f_out = c2(0.0, 0.0);
+    scale_out = 0.0;
+    return;
+  }
+  if (N == 0) {
+    if (tid == 0) {
+      kb_gf_index a = it.f.A, b = it.f.B;
+      a.timesplit = 0;
+      b.timesplit = 0;
+      D.red[0] = g0_contour(it.model, a, b, 0, bad);
+      D.reds[0] = cabs(D.red[0]);
+    }
+    __syncthreads();
+    f_out = D.red[0];
+    scale_out = D.reds[0];
+    __syncthreads();
+    return;
+  }
+  const int M = 2 * N + 1;
+  const int spin = it.f.A.spin;
+  build_G(it, N, 1, D.u, D.flag, D.G1, spin, bad);
+  const double2 *G2 = D.G1;
+  if (!it.spin_symmetric) {
+    build_G(it, N, 1, D.u, D.flag, D.G2, 1 - spin, bad);
+    G2 = D.G2;
+  }
+  __syncthreads();
+  double2 acc = c2(0.0, 0.0);
+  double sc = 0.0;
+  double2 m1[(MAX_ORDER + 1) * (MAX_ORDER + 1)];
+  double2 m2[MAX_ORDER * MAX_ORDER];
+  int pick[MAX_ORDER + 1];
+  const unsigned nconf = 1u << N;
+  for (unsigned cfg = tid; cfg < nconf; cfg += blockDim.x) {
+    for (int i = 0; i < N; ++i) pick[i] = 2 * i + ((cfg >> i) & 1u);
+    pick[N] = 2 * N;
+    for (int i = 0; i <= N; ++i)
+      for (int j = 0; j <= N; ++j) m1[i * (N + 1) + j] = D.G1[pick[i] * M + pick[j]];
+    m1[N * (N + 1) + N] = c2(0.0, 0.0);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) m2[i * N + j] = G2[pick[i] * M + pick[j]];
+    double2 d = cmul(lu_det(m1, N + 1), lu_det(m2, N));
+    if (__popc(cfg) & 1)
+      acc = c2(acc.x - d.x, acc.y - d.y);
+    else
+      acc = cadd(acc, d);
+    if (want_scale) sc += cabs(d);
+  }
+  D.red[tid] = acc;
+  D.reds[tid] = sc;
+  __syncthreads();
+  if (tid == 0) {
+    double2 s = c2(0.0, 0.0);
+    double ss = 0.0;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      s = cadd(s, D.red[t]);
+      ss += D.reds[t];
+    }
+    D.red[0] = s;
+    D.reds[0] = ss;
+  }
+  __syncthreads();
+  f_out = D.red[0];
+  scale_out = D.reds[0];
+  __syncthreads();
+}
+
+__device__ void direct_load_point(const Launch &L, const ItemDev &it, int N, long long gp, bool keep,
+                                  DirectShared &D) {
+  load_points(L, it, N, 1, gp, D.u, D.jac, D.flag, keep);
+  __syncthreads();
+}
+
+// Modes: IN_TIMES / IN_LI (every point, or the points of L.index), IN_SOBOL (per-chunk
+// partial sums, as the tree kernel).
+__global__ void __launch_bounds__(NT) direct_kernel(Launch L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DirectShared &D = *reinterpret_cast<DirectShared *>(smem_raw);
+  __shared__ int s_chunk;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_bad = 0;
+  const bool eval = L.mode != IN_SOBOL;
+  for (;;) {
+    if (tid == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
+    __syncthreads();
+    const int c = s_chunk;
+    if (c >= L.n_chunks) break;
+    const int item = find_item(L.chunk_offsets, L.n_items, c);
+    const ItemDev &it = L.items[item];
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * CHUNK_POINTS;
+    const long long total = eval ? (L.index ? (long long)L.n_index : it.n_points) : it.n_points;
+    const int ccount = (int)min((long long)CHUNK_POINTS, total - cfirst);
+    const int N = it.order;
+    const bool keep = eval ? (L.keep_u_hypercube != 0) : true;
+    double2 csum = c2(0.0, 0.0);
+    unsigned long long cdom = 0;
+    for (int p = 0; p < ccount; ++p) {
+      long long gp = cfirst + p;
+      direct_load_point(L, it, N, gp, keep, D);
+      double2 f;
+      double sc;
+      direct_point(D, it, N, eval && L.out_scale != nullptr, f, sc, &s_bad);
+      if (tid == 0) {
+        bool dom = !(D.flag[0] & 1);
+        double j = D.jac[0];
+        f = dom ? apply_cutoff(f, it.f.cutoff) : c2(0.0, 0.0);
+        if (eval) {
+          long long o = L.index ? (long long)L.index[gp] : gp;
+          L.out_val[o] = c2(f.x * j, f.y * j);
+          if (L.out_jac) L.out_jac[o] = j;
+          if (L.out_dom) L.out_dom[o] = dom ? 1 : 0;
+          if (L.out_scale) L.out_scale[o] = dom ? sc * fabs(j) : 0.0;
+          if (L.out_flag) L.out_flag[o] = 0;
+        } else {
+          csum.x += f.x * j;
+          csum.y += f.y * j;
+          cdom += dom ? 1 : 0;
+        }
+      }
+      __syncthreads();
+    }
+    if (!eval && tid == 0) {
+      ChunkPartial pr;
+      pr.sum_re = csum.x;
+      pr.sum_im = csum.y;
+      pr.n_in_domain = cdom;
+      pr.n_fallback = 0;
+      pr.fb_mask[0] = pr.fb_mask[1] = 0;
+      L.partials[c] = pr;
+    }
+  }
+  if (tid == 0 && s_bad) atomicOr(L.err, 1);
+}
+
+// Points the tree marked in a chunk's fb_mask, evaluated with keldy's algorithm and
+// added to that chunk's partial sum in point order.
+__global__ void __launch_bounds__(NT) fallback_kernel(Launch L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DirectShared &D = *reinterpret_cast<DirectShared *>(smem_raw);
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_bad = 0;
+  __syncthreads();
+  for (int c = blockIdx.x; c < L.n_chunks; c += gridDim.x) {
+    ChunkPartial pr = L.partials[c];
+    if (pr.n_fallback == 0) continue;
+    const int item = find_item(L.chunk_offsets, L.n_items, c);
+    const ItemDev &it = L.items[item];
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * CHUNK_POINTS;
+    for (int bit = 0; bit < CHUNK_POINTS; ++bit) {
+      unsigned long long w = pr.fb_mask[bit >> 6];
+      if (!((w >> (bit & 63)) & 1ull)) continue;
+      direct_load_point(L, it, it.order, cfirst + bit, true, D);
+      double2 f;
+      double sc;
+      direct_point(D, it, it.order, false, f, sc, &s_bad);
+      if (tid == 0) {
+        f = apply_cutoff(f, it.f.cutoff);
+        pr.sum_re += f.x * D.jac[0];
+        pr.sum_im += f.y * D.jac[0];
+      }
+      __syncthreads();
+    }
+    if (tid == 0) L.partials[c] = pr;
+    __syncthreads();
+  }
+  if (tid == 0 && s_bad) atomicOr(L.err, 1);
+}
+
+// acc[item] += sum of the item's chunk partials: each thread adds a contiguous run of
+// chunks in order, then the threads' sums are added in thread order (deterministic).
+__global__ void __launch_bounds__(NT) reduce_kernel(Launch L, kb_accum *acc) {
+  __shared__ double s_re[NT], s_im[NT];
+  __shared__ unsigned long long s_dom[NT], s_fb[NT];
+  const int item = blockIdx.x;
+  const long long c0 = L.chunk_offsets[item], c1 = L.chunk_offsets[item + 1];
+  const long long nc = c1 - c0;
+  const long long per = (nc + NT - 1) / NT;
+  const long long a = c0 + threadIdx.x * per, b = min(c1, a + per);
+  double re = 0.0, im = 0.0;
+  unsigned long long dom = 0, fb = 0;
+  for (long long c = a; c < b; ++c) {
+    ChunkPartial pr = L.partials[c];
+    re += pr.sum_re;
+    im += pr.sum_im;
+    dom += pr.n_in_domain;
+    fb += pr.n_fallback;
+  }
+  s_re[threadIdx.x] = re;
+  s_im[threadIdx.x] = im;
+  s_dom[threadIdx.x] = dom;
+  s_fb[threadIdx.x] = fb;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int t = 1; t < NT; ++t) {
+      re += s_re[t];
+      im += s_im[t];
+      dom += s_dom[t];
+      fb += s_fb[t];
+    }
+    acc[item].sum_re += re;
+    acc[item].sum_im += im;
+    acc[item].n_points += (uint64_t)L.items[item].n_points;
+    acc[item].n_in_domain += dom;
+    acc[item].n_fallback += fb;
+  }
+}
+
+} // namespace
+
+size_t tree_smem_bytes() { return sizeof(TreeShared); }
+
+static size_t direct_smem_bytes() { return sizeof(DirectShared); }
+
+cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
+  static bool configured = false;
+  size_t smem = tree_smem_bytes();
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(tree_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(tree_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  if (L.mode == IN_SOBOL)
+    tree_kernel<false><<<grid, NT, smem, st>>>(L);
+  else
+    tree_kernel<true><<<grid, NT, smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_direct(const Launch &L, int grid, cudaStream_t st) {
+  static bool configured = false;
+  size_t smem = direct_smem_bytes();
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  direct_kernel<<<grid, NT, smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fallback(const Launch &L, int grid, cudaStream_t st) {
+  static bool configured = false;
+  size_t smem = direct_smem_bytes();
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  fallback_kernel<<<grid, NT, smem, st>>>(L);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reduce(const Launch &L, kb_accum *acc_dev, cudaStream_t st) {
+  if (L.n_items == 0) return cudaSuccess;
+  reduce_kernel<<<L.n_items, NT, 0, st>>>(L, acc_dev);
+  return cudaGetLastError();
+}
+
+} // namespace kb

@@ -1,0 +1,117 @@
+"""Host-side g0 tables of the single-level dot with flat-band leads.
+
+keldy builds g0^<(t), g0^>(t) on the uniform mesh [-time_max, time_max] with an odd
+number of points (model.cpp:79-90, 139-177). This module produces the same tables:
+
+* :func:`flatband_analytic` restates keldy's zero-temperature formula
+  (``make_flat_band_analytic``, model.cpp:428-466): beta = infinity, bias 0, eps_d 0.
+* :func:`flatband` evaluates the Fourier transform of the flat-band dot functions
+  (model.hpp:100-112, 129-130; Delta^R = -i Gamma/2 per lead, model.cpp:107-111) for
+  any beta, eps_d and bias: the zero-temperature part in closed form through the
+  complex exponential integral E1, the finite-temperature correction (localised within
+  ~36/beta of each chemical potential) by Gauss-Legendre quadrature. Accurate to
+  ~1e-12; keldy's own "fft"/"contour" methods approximate the same functions.
+
+Conventions follow keldy: g(t) = int dw/2pi e^{-iwt} g(w), mu_left = -V/2,
+mu_right = +V/2, and t < 0 from g(-t) = -conj(g(t)) (model.cpp:302-314).
+"""
+from __future__ import annotations
+
+import numpy as np
+from scipy.special import exp1, expi
+
+
+def time_mesh(time_max, npts):
+    """keldy's retime mesh: npts points on [-time_max, time_max]; an even count is raised
+    by one so that t = 0 is a mesh point (model.cpp:87-90)."""
+    if npts % 2 == 0:
+        npts += 1
+    delta = (time_max - (-time_max)) / (npts - 1)
+    return -time_max + np.arange(npts) * delta
+
+
+def flatband_analytic(gamma, time_max, npts):
+    """Zero-temperature flat band, eps_d = 0, bias 0 (model.cpp:428-466):
+    g^<(t) = [e^{Gt} Ei(-Gt) - e^{-Gt} Ei(Gt)]/(2 pi) + i/2 e^{-|Gt|}, g^<(0) = i/2,
+    g^> = conj(g^<)."""
+    t = time_mesh(time_max, npts)
+    gt = gamma * t
+    with np.errstate(all="ignore"):
+        re = (np.exp(gt) * expi(-gt) - np.exp(-gt) * expi(gt)) / (2 * np.pi)
+    gl = re + 0.5j * np.exp(-np.abs(gt))
+    gl[t == 0.0] = 0.5j
+    return t, gl, np.conj(gl)
+
+
+def _lorentz_below(t, mu, eps, gamma):
+    """K(t) = int_{-inf}^{mu} e^{-iwt} / ((w-eps)^2 + gamma^2) dw for t > 0 (array t)."""
+    out = np.zeros(t.shape, dtype=np.complex128)
+    for sgn in (+1, -1):
+        z = eps + 1j * sgn * gamma
+        v = 1j * (mu - z) * t
+        if sgn < 0 and mu == eps:
+            # the path ends on E1's cut (v = -gamma t): take the limit from below
+            e1 = -expi(gamma * t) + 1j * np.pi
+        else:
+            e1 = exp1(v)
+            # continuation of E1 across its cut when the path Re v = t Im z < 0 passes Im v = 0
+            if sgn < 0 and mu > eps:
+                e1 = e1 + 2j * np.pi
+        J = -np.exp(-1j * z * t) * e1
+        out += sgn * J
+    return out / (2j * gamma)
+
+
+def _fermi_correction(t, mu, eps, gamma, beta, nodes=240):
+    """int dx e^{-i(x+mu)t} d(x) / ((x+mu-eps)^2 + gamma^2), d(x) = n_F(x) - theta(-x)."""
+    W = 36.0 / beta
+    xg, wg = np.polynomial.legendre.leggauss(nodes)
+    out = np.zeros(t.shape, dtype=np.complex128)
+    for a, b in ((-W, 0.0), (0.0, W)):
+        x = 0.5 * (b - a) * xg + 0.5 * (b + a)
+        w = 0.5 * (b - a) * wg
+        ax = np.abs(x)
+        d = np.sign(x) * np.exp(-beta * ax) / (1.0 + np.exp(-beta * ax))
+        f = w * d / ((x + mu - eps) ** 2 + gamma ** 2)
+        for s in range(0, len(t), 8192):
+            ts = t[s:s + 8192]
+            out[s:s + 8192] += np.exp(-1j * np.outer(ts, x + mu)) @ f
+    return out
+
+
+def flatband(gamma, eps_d, bias_V, beta, time_max, npts):
+    """g^<, g^> of the dot coupled to two flat-band leads (each Delta^R = -i gamma/2) at
+    inverse temperature beta (np.inf for zero temperature). Returns (t, lesser, greater)."""
+    t = time_mesh(time_max, npts)
+    tp = t[t > 0]
+    mus = (-bias_V / 2.0, bias_V / 2.0)
+    full = np.pi / gamma * np.exp(-1j * eps_d * tp - gamma * tp)
+    less = np.zeros(tp.shape, dtype=np.complex128)
+    great = np.zeros(tp.shape, dtype=np.complex128)
+    for mu in mus:
+        below = _lorentz_below(tp, mu, eps_d, gamma)
+        corr = _fermi_correction(tp, mu, eps_d, gamma, beta) if np.isfinite(beta) else 0.0
+        less += below + corr
+        great += full - below - corr
+    pref = gamma / (2 * np.pi)
+    gl_pos = 1j * pref * less
+    gg_pos = -1j * pref * great
+    # t = 0: int n(w) / ((w-eps)^2 + gamma^2) dw in closed form at T = 0, plus correction
+    occ = 0.0
+    for mu in mus:
+        k0 = (np.arctan((mu - eps_d) / gamma) + np.pi / 2) / gamma
+        c0 = _fermi_correction(np.zeros(1), mu, eps_d, gamma, beta)[0].real if np.isfinite(beta) else 0.0
+        occ += k0 + c0
+    g0l = 1j * pref * occ
+    g0g = -1j * pref * (2 * np.pi / gamma - occ)
+    n = len(t)
+    mid = n // 2
+    gl = np.empty(n, dtype=np.complex128)
+    gg = np.empty(n, dtype=np.complex128)
+    gl[mid + 1:] = gl_pos
+    gg[mid + 1:] = gg_pos
+    gl[mid] = g0l
+    gg[mid] = g0g
+    gl[:mid] = -np.conj(gl_pos[::-1])
+    gg[:mid] = -np.conj(gg_pos[::-1])
+    return t, gl, gg

@@ -1,0 +1,146 @@
+"""Generates tests/golden/golden.npz and tests/golden/keldy_tests.json.
+
+Run in a checkout that has keldy's sources (KELDY_SRC, default /root/reference) and a
+built oracle/_ref (``make -C oracle``):
+
+    python tests/golden/make_golden.py
+
+* golden.npz: outputs of keldy's own code (digitalseq_b2g.hpp, the warper headers and
+  wick_direct.cpp, compiled by oracle/Makefile) on seeded inputs: Sobol points, warper
+  chains, integrand values (two g0 tables, several external-point pairs, orders 0-6),
+  eval_no_det values and the integrator's sums.
+* keldy_tests.json: known answers read from keldy's test files: the Horvatic-Zlatic
+  charge series and its parameters (test/c++/impurity_oneband/compute_obs_test.cpp),
+  and the plasma-warper vectors (test/c++/warpers/warper_plasma_uv_test.cpp).
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.pyoracle import (Reference, W_EXPONENTIAL, W_IDENTITY, W_INVERSE, W_INVERSE_POWER,  # noqa: E402
+                             W_INVERSE_SQUARE, W_PLASMA_UV, W_UNIFORM)
+from keldy_b200.g0_tables import flatband, flatband_analytic  # noqa: E402
+
+KELDY_SRC = os.environ.get("KELDY_SRC", "/root/reference")
+
+SOBOL_CASES = [  # (dim, seed, do_shift, do_scramble, seed_shift)
+    (1, 0, 0, 0, 0), (3, 0, 0, 0, 0), (8, 0, 0, 0, 0), (12, 0, 0, 0, 0), (8, 1000, 0, 0, 0),
+    (8, 0, 1, 0, 1), (8, 0, 0, 1, 2), (10, 0, 1, 1, 3), (16, 77, 1, 1, -4), (40, 0, 1, 1, 5),
+]
+SOBOL_COUNT = 96
+
+CHAINS = {
+    "plasma": [(W_PLASMA_UV, 20.0, 0.0)],
+    "exponential": [(W_EXPONENTIAL, 20.0, 1.0)],
+    "plasma_exponential": [(W_PLASMA_UV, 20.0, 0.0), (W_EXPONENTIAL, 20.0, 1.0)],
+    "plasma_inverse_square": [(W_PLASMA_UV, 20.0, 0.0), (W_INVERSE_SQUARE, 20.0, 1.0)],
+    "inverse": [(W_INVERSE, 10.0, 1.5)],
+    "inverse_power3": [(W_INVERSE_POWER, 10.0, 1.5, 3)],
+    "uniform": [(W_UNIFORM, 10.0, 0.0)],
+    "identity": [(W_IDENTITY, 0.0, 0.0)],
+    "inverse_exponential": [(W_INVERSE, 10.0, 1.0), (W_EXPONENTIAL, 1.0, 1.0)],
+}
+
+# (name, A, B): gf_index tuples (time, spin, k_idx, timesplit, orbital)
+EXTERNALS = [
+    ("charge", (10.0, 0, 0, 0, 0), (10.0, 0, 1, 0, 0)),
+    ("ab", (4.0, 0, 0, 0, 0), (5.0, 0, 0, 0, 0)),
+    ("down_bwd", (7.5, 1, 1, 0, 0), (2.0, 1, 0, 0, 0)),
+]
+
+
+def keldy_test_values():
+    src = open(os.path.join(KELDY_SRC, "test/c++/impurity_oneband/compute_obs_test.cpp")).read()
+    m = re.search(r"HZ_charge_series = \{([^}]*)\}", src)
+    hz = [float(x) for x in m.group(1).replace("\n", " ").split(",")]
+    pl = open(os.path.join(KELDY_SRC, "test/c++/warpers/warper_plasma_uv_test.cpp")).read()
+    vecs = []
+    for block in re.findall(r"TEST\(ViUiMaps, \w+\).*?\n}\n", pl, re.S):
+        t_max = float(re.search(r"t_max = ([\d.]+)", block).group(1))
+        ui = [float(x) for x in re.search(r"ui_times = \{([^}]*)\}", block).group(1).split(",")]
+        vi = [float(x) for x in re.search(r"vi_result = \{([^}]*)\}", block).group(1).split(",")]
+        vecs.append({"t_max": t_max, "ui": ui, "vi": vi})
+    return {
+        "source": "keldy test/c++/impurity_oneband/compute_obs_test.cpp:93-181, "
+                  "test/c++/warpers/warper_plasma_uv_test.cpp:15-43",
+        "hz_charge_series": hz,
+        "hz_params": {"beta": "inf", "bias_V": 0.0, "eps_d": 0.0, "Gamma": 1.0, "time_max": 30.0,
+                      "nr_time_points_gf": 10001, "alpha": 0.0, "bath_type": "flatband", "ft_method": "analytic",
+                      "t": 20.0, "orders": [1, 6],
+                      "runs": [{"warper": "inverse_square", "w": 1.0, "n_points": 10000, "rtol": [1e-3, 1e-2]},
+                               {"warper": "exponential", "w": 2.0, "n_points": 50000, "rtol": [1e-2, 1e-2]}]},
+        "plasma_vectors": vecs,
+    }
+
+
+def main():
+    ref = Reference()
+    rng = np.random.default_rng(20240601)
+    out = {}
+    # Sobol
+    for i, (dim, seed, sh, sc, ss) in enumerate(SOBOL_CASES):
+        out[f"sobol_{i}"] = ref.sobol_points(dim, seed, SOBOL_COUNT, bool(sh), bool(sc), ss)
+    out["sobol_cases"] = np.array(SOBOL_CASES, dtype=np.int64)
+    # warpers
+    for name, chain in CHAINS.items():
+        x = rng.random((64, 6))
+        u, j = ref.warp(chain, x, "reverse")
+        out[f"warp_{name}_li"] = x
+        out[f"warp_{name}_ui"] = u
+        out[f"warp_{name}_jr"] = j
+        y = np.abs(u) + 0.05 if name not in ("identity",) else x
+        y = np.minimum(y, 9.5)
+        lf, jf = ref.warp(chain, y, "forward")
+        out[f"warp_{name}_fin"] = y
+        out[f"warp_{name}_fout"] = lf
+        out[f"warp_{name}_jf"] = jf
+    # g0 tables: zero-temperature analytic and finite beta, t in [-10, 10]
+    _, l0, g0 = flatband_analytic(1.0, 10.0, 2001)
+    _, l1, g1 = flatband(1.0, 0.3, 0.4, 20.0, 10.0, 2001)
+    out["table_T0_lesser"], out["table_T0_greater"] = l0, g0
+    out["table_beta20_lesser"], out["table_beta20_greater"] = l1, g1
+    for tname, (le, gr) in {"T0": (l0, g0), "beta20": (l1, g1)}.items():
+        for alpha in (0.0, 0.8):
+            model = ref.model(10.0, le, gr, alpha)
+            for ename, A, B in EXTERNALS:
+                for n in range(0, 7):
+                    t = rng.random((24, n)) * 10.0
+                    if n >= 2:
+                        t[0, 1] = t[0, 0]            # equal vertex times
+                        t[1, 0] = -0.5               # out of the domain
+                        t[2, :] = np.sort(t[2, :])[::-1]
+                    if n >= 1:
+                        t[3, 0] = A[0]               # vertex at an external time
+                    key = f"integrand_{tname}_a{alpha}_{ename}_n{n}"
+                    vals, dom = ref.integrand(model, A, B, t)
+                    out[key + "_t"] = t
+                    out[key + "_v"] = vals
+                    out[key + "_d"] = dom
+                    if n <= 2:
+                        nv, nd = ref.integrand(model, A, B, t, no_det=True)
+                        out[key + "_nodet"] = nv
+    # integrator sums (keldy's loop, sobol_unshifted seed 0)
+    model = ref.model(10.0, l1, g1, 0.0)
+    for n in (1, 2, 3, 4):
+        for cname in ("plasma_exponential", "uniform"):
+            chain = [(W_PLASMA_UV, 10.0, 0.0), (W_EXPONENTIAL, 10.0, 1.0)] if cname == "plasma_exponential" \
+                else [(W_UNIFORM, 10.0, 0.0)]
+            s, npts, ndom = ref.integrate(model, EXTERNALS[0][1], EXTERNALS[0][2], chain, n, 4096)
+            out[f"integrate_{cname}_n{n}"] = np.array([s.real, s.imag, npts, ndom])
+    np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
+    with open(os.path.join(HERE, "keldy_tests.json"), "w") as f:
+        json.dump(keldy_test_values(), f, indent=1)
+    print("wrote", len(out), "arrays")
+
+
+if __name__ == "__main__":
+    main()

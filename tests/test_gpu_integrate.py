@@ -1,0 +1,121 @@
+"""integrator::run on the GPU (Sobol -> warper chain -> integrand -> sum), through the C
+ABI, against keldy's integrator (golden.npz), the CPU oracle and keldy's Horvatic-Zlatic
+known answer."""
+import numpy as np
+import pytest
+
+from keldy_b200 import capi
+from keldy_b200.g0_tables import flatband_analytic
+from tests.golden.make_golden import EXTERNALS
+
+pytestmark = pytest.mark.gpu
+
+CHARGE = (EXTERNALS[0][1], EXTERNALS[0][2])
+PLASMA_EXP = [(capi.WARPER_PLASMA_UV, 10.0, 0.0), (capi.WARPER_EXPONENTIAL, 10.0, 1.0)]
+UNIFORM = [(capi.WARPER_UNIFORM, 10.0, 0.0)]
+
+
+def _item(model, rng, chain, order, n, k_first=1, A=CHARGE[0], B=CHARGE[1], cutoff=0.0):
+    return dict(model=model, rng=rng, chain=chain, A=A, B=B, cutoff=cutoff, order=order, k_first=k_first,
+                n_points=n)
+
+
+@pytest.mark.parametrize("algo", [capi.ALGO_AUTO, capi.ALGO_DIRECT])
+def test_integrate_vs_keldy(ctx, oracle, golden, algo):
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    for n in (1, 2, 3, 4):
+        rng = ctx.sobol(n)
+        for cname, chain in (("plasma_exponential", PLASMA_EXP), ("uniform", UNIFORM)):
+            (s, npts, ndom, nfb), = capi.integrate(ctx, [_item(gm, rng, chain, n, 4096)], algo)
+            g = golden[f"integrate_{cname}_n{n}"]
+            _, _, _, sc = oracle.integrate(om, CHARGE[0], CHARGE[1], chain, n, 4096)
+            assert (npts, ndom) == (int(g[2]), int(g[3]))
+            assert abs(s - complex(g[0], g[1])) <= 1e-12 * sc
+
+
+def test_integrate_higher_orders_vs_oracle(ctx, oracle, golden):
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    for n, npts in ((5, 1024), (6, 512), (7, 256), (8, 128), (9, 64), (10, 24)):
+        rng = ctx.sobol(n)
+        (s, np_, nd, _), = capi.integrate(ctx, [_item(gm, rng, PLASMA_EXP, n, npts)])
+        w, onp, ond, sc = oracle.integrate(om, CHARGE[0], CHARGE[1], PLASMA_EXP, n, npts)
+        assert (np_, nd) == (onp, ond)
+        assert abs(s - w) <= 1e-12 * sc, (n, abs(s - w) / sc)
+
+
+def test_batched_items_equal_separate_calls(ctx, golden):
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr)
+    rngs = {n: ctx.sobol(n) for n in range(1, 8)}
+    shifted = ctx.sobol(5, 31, True, True, 17)
+    items = [_item(gm, rngs[n], PLASMA_EXP, n, 3000 + 17 * n, k_first=1 + 5 * n) for n in range(1, 8)]
+    items.append(_item(gm, shifted, UNIFORM, 5, 2000))
+    items.append(_item(gm, rngs[3], PLASMA_EXP, 3, 0))
+    batched = capi.integrate(ctx, items)
+    for it, b in zip(items, batched):
+        assert capi.integrate(ctx, [it])[0] == b
+    # deterministic: the same call twice gives identical sums
+    assert capi.integrate(ctx, items) == batched
+
+
+def test_integrate_equals_sum_of_point_values(ctx, golden):
+    le, gr = golden["table_T0_lesser"], golden["table_T0_greater"]
+    gm = ctx.model(10.0, le, gr)
+    n, N = 4, 777
+    rng = ctx.sobol(n, 31, True, False, 3)
+    (s, npts, ndom, _), = capi.integrate(ctx, [_item(gm, rng, PLASMA_EXP, n, N, k_first=10)])
+    li = rng.points(10, N)
+    v, jac, dom = gm.evaluate_warped(CHARGE[0], CHARGE[1], PLASMA_EXP, li)
+    assert npts == N and ndom == dom.sum()
+    assert abs(s - v.sum()) <= 1e-13 * np.abs(v).sum()
+
+
+def test_integrate_errors(ctx, golden):
+    gm = ctx.model(10.0, golden["table_T0_lesser"], golden["table_T0_greater"])
+    rng = ctx.sobol(3, 12)
+    with pytest.raises(capi.KbError) as e:
+        capi.integrate(ctx, [_item(gm, rng, UNIFORM, 3, 5000)])
+    assert e.value.code == capi.KB_E_EXHAUSTED
+    with pytest.raises(capi.KbError):
+        capi.integrate(ctx, [_item(gm, ctx.sobol(2), UNIFORM, 3, 10)])  # fewer Sobol dimensions than the order
+    with pytest.raises(capi.KbError) as e:  # warper reaching outside the g0 window
+        capi.integrate(ctx, [_item(gm, ctx.sobol(2), [(capi.WARPER_UNIFORM, 25.0, 0.0)], 2, 100)])
+    assert e.value.code == capi.KB_E_RANGE
+
+
+def test_integrate_pivot_guard(ctx, oracle):
+    t = np.linspace(-10, 10, 2001)
+    le = 1j * t * np.exp(-t * t / 8) + 0.2 * np.sin(t)
+    gr = -np.conj(le[::-1])
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    for n in (3, 5):
+        (s, npts, nd, nfb), = capi.integrate(ctx, [_item(gm, ctx.sobol(n), PLASMA_EXP, n, 300)])
+        w, _, ond, sc = oracle.integrate(om, CHARGE[0], CHARGE[1], PLASMA_EXP, n, 300)
+        assert nfb > 0 and nd == ond
+        assert abs(s - w) <= 1e-12 * sc
+
+
+@pytest.mark.parametrize("run", [0, 1])
+def test_horvatic_zlatic_series(ctx, keldy_tests, run):
+    """keldy's known answer (compute_obs_test.cpp:93-181): charge series of the flat-band
+    dot at T = 0 to order 6."""
+    p = keldy_tests["hz_params"]
+    cfg = p["runs"][run]
+    hz = keldy_tests["hz_charge_series"]
+    _, le, gr = flatband_analytic(p["Gamma"], p["time_max"], p["nr_time_points_gf"])
+    gm = ctx.model(p["time_max"], le, gr)
+    t = p["t"]
+    kind = capi.WARPER_INVERSE_SQUARE if cfg["warper"] == "inverse_square" else capi.WARPER_EXPONENTIAL
+    chain = [(capi.WARPER_PLASMA_UV, t, 0.0), (kind, t, cfg["w"])]
+    items = [_item(gm, ctx.sobol(n), chain, n, cfg["n_points"], A=(t, 0, 0), B=(t, 0, 1)) for n in range(1, 7)]
+    res = capi.integrate(ctx, items)
+    i_n = [1, 1j, -1, -1j]
+    for n, (s, npts, _, _) in zip(range(1, 7), res):
+        q = -1j * i_n[n % 4] * s / npts
+        tol = cfg["rtol"][0] if n < 5 else cfg["rtol"][1]
+        assert abs(q - hz[n]) <= tol * abs(hz[n]), (n, q, hz[n])
