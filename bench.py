@@ -333,6 +333,19 @@ def run_ours(args, rank, world, local_rank):
     ctx.close()
 
 
+def run_single(args):
+    from keldy_b200 import capi
+    from keldy_b200.g0_tables import flatband
+    ctx = capi.Context(0)
+    _, le, gr = flatband(GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS)
+    model = ctx.model(T_MAX, le, gr)
+    chain = [(capi.WARPER_PLASMA_UV, T_MAX, 0.0), (capi.WARPER_EXPONENTIAL, T_MAX, 1.0 / GAMMA)]
+    res = capi.integrate(ctx, [dict(model=model, rng=ctx.sobol(args.order), chain=chain, A=(T_MAX, 0, 0, 0, 0),
+                                    B=(T_MAX, 0, 1, 0, 0), order=args.order, k_first=1, n_points=args.points)])
+    print("single", args.order, args.points, res[0])
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,11 +356,15 @@ def main():
     ap.add_argument("--points", type=int, default=1 << 20)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--ref-seconds", type=float, default=2.0, help="seconds of CPU work per reference-arm step")
+    ap.add_argument("--single", action="store_true",
+                    help="one integrate call of --points points at --order and exit (for profiler captures)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
+    if args.single:
+        run_single(args)
+    elif args.impl == "reference":
         run_reference_arm(args, rank, world)
     else:
         run_ours(args, rank, world, local_rank)
