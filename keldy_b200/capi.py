@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -160,9 +161,12 @@ class Context:
         check(L.kb_context_create(device, C.byref(h)))
         self.h = h
         self.L = L
+        self._deps = weakref.WeakSet()  # models and generators, destroyed before the context
 
     def close(self):
         if self.h:
+            for d in list(self._deps):
+                d.close()
             self.L.kb_context_destroy(self.h)
             self.h = None
 
@@ -227,10 +231,16 @@ class Sobol:
         check(ctx.L.kb_sobol_create(ctx.h, dim, log_max_points, int(do_shift), int(do_scramble), int(seed_shift),
                                     C.byref(h)))
         self.h = h
+        ctx._deps.add(self)
+
+    def close(self):
+        if self.h:
+            self.ctx.L.kb_sobol_destroy(self.h)
+            self.h = None
 
     def __del__(self):
         try:
-            self.ctx.L.kb_sobol_destroy(self.h)
+            self.close()
         except Exception:
             pass
 
@@ -252,6 +262,7 @@ class Model:
         h = _VP()
         check(ctx.L.kb_model_create(ctx.h, self.npts, float(time_max), float(alpha), C.byref(h)))
         self.h = h
+        ctx._deps.add(self)
         self.set_table(0, 0, 0, lesser, greater)
         if lesser_down is not None:
             self.set_table(1, 0, 0, lesser_down, greater_down)
@@ -264,9 +275,14 @@ class Model:
         assert le.size == 2 * self.npts and gr.size == 2 * self.npts
         check(self.ctx.L.kb_model_set_table(self.h, spin, o1, o2, _dp(le), _dp(gr)))
 
+    def close(self):
+        if self.h:
+            self.ctx.L.kb_model_destroy(self.h)
+            self.h = None
+
     def __del__(self):
         try:
-            self.ctx.L.kb_model_destroy(self.h)
+            self.close()
         except Exception:
             pass
 

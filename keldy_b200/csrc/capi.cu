@@ -79,8 +79,11 @@ struct kb_context {
   std::mutex mu;
 };
 
+// Models and generators belong to a context and must be destroyed before it; their
+// destroy functions touch only the device they live on.
 struct kb_model {
   kb_context *ctx = nullptr;
+  int device = 0;
   int npts = 0;
   double tmax = 0, alpha = 0;
   double2 *tab[2][2][2] = {};
@@ -90,6 +93,7 @@ struct kb_model {
 
 struct kb_sobol {
   kb_context *ctx = nullptr;
+  int device = 0;
   int dim = 0, m = 0;
   uint32_t *d_Csr = nullptr;
   uint32_t *d_shfr = nullptr;
@@ -187,6 +191,7 @@ int kb_sobol_create(kb_context *ctx, int dim, int log_max_points, int do_shift, 
   sobol_setup(dim, log_max_points, do_shift != 0, do_scramble != 0, seed_shift, Csr.data(), shfr.data());
   auto *s = new kb_sobol;
   s->ctx = ctx;
+  s->device = ctx->device;
   s->dim = dim;
   s->m = log_max_points;
   cudaSetDevice(ctx->device);
@@ -216,7 +221,7 @@ int kb_sobol_matrices(int dim, int log_max_points, int do_shift, int do_scramble
 
 int kb_sobol_destroy(kb_sobol *s) {
   if (!s) return KB_OK;
-  cudaSetDevice(s->ctx->device);
+  cudaSetDevice(s->device); // cudaFree waits for the device's pending work
   cudaFree(s->d_Csr);
   cudaFree(s->d_shfr);
   delete s;
@@ -371,6 +376,7 @@ int kb_model_create(kb_context *ctx, int npts, double time_max, double alpha, kb
   KB_CHECK(time_max > 0.0 && std::isfinite(time_max), "time_max must be > 0");
   auto *m = new kb_model;
   m->ctx = ctx;
+  m->device = ctx->device;
   m->npts = npts;
   m->tmax = time_max;
   m->alpha = alpha;
@@ -380,8 +386,7 @@ int kb_model_create(kb_context *ctx, int npts, double time_max, double alpha, kb
 
 int kb_model_destroy(kb_model *m) {
   if (!m) return KB_OK;
-  cudaSetDevice(m->ctx->device);
-  cudaStreamSynchronize(m->ctx->stream);
+  cudaSetDevice(m->device); // cudaFree waits for the device's pending work
   for (int s = 0; s < 2; ++s)
     for (int a = 0; a < 2; ++a)
       for (int b = 0; b < 2; ++b) cudaFree(m->tab[s][a][b]);
