@@ -182,6 +182,22 @@ typedef struct {
  * sequence on the context's stream; sums are deterministic (fixed reduction order). */
 int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc);
 
+/* Integrate without allocating device memory. No counterpart in keldy: this entry point
+ * is for callers that cannot call cudaMalloc (a host application whose own allocator
+ * owns the device's memory, or a latency-bound loop that must not pay cudaMalloc's
+ * implicit synchronisation). Same work and sums as kb_integrate with KB_ALGO_AUTO, but
+ * its scratch lives in one file-scope device array of KB_NOALLOC_SCRATCH_BYTES (held by
+ * every GPU that loads the library until exit) instead of per-call allocations; the
+ * model tables and Sobol matrices are the caller's existing objects. Limits: at most
+ * KB_NOALLOC_MAX_ITEMS work items and KB_NOALLOC_MAX_CHUNKS * 128 points per call
+ * (KB_E_INVALID beyond). All calls share the array: calls that overlap on the GPU race.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ * make it before any stream capture. */
+#define KB_NOALLOC_MAX_ITEMS 64
+#define KB_NOALLOC_MAX_CHUNKS 65536
+#define KB_NOALLOC_SCRATCH_BYTES (4u << 20)
+int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc);
+
 /* ----------------------------------------------------------------- peaks --- */
 /* Measures the FP64 FMA rate of this device (FLOP/s, 2 per FMA) with a dependent-chain
  * kernel of `iters` FMAs per thread; used as the roofline denominator. */

@@ -32,8 +32,9 @@ EXPORTS = [
     "kb_sobol_points_dev",
     "kb_warp", "kb_model_create", "kb_model_destroy", "kb_model_set_table", "kb_model_set_table_dev",
     "kb_g0_eval", "kb_integrand_eval", "kb_integrand_eval_no_det", "kb_evaluate_warped", "kb_integrate",
-    "kb_fp64_peak",
+    "kb_fp64_peak", "kb_integrate_noalloc",
 ]
+NOALLOC_MAX_ITEMS, NOALLOC_MAX_CHUNKS = 64, 65536
 
 
 class KbError(RuntimeError):
@@ -109,6 +110,7 @@ def load():
                                      C.c_int64, _D, C.c_int, C.c_int, _D, _D, _I]
     L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
     L.kb_fp64_peak.argtypes = [_VP, C.c_int, _D]
+    L.kb_integrate_noalloc.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(Accum)]
     _lib = L
     return L
 
@@ -334,6 +336,29 @@ class Model:
                                             count, _dp(li), int(keep_u_hypercube), algo, _dp(out.view(np.float64)),
                                             _dp(jac), _ip(dom)))
         return out, jac, dom
+
+
+def _works(items):
+    n = len(items)
+    works = (Work * max(1, n))()
+    keep = []
+    for i, it in enumerate(items):
+        arr, L = chain_array(it["chain"])
+        keep.append(arr)
+        works[i] = Work(it["model"].h.value, it["rng"].h.value, C.cast(arr, C.POINTER(Warper)), L,
+                        Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
+                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]))
+    return works, keep
+
+
+def integrate_noalloc(ctx, items):
+    """kb_integrate_noalloc: as integrate(algo=ALGO_AUTO), for callers that cannot allocate
+    device memory; its scratch is a fixed device array inside the library (at most 64
+    items and 8,388,608 points per call)."""
+    works, keep = _works(items)
+    acc = (Accum * max(1, len(items)))()
+    check(ctx.L.kb_integrate_noalloc(ctx.h, works, len(items), acc))
+    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback) for a in acc[:len(items)]]
 
 
 def integrate(ctx, items, algo=ALGO_AUTO):

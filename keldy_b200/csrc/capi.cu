@@ -803,3 +803,158 @@ int kb_fp64_peak(kb_context *ctx, int iters, double *flops_per_s) {
 }
 
 } // extern "C"
+
+// ------------------------------------------------- integrate without allocating
+// kb_integrate_noalloc: the integrate path with its scratch (item descriptors, chunk
+// offsets, the scheduling counter, per-chunk partial sums and the per-item sums) in one
+// file-scope device array instead of memory allocated per call. It serves callers that
+// cannot call cudaMalloc: a host application whose own allocator owns all of the
+// device's memory, or a latency-bound loop that must not pay cudaMalloc's implicit
+// device synchronisation.
+//
+// The array is KB_NOALLOC_SCRATCH_BYTES per device, held by every GPU that loads the
+// library until the process exits. All calls share it and it keeps the last call's
+// contents: each call clears the counter and the sums it needs, and two calls whose
+// work overlaps on the GPU (different streams, contexts or threads on one device) race
+// on it. The device address of the array is looked up with cudaGetSymbolAddress the
+// first time the entry point runs on a device (with that device current); make that
+// first call before any stream capture.
+namespace {
+constexpr int NOALLOC_MAX_DEVICES = 64;
+constexpr size_t NOALLOC_ITEMS_OFF = 0;
+constexpr size_t NOALLOC_OFFS_OFF = NOALLOC_ITEMS_OFF + sizeof(ItemDev) * KB_NOALLOC_MAX_ITEMS;
+constexpr size_t NOALLOC_ACC_OFF = ((NOALLOC_OFFS_OFF + sizeof(long long) * (KB_NOALLOC_MAX_ITEMS + 1)) + 255) / 256 * 256;
+constexpr size_t NOALLOC_CNT_OFF = NOALLOC_ACC_OFF + sizeof(kb_accum) * 2 * KB_NOALLOC_MAX_ITEMS;
+constexpr size_t NOALLOC_PART_OFF = (NOALLOC_CNT_OFF + sizeof(int) + 255) / 256 * 256;
+constexpr size_t NOALLOC_BYTES = NOALLOC_PART_OFF + sizeof(ChunkPartial) * (size_t)KB_NOALLOC_MAX_CHUNKS;
+static_assert(NOALLOC_BYTES <= KB_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the stated maximum");
+
+static __device__ __align__(256) unsigned char kb_noalloc_scratch[KB_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+// Device address of kb_noalloc_scratch on the current device (looked up once per device).
+int noalloc_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= NOALLOC_MAX_DEVICES) return fail(KB_E_INVALID, "device index too large for kb_integrate_noalloc");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, kb_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(KB_E_CUDA, std::string("cudaGetSymbolAddress(kb_noalloc_scratch): ") + cudaGetErrorString(e));
+    g_noalloc_addr[device] = static_cast<unsigned char *>(p);
+  }
+  *out = g_noalloc_addr[device];
+  return KB_OK;
+}
+} // namespace
+
+extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc) {
+  KB_CHECK(ctx && (n_work == 0 || (work && acc)), "kb_integrate_noalloc: null argument");
+  if (n_work < 0 || n_work > KB_NOALLOC_MAX_ITEMS)
+    return fail(KB_E_INVALID, "kb_integrate_noalloc takes at most KB_NOALLOC_MAX_ITEMS (64) work items");
+  if (n_work == 0) return KB_OK;
+  ItemDev items[KB_NOALLOC_MAX_ITEMS];
+  int group_of[KB_NOALLOC_MAX_ITEMS];
+  long long chunks_total = 0;
+  for (int i = 0; i < n_work; ++i) {
+    const kb_work &w = work[i];
+    int st = check_integrand(w.m, &w.f, w.order);
+    if (st) return st;
+    KB_CHECK(w.rng, "work item without a Sobol generator");
+    KB_CHECK(w.n_points >= 0, "n_points must be >= 0");
+    KB_CHECK(w.order >= 1, "integrator dimension must be > 0 (Dimension of the integration space must be > 0.)");
+    if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
+    st = check_sobol_range(w.rng, w.k_first, w.n_points);
+    if (st) return st;
+    ItemDev &it = items[i];
+    it = make_item(w.m, &w.f, w.order);
+    st = make_chain(w.chain, w.chain_len, it.chain);
+    if (st) return st;
+    it.chain_len = w.chain_len;
+    it.chain_start = w.chain_len;
+    it.rng = sobol_dev(w.rng);
+    it.k_first = w.k_first;
+    it.n_points = w.n_points;
+    group_of[i] = it.spin_symmetric ? 0 : 1;
+    chunks_total += (w.n_points + CHUNK_POINTS - 1) / CHUNK_POINTS;
+  }
+  if (chunks_total > KB_NOALLOC_MAX_CHUNKS)
+    return fail(KB_E_INVALID, "kb_integrate_noalloc: more than KB_NOALLOC_MAX_CHUNKS*128 (8,388,608) points in one call");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  unsigned char *base = nullptr;
+  int st = noalloc_scratch(ctx->device, &base);
+  if (st) return st;
+  cudaStream_t stream = ctx->stream;
+  ItemDev *d_items = reinterpret_cast<ItemDev *>(base + NOALLOC_ITEMS_OFF);
+  long long *d_offs = reinterpret_cast<long long *>(base + NOALLOC_OFFS_OFF);
+  kb_accum *d_acc = reinterpret_cast<kb_accum *>(base + NOALLOC_ACC_OFF);
+  int *d_cnt = reinterpret_cast<int *>(base + NOALLOC_CNT_OFF);
+  ChunkPartial *d_part = reinterpret_cast<ChunkPartial *>(base + NOALLOC_PART_OFF);
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), stream));
+  KB_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(kb_accum) * 2 * KB_NOALLOC_MAX_ITEMS, stream));
+  // Group 0 (tree) and group 1 (pivoted LU), heaviest orders first within a group; the
+  // groups use the item and chunk regions in turn, their sums land in separate halves.
+  int ids[2][KB_NOALLOC_MAX_ITEMS];
+  int nids[2] = {0, 0};
+  for (int g = 0; g < 2; ++g) {
+    for (int i = 0; i < n_work; ++i)
+      if (group_of[i] == g && items[i].n_points > 0) ids[g][nids[g]++] = i;
+    for (int a = 1; a < nids[g]; ++a) // stable insertion sort by order, descending
+      for (int b = a; b > 0 && items[ids[g][b]].order > items[ids[g][b - 1]].order; --b) {
+        int t = ids[g][b];
+        ids[g][b] = ids[g][b - 1];
+        ids[g][b - 1] = t;
+      }
+  }
+  ItemDev sorted[KB_NOALLOC_MAX_ITEMS];
+  long long offs[KB_NOALLOC_MAX_ITEMS + 1];
+  for (int g = 0; g < 2; ++g) {
+    if (nids[g] == 0) continue;
+    offs[0] = 0;
+    for (int j = 0; j < nids[g]; ++j) {
+      sorted[j] = items[ids[g][j]];
+      offs[j + 1] = offs[j] + (sorted[j].n_points + CHUNK_POINTS - 1) / CHUNK_POINTS;
+    }
+    KB_CUDA(cudaMemcpyAsync(d_items, sorted, sizeof(ItemDev) * nids[g], cudaMemcpyHostToDevice, stream));
+    KB_CUDA(cudaMemcpyAsync(d_offs, offs, sizeof(long long) * (nids[g] + 1), cudaMemcpyHostToDevice, stream));
+    KB_CUDA(cudaMemsetAsync(d_cnt, 0, sizeof(int), stream));
+    Launch L;
+    memset(&L, 0, sizeof(L));
+    L.items = d_items;
+    L.n_items = nids[g];
+    L.chunk_offsets = d_offs;
+    L.n_chunks = (int)offs[nids[g]];
+    L.chunk_counter = d_cnt;
+    L.mode = IN_SOBOL;
+    L.partials = d_part;
+    L.err = ctx->d_err;
+    if (g == 0) {
+      KB_CUDA(launch_tree(L, (int)std::min<long long>(L.n_chunks, ctx->tree_grid), stream));
+      KB_CUDA(launch_fallback(L, ctx->sm_count * 4, stream));
+    } else {
+      KB_CUDA(launch_direct(L, (int)std::min<long long>(L.n_chunks, ctx->sm_count * 4), stream));
+    }
+    KB_CUDA(launch_reduce(L, d_acc + g * KB_NOALLOC_MAX_ITEMS, stream));
+  }
+  kb_accum part[2][KB_NOALLOC_MAX_ITEMS];
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(part, d_acc, sizeof(part), cudaMemcpyDeviceToHost, stream));
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, stream));
+  KB_CUDA(cudaStreamSynchronize(stream));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  for (int g = 0; g < 2; ++g)
+    for (int j = 0; j < nids[g]; ++j) {
+      kb_accum &a = acc[ids[g][j]];
+      const kb_accum &p = part[g][j];
+      a.sum_re += p.sum_re;
+      a.sum_im += p.sum_im;
+      a.n_points += p.n_points;
+      a.n_in_domain += p.n_in_domain;
+      a.n_fallback += p.n_fallback;
+    }
+  return KB_OK;
+}
+
