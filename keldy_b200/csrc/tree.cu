@@ -42,6 +42,8 @@ struct TreeShared {
   double2 fval[NT];
   double fscale[NT];
   int flag[NT];      // bit 0: out of domain, bit 1: needs the pivoted-LU kernel
+  double2 wsum[NT / 32]; // per-warp partial sums of the per-point reduction
+  double wscale[NT / 32];
 };
 
 __device__ __forceinline__ int find_item(const long long *off, int n_items, long long c) {
@@ -81,6 +83,57 @@ __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, l
       if (x[j * np] < 0.0) dom = 0;
   jac_out[p] = jac;
   flag_out[p] = dom ? 0 : 1;
+}
+
+// Inputs of np points with one thread per (point, coordinate): Sobol coordinates (or
+// given inputs) into u[j*np + p], then the warper chain from its last warper to its
+// first, product warpers per coordinate, the plasma warper per point. The Jacobian
+// products are taken in keldy's order (per warper over the coordinates, then along the
+// chain). wtmp holds np*N doubles.
+__device__ void load_points_par(const Launch &L, const ItemDev &it, int N, int np, long long gp0, double *u,
+                                double *jac, int *flag, double *wtmp, bool keep) {
+  const int tid = threadIdx.x, nt = blockDim.x, total = np * N;
+  for (int r = tid; r < total; r += nt) {
+    int j = r / np, p = r - j * np;
+    long long gp = gp0 + p;
+    if (L.mode == IN_SOBOL) {
+      u[r] = sobol_coord(it.rng, it.k_first + (uint32_t)gp, j);
+    } else {
+      long long src = L.index ? (long long)L.index[gp] : gp;
+      u[r] = L.in[src * N + j];
+    }
+  }
+  if (tid < np) jac[tid] = 1.0;
+  __syncthreads();
+  const int start = (L.mode == IN_SOBOL) ? it.chain_len : (L.mode == IN_LI ? it.chain_start : 0);
+  for (int w = start - 1; w >= 0; --w) {
+    const WarperDev &wd = it.chain[w];
+    if (wd.kind == KB_WARPER_IDENTITY) continue;
+    if (wd.kind == KB_WARPER_PLASMA_UV) {
+      if (tid < np) warp_reverse_one(wd, N, u + tid, np);
+    } else {
+      for (int r = tid; r < total; r += nt) {
+        double x = warper_Finv(wd, u[r]);
+        u[r] = x;
+        wtmp[r] = 1.0 / warper_f1(wd, x);
+      }
+      __syncthreads();
+      if (tid < np) {
+        double jw = 1.0;
+        for (int j = 0; j < N; ++j) jw *= wtmp[j * np + tid];
+        jac[tid] *= jw;
+      }
+    }
+    __syncthreads();
+  }
+  if (tid < np) {
+    int dom = (it.f.A.spin == it.f.B.spin) ? 1 : 0;
+    if (keep)
+      for (int j = 0; j < N; ++j)
+        if (u[j * np + tid] < 0.0) dom = 0;
+    flag[tid] = dom ? 0 : 1;
+  }
+  __syncthreads();
 }
 
 // G (row-major, M = 2N+1) of np points: G[p*M*M + r*M + c]. Out-of-domain points get
@@ -148,29 +201,35 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
   }
 }
 
-// One breadth-first level: every node (size m) of the frontier spawns the children
-// that pivot on its rows 0 and 1 and drop both (size m-2).
-__device__ void tree_level(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *inv,
-                           int *flag, int nodes, int npp, int m, double floor_) {
-  const int mc = m - 2, nchild = 2 * nodes, mm = m * m;
-  for (int c = threadIdx.x; c < nchild; c += blockDim.x) {
+// One breadth-first level, both children of a node from one read of its rows: thread r
+// takes row i of parent `par` and writes row i of children 2 par (pivot on row 0) and
+// 2 par + 1 (pivot on row 1). Nodes per point = 2^lg_npp; m >= 9.
+__device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *inv,
+                            int *flag, int nodes, int lg_npp, int m, double floor_) {
+  const int mc = m - 2, mm = m * m, mcc = mc * mc;
+  for (int c = threadIdx.x; c < 2 * nodes; c += blockDim.x) {
     int par = c >> 1, b = c & 1;
-    double2 piv = cur[par * mm + b * m + b];
-    if (!(cabs1(piv) >= floor_)) flag[par / npp] |= 2;
+    double2 piv = cur[par * mm + b * (m + 1)];
+    if (!(cabs1(piv) >= floor_)) flag[par >> lg_npp] |= 2;
     inv[c] = crcp(piv);
     Dn[c] = cmul(Dc[par], piv);
   }
   __syncthreads();
-  const int rows = nchild * mc;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-    int c = r / mc, i = r - c * mc;
-    int par = c >> 1, b = c & 1;
+  const unsigned rows = (unsigned)(nodes * mc);
+  const unsigned magic = 0xFFFFFFFFu / (unsigned)mc + 1u; // r / mc == umulhi(r, magic) for r < 2^20, mc <= 31
+  for (unsigned r = threadIdx.x; r < rows; r += blockDim.x) {
+    const unsigned par = __umulhi(r, magic);
+    const unsigned i = r - par * (unsigned)mc;
     const double2 *S = cur + par * mm;
-    double2 Lf = cmul(S[(i + 2) * m + b], inv[c]);
-    const double2 *prow = S + b * m + 2;
-    const double2 *srow = S + (i + 2) * m + 2;
-    double2 *o = nxt + c * mc * mc + i * mc;
-    for (int j = 0; j < mc; ++j) o[j] = cfms(srow[j], Lf, prow[j]);
+    const double2 L0 = cmul(S[(i + 2) * m], inv[2 * par]);
+    const double2 L1 = cmul(S[(i + 2) * m + 1], inv[2 * par + 1]);
+    const double2 *srow = S + (i + 2) * m + 2, *p0 = S + 2, *p1 = S + m + 2;
+    double2 *o0 = nxt + (2 * par) * mcc + i * mc, *o1 = o0 + mcc;
+    for (int j = 0; j < mc; ++j) {
+      const double2 v = srow[j];
+      o0[j] = cfms(v, L0, p0[j]);
+      o1[j] = cfms(v, L1, p1[j]);
+    }
   }
   __syncthreads();
 }
@@ -198,11 +257,8 @@ __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *
 // Last two levels of a 5x5 node in registers: children on pivots 0/1, then the four
 // leaves, each leaf term (-1)^|a| det(s2)^2 * (1x1 Schur complement) written without
 // division as Db^2 T_cc (T_cc T_ee - T_ce T_ec).
-__device__ __forceinline__ void tree_bottom5(const double2 *R, double2 D, int parity, double floor_, bool want_scale,
-                                             double2 &sum, double &scale, bool &guard) {
-  double2 s[25];
-#pragma unroll
-  for (int i = 0; i < 25; ++i) s[i] = R[i];
+__device__ __forceinline__ void tree_bottom5r(const double2 (&s)[25], double2 D, int parity, double floor_,
+                                              bool want_scale, double2 &sum, double &scale, bool &guard) {
   sum = c2(0.0, 0.0);
   scale = 0.0;
 #pragma unroll
@@ -231,6 +287,72 @@ __device__ __forceinline__ void tree_bottom5(const double2 *R, double2 D, int pa
     }
   }
   if (parity & 1) sum = c2(-sum.x, -sum.y);
+}
+
+__device__ __forceinline__ void tree_bottom5(const double2 *R, double2 D, int parity, double floor_, bool want_scale,
+                                             double2 &sum, double &scale, bool &guard) {
+  double2 s[25];
+#pragma unroll
+  for (int i = 0; i < 25; ++i) s[i] = R[i];
+  tree_bottom5r(s, D, parity, floor_, want_scale, sum, scale, guard);
+}
+
+// The child on pivot b of a 7x7 node (shared memory), built in registers, then its last
+// two levels: the breadth-first level into 5x5 nodes fused with the bottom.
+__device__ __forceinline__ void tree_bottom7(const double2 *S, double2 D, int b, int parity, double floor_,
+                                             bool want_scale, double2 &sum, double &scale, bool &guard) {
+  const double2 piv = S[b * 8];
+  if (!(cabs1(piv) >= floor_)) guard = true;
+  const double2 inv = crcp(piv);
+  const double2 Db = cmul(D, piv);
+  double2 t[25];
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    const double2 Lf = cmul(S[(i + 2) * 7 + b], inv);
+#pragma unroll
+    for (int j = 0; j < 5; ++j) t[i * 5 + j] = cfms(S[(i + 2) * 7 + j + 2], Lf, S[b * 7 + j + 2]);
+  }
+  tree_bottom5r(t, Db, parity ^ b, floor_, want_scale, sum, scale, guard);
+}
+
+// Sums (v, sc) over aligned groups of G consecutive threads (G a power of two <= NT)
+// and adds group g's sum to fval[g], fscale[g] for g < ngroups. Fixed shuffle pattern:
+// deterministic. Every thread of the CTA calls it.
+__device__ void group_sum(double2 v, double sc, int G, int ngroups, double2 *fval, double *fscale, double2 *wsum,
+                          double *wscale) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gw = G < 32 ? G : 32;
+  for (int off = 1; off < gw; off <<= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+    sc += __shfl_xor_sync(0xffffffffu, sc, off);
+  }
+  if (G <= 32) {
+    const int g = tid / G;
+    if ((lane & (G - 1)) == 0 && g < ngroups) {
+      fval[g] = cadd(fval[g], v);
+      fscale[g] += sc;
+    }
+    __syncthreads();
+  } else {
+    if (lane == 0) {
+      wsum[warp] = v;
+      wscale[warp] = sc;
+    }
+    __syncthreads();
+    const int wpg = G / 32;
+    if (tid < ngroups) {
+      double2 f = fval[tid];
+      double s2 = fscale[tid];
+      for (int w = tid * wpg; w < (tid + 1) * wpg; ++w) {
+        f = cadd(f, wsum[w]);
+        s2 += wscale[w];
+      }
+      fval[tid] = f;
+      fscale[tid] = s2;
+    }
+    __syncthreads();
+  }
 }
 
 // Order 1: the 3x3 root's two leaves directly.
@@ -271,7 +393,7 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   }
   const int R = N < TREE_MAX_SUB ? N : TREE_MAX_SUB;
   const int K0 = N - R;
-  const int LTOP = R >= 2 ? R - 2 : 0;
+  const int LB = R >= 3 ? R - 3 : 0; // breadth-first levels down to 7x7 nodes
   const double floor_ = it.model.pivot_floor;
   const int spin = it.f.A.spin;
   for (int sub = 0; sub < (1 << K0); ++sub) {
@@ -285,41 +407,41 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
       m -= 2;
       cur ^= 1;
     }
-    int nodes = np;
-    for (int k = 0; k < LTOP; ++k) {
-      tree_level(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, nodes, nodes / np, m, floor_);
+    int nodes = np, lg = 0;
+    for (int k = 0; k < LB; ++k) {
+      tree_level2(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, nodes, lg, m, floor_);
       nodes *= 2;
+      lg += 1;
       m -= 2;
       cur ^= 1;
     }
-    // nodes == np << LTOP, each of size m (5, or 3 at order 1)
-    if (tid < nodes) {
-      double2 sum;
-      double sc;
-      bool guard = false;
-      int p = tid >> LTOP;
-      if (m == 5) {
-        int parity = __popc(tid & ((1 << LTOP) - 1)) + __popc(sub);
-        tree_bottom5(S.buf[cur] + tid * 25, S.D[cur][tid], parity, floor_, want_scale, sum, sc, guard);
-      } else {
-        tree_bottom3(S.buf[cur] + tid * 9, sum, sc, want_scale);
+    double2 v = c2(0.0, 0.0);
+    double sc = 0.0;
+    bool guard = false;
+    int G, p = 0;
+    if (m == 7) { // two threads per 7x7 node, one per child
+      G = 2 << lg;
+      if (tid < 2 * nodes) {
+        const int node = tid >> 1, b = tid & 1;
+        p = node >> lg;
+        const int parity = __popc(node & ((1 << lg) - 1)) + __popc(sub);
+        tree_bottom7(S.buf[cur] + node * 49, S.D[cur][node], b, parity, floor_, want_scale, v, sc, guard);
       }
-      if (guard) S.flag[p] |= 2;
-      S.tmp[tid] = sum;
-      S.D[cur ^ 1][tid].x = sc;
-    }
-    __syncthreads();
-    if (tid < np) {
-      double2 f = S.fval[tid];
-      double sc = S.fscale[tid];
-      for (int g = tid << LTOP; g < ((tid + 1) << LTOP); ++g) {
-        f = cadd(f, S.tmp[g]);
-        sc += S.D[cur ^ 1][g].x;
+    } else if (m == 5) { // order 2: the root itself
+      G = 1;
+      if (tid < nodes) {
+        p = tid;
+        tree_bottom5(S.buf[cur] + tid * 25, S.D[cur][tid], __popc(sub), floor_, want_scale, v, sc, guard);
       }
-      S.fval[tid] = f;
-      S.fscale[tid] = sc;
+    } else { // order 1
+      G = 1;
+      if (tid < nodes) {
+        p = tid;
+        tree_bottom3(S.buf[cur] + tid * 9, v, sc, want_scale);
+      }
     }
-    __syncthreads();
+    if (guard) S.flag[p] |= 2;
+    group_sum(v, sc, G, np, S.fval, S.fscale, S.wsum, S.wscale);
   }
   if (tid < np) {
     double2 f = S.fval[tid];
@@ -357,8 +479,7 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
     unsigned long long cdom = 0, cfb = 0, mask0 = 0, mask1 = 0;
     for (int sb = 0; sb < ccount; sb += P) {
       const int np = min(P, ccount - sb);
-      load_points(L, it, N, np, cfirst + sb, S.u, S.jac, S.flag, keep);
-      __syncthreads();
+      load_points_par(L, it, N, np, cfirst + sb, S.u, S.jac, S.flag, reinterpret_cast<double *>(S.tmp), keep);
       tree_points(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
       if (EVAL) {
         if (tid < np) {
