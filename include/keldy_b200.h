@@ -195,7 +195,7 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
  * make it before any stream capture. */
 #define KB_NOALLOC_MAX_ITEMS 64
 #define KB_NOALLOC_MAX_CHUNKS 65536
-#define KB_NOALLOC_SCRATCH_BYTES (4u << 20)
+#define KB_NOALLOC_SCRATCH_BYTES (12u << 20)
 int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc);
 
 /* ----------------------------------------------------------------- peaks --- */

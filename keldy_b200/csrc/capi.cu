@@ -570,6 +570,9 @@ static int run_eval(kb_context *ctx, ItemDev it, int mode, int64_t count, const 
   L.err = ctx->d_err;
   int grid = (int)std::min<long long>(nchunks, use_tree ? ctx->tree_grid : ctx->sm_count * 4);
   if (use_tree) {
+    DevBuf dpts;
+    KB_CUDA(dpts.alloc((size_t)grid * PTS_SLOT * sizeof(double), st));
+    L.pts = dpts.as<double>();
     KB_CUDA(launch_tree(L, grid, st));
     std::vector<int> flags((size_t)count);
     KB_CUDA(cudaMemcpyAsync(flags.data(), dflag.p, count * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -736,9 +739,15 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
     L.mode = IN_SOBOL;
     L.partials = dpart.as<ChunkPartial>();
     L.err = ctx->d_err;
+    DevBuf dpts;
+    const int tgrid = (int)std::min<long long>(nchunks, ctx->tree_grid);
+    if (group == 0) {
+      KB_CUDA(dpts.alloc((size_t)tgrid * PTS_SLOT * sizeof(double), st));
+      L.pts = dpts.as<double>();
+    }
     if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
     if (group == 0)
-      KB_CUDA(launch_tree(L, (int)std::min<long long>(nchunks, ctx->tree_grid), st));
+      KB_CUDA(launch_tree(L, tgrid, st));
     else
       KB_CUDA(launch_direct(L, (int)std::min<long long>(nchunks, ctx->sm_count * 4), st));
     if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[1], st));
@@ -826,8 +835,10 @@ constexpr size_t NOALLOC_OFFS_OFF = NOALLOC_ITEMS_OFF + sizeof(ItemDev) * KB_NOA
 constexpr size_t NOALLOC_ACC_OFF = ((NOALLOC_OFFS_OFF + sizeof(long long) * (KB_NOALLOC_MAX_ITEMS + 1)) + 255) / 256 * 256;
 constexpr size_t NOALLOC_CNT_OFF = NOALLOC_ACC_OFF + sizeof(kb_accum) * 2 * KB_NOALLOC_MAX_ITEMS;
 constexpr size_t NOALLOC_PART_OFF = (NOALLOC_CNT_OFF + sizeof(int) + 255) / 256 * 256;
-constexpr size_t NOALLOC_BYTES = NOALLOC_PART_OFF + sizeof(ChunkPartial) * (size_t)KB_NOALLOC_MAX_CHUNKS;
-static_assert(NOALLOC_BYTES <= KB_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds the stated maximum");
+constexpr size_t NOALLOC_PTS_OFF =
+    (NOALLOC_PART_OFF + sizeof(ChunkPartial) * (size_t)KB_NOALLOC_MAX_CHUNKS + 255) / 256 * 256;
+constexpr size_t NOALLOC_PTS_SLOTS = (KB_NOALLOC_SCRATCH_BYTES - NOALLOC_PTS_OFF) / (PTS_SLOT * sizeof(double));
+static_assert(NOALLOC_PTS_SLOTS >= 296, "scratch too small for one set-up slot per resident CTA");
 
 static __device__ __align__(256) unsigned char kb_noalloc_scratch[KB_NOALLOC_SCRATCH_BYTES];
 
@@ -893,6 +904,7 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
   kb_accum *d_acc = reinterpret_cast<kb_accum *>(base + NOALLOC_ACC_OFF);
   int *d_cnt = reinterpret_cast<int *>(base + NOALLOC_CNT_OFF);
   ChunkPartial *d_part = reinterpret_cast<ChunkPartial *>(base + NOALLOC_PART_OFF);
+  double *d_pts = reinterpret_cast<double *>(base + NOALLOC_PTS_OFF);
   KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), stream));
   KB_CUDA(cudaMemsetAsync(d_acc, 0, sizeof(kb_accum) * 2 * KB_NOALLOC_MAX_ITEMS, stream));
   // Group 0 (tree) and group 1 (pivoted LU), heaviest orders first within a group; the
@@ -930,9 +942,11 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     L.chunk_counter = d_cnt;
     L.mode = IN_SOBOL;
     L.partials = d_part;
+    L.pts = d_pts;
     L.err = ctx->d_err;
     if (g == 0) {
-      KB_CUDA(launch_tree(L, (int)std::min<long long>(L.n_chunks, ctx->tree_grid), stream));
+      const long long slots = (long long)NOALLOC_PTS_SLOTS;
+      KB_CUDA(launch_tree(L, (int)std::min<long long>(std::min<long long>(L.n_chunks, ctx->tree_grid), slots), stream));
       KB_CUDA(launch_fallback(L, ctx->sm_count * 4, stream));
     } else {
       KB_CUDA(launch_direct(L, (int)std::min<long long>(L.n_chunks, ctx->sm_count * 4), stream));

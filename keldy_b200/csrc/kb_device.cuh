@@ -98,14 +98,12 @@ __device__ inline double2 g0_contour(const ModelDev &m, const kb_gf_index &a, co
 // Point number k (k >= 1) of the digital sequence: the state digitalseq_b2g::set_state
 // builds for Gray code gray(k), x_j = 2^-32 (cur_j ^ shift_j) (digitalseq_b2g.hpp:455-471).
 __device__ __forceinline__ double sobol_coord(const SobolDev &s, uint32_t k, int j) {
-  uint32_t g = k ^ (k >> 1);
-  uint32_t cur = 0;
+  const uint32_t g = k ^ (k >> 1); // below 2^m: columns b >= m are never read
   const uint32_t *C = s.Csr + j * s.m;
-  while (g) {
-    int b = __ffs(g) - 1;
-    cur ^= __ldg(C + b);
-    g &= g - 1;
-  }
+  uint32_t cur = 0;
+#pragma unroll
+  for (int b = 0; b < SOBOL_COLS; ++b)
+    if ((g >> b) & 1u) cur ^= __ldg(C + b);
   return 2.3283064365386963e-10 * (double)(cur ^ __ldg(s.shfr + j));
 }
 

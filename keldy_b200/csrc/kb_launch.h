@@ -23,6 +23,9 @@ struct ChunkPartial {
 };
 
 constexpr int CHUNK_POINTS = 128; // points per scheduling chunk (<= 128: two 64-bit masks)
+// Per-CTA slot of the tree kernel's chunk set-up: coordinates [MAX_ORDER][CHUNK_POINTS],
+// then the Jacobians and the domain flags of the chunk's points.
+constexpr int PTS_SLOT = CHUNK_POINTS * (MAX_ORDER + 2);
 
 struct Launch {
   const ItemDev *items; // device
@@ -41,6 +44,8 @@ struct Launch {
   int *out_dom;
   double *out_scale;
   int *out_flag;        // tree: 1 = point needs the pivoted-LU kernel
+  // tree kernel: gridDim.x * PTS_SLOT doubles of set-up scratch
+  double *pts;
   // IN_SOBOL
   ChunkPartial *partials; // [n_chunks]
   // errors

@@ -85,55 +85,28 @@ __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, l
   flag_out[p] = dom ? 0 : 1;
 }
 
-// Inputs of np points with one thread per (point, coordinate): Sobol coordinates (or
-// given inputs) into u[j*np + p], then the warper chain from its last warper to its
-// first, product warpers per coordinate, the plasma warper per point. The Jacobian
-// products are taken in keldy's order (per warper over the coordinates, then along the
-// chain). wtmp holds np*N doubles.
-__device__ void load_points_par(const Launch &L, const ItemDev &it, int N, int np, long long gp0, double *u,
-                                double *jac, int *flag, double *wtmp, bool keep) {
-  const int tid = threadIdx.x, nt = blockDim.x, total = np * N;
-  for (int r = tid; r < total; r += nt) {
-    int j = r / np, p = r - j * np;
-    long long gp = gp0 + p;
-    if (L.mode == IN_SOBOL) {
-      u[r] = sobol_coord(it.rng, it.k_first + (uint32_t)gp, j);
-    } else {
-      long long src = L.index ? (long long)L.index[gp] : gp;
-      u[r] = L.in[src * N + j];
-    }
+// One point of a chunk, on one thread: Sobol coordinates (or the given inputs), the
+// warper chain, the domain flag; written to the CTA's set-up slot at column t.
+__device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long long gp, bool keep, double *slot,
+                              int t) {
+  double x[MAX_ORDER];
+  double jac = 1.0;
+  if (L.mode == IN_SOBOL) {
+    const uint32_t k = it.k_first + (uint32_t)gp;
+    for (int j = 0; j < N; ++j) x[j] = sobol_coord(it.rng, k, j);
+    jac = chain_reverse(it.chain, it.chain_len, 0, N, x, 1);
+  } else {
+    const long long src = L.index ? (long long)L.index[gp] : gp;
+    for (int j = 0; j < N; ++j) x[j] = L.in[src * N + j];
+    if (L.mode == IN_LI) jac = chain_reverse(it.chain, it.chain_start, 0, N, x, 1);
   }
-  if (tid < np) jac[tid] = 1.0;
-  __syncthreads();
-  const int start = (L.mode == IN_SOBOL) ? it.chain_len : (L.mode == IN_LI ? it.chain_start : 0);
-  for (int w = start - 1; w >= 0; --w) {
-    const WarperDev &wd = it.chain[w];
-    if (wd.kind == KB_WARPER_IDENTITY) continue;
-    if (wd.kind == KB_WARPER_PLASMA_UV) {
-      if (tid < np) warp_reverse_one(wd, N, u + tid, np);
-    } else {
-      for (int r = tid; r < total; r += nt) {
-        double x = warper_Finv(wd, u[r]);
-        u[r] = x;
-        wtmp[r] = 1.0 / warper_f1(wd, x);
-      }
-      __syncthreads();
-      if (tid < np) {
-        double jw = 1.0;
-        for (int j = 0; j < N; ++j) jw *= wtmp[j * np + tid];
-        jac[tid] *= jw;
-      }
-    }
-    __syncthreads();
-  }
-  if (tid < np) {
-    int dom = (it.f.A.spin == it.f.B.spin) ? 1 : 0;
-    if (keep)
-      for (int j = 0; j < N; ++j)
-        if (u[j * np + tid] < 0.0) dom = 0;
-    flag[tid] = dom ? 0 : 1;
-  }
-  __syncthreads();
+  int dom = (it.f.A.spin == it.f.B.spin) ? 1 : 0;
+  if (keep)
+    for (int j = 0; j < N; ++j)
+      if (x[j] < 0.0) dom = 0;
+  for (int j = 0; j < N; ++j) slot[j * CHUNK_POINTS + t] = x[j];
+  slot[MAX_ORDER * CHUNK_POINTS + t] = jac;
+  slot[(MAX_ORDER + 1) * CHUNK_POINTS + t] = dom ? 0.0 : 1.0;
 }
 
 // G (row-major, M = 2N+1) of np points: G[p*M*M + r*M + c]. Out-of-domain points get
@@ -477,9 +450,17 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
     const bool keep = (L.mode == IN_SOBOL) ? true : (L.keep_u_hypercube != 0);
     double2 csum = c2(0.0, 0.0);
     unsigned long long cdom = 0, cfb = 0, mask0 = 0, mask1 = 0;
+    double *slot = L.pts + (size_t)blockIdx.x * PTS_SLOT;
+    if (tid < ccount) prepare_point(L, it, N, cfirst + tid, keep, slot, tid);
+    __syncthreads();
     for (int sb = 0; sb < ccount; sb += P) {
       const int np = min(P, ccount - sb);
-      load_points_par(L, it, N, np, cfirst + sb, S.u, S.jac, S.flag, reinterpret_cast<double *>(S.tmp), keep);
+      if (tid < np) {
+        for (int j = 0; j < N; ++j) S.u[j * np + tid] = slot[j * CHUNK_POINTS + sb + tid];
+        S.jac[tid] = slot[MAX_ORDER * CHUNK_POINTS + sb + tid];
+        S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
+      }
+      __syncthreads();
       tree_points(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
       if (EVAL) {
         if (tid < np) {
