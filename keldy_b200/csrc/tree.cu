@@ -111,65 +111,135 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
 
 // G (row-major, M = 2N+1) of np points: G[p*M*M + r*M + c]. Out-of-domain points get
 // the identity (their values are discarded; this keeps every pivot finite).
+// Items per point: the N(N-1) ordered vertex pairs, the N external-row and N
+// external-column entries (one table lookup each: g^< and g^> at one time difference),
+// the N diagonal blocks (g(0)) and the corner. Each thread computes the lookup positions
+// of GK items before issuing their loads, so that GK L2 round trips overlap.
 __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
                         int spin, int *bad) {
+  constexpr int GK = 4;
   const ModelDev &m = it.model;
   const int M = 2 * N + 1;
-  const int per = N * N + N + 1;
+  const int npair = N * (N - 1), nlook = npair + 2 * N, per = nlook + N + 1;
   const kb_gf_index &A = it.f.A, &B = it.f.B;
   const double2 *t00 = m.tab[spin][0][0];
   const double2 *trow = m.tab[spin][A.orbital][0];
   const double2 *tcol = m.tab[spin][0][B.orbital];
-  for (int r = threadIdx.x; r < np * per; r += blockDim.x) {
-    int p = r / per, q = r - p * per;
-    double2 *G = buf + (size_t)p * M * M;
-    const double *x = u + p;
-    bool out = flag[p] & 1;
-    if (q < N * N) {
-      int i = q / N, j = q - i * N;
-      double2 *g = G + (2 * i) * M + 2 * j;
-      if (out) {
-        double2 z = c2(0.0, 0.0), one = c2(1.0, 0.0);
-        g[0] = (i == j) ? one : z;
-        g[M + 1] = (i == j) ? one : z;
-        g[1] = z;
-        g[M] = z;
-      } else if (i != j) {
-        double d = x[i * np] - x[j * np];
-        double2 gl, gg;
-        g0_pair(m, t00, d, gl, gg, bad);
-        bool later = (d != 0.0) ? (d > 0.0) : (i > j);
-        g[0] = later ? gg : gl;      // forward-forward
-        g[M + 1] = later ? gl : gg;  // backward-backward
-        g[1] = gl;                   // forward-backward
-        g[M] = gg;                   // backward-forward
+  const int total = np * per;
+  for (int base = threadIdx.x; base < total; base += GK * blockDim.x) {
+    int kind[GK], pi[GK], qi[GK], ix[GK];
+    double wt[GK], dt[GK];
+    const double2 *tb[GK];
+#pragma unroll
+    for (int k = 0; k < GK; ++k) {
+      const int r = base + k * blockDim.x;
+      kind[k] = 0; // 0: none, 1: pair, 2: row, 3: col, 4: diagonal, 5: corner, 6: out of domain
+      tb[k] = nullptr;
+      ix[k] = 0;
+      wt[k] = 0.0;
+      dt[k] = 0.0;
+      pi[k] = 0;
+      qi[k] = 0;
+      if (r >= total) continue;
+      const int p = r / per, q = r - p * per;
+      pi[k] = p;
+      qi[k] = q;
+      const double *x = u + p;
+      if (flag[p] & 1) {
+        kind[k] = 6;
+        continue;
+      }
+      if (q < npair) {
+        const int i = q / (N - 1), r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
+        kind[k] = 1;
+        dt[k] = x[i * np] - x[j * np];
+        tb[k] = t00;
+      } else if (q < npair + N) {
+        kind[k] = 2;
+        dt[k] = A.time - x[(q - npair) * np];
+        tb[k] = trow;
+      } else if (q < nlook) {
+        kind[k] = 3;
+        dt[k] = x[(q - npair - N) * np] - B.time;
+        tb[k] = tcol;
+      } else if (q < nlook + N) {
+        kind[k] = 4;
+        tb[k] = t00;
       } else {
-        double2 gl, gg;
-        g0_pair(m, t00, 0.0, gl, gg, bad);
-        double2 eq = c2(gl.x, gl.y - m.alpha); // equal contour points, internal
+        kind[k] = 5;
+      }
+      if (tb[k] && !interp_index(m, dt[k], ix[k], wt[k])) {
+        *bad = 1;
+        ix[k] = 0;
+        wt[k] = 0.0;
+      }
+    }
+    double2 gl[GK], gg[GK];
+#pragma unroll
+    for (int k = 0; k < GK; ++k) {
+      if (tb[k])
+        interp_pair(tb[k], ix[k], wt[k], gl[k], gg[k]);
+      else
+        gl[k] = gg[k] = c2(0.0, 0.0);
+    }
+#pragma unroll
+    for (int k = 0; k < GK; ++k) {
+      if (kind[k] == 0) continue;
+      double2 *G = buf + (size_t)pi[k] * M * M;
+      const int q = qi[k];
+      const double *x = u + pi[k];
+      if (kind[k] == 1) {
+        const int i = q / (N - 1), r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
+        double2 *g = G + (2 * i) * M + 2 * j;
+        const double d = dt[k];
+        const bool later = (d != 0.0) ? (d > 0.0) : (i > j);
+        g[0] = later ? gg[k] : gl[k];     // forward-forward
+        g[M + 1] = later ? gl[k] : gg[k]; // backward-backward
+        g[1] = gl[k];                     // forward-backward
+        g[M] = gg[k];                     // backward-forward
+      } else if (kind[k] == 2) {
+        const int j = q - npair;
+        const double uj = x[j * np];
+        double2 *row = G + (2 * N) * M + 2 * j;
+        row[0] = compare_3way(A.time, A.k_idx, N, uj, 0, j) > 0 ? gg[k] : gl[k];
+        row[1] = compare_3way(A.time, A.k_idx, N, uj, 1, j) > 0 ? gg[k] : gl[k];
+      } else if (kind[k] == 3) {
+        const int j = q - npair - N;
+        const double uj = x[j * np];
+        double2 *col = G + (2 * j) * M + 2 * N;
+        col[0] = compare_3way(uj, 0, j, B.time, B.k_idx, N) > 0 ? gg[k] : gl[k];
+        col[M] = compare_3way(uj, 1, j, B.time, B.k_idx, N) > 0 ? gg[k] : gl[k];
+      } else if (kind[k] == 4) {
+        const int i = q - nlook;
+        double2 *g = G + (2 * i) * M + 2 * i;
+        const double2 eq = c2(gl[k].x, gl[k].y - m.alpha); // equal contour points, internal
         g[0] = eq;
         g[M + 1] = eq;
-        g[1] = gl;
-        g[M] = gg;
+        g[1] = gl[k];
+        g[M] = gg[k];
+      } else if (kind[k] == 5) {
+        G[(2 * N) * M + 2 * N] = c2(0.0, 0.0);
+      } else { // out of domain: identity blocks, zero externals
+        const double2 z = c2(0.0, 0.0), one = c2(1.0, 0.0);
+        if (q < npair) {
+          const int i = q / (N - 1), r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
+          double2 *g = G + (2 * i) * M + 2 * j;
+          g[0] = g[1] = g[M] = g[M + 1] = z;
+        } else if (q < npair + N) {
+          double2 *row = G + (2 * N) * M + 2 * (q - npair);
+          row[0] = row[1] = z;
+        } else if (q < nlook) {
+          double2 *col = G + (2 * (q - npair - N)) * M + 2 * N;
+          col[0] = col[M] = z;
+        } else if (q < nlook + N) {
+          const int i = q - nlook;
+          double2 *g = G + (2 * i) * M + 2 * i;
+          g[0] = g[M + 1] = one;
+          g[1] = g[M] = z;
+        } else {
+          G[(2 * N) * M + 2 * N] = one;
+        }
       }
-    } else if (q < N * N + N) {
-      int j = q - N * N;
-      double2 *row = G + (2 * N) * M + 2 * j;
-      double2 *col = G + (2 * j) * M + 2 * N;
-      if (out) {
-        row[0] = row[1] = col[0] = col[M] = c2(0.0, 0.0);
-      } else {
-        double uj = x[j * np];
-        double2 gl, gg;
-        g0_pair(m, trow, A.time - uj, gl, gg, bad);
-        row[0] = compare_3way(A.time, A.k_idx, N, uj, 0, j) > 0 ? gg : gl;
-        row[1] = compare_3way(A.time, A.k_idx, N, uj, 1, j) > 0 ? gg : gl;
-        g0_pair(m, tcol, uj - B.time, gl, gg, bad);
-        col[0] = compare_3way(uj, 0, j, B.time, B.k_idx, N) > 0 ? gg : gl;
-        col[M] = compare_3way(uj, 1, j, B.time, B.k_idx, N) > 0 ? gg : gl;
-      }
-    } else {
-      G[(2 * N) * M + 2 * N] = out ? c2(1.0, 0.0) : c2(0.0, 0.0);
     }
   }
 }
@@ -190,7 +260,14 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
   const unsigned rows = (unsigned)(nodes * mc);
   const unsigned magic = 0xFFFFFFFFu / (unsigned)mc + 1u; // r / mc == umulhi(r, magic) for r < 2^20, mc <= 31
-  for (unsigned r = threadIdx.x; r < rows; r += blockDim.x) {
+  // split rows into column segments while the CTA has idle threads
+  int lgseg = 0;
+  while ((rows << (lgseg + 1)) <= blockDim.x && (mc >> (lgseg + 1)) >= 3) ++lgseg;
+  const int seglen = (mc + (1 << lgseg) - 1) >> lgseg;
+  const unsigned items = rows << lgseg;
+  for (unsigned t = threadIdx.x; t < items; t += blockDim.x) {
+    const unsigned r = t >> lgseg;
+    const int j0 = (int)(t & ((1u << lgseg) - 1)) * seglen, j1 = min(mc, j0 + seglen);
     const unsigned par = __umulhi(r, magic);
     const unsigned i = r - par * (unsigned)mc;
     const double2 *S = cur + par * mm;
@@ -198,7 +275,8 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
     const double2 L1 = cmul(S[(i + 2) * m + 1], inv[2 * par + 1]);
     const double2 *srow = S + (i + 2) * m + 2, *p0 = S + 2, *p1 = S + m + 2;
     double2 *o0 = nxt + (2 * par) * mcc + i * mc, *o1 = o0 + mcc;
-    for (int j = 0; j < mc; ++j) {
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
       const double2 v = srow[j];
       o0[j] = cfms(v, L0, p0[j]);
       o1[j] = cfms(v, L1, p1[j]);
