@@ -67,7 +67,7 @@ int kb_sobol_matrices(int dim, int log_max_points, int do_shift, int do_scramble
                       uint32_t *shfr);
 /* Points k_first .. k_first+count-1, row-major [count][dim] doubles
  * (replaces digitalseq_b2g::next/set_state, digitalseq_b2g.hpp:415-471, and
- * sobol::operator()/seed/discard, qrng.hpp:51-67). KB_E_EXHAUSTED past 2^log_max_points - 1. */
+ * sobol::operator()/seed/discard, qrng.hpp:51-67). KB_E_EXHAUSTED past 2^log_max_points. */
 int kb_sobol_points(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out);
 int kb_sobol_points_dev(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out_dev);
 

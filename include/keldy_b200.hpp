@@ -1,0 +1,504 @@
+// keldy's C++ interface for its QMC hot path, running on the keldy_b200 C ABI.
+//
+// Header-only. The classes keep keldy's names, signatures and value semantics
+// (qrng.hpp, warpers/*.hpp, impurity_oneband/{model,wick_direct,compute_obs}.hpp,
+// integrator.hpp) so that code written against keldy compiles against this header; the
+// work runs on the GPU through include/keldy_b200.h. Errors that keldy raises with
+// TRIQS_RUNTIME_ERROR are thrown as std::runtime_error with keldy's message.
+//
+// Differences from keldy, all forced by running on the device:
+//  * warper_product_1d_simple_t is built by the analytic makers (and the uniform maker
+//    make_product_1d_simple_uniform); its constructor from arbitrary std::function
+//    objects has no device form and throws.
+//  * g0_model is built from tables (g0_model::from_tables); the Python layer builds
+//    them from model_param_t (keldy_b200.g0_tables).
+//  * integrator::reset_rng accepts "sobol_unshifted" and "sobol"; keldy's boost
+//    pseudo-random generators are not on the device.
+//  * one process drives one GPU; keldy_b200.parallel shards Sobol blocks over ranks.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "keldy_b200.h"
+
+namespace keldy_b200 {
+
+inline void check(int status) {
+  if (status != KB_OK) throw std::runtime_error(kb_last_error());
+}
+
+// One context per device, created on first use and kept for the life of the process.
+inline kb_context *default_context(int device = 0) {
+  static std::mutex mu;
+  static kb_context *ctx[64] = {};
+  if (device < 0 || device >= 64) throw std::runtime_error("device index out of range");
+  std::lock_guard<std::mutex> lk(mu);
+  if (!ctx[device]) check(kb_context_create(device, &ctx[device]));
+  return ctx[device];
+}
+
+} // namespace keldy_b200
+
+namespace keldy {
+
+using dcomplex = std::complex<double>;
+using time_real_t = double;
+using orbital_t = int;
+
+enum spin_t { up = 0, down = 1 };
+enum keldysh_idx_t { forward = 0, backward = 1 };
+
+// Point of the Keldysh contour (common.hpp:45-55).
+class contour_pt_t {
+ public:
+  time_real_t time{};
+  keldysh_idx_t k_idx = forward;
+  int timesplit_n = 0;
+  bool operator==(const contour_pt_t &o) const {
+    return time == o.time && k_idx == o.k_idx && timesplit_n == o.timesplit_n;
+  }
+};
+
+// Contour order (common.cpp:47-57): < 0 if a is earlier on the contour than b.
+inline int compare_3way(const contour_pt_t &a, const contour_pt_t &b) {
+  int k3 = a.k_idx - b.k_idx;
+  if (k3 != 0) return k3;
+  double d = a.time - b.time;
+  if (d != 0.0) return (1 - 2 * int(a.k_idx)) * (2 * int(!std::signbit(d)) - 1);
+  return (1 - 2 * int(a.k_idx)) * (a.timesplit_n - b.timesplit_n);
+}
+
+// keldy::sobol (qrng.hpp:49-114). The state is the index k of the last point drawn;
+// operator() returns point k+1 (the first draw after seed(s) is point s+1).
+class sobol {
+  std::shared_ptr<kb_sobol> gen_;
+  int dim_ = 0;
+  int log_max_points_ = 31;
+  uint32_t k_ = 0;
+
+  void make(int dim, bool do_shift, bool do_scramble, int seed_shift) {
+    if (log_max_points_ > 31) throw std::runtime_error("To many points requested from Sobol generator.");
+    kb_sobol *s = nullptr;
+    keldy_b200::check(kb_sobol_create(keldy_b200::default_context(), dim, log_max_points_, do_shift, do_scramble,
+                                      seed_shift, &s));
+    gen_ = std::shared_ptr<kb_sobol>(s, kb_sobol_destroy);
+    dim_ = dim;
+  }
+
+ public:
+  sobol(int dim, int rng_state_seed, int log_max_points_ = 31) : log_max_points_(log_max_points_) {
+    make(dim, false, false, 0);
+    seed(rng_state_seed);
+  }
+  sobol(int dim, int rng_state_seed, bool do_shift, bool do_scramble, int rng_seed_shift, int log_max_points_ = 31)
+     : log_max_points_(log_max_points_) {
+    make(dim, do_shift, do_scramble, rng_seed_shift);
+    seed(rng_state_seed);
+  }
+
+  std::vector<double> operator()() { return points(1); }
+
+  // next `count` points, row-major (an addition to keldy's interface)
+  std::vector<double> points(int64_t count) {
+    if (count > 0 && (uint64_t)k_ >= (1ull << log_max_points_))
+      throw std::runtime_error("More sample points requested then generator can hold.");
+    std::vector<double> out((size_t)(count * dim_));
+    keldy_b200::check(kb_sobol_points(keldy_b200::default_context(), gen_.get(), k_ + 1, count, out.data()));
+    k_ += (uint32_t)count;
+    return out;
+  }
+
+  void seed(int k) { k_ = (uint32_t)k; }
+  void discard(int nr_discard) { k_ += (uint32_t)nr_discard; }
+
+  int dimension() const { return dim_; }
+  uint32_t state() const { return k_; }
+  void set_state(uint32_t k) { k_ = k; }
+  const kb_sobol *handle() const { return gen_.get(); }
+};
+
+namespace warpers {
+
+// Coordinate maps of the plasma warper (plasma_uv.hpp:35-51), on the device.
+inline std::vector<double> vi_from_ui(double t_max, std::vector<double> const &u_times) {
+  kb_warper w{KB_WARPER_PLASMA_UV, 0, t_max, 0.0};
+  std::vector<double> out(u_times.size());
+  if (u_times.empty()) return out;
+  keldy_b200::check(kb_warp(keldy_b200::default_context(), &w, 1, KB_FORWARD, 0, 1, (int)u_times.size(), 1,
+                            u_times.data(), out.data(), nullptr));
+  return out;
+}
+
+inline std::vector<double> ui_from_vi(double t_max, std::vector<double> const &v_times) {
+  kb_warper w{KB_WARPER_PLASMA_UV, 0, t_max, 0.0};
+  std::vector<double> out(v_times.size());
+  if (v_times.empty()) return out;
+  keldy_b200::check(kb_warp(keldy_b200::default_context(), &w, 1, KB_REVERSE, 1, 0, (int)v_times.size(), 1,
+                            v_times.data(), out.data(), nullptr));
+  return out;
+}
+
+namespace detail {
+// map_reverse / map_forward of a chain of warpers on one point.
+inline std::pair<std::vector<double>, double> apply(std::vector<kb_warper> const &chain, int direction, int start,
+                                                    int end, std::vector<double> const &x) {
+  std::vector<double> out(x.size());
+  double jac = 1.0;
+  if (x.empty()) {
+    // keldy's warpers on an empty vector: identity map, Jacobian 1
+    return {out, jac};
+  }
+  keldy_b200::check(kb_warp(keldy_b200::default_context(), chain.data(), (int)chain.size(), direction, start, end,
+                            (int)x.size(), 1, x.data(), out.data(), &jac));
+  return {out, jac};
+}
+} // namespace detail
+
+// The concept of a keldy warper (warpers.hpp): map_reverse, map_forward, ui_from_li,
+// li_from_ui, jacobian_reverse, jacobian_forward.
+class warper_base {
+ protected:
+  kb_warper desc_{};
+
+ public:
+  const kb_warper &desc() const { return desc_; }
+  std::pair<std::vector<double>, double> map_reverse(std::vector<double> const &li_vec) const {
+    return detail::apply({desc_}, KB_REVERSE, 1, 0, li_vec);
+  }
+  std::pair<std::vector<double>, double> map_forward(std::vector<double> const &ui_vec) const {
+    return detail::apply({desc_}, KB_FORWARD, 0, 1, ui_vec);
+  }
+  std::vector<double> ui_from_li(std::vector<double> const &li_vec) const { return map_reverse(li_vec).first; }
+  std::vector<double> li_from_ui(std::vector<double> const &ui_vec) const { return map_forward(ui_vec).first; }
+  double jacobian_reverse(std::vector<double> const &li_vec) const { return map_reverse(li_vec).second; }
+  double jacobian_forward(std::vector<double> const &ui_vec) const { return map_forward(ui_vec).second; }
+};
+
+// warpers/identity.hpp:30-49
+class warper_identity_t : public warper_base {
+ public:
+  warper_identity_t() { desc_ = kb_warper{KB_WARPER_IDENTITY, 0, 0.0, 0.0}; }
+};
+
+// warpers/plasma_uv.hpp:55-81
+class warper_plasma_uv_t : public warper_base {
+ public:
+  warper_plasma_uv_t(double t_max_ = 0.0) { desc_ = kb_warper{KB_WARPER_PLASMA_UV, 0, t_max_, 0.0}; }
+};
+
+// warpers/product_1d_simple.hpp:44-168, built by the makers below.
+class warper_product_1d_simple_t : public warper_base {
+ public:
+  warper_product_1d_simple_t() { desc_ = kb_warper{KB_WARPER_UNIFORM, 0, 1.0, 0.0}; }
+  explicit warper_product_1d_simple_t(kb_warper const &d) { desc_ = d; }
+  template <typename F1, typename F2, typename F3>
+  warper_product_1d_simple_t(F1 &&, F2 &&, F3 &&, double, bool = true) {
+    throw std::runtime_error("warper_product_1d_simple_t from arbitrary functions has no device form; use "
+                             "make_product_1d_simple_exponential/inverse/inverse_square/inverse_power/uniform");
+  }
+  // product of the normalised 1-D densities (product_1d_simple.hpp:161-167)
+  double operator()(std::vector<double> const &ui_vec) const { return jacobian_forward(ui_vec); }
+};
+
+inline warper_product_1d_simple_t make_product_1d_simple_exponential(double domain_u_max, double w_scale) {
+  return warper_product_1d_simple_t(kb_warper{KB_WARPER_EXPONENTIAL, 0, domain_u_max, w_scale});
+}
+inline warper_product_1d_simple_t make_product_1d_simple_inverse(double domain_u_max, double w_scale) {
+  return warper_product_1d_simple_t(kb_warper{KB_WARPER_INVERSE, 0, domain_u_max, w_scale});
+}
+inline warper_product_1d_simple_t make_product_1d_simple_inverse_square(double domain_u_max, double w_scale) {
+  return warper_product_1d_simple_t(kb_warper{KB_WARPER_INVERSE_SQUARE, 0, domain_u_max, w_scale});
+}
+inline warper_product_1d_simple_t make_product_1d_simple_inverse_power(int power, double domain_u_max,
+                                                                         double w_scale) {
+  return warper_product_1d_simple_t(kb_warper{KB_WARPER_INVERSE_POWER, power, domain_u_max, w_scale});
+}
+// f1 = 1/u_max on [0, u_max] (keldy writes it with three lambdas, product_1d_simple_test.cpp:10-23)
+inline warper_product_1d_simple_t make_product_1d_simple_uniform(double domain_u_max) {
+  return warper_product_1d_simple_t(kb_warper{KB_WARPER_UNIFORM, 0, domain_u_max, 0.0});
+}
+
+// warpers.hpp:45-137: a chain, applied last to first by map_reverse.
+class warper_train_t {
+  std::vector<kb_warper> chain_;
+
+ public:
+  warper_train_t() = default;
+  void emplace_back(warper_base const &w) {
+    if (chain_.size() >= KB_MAX_CHAIN) throw std::runtime_error("warper train longer than KB_MAX_CHAIN");
+    chain_.push_back(w.desc());
+  }
+  void reserve(size_t n) { chain_.reserve(n); }
+  void clear() { chain_.clear(); }
+  size_t size() const { return chain_.size(); }
+  std::vector<kb_warper> const &chain() const { return chain_; }
+
+  std::pair<std::vector<double>, double> map_reverse(std::vector<double> const &li_vec, int start_domain_nr,
+                                                     int end_domain_nr) const {
+    if (chain_.empty()) return {li_vec, 1.0};
+    return detail::apply(chain_, KB_REVERSE, start_domain_nr, end_domain_nr, li_vec);
+  }
+  std::pair<std::vector<double>, double> map_forward(std::vector<double> const &ui_vec, int start_domain_nr,
+                                                     int end_domain_nr) const {
+    if (chain_.empty()) return {ui_vec, 1.0};
+    return detail::apply(chain_, KB_FORWARD, start_domain_nr, end_domain_nr, ui_vec);
+  }
+  std::pair<std::vector<double>, double> map_reverse(std::vector<double> const &li_vec) const {
+    return map_reverse(li_vec, (int)chain_.size(), 0);
+  }
+  std::pair<std::vector<double>, double> map_forward(std::vector<double> const &ui_vec) const {
+    return map_forward(ui_vec, 0, (int)chain_.size());
+  }
+  double jacobian_reverse(std::vector<double> const &li_vec) const { return map_reverse(li_vec).second; }
+  double jacobian_forward(std::vector<double> const &ui_vec) const { return map_forward(ui_vec).second; }
+  std::vector<double> ui_from_li(std::vector<double> const &li_vec) const { return map_reverse(li_vec).first; }
+  std::vector<double> li_from_ui(std::vector<double> const &ui_vec) const { return map_forward(ui_vec).first; }
+};
+
+} // namespace warpers
+
+namespace impurity_oneband {
+
+// model.hpp:37-50
+struct model_param_t {
+  double beta = 1.0;
+  double bias_V = 0.0;
+  double eps_d = 0.0;
+  double Gamma = 1.0;
+  double alpha = 0.0;
+  double half_bandwidth = 2.;
+  std::string bath_type = "semicircle";
+  double time_max = +100.0;
+  int nr_time_points_gf = 1000;
+  std::string ft_method = "fft";
+};
+
+// model.hpp:55-78
+class gf_index_t {
+ public:
+  contour_pt_t contour{};
+  spin_t spin = up;
+  orbital_t orbital = 0;
+  gf_index_t() = default;
+  gf_index_t(time_real_t time_, int spin_, int k_idx_) : contour{time_, keldysh_idx_t(k_idx_)}, spin(spin_t(spin_)) {}
+  gf_index_t(time_real_t time_, int spin_, int k_idx_, int timesplit_n_)
+     : contour{time_, keldysh_idx_t(k_idx_), timesplit_n_}, spin(spin_t(spin_)) {}
+  gf_index_t(time_real_t time_, int spin_, int k_idx_, int timesplit_n_, int orbital_)
+     : contour{time_, keldysh_idx_t(k_idx_), timesplit_n_}, spin(spin_t(spin_)), orbital(orbital_t(orbital_)) {}
+  kb_gf_index abi() const {
+    return kb_gf_index{contour.time, int(spin), int(contour.k_idx), contour.timesplit_n, orbital};
+  }
+};
+
+// g^<(t), g^>(t) tables on the uniform mesh [-time_max, time_max] (model.hpp:178-232).
+// Copies share the device tables (immutable after construction).
+class g0_model {
+  std::shared_ptr<kb_model> m_;
+  double time_max_ = 0.0;
+  int npts_ = 0;
+  double alpha_ = 0.0;
+
+ public:
+  bool make_dot_lead = false;
+  model_param_t param{};
+
+  g0_model() = default;
+
+  // lesser/greater: npts complex values of spin up, orbital (0,0); the other blocks
+  // (spin down, dot-lead orbitals) may be added with set_table.
+  static g0_model from_tables(double time_max, std::vector<dcomplex> const &lesser,
+                              std::vector<dcomplex> const &greater, double alpha = 0.0) {
+    if (lesser.size() != greater.size()) throw std::runtime_error("lesser and greater tables differ in length");
+    g0_model g;
+    kb_model *m = nullptr;
+    keldy_b200::check(kb_model_create(keldy_b200::default_context(), (int)lesser.size(), time_max, alpha, &m));
+    g.m_ = std::shared_ptr<kb_model>(m, kb_model_destroy);
+    g.time_max_ = time_max;
+    g.npts_ = (int)lesser.size();
+    g.alpha_ = alpha;
+    g.param.time_max = time_max;
+    g.param.nr_time_points_gf = g.npts_;
+    g.param.alpha = alpha;
+    g.set_table(0, 0, 0, lesser, greater);
+    return g;
+  }
+
+  void set_table(int spin, int o1, int o2, std::vector<dcomplex> const &lesser, std::vector<dcomplex> const &greater) {
+    if ((int)lesser.size() != npts_ || (int)greater.size() != npts_)
+      throw std::runtime_error("table length differs from the model's mesh");
+    keldy_b200::check(kb_model_set_table(m_.get(), spin, o1, o2, reinterpret_cast<const double *>(lesser.data()),
+                                         reinterpret_cast<const double *>(greater.data())));
+  }
+
+  double time_max() const { return time_max_; }
+  int npts() const { return npts_; }
+  double alpha() const { return alpha_; }
+  const kb_model *handle() const { return m_.get(); }
+};
+
+// model.hpp:238-268
+struct g0_keldysh_contour_t {
+  g0_model model;
+  g0_keldysh_contour_t(g0_model model_) : model(std::move(model_)) {}
+
+  dcomplex operator()(gf_index_t const &a, gf_index_t const &b, bool internal_point = true) const {
+    kb_gf_index x = a.abi(), y = b.abi();
+    int internal = internal_point ? 1 : 0;
+    double out[2];
+    keldy_b200::check(kb_g0_eval(keldy_b200::default_context(), model.handle(), &x, &y, &internal, 1, out));
+    return {out[0], out[1]};
+  }
+
+  double get_time_max() const { return model.time_max(); }
+};
+
+// wick_direct.hpp:34-65
+class integrand_g_direct {
+  g0_keldysh_contour_t g0;
+  gf_index_t external_A;
+  gf_index_t external_B;
+  double cutoff;
+  int algo_ = KB_ALGO_AUTO;
+
+  std::pair<dcomplex, int> eval(std::vector<double> const &times, bool keep, bool no_det) const {
+    kb_integrand f = abi();
+    double out[2];
+    int dom = 0;
+    int n = (int)times.size();
+    if (no_det)
+      keldy_b200::check(kb_integrand_eval_no_det(keldy_b200::default_context(), g0.model.handle(), &f, n, 1,
+                                                 times.data(), keep, out, &dom));
+    else
+      keldy_b200::check(kb_integrand_eval(keldy_b200::default_context(), g0.model.handle(), &f, n, 1, times.data(),
+                                          keep, algo_, out, &dom, nullptr));
+    return {dcomplex(out[0], out[1]), dom};
+  }
+
+ public:
+  using result_t = dcomplex;
+
+  integrand_g_direct(g0_keldysh_contour_t g0_, gf_index_t external_A_, gf_index_t external_B_, double cutoff_ = 0.)
+     : g0(std::move(g0_)), external_A(external_A_), external_B(external_B_), cutoff(cutoff_) {
+    if (external_A.contour.time < 0. || external_B.contour.time < 0.)
+      throw std::runtime_error("An external point has negative time.");
+    double const t_max = g0.get_time_max();
+    if (external_A.contour.time > t_max || external_B.contour.time > t_max)
+      throw std::runtime_error("An external point is out of g0 time window.");
+  }
+
+  std::pair<result_t, int> operator()(std::vector<double> const &times, bool const keep_u_hypercube = true) const {
+    return eval(times, keep_u_hypercube, false);
+  }
+  std::pair<result_t, int> eval_no_det(std::vector<double> const &times, bool const keep_u_hypercube = true) const {
+    return eval(times, keep_u_hypercube, true);
+  }
+
+  // algorithm of the device integrand: KB_ALGO_AUTO (default), KB_ALGO_TREE, KB_ALGO_DIRECT
+  void set_algorithm(int algo) { algo_ = algo; }
+  int algorithm() const { return algo_; }
+  kb_integrand abi() const { return kb_integrand{external_A.abi(), external_B.abi(), cutoff}; }
+  g0_keldysh_contour_t const &get_g0() const { return g0; }
+};
+
+// integrator.hpp:42-136 for the integrand_g_direct observables; runs on the device.
+class integrator_g_direct {
+ protected:
+  int dimension = 1;
+  dcomplex result{0.0};
+  uint64_t n_points = 0;
+  uint64_t n_integrand_evals_in_domain = 0;
+  integrand_g_direct integrand;
+  sobol rng_;
+
+ public:
+  warpers::warper_train_t warper{};
+
+  integrator_g_direct(integrand_g_direct integrand_, int dimension_)
+     : dimension(dimension_), integrand(std::move(integrand_)), rng_(dimension_ > 0 ? dimension_ : 1, 0) {
+    if (dimension <= 0) throw std::runtime_error("Dimension of the integration space must be > 0.");
+  }
+
+  std::pair<dcomplex, double> evaluate_warped_integrand(std::vector<double> const &li_vec, int start_domain_nr,
+                                                        bool keep_u_hypercube = true) const {
+    kb_integrand f = integrand.abi();
+    double out[2], jac = 1.0;
+    int dom = 0;
+    auto const &chain = warper.chain();
+    keldy_b200::check(kb_evaluate_warped(keldy_b200::default_context(), integrand.get_g0().model.handle(), &f,
+                                         chain.data(), (int)chain.size(), start_domain_nr, (int)li_vec.size(), 1,
+                                         li_vec.data(), keep_u_hypercube, integrand.algorithm(), out, &jac, &dom));
+    return {dcomplex(out[0], out[1]), double(dom)};
+  }
+  std::pair<dcomplex, double> evaluate_warped_integrand(std::vector<double> const &li_vec) const {
+    return evaluate_warped_integrand(li_vec, (int)warper.size(), true);
+  }
+
+  // nr_steps Sobol points through the warper train and the integrand, summed (integrator.hpp:81-95)
+  void run(int nr_steps) {
+    if (nr_steps <= 0) return;
+    if ((uint64_t)rng_.state() + (uint64_t)nr_steps > (1ull << 31))
+      throw std::runtime_error("More sample points requested then generator can hold.");
+    auto const &chain = warper.chain();
+    kb_work w{integrand.get_g0().model.handle(), rng_.handle(), chain.data(), (int)chain.size(), integrand.abi(),
+              dimension, rng_.state() + 1, nr_steps};
+    kb_accum acc{};
+    keldy_b200::check(kb_integrate(keldy_b200::default_context(), &w, 1, integrand.algorithm(), &acc));
+    rng_.discard(nr_steps);
+    result += dcomplex(acc.sum_re, acc.sum_im);
+    n_points += acc.n_points;
+    n_integrand_evals_in_domain += acc.n_in_domain;
+  }
+
+  // integrator.hpp:97-112 ("sobol_unshifted", "sobol"; the boost generators have no device form)
+  void reset_rng(std::string rng_name, int rng_state_seed, bool do_shift = false, bool do_scramble = false,
+                 int rng_seed_shift = 0) {
+    if (rng_name == "sobol_unshifted")
+      rng_ = sobol(dimension, rng_state_seed);
+    else if (rng_name == "sobol")
+      rng_ = sobol(dimension, rng_state_seed, do_shift, do_scramble, rng_seed_shift);
+    else if (rng_name == "mt19937_64" || rng_name == "ranlux48" || rng_name == "taus88")
+      throw std::runtime_error("rng '" + rng_name + "' has no device form; use sobol_unshifted or sobol");
+    else
+      throw std::runtime_error("No other rng available.");
+  }
+
+  dcomplex reduce_result() const { return result * (1.0 / double(reduce_nr_points_run())); }
+  uint64_t reduce_nr_points_run() const { return n_points; }
+  uint64_t reduce_nr_points_in_domain() const { return n_integrand_evals_in_domain; }
+  dcomplex raw_result() const { return result; }
+  integrand_g_direct get_integrand() const { return integrand; }
+  warpers::warper_train_t get_warper() const { return warper; }
+  sobol const &get_rng() const { return rng_; }
+};
+
+// compute_obs.hpp:51-64: charge G^<_{up,up}(t, t)
+class compute_charge_Q_direct : public integrator_g_direct {
+ public:
+  compute_charge_Q_direct(g0_model model, double time, int order, double cutoff_integrand)
+     : integrator_g_direct(integrand_g_direct{g0_keldysh_contour_t{std::move(model)}, gf_index_t{time, up, forward},
+                                              gf_index_t{time, up, backward}, cutoff_integrand},
+                           order) {}
+};
+
+// compute_obs.hpp:66-80: current, -2e/hbar gamma Re G^<_{lead,dot}(t, t); needs the
+// model's dot-lead blocks (set_table(spin, 1, 0, ...) and (spin, 0, 1, ...)).
+class compute_current_J_direct : public integrator_g_direct {
+ public:
+  compute_current_J_direct(g0_model model, double time, int order, double cutoff_integrand)
+     : integrator_g_direct(integrand_g_direct{g0_keldysh_contour_t{std::move(model)},
+                                              gf_index_t{time, up, forward, 0, 1},
+                                              gf_index_t{time, up, backward, 0, 0}, cutoff_integrand},
+                           order) {}
+};
+
+} // namespace impurity_oneband
+} // namespace keldy

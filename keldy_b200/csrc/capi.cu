@@ -239,8 +239,9 @@ static SobolDev sobol_dev(const kb_sobol *s) {
 
 static int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count) {
   if (k_first < 1) return fail(KB_E_INVALID, "Sobol point index must be >= 1 (first draw of sobol(dim, seed) is seed+1)");
+  // the last point keldy's generator hands out is k = 2^m (past_end() is checked before next())
   uint64_t last = (uint64_t)k_first + (uint64_t)(count > 0 ? count - 1 : 0);
-  if (count > 0 && last >= (1ull << s->m))
+  if (count > 0 && last > (1ull << s->m))
     return fail(KB_E_EXHAUSTED, "More sample points requested then generator can hold.");
   return KB_OK;
 }

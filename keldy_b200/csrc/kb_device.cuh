@@ -97,13 +97,16 @@ __device__ inline double2 g0_contour(const ModelDev &m, const kb_gf_index &a, co
 // ------------------------------------------------------------------ Sobol
 // Point number k (k >= 1) of the digital sequence: the state digitalseq_b2g::set_state
 // builds for Gray code gray(k), x_j = 2^-32 (cur_j ^ shift_j) (digitalseq_b2g.hpp:455-471).
+// k runs up to 2^m inclusive: keldy checks past_end() before next(), so the point
+// k = 2^m is drawn once, with next()'s column ctz(2^m) % m = 0 for the Gray-code bit m.
 __device__ __forceinline__ double sobol_coord(const SobolDev &s, uint32_t k, int j) {
-  const uint32_t g = k ^ (k >> 1); // below 2^m: columns b >= m are never read
+  const uint32_t g = k ^ (k >> 1);
   const uint32_t *C = s.Csr + j * s.m;
   uint32_t cur = 0;
 #pragma unroll
   for (int b = 0; b < SOBOL_COLS; ++b)
-    if ((g >> b) & 1u) cur ^= __ldg(C + b);
+    if (b < s.m && ((g >> b) & 1u)) cur ^= __ldg(C + b);
+  if (s.m < 32 && ((g >> s.m) & 1u)) cur ^= __ldg(C);
   return 2.3283064365386963e-10 * (double)(cur ^ __ldg(s.shfr + j));
 }
 

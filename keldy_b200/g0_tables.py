@@ -115,3 +115,71 @@ def flatband(gamma, eps_d, bias_V, beta, time_max, npts):
     gl[:mid] = -np.conj(gl_pos[::-1])
     gg[:mid] = -np.conj(gg_pos[::-1])
     return t, gl, gg
+
+
+def _fermi(x, beta):
+    if not np.isfinite(beta):
+        return np.where(x < 0, 1.0, np.where(x > 0, 0.0, 0.5))
+    return 0.5 * (1.0 - np.tanh(0.5 * beta * x))
+
+
+def semicircle(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_lead=False, nodes=None):
+    """Dot coupled to two semicircular leads of half-bandwidth D (model.cpp:92-105):
+    Delta^R(w) = Gamma/(2D) (w - i sqrt(D^2 - w^2)) per lead inside the band. As keldy's
+    finite-contour method (model.cpp:220-319), the Fourier integrals run over the band
+    [-D, D]; here in theta with w = -D cos(theta), which removes the square-root edges,
+    by Gauss-Legendre panels split at the chemical potentials.
+
+    Returns (t, lesser, greater) for the dot, and with dot_lead=True also the
+    (lead, dot) and (dot, lead) blocks: (t, lesser, greater, lesser_10, greater_10,
+    lesser_01, greater_01) (right lead, model.hpp:94-99)."""
+    t = time_mesh(time_max, npts)
+    D = float(half_bandwidth)
+    mus = (-bias_V / 2.0, bias_V / 2.0)
+    breaks = sorted({0.0, np.pi} | {float(np.arccos(-mu / D)) for mu in mus if abs(mu) < D})
+    n = nodes or int(96 + 2.0 * D * time_max)
+    xg, wg = np.polynomial.legendre.leggauss(n)
+    th_list, w_list = [], []
+    for a, b in zip(breaks[:-1], breaks[1:]):
+        th_list.append(0.5 * (b - a) * xg + 0.5 * (b + a))
+        w_list.append(0.5 * (b - a) * wg)
+    th = np.concatenate(th_list)
+    wq = np.concatenate(w_list)
+    w = -D * np.cos(th)
+    jac = D * np.sin(th)
+    root = D * np.sin(th)                       # sqrt(D^2 - w^2)
+    delta_r = 0.5 * (gamma / D) * (w - 1j * root)  # per lead
+    gR = 1.0 / (w - eps_d - 2.0 * delta_r)
+    c = (gamma / D) * root                      # -i (Delta^R - Delta^A) per lead
+    nl = [_fermi(w - mu, beta) for mu in mus]
+    less_w = 1j * c * (nl[0] + nl[1]) * np.abs(gR) ** 2
+    great_w = -1j * c * ((1 - nl[0]) + (1 - nl[1])) * np.abs(gR) ** 2
+
+    def ft(gw, times):
+        f = wq * jac * gw / (2 * np.pi)
+        out = np.empty(len(times), dtype=np.complex128)
+        for s in range(0, len(times), 8192):
+            out[s:s + 8192] = np.exp(-1j * np.outer(times[s:s + 8192], w)) @ f
+        return out
+
+    mid = len(t) // 2
+
+    def dot_block(gw):
+        pos = ft(gw, t[mid + 1:])
+        g = np.empty(len(t), dtype=np.complex128)
+        g[mid + 1:] = pos
+        g[mid] = ft(gw, np.zeros(1))[0]
+        g[:mid] = -np.conj(pos[::-1])
+        return g
+
+    gl, gg = dot_block(less_w), dot_block(great_w)
+    if not dot_lead:
+        return t, gl, gg
+    # right lead - dot (model.hpp:94-99): -s n_R^(s) (Delta^R - Delta^A)_R g^A + Delta^R_R g_dot^(s)
+    gA = np.conj(gR)
+    l10_w = -(nl[1]) * (-1j * c) * gA + delta_r * less_w
+    g10_w = (1 - nl[1]) * (-1j * c) * gA + delta_r * great_w
+    l10, g10 = ft(l10_w, t), ft(g10_w, t)
+    l01 = -np.conj(l10[::-1])
+    g01 = -np.conj(g10[::-1])
+    return t, gl, gg, l10, g10, l01, g01

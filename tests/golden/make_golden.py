@@ -10,8 +10,12 @@ built oracle/_ref (``make -C oracle``):
   chains, integrand values (two g0 tables, several external-point pairs, orders 0-6),
   eval_no_det values and the integrator's sums.
 * keldy_tests.json: known answers read from keldy's test files: the Horvatic-Zlatic
-  charge series and its parameters (test/c++/impurity_oneband/compute_obs_test.cpp),
-  and the plasma-warper vectors (test/c++/warpers/warper_plasma_uv_test.cpp).
+  charge series and its parameters and the order-1 current
+  (test/c++/impurity_oneband/compute_obs_test.cpp), the plasma-warper vectors
+  (test/c++/warpers/warper_plasma_uv_test.cpp), and g0 values of the semicircular and
+  flat-band models (model_semicircle_test.cpp, model_flatband_test.cpp).
+
+    python tests/golden/make_golden.py --json-only   # rewrite keldy_tests.json only
 """
 from __future__ import annotations
 
@@ -69,9 +73,51 @@ def keldy_test_values():
         ui = [float(x) for x in re.search(r"ui_times = \{([^}]*)\}", block).group(1).split(",")]
         vi = [float(x) for x in re.search(r"vi_result = \{([^}]*)\}", block).group(1).split(",")]
         vecs.append({"t_max": t_max, "ui": ui, "vi": vi})
+    def params_of(block):
+        out = {}
+        for k, v in re.findall(r"params\.(\w+) = ([^;]+);", block):
+            v = v.strip()
+            out[k] = v.strip('"') if v.startswith('"') else float(v)
+        return out
+
+    def test_block(text, name):
+        return re.search(r"TEST\(" + name + r"\).*?\n}\n", text, re.S).group(0)
+
+    cur = test_block(src, r"ComputeObs, ValueCurrent1")
+    current = {"params": params_of(cur),
+               "t_max": float(re.search(r"double t_max = ([\d.]+);", cur).group(1)),
+               "w_scale": float(re.search(r"make_product_1d_simple_inverse_square\(t_max, ([\d.]+)\)", cur).group(1)),
+               "n_points": int(float(re.search(r"computer\.run\(([\de.]+)\)", cur).group(1))),
+               "value": float(re.search(r"EXPECT_NEAR\([^,]+, ([\d.e-]+), ([\d.e-]+)\)", cur).group(1)),
+               "tol": float(re.search(r"EXPECT_NEAR\([^,]+, ([\d.e-]+), ([\d.e-]+)\)", cur).group(2))}
+    sc = open(os.path.join(KELDY_SRC, "test/c++/impurity_oneband/model_semicircle_test.cpp")).read()
+    semi = []
+    for name in ("g0_model, Semicirc_fft", "g0_model, Semicirc_contour"):
+        blk = test_block(sc, name)
+        vals = re.findall(r"EXPECT_COMPLEX_NEAR\(([-\d.e]+) \+ ([-\d.e]+)i, g0\.g0_lesser\[up\]\(([\d.]+)\)\((\d), (\d)\), "
+                          r"([\d.e-]+)\)", blk)
+        semi.append({"params": params_of(blk), "values": [
+            {"re": float(a), "im": float(b), "t": float(t), "o1": int(i), "o2": int(j), "tol": float(tol)}
+            for a, b, t, i, j, tol in vals]})
+    fb = open(os.path.join(KELDY_SRC, "test/c++/impurity_oneband/model_flatband_test.cpp")).read()
+    flat = []
+    for name in ("g0_model, Flatband_asym_1", "g0_model, Flatband_asym_2"):
+        blk = test_block(fb, name)
+        first = blk.split("g0_model g0_ctr")[0]
+        vals = re.findall(r"EXPECT_COMPLEX_NEAR\(([-\d.e]+) \+ ([-\d.e]+)i, g0_ctr\.g0_lesser\[up\]\(([\d.]+)\)\(0, 0\), "
+                          r"([\d.e-]+)\)", blk)
+        p = params_of(first)
+        p.update(params_of(blk.split("g0_model g0_fft")[1]))  # the contour run's parameters
+        flat.append({"params": p, "values": [{"re": float(a), "im": float(b), "t": float(t), "tol": float(tol)}
+                                             for a, b, t, tol in vals]})
     return {
-        "source": "keldy test/c++/impurity_oneband/compute_obs_test.cpp:93-181, "
-                  "test/c++/warpers/warper_plasma_uv_test.cpp:15-43",
+        "source": "keldy test/c++/impurity_oneband/compute_obs_test.cpp:93-206, "
+                  "test/c++/warpers/warper_plasma_uv_test.cpp:15-43, "
+                  "test/c++/impurity_oneband/model_semicircle_test.cpp:30-86, "
+                  "test/c++/impurity_oneband/model_flatband_test.cpp:154-220",
+        "current_kat": current,
+        "semicircle_kat": semi,
+        "flatband_kat": flat,
         "hz_charge_series": hz,
         "hz_params": {"beta": "inf", "bias_V": 0.0, "eps_d": 0.0, "Gamma": 1.0, "time_max": 30.0,
                       "nr_time_points_gf": 10001, "alpha": 0.0, "bath_type": "flatband", "ft_method": "analytic",
@@ -83,6 +129,10 @@ def keldy_test_values():
 
 
 def main():
+    if "--json-only" in sys.argv:
+        with open(os.path.join(HERE, "keldy_tests.json"), "w") as f:
+            json.dump(keldy_test_values(), f, indent=1)
+        return
     ref = Reference()
     rng = np.random.default_rng(20240601)
     out = {}

@@ -24,6 +24,14 @@ def test_sobol_far_indices_and_short_sequences(ctx, oracle):
         assert np.array_equal(got, want)
 
 
+def test_sobol_last_points(ctx, oracle):
+    # keldy checks past_end() before next(): with 2^m points, k = 2^m is the last one drawn
+    for dim, m, sh, sc in [(5, 10, 0, 0), (7, 12, 1, 1)]:
+        got = ctx.sobol(dim, m, bool(sh), bool(sc), 4).points((1 << m) - 3, 4)
+        want = oracle.sobol_points(dim, (1 << m) - 4, 4, bool(sh), bool(sc), 4, log_max_points=m)
+        assert np.array_equal(got, want)
+
+
 def test_sobol_errors(ctx):
     s = ctx.sobol(4, 10)
     with pytest.raises(capi.KbError) as e:
