@@ -1,0 +1,52 @@
+"""Randomised quasi-Monte Carlo error bars on the GPU.
+
+R independent random digital shifts of the same Sobol sequence (keldy's
+sobol(dim, seed, do_shift=true, do_scramble, rng_seed_shift = 1..R), qrng.hpp:77-109)
+give R unbiased estimates of the integral; their mean is the estimate and their
+standard deviation / sqrt(R) its standard error. All replicas of all orders run in one
+kb_integrate call (one batched launch).
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import capi
+
+
+def estimate(ctx, model, A, B, chain, order, n_points, replicas=16, seed_shift0=1, scramble=False, k_first=1,
+             cutoff=0.0, algo=capi.ALGO_AUTO, rngs=None):
+    """Mean, standard error and per-replica means of int f(warp(x)) J dx over [0,1]^order.
+    rngs: optional list of `replicas` prebuilt shifted generators (reused across calls)."""
+    if rngs is None:
+        rngs = [ctx.sobol(order, 31, True, scramble, seed_shift0 + r) for r in range(replicas)]
+    items = [dict(model=model, rng=g, chain=chain, A=A, B=B, cutoff=cutoff, order=order, k_first=k_first,
+                  n_points=n_points) for g in rngs]
+    res = capi.integrate(ctx, items, algo)
+    means = np.array([s / n for s, n, _, _ in res])
+    mean = means.mean()
+    r = len(means)
+    err = math.sqrt((np.abs(means - mean) ** 2).sum() / (r - 1) / r) if r > 1 else float("nan")
+    return mean, err, means
+
+
+def time_to_relative_error(ctx, model, A, B, chain, order, target=1e-3, replicas=16, start_points=1 << 12,
+                           max_points=1 << 24, seed_shift0=1, scramble=False):
+    """Doubles the points per replica until stderr / |mean| <= target (or max_points is
+    reached). Returns dict(mean, stderr, rel, points_per_replica, evaluations, seconds):
+    `seconds` is the wall time of the run that met the target (the GPU work needed at
+    that size, excluding the smaller probing runs)."""
+    rngs = [ctx.sobol(order, 31, True, scramble, seed_shift0 + r) for r in range(replicas)]
+    n = start_points
+    while True:
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        mean, err, _ = estimate(ctx, model, A, B, chain, order, n, replicas, rngs=rngs)
+        dt = time.perf_counter() - t0
+        rel = err / abs(mean) if mean != 0 else float("inf")
+        if rel <= target or n >= max_points:
+            return dict(mean=mean, stderr=err, rel=rel, points_per_replica=n, evaluations=n * replicas, seconds=dt,
+                        reached=rel <= target)
+        n *= 2
