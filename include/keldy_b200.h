@@ -198,6 +198,29 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
 #define KB_NOALLOC_SCRATCH_BYTES (12u << 20)
 int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc);
 
+/* ------------------------------------------------------------------ plans --- */
+/* A batched integration set up once and launched many times: the work items' descriptors
+ * and scratch stay on the device, and the launch sequence (tree or pivoted-LU kernel,
+ * guarded-pivot pass, reduction) is captured into a CUDA graph on the first launch and
+ * replayed after. Replaces keldy's per-point integrator::run loop (integrator.hpp:81-95)
+ * for a fixed set of (model, order, generator, warper chain) runs. */
+typedef struct kb_plan kb_plan;
+int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_plan **out);
+int kb_plan_destroy(kb_plan *plan);
+/* Enqueue one run on the context's stream; the sums of this run land in the plan's device
+ * accumulators (read them with kb_plan_result). */
+int kb_plan_launch(kb_context *ctx, kb_plan *plan);
+/* Wait for the last launch and add its sums to acc[n_work]. */
+int kb_plan_result(kb_context *ctx, kb_plan *plan, kb_accum *acc);
+/* Move work item i to Sobol points k_first .. k_first + n_points - 1 for the next launch
+ * (the generator state advances without rebuilding the plan). */
+int kb_plan_set_k_first(kb_context *ctx, kb_plan *plan, int item, uint32_t k_first);
+
+/* Launch shape of the tree kernel: points per scheduling chunk for `order` (1..128;
+ * order -1 sets every order) and resident CTAs per SM (1 or 2; 0 keeps the value). */
+int kb_context_set_launch(kb_context *ctx, int order, int chunk_points, int ctas_per_sm);
+int kb_context_get_launch(kb_context *ctx, int order, int *chunk_points, int *ctas_per_sm);
+
 /* ----------------------------------------------------------------- peaks --- */
 /* Measures the FP64 FMA rate of this device (FLOP/s, 2 per FMA) with a dependent-chain
  * kernel of `iters` FMAs per thread; used as the roofline denominator. */

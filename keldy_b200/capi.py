@@ -32,7 +32,8 @@ EXPORTS = [
     "kb_sobol_points_dev",
     "kb_warp", "kb_model_create", "kb_model_destroy", "kb_model_set_table", "kb_model_set_table_dev",
     "kb_g0_eval", "kb_integrand_eval", "kb_integrand_eval_no_det", "kb_evaluate_warped", "kb_integrate",
-    "kb_fp64_peak", "kb_integrate_noalloc",
+    "kb_fp64_peak", "kb_integrate_noalloc", "kb_plan_create", "kb_plan_destroy", "kb_plan_launch",
+    "kb_plan_result", "kb_plan_set_k_first", "kb_context_set_launch", "kb_context_get_launch",
 ]
 NOALLOC_MAX_ITEMS, NOALLOC_MAX_CHUNKS = 64, 65536
 
@@ -111,6 +112,13 @@ def load():
     L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
     L.kb_fp64_peak.argtypes = [_VP, C.c_int, _D]
     L.kb_integrate_noalloc.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(Accum)]
+    L.kb_plan_create.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(_VP)]
+    L.kb_plan_destroy.argtypes = [_VP]
+    L.kb_plan_launch.argtypes = [_VP, _VP]
+    L.kb_plan_result.argtypes = [_VP, _VP, C.POINTER(Accum)]
+    L.kb_plan_set_k_first.argtypes = [_VP, _VP, C.c_int, C.c_uint32]
+    L.kb_context_set_launch.argtypes = [_VP, C.c_int, C.c_int, C.c_int]
+    L.kb_context_get_launch.argtypes = [_VP, C.c_int, _I, _I]
     _lib = L
     return L
 
@@ -187,6 +195,16 @@ class Context:
 
     def set_timing(self, enable=True):
         check(self.L.kb_context_set_timing(self.h, int(enable)))
+
+    def set_launch(self, order=-1, chunk_points=128, ctas_per_sm=0):
+        """Tree-kernel launch shape: points per scheduling chunk of `order` (-1: all) and
+        resident CTAs per SM (0 keeps the current value)."""
+        check(self.L.kb_context_set_launch(self.h, order, chunk_points, ctas_per_sm))
+
+    def get_launch(self, order):
+        a, b = C.c_int(), C.c_int()
+        check(self.L.kb_context_get_launch(self.h, order, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def last_timing(self):
         """(integrand_ms, fallback_ms, reduce_ms, launches) of the last kb_integrate."""
@@ -349,6 +367,46 @@ def _works(items):
                         Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
                         int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]))
     return works, keep
+
+
+class Plan:
+    """A batched integration set up once and launched many times (captured into a CUDA
+    graph on its first launch)."""
+
+    def __init__(self, ctx, items, algo=ALGO_AUTO):
+        self.ctx = ctx
+        self.items = list(items)
+        works, self._keep = _works(self.items)
+        h = _VP()
+        check(ctx.L.kb_plan_create(ctx.h, works, len(self.items), algo, C.byref(h)))
+        self.h = h
+        ctx._deps.add(self)
+
+    def launch(self):
+        check(self.ctx.L.kb_plan_launch(self.ctx.h, self.h))
+
+    def result(self):
+        acc = (Accum * max(1, len(self.items)))()
+        check(self.ctx.L.kb_plan_result(self.ctx.h, self.h, acc))
+        return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback) for a in acc[:len(self.items)]]
+
+    def run(self):
+        self.launch()
+        return self.result()
+
+    def set_k_first(self, item, k_first):
+        check(self.ctx.L.kb_plan_set_k_first(self.ctx.h, self.h, item, k_first))
+
+    def close(self):
+        if self.h:
+            self.ctx.L.kb_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def integrate_noalloc(ctx, items):

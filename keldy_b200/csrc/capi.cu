@@ -72,6 +72,8 @@ struct kb_context {
   int sm_count = 0;
   int tree_grid = 0;
   int *d_err = nullptr; // error flags written by kernels
+  int chunk_points[MAX_ORDER + 1]; // scheduling chunk of each order (autotuned; default 128)
+  int ctas_per_sm = 2;             // resident tree CTAs per SM
   bool timing = false;
   cudaEvent_t ev[4] = {};
   double last_ms[3] = {0, 0, 0};
@@ -118,9 +120,11 @@ int kb_context_create(int device, kb_context **out) {
   KB_CUDA(cudaGetDeviceProperties(&prop, device));
   if (prop.major < 10)
     return fail(KB_E_NODEVICE, std::string("keldy_b200 is built for sm_100a; device is ") + prop.name);
+  KB_CUDA(configure_kernels());
   auto *ctx = new kb_context;
   ctx->device = device;
   ctx->sm_count = prop.multiProcessorCount;
+  for (int n = 0; n <= MAX_ORDER; ++n) ctx->chunk_points[n] = CHUNK_POINTS;
   e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     delete ctx;
@@ -518,6 +522,7 @@ static ItemDev make_item(const kb_model *m, const kb_integrand *f, int order) {
   it.spin_symmetric = sym ? 1 : 0;
   it.f = *f;
   it.order = order;
+  it.chunk_points = CHUNK_POINTS;
   return it;
 }
 
@@ -691,6 +696,7 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
     it.rng = sobol_dev(w.rng);
     it.k_first = w.k_first;
     it.n_points = w.n_points;
+    it.chunk_points = ctx->chunk_points[w.order];
     if (algo == KB_ALGO_TREE && !it.spin_symmetric)
       return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
     use_tree[(size_t)i] = (algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric);
@@ -716,7 +722,8 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
     std::vector<long long> offs(1, 0);
     for (int i : ids) {
       sorted.push_back(items[(size_t)i]);
-      offs.push_back(offs.back() + (items[(size_t)i].n_points + CHUNK_POINTS - 1) / CHUNK_POINTS);
+      const long long cp = items[(size_t)i].chunk_points;
+      offs.push_back(offs.back() + (items[(size_t)i].n_points + cp - 1) / cp);
     }
     const long long nchunks = offs.back();
     if (nchunks > INT32_MAX) return fail(KB_E_INVALID, "too many points in one kb_integrate call");
@@ -741,7 +748,7 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
     L.partials = dpart.as<ChunkPartial>();
     L.err = ctx->d_err;
     DevBuf dpts;
-    const int tgrid = (int)std::min<long long>(nchunks, ctx->tree_grid);
+    const int tgrid = (int)std::min<long long>(nchunks, (long long)ctx->sm_count * ctx->ctas_per_sm);
     if (group == 0) {
       KB_CUDA(dpts.alloc((size_t)tgrid * PTS_SLOT * sizeof(double), st));
       L.pts = dpts.as<double>();
@@ -785,6 +792,252 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
   KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   KB_CUDA(cudaStreamSynchronize(st));
   if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  return KB_OK;
+}
+
+
+// ------------------------------------------------------------------ plans
+struct kb_plan {
+  struct Group {
+    int n_items = 0;
+    std::vector<int> ids;      // original work index of each sorted item
+    std::vector<ItemDev> items; // host copy (k_first updates)
+    long long n_chunks = 0;
+    int grid = 0;
+    ItemDev *d_items = nullptr;
+    long long *d_offs = nullptr;
+    int *d_cnt = nullptr;
+    ChunkPartial *d_part = nullptr;
+    double *d_pts = nullptr;
+    kb_accum *d_acc = nullptr;
+  } g[2];
+  int n_work = 0;
+  std::vector<int> where_group, where_pos; // work index -> (group, sorted position)
+  std::vector<const kb_sobol *> rng;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+static void plan_free(kb_plan *p) {
+  cudaSetDevice(p->device);
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  for (auto &g : p->g) {
+    cudaFree(g.d_items);
+    cudaFree(g.d_offs);
+    cudaFree(g.d_cnt);
+    cudaFree(g.d_part);
+    cudaFree(g.d_pts);
+    cudaFree(g.d_acc);
+  }
+  delete p;
+}
+
+int kb_plan_destroy(kb_plan *plan) {
+  if (plan) plan_free(plan);
+  return KB_OK;
+}
+
+int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_plan **out) {
+  KB_CHECK(ctx && out && (n_work == 0 || work), "kb_plan_create: null argument");
+  KB_CHECK(algo == KB_ALGO_AUTO || algo == KB_ALGO_TREE || algo == KB_ALGO_DIRECT, "unknown algorithm");
+  std::vector<ItemDev> items((size_t)n_work);
+  std::vector<int> grp((size_t)n_work);
+  for (int i = 0; i < n_work; ++i) {
+    const kb_work &w = work[i];
+    int st = check_integrand(w.m, &w.f, w.order);
+    if (st) return st;
+    KB_CHECK(w.rng, "work item without a Sobol generator");
+    KB_CHECK(w.n_points >= 0, "n_points must be >= 0");
+    KB_CHECK(w.order >= 1, "integrator dimension must be > 0 (Dimension of the integration space must be > 0.)");
+    if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
+    st = check_sobol_range(w.rng, w.k_first, w.n_points);
+    if (st) return st;
+    ItemDev &it = items[(size_t)i];
+    it = make_item(w.m, &w.f, w.order);
+    st = make_chain(w.chain, w.chain_len, it.chain);
+    if (st) return st;
+    it.chain_len = w.chain_len;
+    it.chain_start = w.chain_len;
+    it.rng = sobol_dev(w.rng);
+    it.k_first = w.k_first;
+    it.n_points = w.n_points;
+    it.chunk_points = ctx->chunk_points[w.order];
+    if (algo == KB_ALGO_TREE && !it.spin_symmetric)
+      return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
+    grp[(size_t)i] = ((algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric)) ? 0 : 1;
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  auto *p = new kb_plan;
+  p->device = ctx->device;
+  p->n_work = n_work;
+  p->where_group.assign((size_t)n_work, -1);
+  p->where_pos.assign((size_t)n_work, -1);
+  for (int i = 0; i < n_work; ++i) p->rng.push_back(work[i].rng);
+  for (int gi = 0; gi < 2; ++gi) {
+    auto &g = p->g[gi];
+    for (int i = 0; i < n_work; ++i)
+      if (grp[(size_t)i] == gi && items[(size_t)i].n_points > 0) g.ids.push_back(i);
+    std::stable_sort(g.ids.begin(), g.ids.end(),
+                     [&](int a, int b) { return items[(size_t)a].order > items[(size_t)b].order; });
+    g.n_items = (int)g.ids.size();
+    if (!g.n_items) continue;
+    std::vector<long long> offs(1, 0);
+    for (int j = 0; j < g.n_items; ++j) {
+      const ItemDev &it = items[(size_t)g.ids[(size_t)j]];
+      g.items.push_back(it);
+      offs.push_back(offs.back() + (it.n_points + it.chunk_points - 1) / it.chunk_points);
+      p->where_group[(size_t)g.ids[(size_t)j]] = gi;
+      p->where_pos[(size_t)g.ids[(size_t)j]] = j;
+    }
+    g.n_chunks = offs.back();
+    if (g.n_chunks > INT32_MAX) {
+      plan_free(p);
+      return fail(KB_E_INVALID, "too many points in one plan");
+    }
+    g.grid = (int)std::min<long long>(g.n_chunks, gi == 0 ? (long long)ctx->sm_count * ctx->ctas_per_sm
+                                                          : (long long)ctx->sm_count * 4);
+    cudaError_t e = cudaMalloc(&g.d_items, sizeof(ItemDev) * g.n_items);
+    if (e == cudaSuccess) e = cudaMalloc(&g.d_offs, sizeof(long long) * offs.size());
+    if (e == cudaSuccess) e = cudaMalloc(&g.d_cnt, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&g.d_part, sizeof(ChunkPartial) * (size_t)g.n_chunks);
+    if (e == cudaSuccess && gi == 0) e = cudaMalloc(&g.d_pts, sizeof(double) * PTS_SLOT * (size_t)g.grid);
+    if (e == cudaSuccess) e = cudaMalloc(&g.d_acc, sizeof(kb_accum) * g.n_items);
+    if (e == cudaSuccess) e = cudaMemcpy(g.d_items, g.items.data(), sizeof(ItemDev) * g.n_items, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(g.d_offs, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      plan_free(p);
+      return fail(KB_E_NOMEM, std::string("kb_plan_create: ") + cudaGetErrorString(e));
+    }
+  }
+  *out = p;
+  return KB_OK;
+}
+
+// The launch sequence of one run (captured into the plan's graph).
+static int plan_enqueue(kb_context *ctx, kb_plan *p, cudaStream_t st) {
+  for (int gi = 0; gi < 2; ++gi) {
+    auto &g = p->g[gi];
+    if (!g.n_items) continue;
+    KB_CUDA(cudaMemsetAsync(g.d_acc, 0, sizeof(kb_accum) * g.n_items, st));
+    KB_CUDA(cudaMemsetAsync(g.d_cnt, 0, sizeof(int), st));
+    Launch L;
+    memset(&L, 0, sizeof(L));
+    L.items = g.d_items;
+    L.n_items = g.n_items;
+    L.chunk_offsets = g.d_offs;
+    L.n_chunks = (int)g.n_chunks;
+    L.chunk_counter = g.d_cnt;
+    L.mode = IN_SOBOL;
+    L.partials = g.d_part;
+    L.pts = g.d_pts;
+    L.err = ctx->d_err;
+    if (gi == 0) {
+      KB_CUDA(launch_tree(L, g.grid, st));
+      KB_CUDA(launch_fallback(L, ctx->sm_count * 4, st));
+    } else {
+      KB_CUDA(launch_direct(L, g.grid, st));
+    }
+    KB_CUDA(launch_reduce(L, g.d_acc, st));
+  }
+  return KB_OK;
+}
+
+int kb_plan_launch(kb_context *ctx, kb_plan *plan) {
+  KB_CHECK(ctx && plan, "kb_plan_launch: null argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  if (!plan->exec) {
+    cudaGraph_t graph = nullptr;
+    KB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = plan_enqueue(ctx, plan, st);
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return fail(KB_E_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&plan->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(KB_E_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  }
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
+  KB_CUDA(cudaGraphLaunch(plan->exec, st));
+  if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[1], st));
+  return KB_OK;
+}
+
+int kb_plan_result(kb_context *ctx, kb_plan *plan, kb_accum *acc) {
+  KB_CHECK(ctx && plan && (plan->n_work == 0 || acc), "kb_plan_result: null argument");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  std::vector<kb_accum> part[2];
+  for (int gi = 0; gi < 2; ++gi) {
+    part[gi].resize((size_t)plan->g[gi].n_items);
+    if (plan->g[gi].n_items)
+      KB_CUDA(cudaMemcpyAsync(part[gi].data(), plan->g[gi].d_acc, sizeof(kb_accum) * plan->g[gi].n_items,
+                              cudaMemcpyDeviceToHost, st));
+  }
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (ctx->timing) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]) == cudaSuccess) {
+      ctx->last_ms[0] = ms;
+      ctx->last_ms[1] = ctx->last_ms[2] = 0.0;
+    }
+  }
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  for (int gi = 0; gi < 2; ++gi)
+    for (int j = 0; j < plan->g[gi].n_items; ++j) {
+      kb_accum &a = acc[plan->g[gi].ids[(size_t)j]];
+      const kb_accum &q = part[gi][(size_t)j];
+      a.sum_re += q.sum_re;
+      a.sum_im += q.sum_im;
+      a.n_points += q.n_points;
+      a.n_in_domain += q.n_in_domain;
+      a.n_fallback += q.n_fallback;
+    }
+  return KB_OK;
+}
+
+int kb_plan_set_k_first(kb_context *ctx, kb_plan *plan, int item, uint32_t k_first) {
+  KB_CHECK(ctx && plan, "kb_plan_set_k_first: null argument");
+  KB_CHECK(item >= 0 && item < plan->n_work, "work item index out of range");
+  const int gi = plan->where_group[(size_t)item], pos = plan->where_pos[(size_t)item];
+  if (gi < 0) return KB_OK; // no points
+  ItemDev &it = plan->g[gi].items[(size_t)pos];
+  int st = check_sobol_range(plan->rng[(size_t)item], k_first, it.n_points);
+  if (st) return st;
+  it.k_first = k_first;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  KB_CUDA(cudaMemcpyAsync(&plan->g[gi].d_items[pos].k_first, &it.k_first, sizeof(uint32_t), cudaMemcpyHostToDevice,
+                          ctx->stream));
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return KB_OK;
+}
+
+int kb_context_set_launch(kb_context *ctx, int order, int chunk_points, int ctas_per_sm) {
+  KB_CHECK(ctx, "null context");
+  KB_CHECK(order == -1 || (order >= 0 && order <= MAX_ORDER), "order must be -1 or in [0, 16]");
+  KB_CHECK(chunk_points >= 1 && chunk_points <= CHUNK_POINTS, "chunk_points must be in [1, 128]");
+  KB_CHECK(ctas_per_sm >= 0 && ctas_per_sm <= 2, "ctas_per_sm must be 0 (keep), 1 or 2");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  for (int n = 0; n <= MAX_ORDER; ++n)
+    if (order == -1 || order == n) ctx->chunk_points[n] = chunk_points;
+  if (ctas_per_sm) ctx->ctas_per_sm = ctas_per_sm;
+  return KB_OK;
+}
+
+int kb_context_get_launch(kb_context *ctx, int order, int *chunk_points, int *ctas_per_sm) {
+  KB_CHECK(ctx && order >= 0 && order <= MAX_ORDER, "kb_context_get_launch: bad argument");
+  if (chunk_points) *chunk_points = ctx->chunk_points[order];
+  if (ctas_per_sm) *ctas_per_sm = ctx->ctas_per_sm;
   return KB_OK;
 }
 

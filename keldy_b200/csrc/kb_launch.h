@@ -53,6 +53,8 @@ struct Launch {
 };
 
 size_t tree_smem_bytes();
+// sets the kernels' shared-memory attributes (before any stream capture)
+cudaError_t configure_kernels();
 cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st);
 cudaError_t launch_direct(const Launch &L, int grid, cudaStream_t st);
 // pivoted-LU evaluation of the points marked in the chunk partials' fb_mask

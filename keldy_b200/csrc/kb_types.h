@@ -50,6 +50,7 @@ struct ItemDev {
   int order;
   int spin_symmetric; // spin-down tables equal spin-up ones: det(s2) = det of s1's vertex block
   uint32_t k_first;
+  int chunk_points; // points per scheduling chunk of this item (<= 128)
   int64_t n_points;
 };
 

@@ -520,9 +520,9 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
     if (c >= L.n_chunks) break;
     const int item = find_item(L.chunk_offsets, L.n_items, c);
     const ItemDev &it = L.items[item];
-    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * CHUNK_POINTS;
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * it.chunk_points;
     const long long total = EVAL ? (L.index ? (long long)L.n_index : it.n_points) : it.n_points;
-    const int ccount = (int)min((long long)CHUNK_POINTS, total - cfirst);
+    const int ccount = (int)min((long long)it.chunk_points, total - cfirst);
     const int N = it.order;
     const int P = tree_points_per_chunk(N);
     const bool keep = (L.mode == IN_SOBOL) ? true : (L.keep_u_hypercube != 0);
@@ -731,9 +731,9 @@ __global__ void __launch_bounds__(NT) direct_kernel(Launch L) {
     if (c >= L.n_chunks) break;
     const int item = find_item(L.chunk_offsets, L.n_items, c);
     const ItemDev &it = L.items[item];
-    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * CHUNK_POINTS;
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * it.chunk_points;
     const long long total = eval ? (L.index ? (long long)L.n_index : it.n_points) : it.n_points;
-    const int ccount = (int)min((long long)CHUNK_POINTS, total - cfirst);
+    const int ccount = (int)min((long long)it.chunk_points, total - cfirst);
     const int N = it.order;
     const bool keep = eval ? (L.keep_u_hypercube != 0) : true;
     double2 csum = c2(0.0, 0.0);
@@ -790,8 +790,8 @@ __global__ void __launch_bounds__(NT) fallback_kernel(Launch L) {
     if (pr.n_fallback == 0) continue;
     const int item = find_item(L.chunk_offsets, L.n_items, c);
     const ItemDev &it = L.items[item];
-    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * CHUNK_POINTS;
-    for (int bit = 0; bit < CHUNK_POINTS; ++bit) {
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * it.chunk_points;
+    for (int bit = 0; bit < it.chunk_points; ++bit) {
       unsigned long long w = pr.fb_mask[bit >> 6];
       if (!((w >> (bit & 63)) & 1ull)) continue;
       direct_load_point(L, it, it.order, cfirst + bit, true, D);
@@ -853,6 +853,18 @@ __global__ void __launch_bounds__(NT) reduce_kernel(Launch L, kb_accum *acc) {
 } // namespace
 
 size_t tree_smem_bytes() { return sizeof(TreeShared); }
+
+cudaError_t configure_kernels() {
+  cudaError_t e = cudaFuncSetAttribute(tree_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(TreeShared));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tree_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TreeShared));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirectShared));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirectShared));
+  return e;
+}
 
 static size_t direct_smem_bytes() { return sizeof(DirectShared); }
 
