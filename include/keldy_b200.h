@@ -164,8 +164,12 @@ typedef struct {
   uint64_t n_fallback;  /* points the tree handed to the pivoted-LU kernel (guarded pivots) */
 } kb_accum;
 
+typedef struct kb_flow kb_flow;
+
 /* One unit of QMC work: `n_points` Sobol points k_first.. of `rng` through `chain` into
- * the integrand of `order` on model `m`. */
+ * the integrand of `order` on model `m`. `flow` (optional, NULL = none): a learned
+ * coupling flow of dimension `order` applied to each Sobol point before the chain, its
+ * Jacobian multiplying the chain's (see kb_flow_create). */
 typedef struct {
   const kb_model *m;
   const kb_sobol *rng;
@@ -175,6 +179,7 @@ typedef struct {
   int order;
   uint32_t k_first;
   int64_t n_points;
+  const kb_flow *flow;
 } kb_work;
 
 /* integrator::run(nr_steps) (integrator.hpp:81-95) for every work item, summed into
@@ -220,6 +225,55 @@ int kb_plan_set_k_first(kb_context *ctx, kb_plan *plan, int item, uint32_t k_fir
  * order -1 sets every order) and resident CTAs per SM (1 or 2; 0 keeps the value). */
 int kb_context_set_launch(kb_context *ctx, int order, int chunk_points, int ctas_per_sm);
 int kb_context_get_launch(kb_context *ctx, int order, int *chunk_points, int *ctas_per_sm);
+
+/* ------------------------------------------------------ learned flow warper --- */
+/* No counterpart in keldy: a learned first stage of the warper chain. A flow of
+ * dimension n (2..8) maps the Sobol point z in [0,1]^n to the chain's input li with an
+ * exact Jacobian; six coupling layers, each redrawing half of the dims through 32-bin
+ * piecewise-linear CDFs whose logits come from a 128-wide two-hidden-layer ReLU MLP of
+ * the other half (bf16 weights, fp32 accumulation on the tensor cores, CDFs in fp64 when
+ * sampling). Trained by weighted maximum likelihood on points li with weights |f(li) J|
+ * of the plain warper chain, its density approaches |integrand|, which lowers the
+ * variance of the estimate; the plain chain alone remains the method without it.
+ * Parameters: KB_FLOW_PARAMS floats, [layer][matrix W1, W2, W3][out][in], 128 x 128
+ * each; the biases are column 16*T_l[0] of W1 (constant input) and column 127 of W2, W3
+ * (hidden unit 127 is fixed to 1). */
+#define KB_FLOW_LAYERS 6
+#define KB_FLOW_WIDTH 128
+#define KB_FLOW_MAX_DIM 8
+#define KB_FLOW_PARAMS (KB_FLOW_LAYERS * 3 * KB_FLOW_WIDTH * KB_FLOW_WIDTH)
+/* W1, W2 uniform in +-sqrt(6/128) from mt19937_64(seed), W3 = 0 (identity flow). */
+int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out);
+int kb_flow_destroy(kb_flow *flow);
+int kb_flow_dim(const kb_flow *flow);
+int kb_flow_get_params(kb_flow *flow, float *params);
+int kb_flow_set_params(kb_flow *flow, const float *params);
+/* direction 0 (density): x [count][dim] -> z, out2 = log q(x); direction 1 (sampling):
+ * z -> x, out2 = dx/dz = 1/q(x). Host arrays. */
+int kb_flow_map(kb_flow *flow, int direction, int64_t count, const double *in, double *out, double *out2);
+/* Sampling direction on Sobol points k_first.. of rng (host outputs). */
+int kb_flow_sample(kb_flow *flow, const kb_sobol *rng, uint32_t k_first, int64_t count, double *x, double *jac);
+/* Loss sum_p w_p (-log q(x_p)) / count and its gradient (KB_FLOW_PARAMS floats, layout of
+ * kb_flow_get_params) on the GPU's own forward and backward kernels. */
+int kb_flow_gradient(kb_flow *flow, int64_t count, const double *x, const double *w, float *grad, double *loss);
+typedef struct {
+  int epochs;       /* passes over the samples */
+  int batch;        /* points per step (multiple of 128 recommended) */
+  float lr;         /* Adam step size, cosine-decayed to lr_final */
+  float lr_final;
+  float beta1, beta2, eps;
+  uint64_t seed;    /* shuffling of the samples per epoch */
+} kb_flow_train_cfg;
+/* Adam on the weighted negative log-likelihood of samples x [count][dim] (in [0,1]) with
+ * weights w >= 0 (normalised to mean 1 internally). loss_hist (optional): the loss of
+ * every step, *n_steps of them. */
+int kb_flow_train(kb_flow *flow, int64_t count, const double *x, const double *w, const kb_flow_train_cfg *cfg,
+                  double *loss_hist, int *n_steps);
+/* Generates n_samples points with the plain method (Sobol points k_first.. of rng,
+ * weights |f(chain(li)) J_chain|) and trains the flow on them. */
+int kb_flow_fit(kb_flow *flow, const kb_model *m, const kb_integrand *f, const kb_warper *chain, int chain_len,
+                const kb_sobol *rng, uint32_t k_first, int64_t n_samples, const kb_flow_train_cfg *cfg,
+                double *final_loss);
 
 /* ----------------------------------------------------------------- peaks --- */
 /* Measures the FP64 FMA rate of this device (FLOP/s, 2 per FMA) with a dependent-chain

@@ -34,7 +34,11 @@ EXPORTS = [
     "kb_g0_eval", "kb_integrand_eval", "kb_integrand_eval_no_det", "kb_evaluate_warped", "kb_integrate",
     "kb_fp64_peak", "kb_integrate_noalloc", "kb_plan_create", "kb_plan_destroy", "kb_plan_launch",
     "kb_plan_result", "kb_plan_set_k_first", "kb_context_set_launch", "kb_context_get_launch",
+    "kb_flow_create", "kb_flow_destroy", "kb_flow_dim", "kb_flow_get_params", "kb_flow_set_params", "kb_flow_map",
+    "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit",
 ]
+FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
+FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
 NOALLOC_MAX_ITEMS, NOALLOC_MAX_CHUNKS = 64, 65536
 
 
@@ -64,7 +68,13 @@ class Accum(C.Structure):
 
 class Work(C.Structure):
     _fields_ = [("m", C.c_void_p), ("rng", C.c_void_p), ("chain", C.POINTER(Warper)), ("chain_len", C.c_int),
-                ("f", Integrand), ("order", C.c_int), ("k_first", C.c_uint32), ("n_points", C.c_int64)]
+                ("f", Integrand), ("order", C.c_int), ("k_first", C.c_uint32), ("n_points", C.c_int64),
+                ("flow", C.c_void_p)]
+
+
+class FlowTrainCfg(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("lr_final", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_uint64)]
 
 
 _D = C.POINTER(C.c_double)
@@ -119,6 +129,18 @@ def load():
     L.kb_plan_set_k_first.argtypes = [_VP, _VP, C.c_int, C.c_uint32]
     L.kb_context_set_launch.argtypes = [_VP, C.c_int, C.c_int, C.c_int]
     L.kb_context_get_launch.argtypes = [_VP, C.c_int, _I, _I]
+    _F = C.POINTER(C.c_float)
+    L.kb_flow_create.argtypes = [_VP, C.c_int, C.c_uint64, C.POINTER(_VP)]
+    L.kb_flow_destroy.argtypes = [_VP]
+    L.kb_flow_dim.argtypes = [_VP]
+    L.kb_flow_get_params.argtypes = [_VP, _F]
+    L.kb_flow_set_params.argtypes = [_VP, _F]
+    L.kb_flow_map.argtypes = [_VP, C.c_int, C.c_int64, _D, _D, _D]
+    L.kb_flow_sample.argtypes = [_VP, _VP, C.c_uint32, C.c_int64, _D, _D]
+    L.kb_flow_gradient.argtypes = [_VP, C.c_int64, _D, _D, _F, _D]
+    L.kb_flow_train.argtypes = [_VP, C.c_int64, _D, _D, C.POINTER(FlowTrainCfg), _D, _I]
+    L.kb_flow_fit.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, _VP, C.c_uint32, C.c_int64,
+                              C.POINTER(FlowTrainCfg), _D]
     _lib = L
     return L
 
@@ -240,6 +262,10 @@ class Context:
     # --- model ---------------------------------------------------------------
     def model(self, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None, blocks=None):
         return Model(self, time_max, lesser, greater, alpha, lesser_down, greater_down, blocks)
+
+    # --- learned flow ------------------------------------------------------
+    def flow(self, dim, seed=0):
+        return Flow(self, dim, seed)
 
 
 class Sobol:
@@ -363,9 +389,11 @@ def _works(items):
     for i, it in enumerate(items):
         arr, L = chain_array(it["chain"])
         keep.append(arr)
+        flow = it.get("flow")
         works[i] = Work(it["model"].h.value, it["rng"].h.value, C.cast(arr, C.POINTER(Warper)), L,
                         Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
-                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]))
+                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]),
+                        flow.h.value if flow is not None else None)
     return works, keep
 
 
@@ -428,9 +456,107 @@ def integrate(ctx, items, algo=ALGO_AUTO):
     for i, it in enumerate(items):
         arr, L = chain_array(it["chain"])
         keep.append(arr)
+        flow = it.get("flow")
         works[i] = Work(it["model"].h.value, it["rng"].h.value, C.cast(arr, C.POINTER(Warper)), L,
                         Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
-                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]))
+                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]),
+                        flow.h.value if flow is not None else None)
     acc = (Accum * n)()
     check(ctx.L.kb_integrate(ctx.h, works, n, algo, acc))
     return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback) for a in acc]
+
+
+def train_cfg(epochs=20, batch=16384, lr=2e-3, lr_final=1e-4, beta1=0.9, beta2=0.999, eps=1e-8, seed=0):
+    return FlowTrainCfg(int(epochs), int(batch), float(lr), float(lr_final), float(beta1), float(beta2), float(eps),
+                        int(seed))
+
+
+class Flow:
+    """Learned coupling-flow warper of dimension `dim` (2..8) on the device: a first
+    stage before the warper chain, trained on |integrand| samples of the plain method
+    (kb_flow_* in include/keldy_b200.h)."""
+
+    def __init__(self, ctx, dim, seed=0):
+        self.ctx = ctx
+        self.dim = dim
+        h = _VP()
+        check(ctx.L.kb_flow_create(ctx.h, dim, int(seed), C.byref(h)))
+        self.h = h
+        ctx._deps.add(self)
+
+    def close(self):
+        if self.h:
+            self.ctx.L.kb_flow_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        """float32 [layer][matrix W1, W2, W3][out][in]."""
+        p = np.empty((FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH), dtype=np.float32)
+        check(self.ctx.L.kb_flow_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == FLOW_PARAMS
+        check(self.ctx.L.kb_flow_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
+
+    def map(self, x, direction):
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        count = x.shape[0]
+        assert x.shape[1] == self.dim
+        out = np.empty_like(x)
+        out2 = np.empty(count)
+        check(self.ctx.L.kb_flow_map(self.h, int(direction), count, _dp(x), _dp(out), _dp(out2)))
+        return out, out2
+
+    def density(self, x):
+        """(z, log q(x)): normalising direction."""
+        return self.map(x, 0)
+
+    def sample(self, z):
+        """(x, dx/dz): sampling direction."""
+        return self.map(z, 1)
+
+    def sample_sobol(self, rng, k_first, count):
+        x = np.empty((count, self.dim))
+        jac = np.empty(count)
+        check(self.ctx.L.kb_flow_sample(self.h, rng.h, k_first, count, _dp(x), _dp(jac)))
+        return x, jac
+
+    def gradient(self, x, w):
+        """(loss, grad [layer][matrix][out][in]) of sum w (-log q(x)) / len(x)."""
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        g = np.empty((FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH), dtype=np.float32)
+        loss = C.c_double()
+        check(self.ctx.L.kb_flow_gradient(self.h, x.shape[0], _dp(x), _dp(w), g.ctypes.data_as(C.POINTER(C.c_float)),
+                                          C.byref(loss)))
+        return loss.value, g
+
+    def train(self, x, w, **cfg):
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        c = train_cfg(**cfg)
+        b = min(c.batch, x.shape[0])
+        steps = max(1, x.shape[0] // b) * c.epochs
+        hist = np.empty(steps)
+        ns = C.c_int()
+        check(self.ctx.L.kb_flow_train(self.h, x.shape[0], _dp(x), _dp(w), C.byref(c), _dp(hist), C.byref(ns)))
+        return hist[:ns.value]
+
+    def fit(self, model, A, B, chain, rng, n_samples, k_first=1, cutoff=0.0, **cfg):
+        """Samples the plain method (Sobol points k_first.. of rng through chain, weights
+        |f J|) and trains on them; returns the mean loss of the last epoch."""
+        arr, L = chain_array(chain)
+        f = Integrand(gf_index(A), gf_index(B), float(cutoff))
+        c = train_cfg(**cfg)
+        loss = C.c_double()
+        check(self.ctx.L.kb_flow_fit(self.h, model.h, C.byref(f), arr, L, rng.h, k_first, n_samples, C.byref(c),
+                                     C.byref(loss)))
+        return loss.value

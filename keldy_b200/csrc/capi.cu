@@ -12,8 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "kb_launch.h"
-#include "kb_types.h"
+#include "kb_host.h"
 
 namespace kb {
 void sobol_setup(int dim, int m, bool do_shift, bool do_scramble, int seed_shift, uint32_t *Csr, uint32_t *shfr);
@@ -21,85 +20,15 @@ void sobol_setup(int dim, int m, bool do_shift, bool do_scramble, int seed_shift
 
 using namespace kb;
 
-// ------------------------------------------------------------------ errors
+namespace kb {
 namespace {
 thread_local std::string g_last_error;
-
+}
 int fail(int code, const std::string &msg) {
   g_last_error = msg;
   return code;
 }
-
-#define KB_CUDA(call)                                                                                        \
-  do {                                                                                                       \
-    cudaError_t e_ = (call);                                                                                 \
-    if (e_ != cudaSuccess) return fail(KB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));       \
-  } while (0)
-
-#define KB_CHECK(cond, msg)                                                                                  \
-  do {                                                                                                       \
-    if (!(cond)) return fail(KB_E_INVALID, msg);                                                            \
-  } while (0)
-
-// Stream-ordered device buffer released at scope exit (on the same stream).
-struct DevBuf {
-  void *p = nullptr;
-  cudaStream_t st = nullptr;
-  DevBuf() = default;
-  DevBuf(const DevBuf &) = delete;
-  DevBuf &operator=(const DevBuf &) = delete;
-  cudaError_t alloc(size_t bytes, cudaStream_t s) {
-    st = s;
-    return cudaMallocAsync(&p, bytes ? bytes : 16, s);
-  }
-  ~DevBuf() {
-    if (p) cudaFreeAsync(p, st);
-  }
-  template <typename T> T *as() const { return static_cast<T *>(p); }
-};
-
-uint64_t fnv1a(const void *data, size_t n) {
-  const unsigned char *c = static_cast<const unsigned char *>(data);
-  uint64_t h = 1469598103934665603ULL;
-  for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ULL;
-  return h;
-}
-} // namespace
-
-struct kb_context {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  int sm_count = 0;
-  int tree_grid = 0;
-  int *d_err = nullptr; // error flags written by kernels
-  int chunk_points[MAX_ORDER + 1]; // scheduling chunk of each order (autotuned; default 128)
-  int ctas_per_sm = 2;             // resident tree CTAs per SM
-  bool timing = false;
-  cudaEvent_t ev[4] = {};
-  double last_ms[3] = {0, 0, 0};
-  int last_launches = 0;
-  std::mutex mu;
-};
-
-// Models and generators belong to a context and must be destroyed before it; their
-// destroy functions touch only the device they live on.
-struct kb_model {
-  kb_context *ctx = nullptr;
-  int device = 0;
-  int npts = 0;
-  double tmax = 0, alpha = 0;
-  double2 *tab[2][2][2] = {};
-  uint64_t hash[2][2][2] = {}; // 0 = unknown (device upload)
-  double tabmax = 0;
-};
-
-struct kb_sobol {
-  kb_context *ctx = nullptr;
-  int device = 0;
-  int dim = 0, m = 0;
-  uint32_t *d_Csr = nullptr;
-  uint32_t *d_shfr = nullptr;
-};
+} // namespace kb
 
 extern "C" {
 
@@ -121,6 +50,7 @@ int kb_context_create(int device, kb_context **out) {
   if (prop.major < 10)
     return fail(KB_E_NODEVICE, std::string("keldy_b200 is built for sm_100a; device is ") + prop.name);
   KB_CUDA(configure_kernels());
+  KB_CUDA(flow_configure());
   auto *ctx = new kb_context;
   ctx->device = device;
   ctx->sm_count = prop.multiProcessorCount;
@@ -232,7 +162,9 @@ int kb_sobol_destroy(kb_sobol *s) {
   return KB_OK;
 }
 
-static SobolDev sobol_dev(const kb_sobol *s) {
+} // extern "C"
+
+SobolDev kb::sobol_dev(const kb_sobol *s) {
   SobolDev d;
   d.Csr = s->d_Csr;
   d.shfr = s->d_shfr;
@@ -241,7 +173,7 @@ static SobolDev sobol_dev(const kb_sobol *s) {
   return d;
 }
 
-static int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count) {
+int kb::check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count) {
   if (k_first < 1) return fail(KB_E_INVALID, "Sobol point index must be >= 1 (first draw of sobol(dim, seed) is seed+1)");
   // the last point keldy's generator hands out is k = 2^m (past_end() is checked before next())
   uint64_t last = (uint64_t)k_first + (uint64_t)(count > 0 ? count - 1 : 0);
@@ -249,6 +181,8 @@ static int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count)
     return fail(KB_E_EXHAUSTED, "More sample points requested then generator can hold.");
   return KB_OK;
 }
+
+extern "C" {
 
 int kb_sobol_points_dev(kb_context *ctx, const kb_sobol *s, uint32_t k_first, int64_t count, double *out_dev) {
   KB_CHECK(ctx && s, "kb_sobol_points: null argument");
@@ -671,47 +605,15 @@ int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integr
 }
 
 // ------------------------------------------------------------- integrator
-int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc) {
-  KB_CHECK(ctx && (n_work == 0 || (work && acc)), "kb_integrate: null argument");
-  KB_CHECK(algo == KB_ALGO_AUTO || algo == KB_ALGO_TREE || algo == KB_ALGO_DIRECT, "unknown algorithm");
-  if (n_work == 0) return KB_OK;
-  std::vector<ItemDev> items((size_t)n_work);
-  std::vector<int> use_tree((size_t)n_work);
-  for (int i = 0; i < n_work; ++i) {
-    const kb_work &w = work[i];
-    int st = check_integrand(w.m, &w.f, w.order);
-    if (st) return st;
-    KB_CHECK(w.rng, "work item without a Sobol generator");
-    KB_CHECK(w.n_points >= 0, "n_points must be >= 0");
-    KB_CHECK(w.order >= 1, "integrator dimension must be > 0 (Dimension of the integration space must be > 0.)");
-    if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
-    st = check_sobol_range(w.rng, w.k_first, w.n_points);
-    if (st) return st;
-    ItemDev &it = items[(size_t)i];
-    it = make_item(w.m, &w.f, w.order);
-    st = make_chain(w.chain, w.chain_len, it.chain);
-    if (st) return st;
-    it.chain_len = w.chain_len;
-    it.chain_start = w.chain_len;
-    it.rng = sobol_dev(w.rng);
-    it.k_first = w.k_first;
-    it.n_points = w.n_points;
-    it.chunk_points = ctx->chunk_points[w.order];
-    if (algo == KB_ALGO_TREE && !it.spin_symmetric)
-      return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
-    use_tree[(size_t)i] = (algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric);
-  }
-  std::lock_guard<std::mutex> lk(ctx->mu);
-  KB_CUDA(cudaSetDevice(ctx->device));
+} // extern "C"
+
+namespace {
+// One batched pass over `items`: two groups (tree / pivoted LU), each one persistent
+// launch over its items, heaviest orders first. Sums are added to acc[acc_index[i]].
+int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std::vector<int> &use_tree,
+                  const std::vector<int> &acc_index, kb_accum *acc) {
   cudaStream_t st = ctx->stream;
-  ctx->last_ms[0] = ctx->last_ms[1] = ctx->last_ms[2] = 0.0;
-  ctx->last_launches = 0;
-  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
-  DevBuf dacc;
-  KB_CUDA(dacc.alloc((size_t)n_work * sizeof(kb_accum), st));
-  KB_CUDA(cudaMemsetAsync(dacc.p, 0, (size_t)n_work * sizeof(kb_accum), st));
-  // Two groups (tree / pivoted LU), each one persistent launch over its items, heaviest
-  // orders first.
+  const int n_work = (int)items.size();
   for (int group = 0; group < 2; ++group) {
     std::vector<int> ids;
     for (int i = 0; i < n_work; ++i)
@@ -780,7 +682,7 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
       ctx->last_ms[2] += c;
     }
     for (size_t j = 0; j < ids.size(); ++j) {
-      kb_accum &a = acc[ids[j]];
+      kb_accum &a = acc[acc_index[(size_t)ids[j]]];
       a.sum_re += part[j].sum_re;
       a.sum_im += part[j].sum_im;
       a.n_points += part[j].n_points;
@@ -788,13 +690,132 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
       a.n_fallback += part[j].n_fallback;
     }
   }
+  return KB_OK;
+}
+
+constexpr int64_t FLOW_PIECE = 1 << 22;            // points per flow-mapped piece
+constexpr size_t FLOW_ROUND_BYTES = (size_t)1 << 30; // flow-mapped points held at once
+
+// Checks of a work item shared by kb_integrate and kb_plan_create; fills `it`.
+int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tree) {
+  int st = check_integrand(w.m, &w.f, w.order);
+  if (st) return st;
+  KB_CHECK(w.rng, "work item without a Sobol generator");
+  KB_CHECK(w.n_points >= 0, "n_points must be >= 0");
+  KB_CHECK(w.order >= 1, "integrator dimension must be > 0 (Dimension of the integration space must be > 0.)");
+  if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
+  st = check_sobol_range(w.rng, w.k_first, w.n_points);
+  if (st) return st;
+  if (w.flow) {
+    KB_CHECK(w.flow->dim == w.order, "the flow's dimension differs from the work item's order");
+    KB_CHECK(w.flow->device == ctx->device, "the flow lives on another device");
+  }
+  it = make_item(w.m, &w.f, w.order);
+  st = make_chain(w.chain, w.chain_len, it.chain);
+  if (st) return st;
+  it.chain_len = w.chain_len;
+  it.chain_start = w.chain_len;
+  it.rng = sobol_dev(w.rng);
+  it.k_first = w.k_first;
+  it.n_points = w.n_points;
+  it.chunk_points = ctx->chunk_points[w.order];
+  if (algo == KB_ALGO_TREE && !it.spin_symmetric)
+    return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
+  tree = ((algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric)) ? 1 : 0;
+  return KB_OK;
+}
+} // namespace
+
+extern "C" {
+
+int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc) {
+  KB_CHECK(ctx && (n_work == 0 || (work && acc)), "kb_integrate: null argument");
+  KB_CHECK(algo == KB_ALGO_AUTO || algo == KB_ALGO_TREE || algo == KB_ALGO_DIRECT, "unknown algorithm");
+  if (n_work == 0) return KB_OK;
+  std::vector<ItemDev> items((size_t)n_work);
+  std::vector<int> use_tree((size_t)n_work), index((size_t)n_work);
+  bool any_flow = false;
+  for (int i = 0; i < n_work; ++i) {
+    int st = work_item(ctx, work[i], algo, items[(size_t)i], use_tree[(size_t)i]);
+    if (st) return st;
+    index[(size_t)i] = i;
+    any_flow = any_flow || (work[i].flow && work[i].n_points > 0);
+  }
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  ctx->last_ms[0] = ctx->last_ms[1] = ctx->last_ms[2] = 0.0;
+  ctx->last_launches = 0;
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  if (!any_flow) {
+    int rc = run_integrate(ctx, items, use_tree, index, acc);
+    if (rc) return rc;
+  } else {
+    // Items with a flow run in pieces whose flow-mapped points (li, Jacobian) are made by
+    // the flow's sampling kernel right before the pass that integrates them.
+    struct Piece {
+      ItemDev it;
+      int tree, acc;
+      const kb_flow *flow;
+      size_t bytes;
+    };
+    std::vector<Piece> plain, flowed;
+    for (int i = 0; i < n_work; ++i) {
+      const ItemDev &it = items[(size_t)i];
+      if (!work[i].flow) {
+        plain.push_back({it, use_tree[(size_t)i], i, nullptr, 0});
+        continue;
+      }
+      for (int64_t off = 0; off < it.n_points; off += FLOW_PIECE) {
+        Piece p{it, use_tree[(size_t)i], i, work[i].flow, 0};
+        p.it.k_first = it.k_first + (uint32_t)off;
+        p.it.n_points = std::min<int64_t>(FLOW_PIECE, it.n_points - off);
+        p.bytes = (size_t)p.it.n_points * (size_t)(it.order + 1) * sizeof(double);
+        flowed.push_back(p);
+      }
+    }
+    size_t next = 0;
+    bool first_round = true;
+    while (first_round || next < flowed.size()) {
+      std::vector<Piece> round = first_round ? plain : std::vector<Piece>();
+      size_t bytes = 0;
+      const size_t begin = next;
+      while (next < flowed.size() && (next == begin || bytes + flowed[next].bytes <= FLOW_ROUND_BYTES))
+        bytes += flowed[next++].bytes;
+      DevBuf fbuf;
+      if (bytes) KB_CUDA(fbuf.alloc(bytes, st));
+      size_t off = 0;
+      for (size_t j = begin; j < next; ++j) {
+        Piece p = flowed[j];
+        double *x = reinterpret_cast<double *>(fbuf.as<unsigned char>() + off);
+        double *jac = x + (size_t)p.it.n_points * p.it.order;
+        KB_CUDA(launch_flow_map(p.flow->layout, 1, p.it.n_points, nullptr, p.it.rng, p.it.k_first, nullptr, 1, x, jac,
+                                ctx->d_err, ctx->sm_count, st));
+        ctx->last_launches++;
+        p.it.flow_x = x;
+        p.it.flow_jac = jac;
+        off += p.bytes;
+        round.push_back(p);
+      }
+      std::vector<ItemDev> ritems;
+      std::vector<int> rtree, racc;
+      for (const Piece &p : round) {
+        ritems.push_back(p.it);
+        rtree.push_back(p.tree);
+        racc.push_back(p.acc);
+      }
+      int rc = run_integrate(ctx, ritems, rtree, racc, acc);
+      if (rc) return rc;
+      first_round = false;
+    }
+  }
   int err = 0;
   KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   KB_CUDA(cudaStreamSynchronize(st));
   if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  if (err & 2) return fail(KB_E_CUDA, "a flow kernel's wait on the tensor cores ran out");
   return KB_OK;
 }
-
 
 // ------------------------------------------------------------------ plans
 struct kb_plan {
@@ -814,6 +835,16 @@ struct kb_plan {
   int n_work = 0;
   std::vector<int> where_group, where_pos; // work index -> (group, sorted position)
   std::vector<const kb_sobol *> rng;
+  // items with a learned flow: their points are mapped into `buf` at every launch
+  struct Fill {
+    FlowDev layout;
+    SobolDev rng;
+    int gi, pos;
+    int64_t n;
+    int order;
+    double *buf = nullptr; // [n][order] points, then [n] Jacobians
+  };
+  std::vector<Fill> fills;
   cudaGraphExec_t exec = nullptr;
   int device = 0;
 };
@@ -829,6 +860,7 @@ static void plan_free(kb_plan *p) {
     cudaFree(g.d_pts);
     cudaFree(g.d_acc);
   }
+  for (auto &f : p->fills) cudaFree(f.buf);
   delete p;
 }
 
@@ -843,28 +875,10 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
   std::vector<ItemDev> items((size_t)n_work);
   std::vector<int> grp((size_t)n_work);
   for (int i = 0; i < n_work; ++i) {
-    const kb_work &w = work[i];
-    int st = check_integrand(w.m, &w.f, w.order);
+    int tree = 0;
+    int st = work_item(ctx, work[i], algo, items[(size_t)i], tree);
     if (st) return st;
-    KB_CHECK(w.rng, "work item without a Sobol generator");
-    KB_CHECK(w.n_points >= 0, "n_points must be >= 0");
-    KB_CHECK(w.order >= 1, "integrator dimension must be > 0 (Dimension of the integration space must be > 0.)");
-    if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
-    st = check_sobol_range(w.rng, w.k_first, w.n_points);
-    if (st) return st;
-    ItemDev &it = items[(size_t)i];
-    it = make_item(w.m, &w.f, w.order);
-    st = make_chain(w.chain, w.chain_len, it.chain);
-    if (st) return st;
-    it.chain_len = w.chain_len;
-    it.chain_start = w.chain_len;
-    it.rng = sobol_dev(w.rng);
-    it.k_first = w.k_first;
-    it.n_points = w.n_points;
-    it.chunk_points = ctx->chunk_points[w.order];
-    if (algo == KB_ALGO_TREE && !it.spin_symmetric)
-      return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
-    grp[(size_t)i] = ((algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric)) ? 0 : 1;
+    grp[(size_t)i] = tree ? 0 : 1;
   }
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
@@ -874,6 +888,26 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
   p->where_group.assign((size_t)n_work, -1);
   p->where_pos.assign((size_t)n_work, -1);
   for (int i = 0; i < n_work; ++i) p->rng.push_back(work[i].rng);
+  for (int i = 0; i < n_work; ++i) {
+    const kb_work &w = work[i];
+    if (!w.flow || w.n_points == 0) continue;
+    kb_plan::Fill f;
+    f.layout = w.flow->layout;
+    f.rng = items[(size_t)i].rng;
+    f.n = w.n_points;
+    f.order = w.order;
+    f.gi = grp[(size_t)i];
+    f.pos = -1;
+    cudaError_t e = cudaMalloc(&f.buf, (size_t)f.n * (size_t)(f.order + 1) * sizeof(double));
+    if (e != cudaSuccess) {
+      plan_free(p);
+      return fail(KB_E_NOMEM, std::string("kb_plan_create: ") + cudaGetErrorString(e));
+    }
+    items[(size_t)i].flow_x = f.buf;
+    items[(size_t)i].flow_jac = f.buf + (size_t)f.n * f.order;
+    f.pos = i; // work index until the groups are sorted
+    p->fills.push_back(f);
+  }
   for (int gi = 0; gi < 2; ++gi) {
     auto &g = p->g[gi];
     for (int i = 0; i < n_work; ++i)
@@ -910,12 +944,18 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
       return fail(KB_E_NOMEM, std::string("kb_plan_create: ") + cudaGetErrorString(e));
     }
   }
+  for (auto &f : p->fills) f.pos = p->where_pos[(size_t)f.pos];
   *out = p;
   return KB_OK;
 }
 
 // The launch sequence of one run (captured into the plan's graph).
 static int plan_enqueue(kb_context *ctx, kb_plan *p, cudaStream_t st) {
+  for (const auto &f : p->fills) {
+    const uint32_t *kf = &p->g[f.gi].d_items[f.pos].k_first;
+    KB_CUDA(launch_flow_map(f.layout, 1, f.n, nullptr, f.rng, 0, kf, 1, f.buf, f.buf + (size_t)f.n * f.order, ctx->d_err,
+                            ctx->sm_count, st));
+  }
   for (int gi = 0; gi < 2; ++gi) {
     auto &g = p->g[gi];
     if (!g.n_items) continue;
@@ -992,6 +1032,7 @@ int kb_plan_result(kb_context *ctx, kb_plan *plan, kb_accum *acc) {
     }
   }
   if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  if (err & 2) return fail(KB_E_CUDA, "a flow kernel's wait on the tensor cores ran out");
   for (int gi = 0; gi < 2; ++gi)
     for (int j = 0; j < plan->g[gi].n_items; ++j) {
       kb_accum &a = acc[plan->g[gi].ids[(size_t)j]];
@@ -1133,6 +1174,7 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     if (w.rng->dim < w.order) return fail(KB_E_INVALID, "Sobol generator has fewer dimensions than the order");
     st = check_sobol_range(w.rng, w.k_first, w.n_points);
     if (st) return st;
+    KB_CHECK(!w.flow, "kb_integrate_noalloc does not take work items with a learned flow");
     ItemDev &it = items[i];
     it = make_item(w.m, &w.f, w.order);
     st = make_chain(w.chain, w.chain_len, it.chain);

@@ -1,0 +1,109 @@
+// Host-side objects of the C ABI shared by capi.cu and flow_capi.cu: error
+// reporting, stream-ordered device buffers, and the opaque handle types of
+// include/keldy_b200.h.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+
+#include "kb_flow.h"
+#include "kb_launch.h"
+#include "kb_types.h"
+
+namespace kb {
+// Records msg as the calling thread's last error (kb_last_error) and returns code.
+int fail(int code, const std::string &msg);
+
+// Stream-ordered device buffer released at scope exit (on the same stream).
+struct DevBuf {
+  void *p = nullptr;
+  cudaStream_t st = nullptr;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  cudaError_t alloc(size_t bytes, cudaStream_t s) {
+    st = s;
+    return cudaMallocAsync(&p, bytes ? bytes : 16, s);
+  }
+  ~DevBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+inline uint64_t fnv1a(const void *data, size_t n) {
+  const unsigned char *c = static_cast<const unsigned char *>(data);
+  uint64_t h = 1469598103934665603ULL;
+  for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ULL;
+  return h;
+}
+
+} // namespace kb
+
+#define KB_CUDA(call)                                                                                        \
+  do {                                                                                                       \
+    cudaError_t e_ = (call);                                                                                 \
+    if (e_ != cudaSuccess) return kb::fail(KB_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+#define KB_CHECK(cond, msg)                                                                                  \
+  do {                                                                                                       \
+    if (!(cond)) return kb::fail(KB_E_INVALID, msg);                                                        \
+  } while (0)
+
+struct kb_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sm_count = 0;
+  int tree_grid = 0;
+  int *d_err = nullptr; // error flags written by kernels
+  int chunk_points[kb::MAX_ORDER + 1]; // scheduling chunk of each order (autotuned; default 128)
+  int ctas_per_sm = 2;                 // resident tree CTAs per SM
+  bool timing = false;
+  cudaEvent_t ev[4] = {};
+  double last_ms[3] = {0, 0, 0};
+  int last_launches = 0;
+  std::mutex mu;
+};
+
+// Models, generators and flows belong to a context and must be destroyed before it;
+// their destroy functions touch only the device they live on.
+struct kb_model {
+  kb_context *ctx = nullptr;
+  int device = 0;
+  int npts = 0;
+  double tmax = 0, alpha = 0;
+  double2 *tab[2][2][2] = {};
+  uint64_t hash[2][2][2] = {}; // 0 = unknown (device upload)
+  double tabmax = 0;
+};
+
+struct kb_sobol {
+  kb_context *ctx = nullptr;
+  int device = 0;
+  int dim = 0, m = 0;
+  uint32_t *d_Csr = nullptr;
+  uint32_t *d_shfr = nullptr;
+};
+
+namespace kb {
+SobolDev sobol_dev(const kb_sobol *s);
+// KB_E_EXHAUSTED when points k_first .. k_first+count-1 pass the generator's end
+int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count);
+} // namespace kb
+
+// Learned coupling-flow warper: fp32 master weights and Adam moments in the internal
+// order [matrix][in][out], bf16 images for the tensor cores.
+struct kb_flow {
+  kb_context *ctx = nullptr;
+  int device = 0;
+  int dim = 0;
+  kb::FlowDev layout{};    // img set to `img`
+  float *master = nullptr; // [FLOW_NPARAM]
+  float *adam_m = nullptr;
+  float *adam_v = nullptr;
+  uint16_t *img = nullptr; // [FLOW_NPARAM] bf16
+  int64_t adam_step = 0;
+};

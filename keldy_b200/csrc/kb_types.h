@@ -52,6 +52,10 @@ struct ItemDev {
   uint32_t k_first;
   int chunk_points; // points per scheduling chunk of this item (<= 128)
   int64_t n_points;
+  // learned flow (integrate mode): point gp of the item is flow_x[gp*order..] with flow
+  // Jacobian flow_jac[gp] instead of its Sobol point; null = plain Sobol points
+  const double *flow_x;
+  const double *flow_jac;
 };
 
 // One chunk of points of one item, processed by one CTA iteration.

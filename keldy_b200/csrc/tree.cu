@@ -68,9 +68,14 @@ __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, l
   double *x = u + p;
   double jac = 1.0;
   if (L.mode == IN_SOBOL) {
-    uint32_t k = it.k_first + (uint32_t)gp;
-    for (int j = 0; j < N; ++j) x[j * np] = sobol_coord(it.rng, k, j);
-    jac = chain_reverse(it.chain, it.chain_len, 0, N, x, np);
+    if (it.flow_x) { // Sobol point already mapped by the learned flow
+      for (int j = 0; j < N; ++j) x[j * np] = it.flow_x[gp * N + j];
+      jac = it.flow_jac[gp];
+    } else {
+      uint32_t k = it.k_first + (uint32_t)gp;
+      for (int j = 0; j < N; ++j) x[j * np] = sobol_coord(it.rng, k, j);
+    }
+    jac *= chain_reverse(it.chain, it.chain_len, 0, N, x, np);
   } else {
     long long src = L.index ? (long long)L.index[gp] : gp;
     for (int j = 0; j < N; ++j) x[j * np] = L.in[src * N + j];
@@ -92,9 +97,14 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
   double x[MAX_ORDER];
   double jac = 1.0;
   if (L.mode == IN_SOBOL) {
-    const uint32_t k = it.k_first + (uint32_t)gp;
-    for (int j = 0; j < N; ++j) x[j] = sobol_coord(it.rng, k, j);
-    jac = chain_reverse(it.chain, it.chain_len, 0, N, x, 1);
+    if (it.flow_x) { // Sobol point already mapped by the learned flow
+      for (int j = 0; j < N; ++j) x[j] = it.flow_x[gp * N + j];
+      jac = it.flow_jac[gp];
+    } else {
+      const uint32_t k = it.k_first + (uint32_t)gp;
+      for (int j = 0; j < N; ++j) x[j] = sobol_coord(it.rng, k, j);
+    }
+    jac *= chain_reverse(it.chain, it.chain_len, 0, N, x, 1);
   } else {
     const long long src = L.index ? (long long)L.index[gp] : gp;
     for (int j = 0; j < N; ++j) x[j] = L.in[src * N + j];
