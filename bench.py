@@ -193,6 +193,94 @@ def workload_config(order, points):
             "l2": "flushed between timed steps (256 MiB write)"}
 
 
+def measure_biased_dot(ctx):
+    """Biased dot, orders 6..12 in one CUDA-graph plan: V = 1, eps_d = 0.5, beta = 100,
+    Gamma = 1, g0 on 100,001 points over [-50, 50] (built on the GPU), charge at t = 50,
+    chain [plasma_uv(50), exponential(50, 1)], 2^22 Sobol points per order."""
+    from keldy_b200 import capi
+    t0 = time.perf_counter()
+    model, = capi.flatband_models(ctx, [(1.0, 0.5, 1.0, 100.0)], 50.0, 100001)
+    ctx.synchronize()
+    build_s = time.perf_counter() - t0
+    chain = [(capi.WARPER_PLASMA_UV, 50.0, 0.0), (capi.WARPER_EXPONENTIAL, 50.0, 1.0)]
+    orders = list(range(6, 13))
+    items = [dict(model=model, rng=ctx.sobol(n), chain=chain, A=(50.0, 0, 0, 0, 0), B=(50.0, 0, 1, 0, 0), order=n,
+                  n_points=1 << 22) for n in orders]
+    plan = capi.Plan(ctx, items)
+    plan.run()
+    res = plan.run()
+    ms = ctx.last_timing()[0]
+    plan.close()
+    ref = sum(reference_flops(n) << 22 for n in orders)
+    return {"workload": "biased dot V=1 eps_d=0.5 beta=100, charge G^<(t=50), g0 100,001 points on [-50,50] "
+                        "(GPU-built, linear interpolation), chain [plasma_uv(50), exponential(50,1)], "
+                        "orders 6..12 x 2^22 Sobol points, one graph launch",
+            "ms": ms, "evals_per_s": len(orders) * (1 << 22) / (ms * 1e-3),
+            "reference_equivalent_tflops": ref / (ms * 1e-3) / 1e12, "g0_build_s": build_s,
+            "charge_by_order": {str(n): [r[0].real / r[1], r[0].imag / r[1]] for n, r in zip(orders, res)},
+            "fallback_points": sum(r[3] for r in res)}
+
+
+def measure_sweep(ctx):
+    """256 models (V in [0,2] x eps_d in [-1,1] x beta in {10,50,200}, Gamma = 1), each with
+    its own 20,001-point g0 table built on the GPU in one launch; model i integrates order
+    2 + i % 9 (uneven costs) with 2^18 Sobol points; all 256 items in one graph launch."""
+    import numpy as np
+    from keldy_b200 import capi
+    params = [(1.0, e, v, b) for b in (10.0, 50.0, 200.0) for v in np.linspace(0.0, 2.0, 8)
+              for e in np.linspace(-1.0, 1.0, 11)][:256]
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    models = capi.flatband_models(ctx, params, 20.0, 20001)
+    ctx.synchronize()
+    build_s = time.perf_counter() - t0
+    chain = [(capi.WARPER_PLASMA_UV, 20.0, 0.0), (capi.WARPER_EXPONENTIAL, 20.0, 1.0)]
+    rngs = {n: ctx.sobol(n) for n in range(2, 11)}
+    items = [dict(model=models[i], rng=rngs[2 + i % 9], chain=chain, A=(20.0, 0, 0, 0, 0), B=(20.0, 0, 1, 0, 0),
+                  order=2 + i % 9, n_points=1 << 18) for i in range(len(models))]
+    plan = capi.Plan(ctx, items)
+    plan.run()
+    plan.run()
+    ms = ctx.last_timing()[0]
+    plan.close()
+    ref = sum(reference_flops(it["order"]) << 18 for it in items)
+    for m in models:
+        m.close()
+    return {"workload": "256 flat-band models (V in [0,2] x eps_d in [-1,1] x beta in {10,50,200}), own "
+                        "20,001-point g0 table each (GPU-built in one launch), orders 2..10 by model, "
+                        "2^18 Sobol points per (model, order), one graph launch",
+            "ms": ms, "evals_per_s": len(items) * (1 << 18) / (ms * 1e-3),
+            "reference_equivalent_tflops": ref / (ms * 1e-3) / 1e12, "g0_build_ms": build_s * 1e3}
+
+
+def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8)):
+    """Learned flow vs the plain chain per order: training time, per-point variance gain,
+    RQMC standard errors at a fixed 2^24-evaluation budget (16 shifts x 2^20 points) and
+    wall time to a 1e-3 relative standard error (16 shifts, points doubled from 2^8)."""
+    from keldy_b200 import learned, rqmc
+    out = {}
+    for n in orders:
+        flow, fit_s, loss = learned.fit(ctx, model, A, B, chain, n, 1 << 18, seed=n)
+        budget = learned.compare(ctx, model, A, B, chain, n, flow, 1 << 20, 16)
+        tp = rqmc.time_to_relative_error(ctx, model, A, B, chain, n, 1e-3, 16, start_points=1 << 8)
+        tl = rqmc.time_to_relative_error(ctx, model, A, B, chain, n, 1e-3, 16, start_points=1 << 8, flow=flow)
+        out[str(n)] = {
+            "fit_s": fit_s, "fit_loss": loss,
+            "per_point_variance_gain": learned.variance_gain(ctx, model, A, B, chain, flow),
+            "budget_2e24": {"plain_stderr": budget["plain"]["stderr"], "learned_stderr": budget["learned"]["stderr"],
+                            "plain_rel": budget["plain"]["rel"], "learned_rel": budget["learned"]["rel"],
+                            "stderr_ratio_plain_over_learned": budget["stderr_ratio"],
+                            "diff_in_combined_sigma": budget["diff_sigma"],
+                            "plain_s": budget["plain"]["seconds"], "learned_s": budget["learned"]["seconds"]},
+            "time_to_1e-3": {"plain_s": tp["seconds"], "plain_points_per_shift": tp["points_per_replica"],
+                             "learned_s": tl["seconds"], "learned_points_per_shift": tl["points_per_replica"],
+                             "learned_incl_training_s": tl["seconds"] + fit_s,
+                             "speedup_plain_over_learned": tp["seconds"] / tl["seconds"]},
+        }
+        flow.close()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -334,6 +422,10 @@ def run_ours(args, rank, world, local_rank):
                              for k, v in tuned.items()},
             "clocks": clocks,
         }
+        if not args.no_extras:
+            line["biased_dot_orders_6_12"] = measure_biased_dot(ctx)
+            line["sweep_256_models"] = measure_sweep(ctx)
+            line["learned_vs_plain"] = measure_learned(ctx, model, A, B, chain)
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)
@@ -366,6 +458,8 @@ def main():
     ap.add_argument("--order", type=int, default=8)
     ap.add_argument("--points", type=int, default=1 << 20)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the biased-dot, 256-model sweep and learned-warper measurements")
     ap.add_argument("--ref-seconds", type=float, default=2.0, help="seconds of CPU work per reference-arm step")
     ap.add_argument("--single", action="store_true",
                     help="one integrate call of --points points at --order and exit (for profiler captures)")

@@ -109,6 +109,19 @@ int kb_model_set_table(kb_model *m, int spin, int o1, int o2, const double *less
 /* Same from device memory. */
 int kb_model_set_table_dev(kb_model *m, int spin, int o1, int o2, const double *lesser_dev,
                            const double *greater_dev);
+/* Copies a model's g0^< and g0^> table of (spin, o1, o2) to the host (interleaved complex,
+ * npts each): keldy's public g0_model::g0_lesser / g0_greater members (model.hpp:184-188).
+ * A spin never uploaded reads the other spin's table. */
+int kb_model_get_table(kb_model *m, int spin, int o1, int o2, double *lesser, double *greater);
+/* Builds the spin-up orbital (0,0) tables of n models on the GPU, the single-level dot
+ * coupled to two flat-band leads (keldy's make_g0_flat_band with the contour/fft
+ * methods' functions, impurity_oneband/model.hpp:100-130, model.cpp:107-111, evaluated
+ * in closed form through the exponential integral plus a quadrature of the
+ * finite-temperature correction; the same functions as the package's host builder
+ * g0_tables.flatband). params [n][4] = {Gamma, eps_d, V, beta} (beta = INFINITY: zero
+ * temperature; mu_left = -V/2, mu_right = +V/2). All models share one context and one
+ * time mesh (odd npts). */
+int kb_models_set_flatband(int n, kb_model *const *models, const double *params);
 
 /* A point of the Keldysh contour with spin and orbital: keldy's gf_index_t (model.hpp:55-78). */
 typedef struct {

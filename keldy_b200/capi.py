@@ -29,7 +29,7 @@ ALGO_AUTO, ALGO_TREE, ALGO_DIRECT = 0, 1, 2
 EXPORTS = [
     "kb_last_error", "kb_version", "kb_context_create", "kb_context_destroy", "kb_context_synchronize",
     "kb_context_stream", "kb_context_set_timing", "kb_context_last_timing", "kb_sobol_create", "kb_sobol_destroy", "kb_sobol_matrices", "kb_sobol_points",
-    "kb_sobol_points_dev",
+    "kb_sobol_points_dev", "kb_models_set_flatband", "kb_model_get_table",
     "kb_warp", "kb_model_create", "kb_model_destroy", "kb_model_set_table", "kb_model_set_table_dev",
     "kb_g0_eval", "kb_integrand_eval", "kb_integrand_eval_no_det", "kb_evaluate_warped", "kb_integrate",
     "kb_fp64_peak", "kb_integrate_noalloc", "kb_plan_create", "kb_plan_destroy", "kb_plan_launch",
@@ -112,6 +112,8 @@ def load():
     L.kb_model_destroy.argtypes = [_VP]
     L.kb_model_set_table.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D]
     L.kb_model_set_table_dev.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _VP, _VP]
+    L.kb_models_set_flatband.argtypes = [C.c_int, C.POINTER(_VP), _D]
+    L.kb_model_get_table.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D]
     L.kb_g0_eval.argtypes = [_VP, _VP, C.POINTER(GfIndex), C.POINTER(GfIndex), _I, C.c_int64, _D]
     L.kb_integrand_eval.argtypes = [_VP, _VP, C.POINTER(Integrand), C.c_int, C.c_int64, _D, C.c_int, C.c_int, _D,
                                     _I, _D]
@@ -299,16 +301,18 @@ class Sobol:
 class Model:
     """g0 tables (complex arrays on [-time_max, time_max]) uploaded to the device."""
 
-    def __init__(self, ctx, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None, blocks=None):
+    def __init__(self, ctx, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None, blocks=None,
+                 npts=None):
+        """lesser/greater None: no table uploaded (npts gives the mesh; see flatband_models)."""
         self.ctx = ctx
-        lesser = np.ascontiguousarray(lesser, dtype=np.complex128)
-        greater = np.ascontiguousarray(greater, dtype=np.complex128)
-        self.npts = len(lesser)
+        self.npts = int(npts) if lesser is None else len(lesser)
         self.time_max = time_max
         h = _VP()
         check(ctx.L.kb_model_create(ctx.h, self.npts, float(time_max), float(alpha), C.byref(h)))
         self.h = h
         ctx._deps.add(self)
+        if lesser is None:
+            return
         self.set_table(0, 0, 0, lesser, greater)
         if lesser_down is not None:
             self.set_table(1, 0, 0, lesser_down, greater_down)
@@ -320,6 +324,13 @@ class Model:
         gr = np.ascontiguousarray(greater, dtype=np.complex128).view(np.float64)
         assert le.size == 2 * self.npts and gr.size == 2 * self.npts
         check(self.ctx.L.kb_model_set_table(self.h, spin, o1, o2, _dp(le), _dp(gr)))
+
+    def table(self, spin=0, o1=0, o2=0):
+        """(lesser, greater) complex arrays of one block, read back from the device."""
+        le = np.empty(self.npts, dtype=np.complex128)
+        gr = np.empty(self.npts, dtype=np.complex128)
+        check(self.ctx.L.kb_model_get_table(self.h, spin, o1, o2, _dp(le.view(np.float64)), _dp(gr.view(np.float64))))
+        return le, gr
 
     def close(self):
         if self.h:
@@ -380,6 +391,16 @@ class Model:
                                             count, _dp(li), int(keep_u_hypercube), algo, _dp(out.view(np.float64)),
                                             _dp(jac), _ip(dom)))
         return out, jac, dom
+
+
+def flatband_models(ctx, params, time_max, npts, alpha=0.0):
+    """Models of the dot with flat-band leads, their g0 tables built on the GPU in one
+    launch (kb_models_set_flatband). params: rows (Gamma, eps_d, V, beta); npts odd."""
+    params = np.ascontiguousarray(np.atleast_2d(params), dtype=np.float64)
+    models = [Model(ctx, time_max, None, None, alpha, npts=npts) for _ in range(len(params))]
+    hs = (_VP * max(1, len(models)))(*[m.h for m in models])
+    check(ctx.L.kb_models_set_flatband(len(models), hs, _dp(params)))
+    return models
 
 
 def _works(items):

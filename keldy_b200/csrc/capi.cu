@@ -379,6 +379,105 @@ int kb_model_set_table_dev(kb_model *m, int spin, int o1, int o2, const double *
   return set_table(m, spin, o1, o2, lesser_dev, greater_dev, cudaMemcpyDeviceToDevice);
 }
 
+} // extern "C"
+
+namespace {
+// Gauss-Legendre rule of n nodes on [-1, 1]: Newton iteration on P_n from the
+// Chebyshev-like first guesses, P_n and P_n' by the three-term recurrence.
+void gauss_legendre(int n, double *x, double *w) {
+  const double pi = 3.14159265358979323846;
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double z = std::cos(pi * (i + 0.75) / (n + 0.5)), dp = 1.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        const double p2 = p1;
+        p1 = p0;
+        p0 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p2) / j;
+      }
+      dp = n * (z * p0 - p1) / (z * z - 1.0);
+      const double dz = p0 / dp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    x[i] = -z;
+    x[n - 1 - i] = z;
+    w[i] = w[n - 1 - i] = 2.0 / ((1.0 - z * z) * dp * dp);
+  }
+}
+} // namespace
+
+extern "C" {
+
+int kb_model_get_table(kb_model *m, int spin, int o1, int o2, double *lesser, double *greater) {
+  KB_CHECK(m && lesser && greater, "kb_model_get_table: null argument");
+  KB_CHECK(spin >= 0 && spin < 2 && o1 >= 0 && o1 < 2 && o2 >= 0 && o2 < 2, "spin/orbital index out of range");
+  const double2 *src = m->tab[spin][o1][o2] ? m->tab[spin][o1][o2] : m->tab[1 - spin][o1][o2];
+  if (!src) return fail(KB_E_INVALID, "kb_model_get_table: no table for this block");
+  kb_context *ctx = m->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)m->npts;
+  KB_CUDA(cudaMemcpy2DAsync(lesser, sizeof(double2), src, 2 * sizeof(double2), sizeof(double2), n,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  KB_CUDA(cudaMemcpy2DAsync(greater, sizeof(double2), src + 1, 2 * sizeof(double2), sizeof(double2), n,
+                            cudaMemcpyDeviceToHost, ctx->stream));
+  KB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return KB_OK;
+}
+
+int kb_models_set_flatband(int n, kb_model *const *models, const double *params) {
+  KB_CHECK(n >= 0 && (n == 0 || (models && params)), "kb_models_set_flatband: null argument");
+  if (n == 0) return KB_OK;
+  kb_context *ctx = models[0] ? models[0]->ctx : nullptr;
+  KB_CHECK(ctx, "kb_models_set_flatband: null model");
+  const int npts = models[0]->npts;
+  const double tmax = models[0]->tmax;
+  KB_CHECK(npts % 2 == 1 && npts >= 3, "the flat-band builder needs an odd number of mesh points (t = 0 on the mesh)");
+  for (int i = 0; i < n; ++i) {
+    KB_CHECK(models[i] && models[i]->ctx == ctx, "all models of one call must belong to one context");
+    KB_CHECK(models[i]->npts == npts && models[i]->tmax == tmax, "all models of one call must share their time mesh");
+    const double *p = params + 4 * i;
+    KB_CHECK(p[0] > 0.0 && std::isfinite(p[0]), "Gamma must be > 0");
+    KB_CHECK(std::isfinite(p[1]) && std::isfinite(p[2]), "eps_d and V must be finite");
+    KB_CHECK(p[3] > 0.0, "beta must be > 0 (INFINITY: zero temperature)");
+  }
+  constexpr int NODES = 240;
+  std::vector<double> gx(NODES), gw(NODES);
+  gauss_legendre(NODES, gx.data(), gw.data());
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  std::vector<double2 *> tabs((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    kb_model *m = models[i];
+    if (!m->tab[0][0][0]) KB_CUDA(cudaMalloc(&m->tab[0][0][0], (size_t)npts * 2 * sizeof(double2)));
+    tabs[(size_t)i] = m->tab[0][0][0];
+  }
+  DevBuf dpar, dtab, dx, dw, dmax;
+  KB_CUDA(dpar.alloc((size_t)n * 4 * sizeof(double), st));
+  KB_CUDA(dtab.alloc((size_t)n * sizeof(double2 *), st));
+  KB_CUDA(dx.alloc(NODES * sizeof(double), st));
+  KB_CUDA(dw.alloc(NODES * sizeof(double), st));
+  KB_CUDA(dmax.alloc((size_t)n * sizeof(double), st));
+  KB_CUDA(cudaMemcpyAsync(dpar.p, params, (size_t)n * 4 * sizeof(double), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dtab.p, tabs.data(), (size_t)n * sizeof(double2 *), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dx.p, gx.data(), NODES * sizeof(double), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dw.p, gw.data(), NODES * sizeof(double), cudaMemcpyHostToDevice, st));
+  KB_CUDA(launch_flatband_tables(n, dpar.as<double>(), dtab.as<double2 *>(), npts, tmax, dx.as<double>(),
+                                 dw.as<double>(), NODES, st));
+  for (int i = 0; i < n; ++i) KB_CUDA(launch_table_max(tabs[(size_t)i], npts, dmax.as<double>() + i, st));
+  std::vector<double> mx((size_t)n);
+  KB_CUDA(cudaMemcpyAsync(mx.data(), dmax.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  for (int i = 0; i < n; ++i) {
+    if (!std::isfinite(mx[(size_t)i])) return fail(KB_E_INVALID, "flat-band table has non-finite values");
+    models[i]->hash[0][0][0] = 0;
+    models[i]->tabmax = std::max(models[i]->tabmax, mx[(size_t)i]);
+  }
+  return KB_OK;
+}
+
 // Device view of a model. A spin whose (o1,o2) block was never uploaded uses the
 // other spin's block (keldy's models are spin symmetric, model.cpp:209-211).
 static ModelDev model_dev(const kb_model *m, bool *spin_symmetric) {

@@ -1,0 +1,188 @@
+// g0 tables of the single-level dot with flat-band leads, built on the GPU: the step
+// before the hot path when many models run at once (parameter sweeps).
+//
+// Same functions as the host builder (keldy_b200/g0_tables.py: flatband), restated per
+// mesh point: keldy's flat-band dot (impurity_oneband/model.hpp:100-112, 129-130;
+// Delta^R = -i Gamma/2 per lead, model.cpp:107-111) Fourier-transformed as
+//   g^<(t) = i Gamma/(2 pi) sum_mu [K_mu(t) + C_mu(t)],
+//   g^>(t) = -i Gamma/(2 pi) sum_mu [pi/Gamma e^{-i eps t - Gamma t} - K_mu(t) - C_mu(t)],
+// K_mu(t) = int_{-inf}^{mu} e^{-i w t} / ((w - eps)^2 + Gamma^2) dw in closed form through
+// the exponential integral E1 (complex argument), C_mu(t) the finite-temperature
+// correction int e^{-i w t} (n_F - theta)(w - mu) / ((w - eps)^2 + Gamma^2) dw by
+// Gauss-Legendre quadrature on [mu - 36/beta, mu + 36/beta]. t = 0 in closed form
+// (arctan), t < 0 from g(-t) = -conj(g(t)) (model.cpp:302-314).
+//
+// E1: power series E1(z) = -gamma - ln z - sum_k (-z)^k / (k k!) for small |z| or near
+// the negative real axis, otherwise the even continued fraction
+// E1(z) = e^{-z} / (z + 1 - 1/(z + 3 - 4/(z + 5 - ...))) evaluated by the modified Lentz
+// method (Abramowitz & Stegun 5.1.11 and 5.1.22; Press et al., Numerical Recipes 6.3).
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "kb_device.cuh"
+#include "kb_launch.h"
+
+namespace kb {
+
+namespace {
+
+constexpr double EULER_GAMMA = 0.57721566490153286061;
+constexpr double PI = 3.14159265358979323846;
+
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) { return cmul(a, crcp(b)); }
+__device__ __forceinline__ double2 cexpd(double2 z) {
+  double s, c;
+  sincos(z.y, &s, &c);
+  const double e = exp(z.x);
+  return c2(e * c, e * s);
+}
+__device__ __forceinline__ double2 clogd(double2 z) { return c2(log(hypot(z.x, z.y)), atan2(z.y, z.x)); }
+
+// E1(z), principal branch (cut on the negative real axis).
+__device__ double2 e1_complex(double2 z) {
+  const double az = hypot(z.x, z.y);
+  const bool series = az < 1.5 || (z.x < 0.0 && fabs(z.y) < 0.6 * fabs(z.x));
+  if (series) {
+    // sum_{k>=1} (-z)^k / (k k!)
+    double2 term = c2(1.0, 0.0), sum = c2(0.0, 0.0);
+    const double2 mz = c2(-z.x, -z.y);
+    for (int k = 1; k < 400; ++k) {
+      term = cmul(term, mz);
+      term = c2(term.x / k, term.y / k); // (-z)^k / k!
+      const double2 t = c2(term.x / k, term.y / k);
+      sum = cadd(sum, t);
+      if (k > az && hypot(t.x, t.y) <= 1e-17 * hypot(sum.x, sum.y)) break;
+    }
+    const double2 lz = clogd(z);
+    return c2(-EULER_GAMMA - lz.x - sum.x, -lz.y - sum.y);
+  }
+  double2 b = c2(z.x + 1.0, z.y);
+  double2 c = c2(1e300, 0.0);
+  double2 d = crcp(b);
+  double2 h = d;
+  for (int i = 1; i < 2000; ++i) {
+    const double an = -(double)i * (double)i;
+    b = c2(b.x + 2.0, b.y);
+    d = crcp(c2(an * d.x + b.x, an * d.y + b.y));
+    const double2 q = cdiv(c2(an, 0.0), c);
+    c = c2(b.x + q.x, b.y + q.y);
+    const double2 del = cmul(c, d);
+    h = cmul(h, del);
+    if (fabs(del.x - 1.0) + fabs(del.y) < 1e-16) break;
+  }
+  return cmul(h, cexpd(c2(-z.x, -z.y)));
+}
+
+// Ei(x) for real x > 0: gamma + ln x + sum x^k / (k k!) (all terms positive).
+__device__ double ei_positive(double x) {
+  double term = 1.0, sum = 0.0;
+  for (int k = 1; k < 600; ++k) {
+    term *= x / k;
+    const double t = term / k;
+    sum += t;
+    if (k > x && t <= 1e-17 * sum) break;
+  }
+  return EULER_GAMMA + log(x) + sum;
+}
+
+// K_mu(t) for t > 0 (the host builder's _lorentz_below).
+__device__ double2 lorentz_below(double t, double mu, double eps, double gamma) {
+  double2 out = c2(0.0, 0.0);
+  for (int sgn = 1; sgn >= -1; sgn -= 2) {
+    const double2 z = c2(eps, sgn * gamma);
+    const double2 v = c2(sgn * gamma * t, (mu - eps) * t); // i (mu - z) t
+    double2 e1;
+    if (sgn < 0 && mu == eps) {
+      e1 = c2(-ei_positive(gamma * t), PI); // the path ends on the cut: limit from below
+    } else {
+      e1 = e1_complex(v);
+      if (sgn < 0 && mu > eps) e1.y += 2.0 * PI; // continuation across the cut
+    }
+    const double2 ez = cexpd(c2(z.y * t, -z.x * t)); // exp(-i z t)
+    const double2 J = cmul(c2(-ez.x, -ez.y), e1);
+    out = c2(out.x + sgn * J.x, out.y + sgn * J.y);
+  }
+  // / (2 i gamma)
+  return c2(out.y / (2.0 * gamma), -out.x / (2.0 * gamma));
+}
+
+struct FlatbandParams {
+  double gamma, eps, bias, beta;
+};
+
+// One table per blockIdx.y; thread k >= 1 of the positive half builds mesh point mid+k
+// and its mirror mid-k; k = 0 builds t = 0.
+__global__ void flatband_kernel(const FlatbandParams *params, double2 *const *tabs, int npts, double tmax,
+                                const double *nodes, const double *weights, int n_nodes) {
+  const FlatbandParams P = params[blockIdx.y];
+  double2 *tab = tabs[blockIdx.y];
+  const int mid = npts / 2;
+  const double delta = (tmax - (-tmax)) / (double)(npts - 1);
+  const double pref = P.gamma / (2.0 * PI);
+  const double mus[2] = {-P.bias / 2.0, P.bias / 2.0};
+  const bool finite = isfinite(P.beta);
+  const double W = 36.0 / P.beta;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k <= npts - 1 - mid; k += gridDim.x * blockDim.x) {
+    const int i = mid + k;
+    const double t = -tmax + i * delta;
+    double2 less = c2(0.0, 0.0), great = c2(0.0, 0.0);
+    double occ = 0.0;
+    for (int l = 0; l < 2; ++l) {
+      const double mu = mus[l];
+      // finite-temperature correction: two Gauss-Legendre panels [-W, 0], [0, W]
+      double2 corr = c2(0.0, 0.0);
+      if (finite) {
+        for (int pnl = 0; pnl < 2; ++pnl) {
+          const double a = pnl == 0 ? -W : 0.0, b = pnl == 0 ? 0.0 : W;
+          for (int q = 0; q < n_nodes; ++q) {
+            const double x = 0.5 * (b - a) * nodes[q] + 0.5 * (b + a);
+            const double wq = 0.5 * (b - a) * weights[q];
+            const double ax = fabs(x);
+            const double e = exp(-P.beta * ax);
+            const double d = (x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0)) * e / (1.0 + e);
+            const double dx = x + mu - P.eps;
+            const double f = wq * d / (dx * dx + P.gamma * P.gamma);
+            double s, c;
+            sincos(-(x + mu) * (k == 0 ? 0.0 : t), &s, &c);
+            corr = c2(corr.x + f * c, corr.y + f * s);
+          }
+        }
+      }
+      if (k == 0) {
+        occ += (atan((mu - P.eps) / P.gamma) + PI / 2.0) / P.gamma + corr.x;
+      } else {
+        const double2 below = lorentz_below(t, mu, P.eps, P.gamma);
+        const double2 full = cmul(c2(PI / P.gamma, 0.0), cexpd(c2(-P.gamma * t, -P.eps * t)));
+        less = cadd(less, cadd(below, corr));
+        great = c2(great.x + full.x - below.x - corr.x, great.y + full.y - below.y - corr.y);
+      }
+    }
+    if (k == 0) {
+      tab[2 * mid] = c2(0.0, pref * occ);
+      tab[2 * mid + 1] = c2(0.0, -pref * (2.0 * PI / P.gamma - occ));
+    } else {
+      const double2 gl = c2(-pref * less.y, pref * less.x);   // i pref less
+      const double2 gg = c2(pref * great.y, -pref * great.x); // -i pref great
+      tab[2 * i] = gl;
+      tab[2 * i + 1] = gg;
+      const int j = npts - 1 - i; // mirror point of -t
+      tab[2 * j] = c2(-gl.x, gl.y);
+      tab[2 * j + 1] = c2(-gg.x, gg.y);
+    }
+  }
+}
+
+} // namespace
+
+cudaError_t launch_flatband_tables(int n_models, const double *params_dev, double2 *const *tabs_dev, int npts,
+                                   double tmax, const double *nodes_dev, const double *weights_dev, int n_nodes,
+                                   cudaStream_t st) {
+  if (n_models <= 0) return cudaSuccess;
+  const int half = npts - npts / 2;
+  dim3 grid((half + 127) / 128, n_models);
+  flatband_kernel<<<grid, 128, 0, st>>>(reinterpret_cast<const FlatbandParams *>(params_dev), tabs_dev, npts, tmax,
+                                        nodes_dev, weights_dev, n_nodes);
+  return cudaGetLastError();
+}
+
+} // namespace kb

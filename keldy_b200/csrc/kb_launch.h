@@ -71,5 +71,10 @@ cudaError_t launch_no_det(ModelDev m, kb_integrand f, int order, long long count
                           double2 *out, int *dom, int *err, cudaStream_t st);
 cudaError_t launch_table_max(const double2 *tab, int npts, double *out, cudaStream_t st);
 cudaError_t launch_fp64_peak(int iters, double *sink, int grid, int block, cudaStream_t st);
+// Flat-band dot g0 tables of n models ({Gamma, eps_d, V, beta} each) on the mesh of
+// npts points over [-tmax, tmax] (g0_build.cu); Gauss-Legendre rule on [-1, 1].
+cudaError_t launch_flatband_tables(int n_models, const double *params_dev, double2 *const *tabs_dev, int npts,
+                                   double tmax, const double *nodes_dev, const double *weights_dev, int n_nodes,
+                                   cudaStream_t st);
 
 } // namespace kb

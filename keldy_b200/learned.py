@@ -1,0 +1,67 @@
+"""The learned warper workflow: a coupling flow per perturbation order, trained on the
+GPU on |integrand| samples of the plain method, judged against the plain warper chain.
+
+The flow (kb_flow_*, keldy_b200/csrc/flow.cu) is a first stage before keldy's warper
+chain (warpers.hpp:72-85); the plain chain alone is the method without it. Both are
+estimated with randomised QMC (R random digital shifts of the Sobol sequence,
+qrng.hpp:77-109), so their standard errors and their agreement are measured the same way.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import capi, rqmc
+
+DEFAULT_TRAIN = dict(epochs=10, batch=8192, lr=2e-3, lr_final=1e-4)
+
+
+def fit(ctx, model, A, B, chain, order, n_samples=1 << 18, seed=0, k_first=1, **cfg):
+    """Creates and trains a flow of dimension `order` on n_samples plain-method points.
+    Returns (flow, seconds, final loss)."""
+    c = dict(DEFAULT_TRAIN, **cfg)
+    c.setdefault("seed", seed)
+    flow = ctx.flow(order, seed=seed)
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    loss = flow.fit(model, A, B, chain, ctx.sobol(order), n_samples, k_first=k_first, **c)
+    ctx.synchronize()
+    return flow, time.perf_counter() - t0, loss
+
+
+def variance_gain(ctx, model, A, B, chain, flow, n_points=1 << 15, seed_shift=977):
+    """Per-point variance of f J through the chain alone over that through flow + chain, on
+    the same shifted Sobol points (the plain Monte Carlo gain of the flow)."""
+    rng = ctx.sobol(flow.dim, 31, True, False, seed_shift)
+    z = rng.points(1, n_points)
+    plain = model.evaluate_warped(A, B, chain, z)[0]
+    x, jac = flow.sample_sobol(rng, 1, n_points)
+    learned = model.evaluate_warped(A, B, chain, x)[0] * jac
+    return float(np.var(plain) / np.var(learned))
+
+
+def compare(ctx, model, A, B, chain, order, flow, n_points, replicas=16, seed_shift0=1):
+    """Plain and learned RQMC estimates at n_points per replica: dict with mean, stderr,
+    seconds (wall, one batched call each) and the difference in combined standard errors."""
+    out = {}
+    for name, f in (("plain", None), ("learned", flow)):
+        rngs = [ctx.sobol(order, 31, True, False, seed_shift0 + r) for r in range(replicas)]
+        rqmc.estimate(ctx, model, A, B, chain, order, min(n_points, 1 << 10), replicas, rngs=rngs, flow=f)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        mean, err, _ = rqmc.estimate(ctx, model, A, B, chain, order, n_points, replicas, rngs=rngs, flow=f)
+        dt = time.perf_counter() - t0
+        out[name] = dict(mean=complex(mean), stderr=float(err), rel=float(err / abs(mean)), seconds=dt)
+    p, l = out["plain"], out["learned"]
+    out["diff_sigma"] = abs(l["mean"] - p["mean"]) / math.hypot(p["stderr"], l["stderr"])
+    out["stderr_ratio"] = p["stderr"] / l["stderr"]
+    return out
+
+
+def select(ctx, model, A, B, chain, order, flow, pilot_points=1 << 14, replicas=16):
+    """The plain estimator judges the flow: returns the flow when its RQMC standard error on
+    a pilot run is below the plain chain's, else None (use the plain chain)."""
+    c = compare(ctx, model, A, B, chain, order, flow, pilot_points, replicas, seed_shift0=10_001)
+    return (flow if c["learned"]["stderr"] < c["plain"]["stderr"] else None), c

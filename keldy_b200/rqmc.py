@@ -17,13 +17,14 @@ from . import capi
 
 
 def estimate(ctx, model, A, B, chain, order, n_points, replicas=16, seed_shift0=1, scramble=False, k_first=1,
-             cutoff=0.0, algo=capi.ALGO_AUTO, rngs=None):
+             cutoff=0.0, algo=capi.ALGO_AUTO, rngs=None, flow=None):
     """Mean, standard error and per-replica means of int f(warp(x)) J dx over [0,1]^order.
-    rngs: optional list of `replicas` prebuilt shifted generators (reused across calls)."""
+    rngs: optional list of `replicas` prebuilt shifted generators (reused across calls).
+    flow: optional learned flow applied before the chain."""
     if rngs is None:
         rngs = [ctx.sobol(order, 31, True, scramble, seed_shift0 + r) for r in range(replicas)]
     items = [dict(model=model, rng=g, chain=chain, A=A, B=B, cutoff=cutoff, order=order, k_first=k_first,
-                  n_points=n_points) for g in rngs]
+                  n_points=n_points, flow=flow) for g in rngs]
     res = capi.integrate(ctx, items, algo)
     means = np.array([s / n for s, n, _, _ in res])
     mean = means.mean()
@@ -33,7 +34,7 @@ def estimate(ctx, model, A, B, chain, order, n_points, replicas=16, seed_shift0=
 
 
 def time_to_relative_error(ctx, model, A, B, chain, order, target=1e-3, replicas=16, start_points=1 << 12,
-                           max_points=1 << 24, seed_shift0=1, scramble=False):
+                           max_points=1 << 24, seed_shift0=1, scramble=False, flow=None):
     """Doubles the points per replica until stderr / |mean| <= target (or max_points is
     reached). Returns dict(mean, stderr, rel, points_per_replica, evaluations, seconds):
     `seconds` is the wall time of the run that met the target (the GPU work needed at
@@ -43,7 +44,7 @@ def time_to_relative_error(ctx, model, A, B, chain, order, target=1e-3, replicas
     while True:
         ctx.synchronize()
         t0 = time.perf_counter()
-        mean, err, _ = estimate(ctx, model, A, B, chain, order, n, replicas, rngs=rngs)
+        mean, err, _ = estimate(ctx, model, A, B, chain, order, n, replicas, rngs=rngs, flow=flow)
         dt = time.perf_counter() - t0
         rel = err / abs(mean) if mean != 0 else float("inf")
         if rel <= target or n >= max_points:

@@ -2,7 +2,7 @@
 gradient of the training kernel against the CPU oracle (oracle/flow_oracle.py, bf16
 operands emulated), the exact inverse / Jacobian relations, training on a known
 density, and integration through the flow: unbiased against the plain warper chain and
-with a smaller standard error for the same number of points."""
+with a smaller per-point variance than the chain alone."""
 import math
 
 import numpy as np
