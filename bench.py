@@ -446,6 +446,16 @@ def run_single(args):
     res = capi.integrate(ctx, [dict(model=model, rng=ctx.sobol(args.order), chain=chain, A=(T_MAX, 0, 0, 0, 0),
                                     B=(T_MAX, 0, 1, 0, 0), order=args.order, k_first=1, n_points=args.points)])
     print("single", args.order, args.points, res[0])
+    if args.single_flow:
+        # a learned flow of the same order: one epoch of training (flow_train_kernel), then
+        # the same integration through it (flow_map_kernel)
+        flow = ctx.flow(args.order, seed=1)
+        loss = flow.fit(model, (T_MAX, 0, 0, 0, 0), (T_MAX, 0, 1, 0, 0), chain, ctx.sobol(args.order), 1 << 16,
+                        epochs=1, batch=8192)
+        res = capi.integrate(ctx, [dict(model=model, rng=ctx.sobol(args.order), chain=chain, A=(T_MAX, 0, 0, 0, 0),
+                                        B=(T_MAX, 0, 1, 0, 0), order=args.order, k_first=1, n_points=args.points,
+                                        flow=flow)])
+        print("single-flow", args.order, args.points, loss, res[0])
     ctx.close()
 
 
@@ -463,6 +473,8 @@ def main():
     ap.add_argument("--ref-seconds", type=float, default=2.0, help="seconds of CPU work per reference-arm step")
     ap.add_argument("--single", action="store_true",
                     help="one integrate call of --points points at --order and exit (for profiler captures)")
+    ap.add_argument("--single-flow", action="store_true",
+                    help="with --single: also train a learned flow for one epoch and integrate through it")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
