@@ -32,6 +32,9 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
+# DRAM bytes (read + write) of one tree_kernel launch of this workload (2^20 points,
+# order 8), from an ncu capture of that launch
+TREE_LAUNCH_DRAM_BYTES = 1_870_000
 
 
 def flop_lu(m):
@@ -67,7 +70,10 @@ class ClockSampler:
         self.lines = []
         self.proc = None
 
-    def start(self):
+    def start(self, wait_first=True):
+        """Starts sampling; waits (up to 10 s) for the first sample, so that nvidia-smi's
+        start-up, which stalls this process's CUDA calls for up to a second, ends before the
+        measured regions."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -75,10 +81,19 @@ class ClockSampler:
             threading.Thread(target=self._read, daemon=True).start()
         except OSError:
             self.proc = None
+            return
+        t0 = time.time()
+        while wait_first and not self.lines and time.time() - t0 < 10.0:
+            time.sleep(0.05)
+        time.sleep(0.3)
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def mark(self):
+        """Index of the next sample (start/end of a measured window)."""
+        return len(self.lines)
 
     def stop(self):
         if self.proc:
@@ -87,9 +102,12 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+
+    def summary(self, a=0, b=None):
+        """Median SM clock, max clock and throttle reasons of samples a..b."""
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for line in self.lines[a:b]:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 8:
                 continue
@@ -325,6 +343,8 @@ def run_ours(args, rank, world, local_rank):
     tuned = autotune.tune(ctx, orders=sorted({order} | set(range(1, 11))), repeats=2)
     autotune.apply(ctx, tuned)
     plan = capi.Plan(ctx, [item(0)])
+    sampler = ClockSampler(local_rank)
+    sampler.start()
     for s in range(args.warmup):
         plan.set_k_first(0, item(s)["k_first"])
         allreduce(plan.run())
@@ -335,9 +355,8 @@ def run_ours(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    sampler = ClockSampler(local_rank)
-    sampler.start()
     barrier()
+    w0 = sampler.mark()
     dev_ms, integ_ms, launches, in_domain, fallback = 0.0, 0.0, 0, 0, 0
     for s in range(args.steps):
         flush.fill_(s & 0xFF)
@@ -351,7 +370,7 @@ def run_ours(args, rank, world, local_rank):
         in_domain += res[0][2]
         fallback += res[0][3]
     barrier()
-    clocks = sampler.stop()
+    w1 = sampler.mark()
     plan.close()
     # end to end through the public API with host buffers: per step, upload the g0
     # tables from pinned memory, integrate, read the sums back
@@ -363,6 +382,9 @@ def run_ours(args, rank, world, local_rank):
         del m2
     barrier()
     e2e_s = time.perf_counter() - t0
+    sampler.stop()
+    clocks = sampler.summary(w0, max(w1, w0 + 1))
+    clocks["e2e"] = sampler.summary(w1)
 
     t_max_ms = dev_ms
     e2e_max = e2e_s
@@ -406,7 +428,11 @@ def run_ours(args, rank, world, local_rank):
                     "d2h_bytes_per_step": 40},
             "gpu_launches": launches,
             "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": TREE_LAUNCH_DRAM_BYTES if order == 8 and N == 1 << 20 else None,
+                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-point order-8 "
+                                           "tree_kernel launch (ncu, profiles/tree_kernel_order8_65536pts.md): the "
+                                           "g0 table and chunk partials; the 17,440 B per evaluation of table "
+                                           "gathers are served by L2/L1",
                          "numerator": f"reference-equivalent: {reference_flops(order)} FLOP per evaluation "
                                       f"(keldy's 2^n LU pairs); the tree executes ~{tree_flops(order)}",
                          "peak_source": "FP64 FMA rate measured in this run (kb_fp64_peak, 8 independent "
@@ -462,7 +488,7 @@ def run_single(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--order", type=int, default=8)

@@ -200,6 +200,21 @@ typedef struct {
  * sequence on the context's stream; sums are deterministic (fixed reduction order). */
 int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc);
 
+/* Time bins of integrand_g_direct_time (wick_direct_time.cpp:42-163): each point's f*J
+ * goes to the bin of its earliest vertex time in the binner (xmin, xmax, nbins) of
+ * binner_t (binner.hpp:163-176, 241-260: points outside [xmin, xmax] are dropped, xmax
+ * itself falls in the last bin); out-of-domain points add 0 to their bin's sum and count.
+ * compute_charge_Q_direct_time (compute_obs.hpp:85-101) bins [0, t] in nr_time_slices. */
+typedef struct {
+  int nbins;
+  double xmin, xmax;
+} kb_time_bins;
+/* kb_integrate plus, per work item, the binned sums bin_sums[n_work][nbins] (interleaved
+ * complex), the counts bin_counts[n_work][nbins] of values added and dropped[n_work]: all
+ * added to. nbins in [1, 4096]. */
+int kb_integrate_binned(kb_context *ctx, const kb_work *work, int n_work, int algo, const kb_time_bins *bins,
+                        kb_accum *acc, double *bin_sums, uint64_t *bin_counts, uint64_t *dropped);
+
 /* Integrate without allocating device memory. No counterpart in keldy: this entry point
  * is for callers that cannot call cudaMalloc (a host application whose own allocator
  * owns the device's memory, or a latency-bound loop that must not pay cudaMalloc's

@@ -500,5 +500,101 @@ class compute_current_J_direct : public integrator_g_direct {
                            order) {}
 };
 
+// keldy::binner::binner_t<1> (binner.hpp:163-300): a continuous axis [xmin, xmax] in
+// nr_bins bins; per bin the sum of the values added and their number; values outside the
+// axis counted as dropped.
+class binner_1d {
+  double xmin_ = 0.0, xmax_ = 1.0, bin_size_ = 1.0;
+  std::vector<dcomplex> data_;
+  std::vector<long> nr_values_added_;
+
+ public:
+  long nr_values_dropped = 0;
+
+  binner_1d(double xmin, double xmax, long nr_bins) : xmin_(xmin), xmax_(xmax) {
+    if (xmin >= xmax)
+      throw std::runtime_error("Boundaries of binning range are in wrong order (" + std::to_string(xmin) +
+                               " >= " + std::to_string(xmax) + ")");
+    if (nr_bins < 1 || nr_bins > 4096) throw std::runtime_error("the number of time bins must be in [1, 4096]");
+    bin_size_ = (xmax - xmin) / double(nr_bins);
+    data_.assign((size_t)nr_bins, dcomplex(0.0));
+    nr_values_added_.assign((size_t)nr_bins, 0);
+  }
+  std::vector<dcomplex> const &get_data() const { return data_; }
+  std::vector<long> const &get_nr_values_added() const { return nr_values_added_; }
+  long get_nr_values_dropped() const { return nr_values_dropped; }
+  int get_nr_bins() const { return (int)data_.size(); }
+  double get_bin_size() const { return bin_size_; }
+  double get_xmin() const { return xmin_; }
+  double get_xmax() const { return xmax_; }
+  std::vector<double> get_bin_coord() const {
+    std::vector<double> c(data_.size());
+    for (size_t i = 0; i < c.size(); ++i) c[i] = xmin_ + (double(i) + 0.5) * bin_size_;
+    return c;
+  }
+  binner_1d &operator*=(dcomplex s) {
+    for (auto &v : data_) v *= s;
+    return *this;
+  }
+  // adds kb_integrate_binned's outputs of one work item
+  void add(const double *sums, const uint64_t *counts, uint64_t dropped) {
+    for (size_t b = 0; b < data_.size(); ++b) {
+      data_[b] += dcomplex(sums[2 * b], sums[2 * b + 1]);
+      nr_values_added_[b] += (long)counts[b];
+    }
+    nr_values_dropped += (long)dropped;
+  }
+};
+
+// integrator<binner_t<1>, integrand_g_direct_time> (wick_direct_time.cpp:42-163,
+// integrator.hpp:81-131): the direct integrand, each point's f*J binned by its earliest
+// vertex time. evaluate_warped_integrand returns the unbinned value.
+class integrator_g_direct_time : public integrator_g_direct {
+ protected:
+  binner_1d bins_;
+
+ public:
+  integrator_g_direct_time(binner_1d bins, integrand_g_direct integrand_, int dimension_)
+     : integrator_g_direct(std::move(integrand_), dimension_), bins_(std::move(bins)) {}
+
+  void run(int nr_steps) {
+    if (nr_steps <= 0) return;
+    if ((uint64_t)rng_.state() + (uint64_t)nr_steps > (1ull << 31))
+      throw std::runtime_error("More sample points requested then generator can hold.");
+    auto const &chain = warper.chain();
+    kb_work w{integrand.get_g0().model.handle(), rng_.handle(), chain.data(), (int)chain.size(), integrand.abi(),
+              dimension, rng_.state() + 1, nr_steps};
+    kb_time_bins tb{bins_.get_nr_bins(), bins_.get_xmin(), bins_.get_xmax()};
+    std::vector<double> sums(2 * (size_t)tb.nbins, 0.0);
+    std::vector<uint64_t> counts((size_t)tb.nbins, 0);
+    uint64_t dropped = 0;
+    kb_accum acc{};
+    keldy_b200::check(kb_integrate_binned(keldy_b200::default_context(), &w, 1, integrand.algorithm(), &tb, &acc,
+                                          sums.data(), counts.data(), &dropped));
+    rng_.discard(nr_steps);
+    bins_.add(sums.data(), counts.data(), dropped);
+    result += dcomplex(acc.sum_re, acc.sum_im);
+    n_points += acc.n_points;
+    n_integrand_evals_in_domain += acc.n_in_domain;
+  }
+
+  // result / n_points, as integrator::reduce_result (integrator.hpp:123-127)
+  binner_1d reduce_result() const {
+    binner_1d r = bins_;
+    r *= dcomplex(1.0 / double(reduce_nr_points_run()));
+    return r;
+  }
+};
+
+// compute_obs.hpp:85-101: charge G^<_{up,up}(t, t) binned over [0, t] in nr_time_slices.
+class compute_charge_Q_direct_time : public integrator_g_direct_time {
+ public:
+  compute_charge_Q_direct_time(g0_model model, double time, int order, int nr_time_slices, double cutoff_integrand)
+     : integrator_g_direct_time(binner_1d(0.0, time, nr_time_slices),
+                                integrand_g_direct{g0_keldysh_contour_t{std::move(model)}, gf_index_t{time, up, forward},
+                                                   gf_index_t{time, up, backward}, cutoff_integrand},
+                                order) {}
+};
+
 } // namespace impurity_oneband
 } // namespace keldy

@@ -35,7 +35,7 @@ EXPORTS = [
     "kb_fp64_peak", "kb_integrate_noalloc", "kb_plan_create", "kb_plan_destroy", "kb_plan_launch",
     "kb_plan_result", "kb_plan_set_k_first", "kb_context_set_launch", "kb_context_get_launch",
     "kb_flow_create", "kb_flow_destroy", "kb_flow_dim", "kb_flow_get_params", "kb_flow_set_params", "kb_flow_map",
-    "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit",
+    "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
 ]
 FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
 FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
@@ -70,6 +70,10 @@ class Work(C.Structure):
     _fields_ = [("m", C.c_void_p), ("rng", C.c_void_p), ("chain", C.POINTER(Warper)), ("chain_len", C.c_int),
                 ("f", Integrand), ("order", C.c_int), ("k_first", C.c_uint32), ("n_points", C.c_int64),
                 ("flow", C.c_void_p)]
+
+
+class TimeBins(C.Structure):
+    _fields_ = [("nbins", C.c_int), ("xmin", C.c_double), ("xmax", C.c_double)]
 
 
 class FlowTrainCfg(C.Structure):
@@ -122,6 +126,8 @@ def load():
     L.kb_evaluate_warped.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, C.c_int, C.c_int,
                                      C.c_int64, _D, C.c_int, C.c_int, _D, _D, _I]
     L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
+    L.kb_integrate_binned.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(TimeBins), C.POINTER(Accum),
+                                      _D, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.kb_fp64_peak.argtypes = [_VP, C.c_int, _D]
     L.kb_integrate_noalloc.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(Accum)]
     L.kb_plan_create.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(_VP)]
@@ -456,6 +462,24 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def integrate_binned(ctx, items, nbins, xmin, xmax, algo=ALGO_AUTO):
+    """kb_integrate_binned: per item (sum, n_points, n_in_domain, n_fallback, bins complex[nbins],
+    counts[nbins], dropped) - keldy's integrand_g_direct_time binned by the earliest vertex
+    time into binner_t(xmin, xmax, nbins)."""
+    works, keep = _works(items)
+    n = len(items)
+    acc = (Accum * max(1, n))()
+    sums = np.zeros((max(1, n), nbins), dtype=np.complex128)
+    counts = np.zeros((max(1, n), nbins), dtype=np.uint64)
+    dropped = np.zeros(max(1, n), dtype=np.uint64)
+    U = C.POINTER(C.c_uint64)
+    check(ctx.L.kb_integrate_binned(ctx.h, works, n, algo, C.byref(TimeBins(int(nbins), float(xmin), float(xmax))),
+                                    acc, _dp(sums.view(np.float64)), counts.ctypes.data_as(U),
+                                    dropped.ctypes.data_as(U)))
+    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback, sums[i], counts[i].astype(np.int64),
+             int(dropped[i])) for i, a in enumerate(acc[:n])]
 
 
 def integrate_noalloc(ctx, items):

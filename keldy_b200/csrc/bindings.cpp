@@ -204,4 +204,16 @@ PYBIND11_MODULE(_keldy, m) {
                 .def(py::init<g0_model, double, int, double>(), py::arg("model"), py::arg("time"), py::arg("order"),
                      py::arg("cutoff_integrand"));
   integrator_methods<compute_current_J_direct>(cj);
+  py::class_<binner_1d>(m, "BinnerT1")
+      .def(py::init<double, double, long>(), py::arg("xmin"), py::arg("xmax"), py::arg("nr_bins"))
+      .def("get_data", &binner_1d::get_data)
+      .def("get_nr_values_added", &binner_1d::get_nr_values_added)
+      .def("get_nr_values_dropped", &binner_1d::get_nr_values_dropped)
+      .def("get_nr_bins", &binner_1d::get_nr_bins)
+      .def("get_bin_size", &binner_1d::get_bin_size)
+      .def("get_bin_coord", &binner_1d::get_bin_coord);
+  auto cqt = py::class_<compute_charge_Q_direct_time>(m, "ComputeChargeQDirectTime")
+                 .def(py::init<g0_model, double, int, int, double>(), py::arg("model"), py::arg("time"),
+                      py::arg("order"), py::arg("nr_time_slices"), py::arg("cutoff_integrand"));
+  integrator_methods<compute_charge_Q_direct_time>(cqt);
 }

@@ -707,10 +707,20 @@ int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integr
 } // extern "C"
 
 namespace {
+// Time bins of an integration (integrand_g_direct_time) and the caller's outputs.
+struct TimeBins {
+  int nbins;
+  double xmin, xmax;
+  double *sums;      // [n_work][nbins] interleaved complex, added to
+  uint64_t *counts;  // [n_work][nbins], added to
+  uint64_t *dropped; // [n_work], added to
+};
+
 // One batched pass over `items`: two groups (tree / pivoted LU), each one persistent
-// launch over its items, heaviest orders first. Sums are added to acc[acc_index[i]].
+// launch over its items, heaviest orders first. Sums are added to acc[acc_index[i]]
+// (and to the time bins of that work item when `bins` is given).
 int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std::vector<int> &use_tree,
-                  const std::vector<int> &acc_index, kb_accum *acc) {
+                  const std::vector<int> &acc_index, kb_accum *acc, const TimeBins *bins = nullptr) {
   cudaStream_t st = ctx->stream;
   const int n_work = (int)items.size();
   for (int group = 0; group < 2; ++group) {
@@ -748,6 +758,23 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
     L.mode = IN_SOBOL;
     L.partials = dpart.as<ChunkPartial>();
     L.err = ctx->d_err;
+    DevBuf dbs, dbc, dbd, dos, doc, dod;
+    if (bins) {
+      const size_t nb = (size_t)bins->nbins;
+      KB_CUDA(dbs.alloc((size_t)nchunks * nb * sizeof(double2), st));
+      KB_CUDA(dbc.alloc((size_t)nchunks * nb * sizeof(unsigned), st));
+      KB_CUDA(dbd.alloc((size_t)nchunks * sizeof(unsigned), st));
+      KB_CUDA(dos.alloc(sorted.size() * nb * sizeof(double2), st));
+      KB_CUDA(doc.alloc(sorted.size() * nb * sizeof(unsigned long long), st));
+      KB_CUDA(dod.alloc(sorted.size() * sizeof(unsigned long long), st));
+      L.nbins = bins->nbins;
+      L.bin_xmin = bins->xmin;
+      L.bin_xmax = bins->xmax;
+      L.bin_size = (bins->xmax - bins->xmin) / bins->nbins;
+      L.bin_sums = dbs.as<double2>();
+      L.bin_counts = dbc.as<unsigned>();
+      L.bin_dropped = dbd.as<unsigned>();
+    }
     DevBuf dpts;
     const int tgrid = (int)std::min<long long>(nchunks, (long long)ctx->sm_count * ctx->ctas_per_sm);
     if (group == 0) {
@@ -766,10 +793,25 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
     }
     if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[2], st));
     KB_CUDA(launch_reduce(L, dacc_s.as<kb_accum>(), st));
+    if (bins) {
+      KB_CUDA(launch_reduce_bins(L, dos.as<double2>(), doc.as<unsigned long long>(), dod.as<unsigned long long>(), st));
+      ctx->last_launches++;
+    }
     if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[3], st));
     ctx->last_launches += 2;
     std::vector<kb_accum> part(sorted.size());
     KB_CUDA(cudaMemcpyAsync(part.data(), dacc_s.p, part.size() * sizeof(kb_accum), cudaMemcpyDeviceToHost, st));
+    std::vector<double> hbs;
+    std::vector<unsigned long long> hbc, hbd;
+    if (bins) {
+      const size_t nb = (size_t)bins->nbins;
+      hbs.resize(sorted.size() * nb * 2);
+      hbc.resize(sorted.size() * nb);
+      hbd.resize(sorted.size());
+      KB_CUDA(cudaMemcpyAsync(hbs.data(), dos.p, hbs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+      KB_CUDA(cudaMemcpyAsync(hbc.data(), doc.p, hbc.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      KB_CUDA(cudaMemcpyAsync(hbd.data(), dod.p, hbd.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    }
     KB_CUDA(cudaStreamSynchronize(st));
     if (ctx->timing) {
       float a = 0, b = 0, c = 0;
@@ -781,12 +823,22 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
       ctx->last_ms[2] += c;
     }
     for (size_t j = 0; j < ids.size(); ++j) {
-      kb_accum &a = acc[acc_index[(size_t)ids[j]]];
+      const int w = acc_index[(size_t)ids[j]];
+      kb_accum &a = acc[w];
       a.sum_re += part[j].sum_re;
       a.sum_im += part[j].sum_im;
       a.n_points += part[j].n_points;
       a.n_in_domain += part[j].n_in_domain;
       a.n_fallback += part[j].n_fallback;
+      if (bins) {
+        const size_t nb = (size_t)bins->nbins;
+        for (size_t b = 0; b < nb; ++b) {
+          bins->sums[2 * ((size_t)w * nb + b)] += hbs[2 * (j * nb + b)];
+          bins->sums[2 * ((size_t)w * nb + b) + 1] += hbs[2 * (j * nb + b) + 1];
+          bins->counts[(size_t)w * nb + b] += hbc[j * nb + b];
+        }
+        bins->dropped[w] += hbd[j];
+      }
     }
   }
   return KB_OK;
@@ -823,11 +875,31 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
   tree = ((algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric)) ? 1 : 0;
   return KB_OK;
 }
+
+int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc, const TimeBins *tb);
 } // namespace
 
 extern "C" {
 
 int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc) {
+  return integrate_impl(ctx, work, n_work, algo, acc, nullptr);
+}
+
+int kb_integrate_binned(kb_context *ctx, const kb_work *work, int n_work, int algo, const kb_time_bins *bins,
+                        kb_accum *acc, double *bin_sums, uint64_t *bin_counts, uint64_t *dropped) {
+  KB_CHECK(bins && (n_work == 0 || (bin_sums && bin_counts && dropped)), "kb_integrate_binned: null argument");
+  KB_CHECK(bins->nbins >= 1 && bins->nbins <= 4096, "the number of time bins must be in [1, 4096]");
+  if (!(bins->xmin < bins->xmax))
+    return fail(KB_E_INVALID, "Boundaries of binning range are in wrong order (" + std::to_string(bins->xmin) +
+                                  " >= " + std::to_string(bins->xmax) + ")");
+  TimeBins tb{bins->nbins, bins->xmin, bins->xmax, bin_sums, bin_counts, dropped};
+  return integrate_impl(ctx, work, n_work, algo, acc, &tb);
+}
+
+} // extern "C"
+
+namespace {
+int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc, const TimeBins *tb) {
   KB_CHECK(ctx && (n_work == 0 || (work && acc)), "kb_integrate: null argument");
   KB_CHECK(algo == KB_ALGO_AUTO || algo == KB_ALGO_TREE || algo == KB_ALGO_DIRECT, "unknown algorithm");
   if (n_work == 0) return KB_OK;
@@ -847,7 +919,7 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
   ctx->last_launches = 0;
   KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
   if (!any_flow) {
-    int rc = run_integrate(ctx, items, use_tree, index, acc);
+    int rc = run_integrate(ctx, items, use_tree, index, acc, tb);
     if (rc) return rc;
   } else {
     // Items with a flow run in pieces whose flow-mapped points (li, Jacobian) are made by
@@ -903,7 +975,7 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
         rtree.push_back(p.tree);
         racc.push_back(p.acc);
       }
-      int rc = run_integrate(ctx, ritems, rtree, racc, acc);
+      int rc = run_integrate(ctx, ritems, rtree, racc, acc, tb);
       if (rc) return rc;
       first_round = false;
     }
@@ -915,6 +987,9 @@ int kb_integrate(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_
   if (err & 2) return fail(KB_E_CUDA, "a flow kernel's wait on the tensor cores ran out");
   return KB_OK;
 }
+} // namespace
+
+extern "C" {
 
 // ------------------------------------------------------------------ plans
 struct kb_plan {

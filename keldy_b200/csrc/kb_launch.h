@@ -48,6 +48,13 @@ struct Launch {
   double *pts;
   // IN_SOBOL
   ChunkPartial *partials; // [n_chunks]
+  // IN_SOBOL with time bins (integrand_g_direct_time): every point's f*J also goes to the
+  // bin of its earliest vertex time; per chunk: sums [n_chunks][nbins], counts, dropped
+  int nbins; // 0: no bins
+  double bin_xmin, bin_xmax, bin_size;
+  double2 *bin_sums;
+  unsigned *bin_counts;
+  unsigned *bin_dropped; // [n_chunks]
   // errors
   int *err; // bit 0: g0 evaluated outside its window
 };
@@ -61,6 +68,10 @@ cudaError_t launch_direct(const Launch &L, int grid, cudaStream_t st);
 cudaError_t launch_fallback(const Launch &L, int grid, cudaStream_t st);
 // acc[item] += sum over the item's chunks in chunk order
 cudaError_t launch_reduce(const Launch &L, kb_accum *acc_dev, cudaStream_t st);
+// per item: bin sums [n_items][nbins], counts [n_items][nbins], dropped [n_items] summed
+// over the item's chunks in chunk order (written, not added)
+cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long long *counts,
+                               unsigned long long *dropped, cudaStream_t st);
 
 cudaError_t launch_sobol_points(SobolDev s, uint32_t k_first, long long count, double *out, cudaStream_t st);
 cudaError_t launch_warp(const WarperDev *chain_dev, int start, int end, int direction, int n, long long count,

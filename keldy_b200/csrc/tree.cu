@@ -515,6 +515,27 @@ __device__ __forceinline__ double2 apply_cutoff(double2 f, double cutoff) {
   return (cabs(f) < cutoff) ? c2(0.0, 0.0) : f;
 }
 
+// Bin of the earliest vertex time (binner_t::in_bounds and coord2index, binner.hpp:163-176:
+// in [xmin, xmax], xmax itself in the last bin); -1: dropped. An index that rounds up to
+// nbins just below xmax goes to the last bin.
+__device__ __forceinline__ int time_bin(const Launch &L, const double *u, int stride, int N) {
+  double t = u[0];
+  for (int j = 1; j < N; ++j) t = fmin(t, u[j * stride]);
+  if (!(L.bin_xmin <= t && t <= L.bin_xmax)) return -1;
+  if (t == L.bin_xmax) return L.nbins - 1;
+  return min((int)((t - L.bin_xmin) / L.bin_size), L.nbins - 1);
+}
+
+// Zeroes chunk c's bins (all threads of the CTA; a barrier follows before their use).
+__device__ __forceinline__ void clear_bins(const Launch &L, int c) {
+  if (!L.nbins) return;
+  for (int b = threadIdx.x; b < L.nbins; b += blockDim.x) {
+    L.bin_sums[(size_t)c * L.nbins + b] = c2(0.0, 0.0);
+    L.bin_counts[(size_t)c * L.nbins + b] = 0u;
+  }
+  if (threadIdx.x == 0) L.bin_dropped[c] = 0u;
+}
+
 template <bool EVAL>
 __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -540,6 +561,7 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
     unsigned long long cdom = 0, cfb = 0, mask0 = 0, mask1 = 0;
     double *slot = L.pts + (size_t)blockIdx.x * PTS_SLOT;
     if (tid < ccount) prepare_point(L, it, N, cfirst + tid, keep, slot, tid);
+    if (!EVAL) clear_bins(L, c);
     __syncthreads();
     for (int sb = 0; sb < ccount; sb += P) {
       const int np = min(P, ccount - sb);
@@ -566,6 +588,14 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
       } else if (tid == 0) {
         for (int p = 0; p < np; ++p) {
           int fl = S.flag[p];
+          int bin = -2;
+          if (L.nbins) {
+            bin = time_bin(L, slot + sb + p, CHUNK_POINTS, N);
+            if (bin < 0)
+              L.bin_dropped[c]++;
+            else
+              L.bin_counts[(size_t)c * L.nbins + bin]++;
+          }
           if (fl & 1) continue;
           cdom++;
           if (fl & 2) {
@@ -581,6 +611,10 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
           double j = S.jac[p];
           csum.x += f.x * j;
           csum.y += f.y * j;
+          if (bin >= 0) {
+            double2 &bs = L.bin_sums[(size_t)c * L.nbins + bin];
+            bs = c2(bs.x + f.x * j, bs.y + f.y * j);
+          }
         }
       }
       __syncthreads();
@@ -748,6 +782,10 @@ __global__ void __launch_bounds__(NT) direct_kernel(Launch L) {
     const bool keep = eval ? (L.keep_u_hypercube != 0) : true;
     double2 csum = c2(0.0, 0.0);
     unsigned long long cdom = 0;
+    if (!eval) {
+      clear_bins(L, c);
+      __syncthreads();
+    }
     for (int p = 0; p < ccount; ++p) {
       long long gp = cfirst + p;
       direct_load_point(L, it, N, gp, keep, D);
@@ -769,6 +807,16 @@ __global__ void __launch_bounds__(NT) direct_kernel(Launch L) {
           csum.x += f.x * j;
           csum.y += f.y * j;
           cdom += dom ? 1 : 0;
+          if (L.nbins) {
+            const int bin = time_bin(L, D.u, 1, N);
+            if (bin < 0) {
+              L.bin_dropped[c]++;
+            } else {
+              L.bin_counts[(size_t)c * L.nbins + bin]++;
+              double2 &bs = L.bin_sums[(size_t)c * L.nbins + bin];
+              bs = c2(bs.x + f.x * j, bs.y + f.y * j);
+            }
+          }
         }
       }
       __syncthreads();
@@ -812,6 +860,13 @@ __global__ void __launch_bounds__(NT) fallback_kernel(Launch L) {
         f = apply_cutoff(f, it.f.cutoff);
         pr.sum_re += f.x * D.jac[0];
         pr.sum_im += f.y * D.jac[0];
+        if (L.nbins) { // counted by the tree kernel; the value is added here
+          const int bin = time_bin(L, D.u, 1, it.order);
+          if (bin >= 0) {
+            double2 &bs = L.bin_sums[(size_t)c * L.nbins + bin];
+            bs = c2(bs.x + f.x * D.jac[0], bs.y + f.y * D.jac[0]);
+          }
+        }
       }
       __syncthreads();
     }
@@ -860,7 +915,36 @@ __global__ void __launch_bounds__(NT) reduce_kernel(Launch L, kb_accum *acc) {
   }
 }
 
+// Thread t of block `item` sums bins t, t + NT, ... over the item's chunks in chunk order.
+__global__ void __launch_bounds__(NT) reduce_bins_kernel(Launch L, double2 *sums, unsigned long long *counts,
+                                                         unsigned long long *dropped) {
+  const int item = blockIdx.x;
+  const long long c0 = L.chunk_offsets[item], c1 = L.chunk_offsets[item + 1];
+  for (int b = threadIdx.x; b < L.nbins; b += blockDim.x) {
+    double2 s = c2(0.0, 0.0);
+    unsigned long long n = 0;
+    for (long long c = c0; c < c1; ++c) {
+      s = cadd(s, L.bin_sums[(size_t)c * L.nbins + b]);
+      n += L.bin_counts[(size_t)c * L.nbins + b];
+    }
+    sums[(size_t)item * L.nbins + b] = s;
+    counts[(size_t)item * L.nbins + b] = n;
+  }
+  if (threadIdx.x == 0) {
+    unsigned long long d = 0;
+    for (long long c = c0; c < c1; ++c) d += L.bin_dropped[c];
+    dropped[item] = d;
+  }
+}
+
 } // namespace
+
+cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long long *counts,
+                               unsigned long long *dropped, cudaStream_t st) {
+  if (L.n_items == 0 || L.nbins == 0) return cudaSuccess;
+  reduce_bins_kernel<<<L.n_items, NT, 0, st>>>(L, sums, counts, dropped);
+  return cudaGetLastError();
+}
 
 size_t tree_smem_bytes() { return sizeof(TreeShared); }
 

@@ -13,7 +13,8 @@ import warnings
 import numpy as np
 
 from . import g0_tables
-from ._keldy import (ComputeChargeQDirect as _ComputeChargeQDirect,  # noqa: F401
+from ._keldy import (BinnerT1, ComputeChargeQDirect as _ComputeChargeQDirect,  # noqa: F401
+                     ComputeChargeQDirectTime as _ComputeChargeQDirectTime,
                      ComputeCurrentJDirect as _ComputeCurrentJDirect, G0KeldyshContourT, G0ModelTables, GfIndexT,
                      IntegrandGDirect)
 
@@ -122,6 +123,14 @@ def ComputeChargeQDirect(model, time, order, cutoff_integrand):
     return _ComputeChargeQDirect(_model(model, False), float(time), int(order), float(cutoff_integrand))
 
 
+def ComputeChargeQDirectTime(model, time, order, nr_time_slices, cutoff_integrand):
+    """compute_charge_Q_direct_time(model or params, time, order, nr_time_slices, cutoff)
+    (compute_obs.hpp:85-101): the charge binned by the earliest vertex time over [0, time];
+    reduce_result() returns the binner (BinnerT1)."""
+    return _ComputeChargeQDirectTime(_model(model, False), float(time), int(order), int(nr_time_slices),
+                                     float(cutoff_integrand))
+
+
 def ComputeCurrentJDirect(model, time, order, cutoff_integrand):
     """compute_current_J_direct(model or params, time, order, cutoff) (compute_obs.hpp:66-80)."""
     m = _model(model, True)
@@ -131,4 +140,4 @@ def ComputeCurrentJDirect(model, time, order, cutoff_integrand):
 
 
 __all__ = ["GfIndexT", "G0Model", "G0KeldyshContourT", "IntegrandGDirect", "ComputeChargeQDirect",
-           "ComputeCurrentJDirect", "model_param_t", "MODEL_PARAM_DEFAULTS"]
+           "ComputeChargeQDirectTime", "BinnerT1", "ComputeCurrentJDirect", "model_param_t", "MODEL_PARAM_DEFAULTS"]

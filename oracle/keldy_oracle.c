@@ -711,3 +711,50 @@ int or_integrate(const or_model *mdl, const or_gf_index *A, const or_gf_index *B
   result[4] = ssc;
   return st;
 }
+
+/* integrator<binner_t<1>, integrand_g_direct_time>::run: as or_integrate, each point's
+ * f*J also added to the bin of its earliest warped vertex time
+ * (wick_direct_time.cpp:55, 160; binner_t<1>(xmin, xmax, nbins), binner.hpp:163-176,
+ * 241-260: in_bounds xmin <= x <= xmax, index (x - xmin) / bin_size truncated, x == xmax
+ * in the last bin, out-of-bounds values counted as dropped). Out-of-domain points add 0.
+ * bins[2 * nbins] (complex sums), counts[nbins], *dropped: added to. */
+int or_integrate_binned(const or_model *mdl, const or_gf_index *A, const or_gf_index *B, double cutoff,
+                        const or_warper *chain, int len, int n, const uint32_t *Csr, const uint32_t *shfr, int m,
+                        uint32_t k_first, int64_t nr_steps, int nbins, double xmin, double xmax, double *result,
+                        double *bins, double *counts, double *dropped) {
+  double li[64], ui[64], v[3], sc, jac;
+  int dom;
+  const double bin_size = (xmax - xmin) / nbins;
+  double sre = 0.0, sim = 0.0, ssc = 0.0;
+  uint64_t npts = 0, ndom = 0;
+  int st = 0;
+  for (int64_t i = 0; i < nr_steps; ++i) {
+    or_sobol_points(n, m, Csr, shfr, k_first + (uint32_t)i, 1, li);
+    if (or_evaluate_warped(mdl, A, B, cutoff, chain, len, n, li, v, &dom, &sc) != 0) st = -1;
+    jac = 1.0;
+    or_map_reverse(chain, len, len, 0, n, li, ui, &jac);
+    double t = ui[0];
+    for (int j = 1; j < n; ++j)
+      if (ui[j] < t) t = ui[j];
+    if (xmin <= t && t <= xmax) {
+      int b = (t == xmax) ? nbins - 1 : (int)((t - xmin) / bin_size);
+      if (b > nbins - 1) b = nbins - 1;
+      bins[2 * b] += v[0];
+      bins[2 * b + 1] += v[1];
+      counts[b] += 1.0;
+    } else {
+      *dropped += 1.0;
+    }
+    sre += v[0];
+    sim += v[1];
+    ssc += sc;
+    npts++;
+    ndom += (uint64_t)dom;
+  }
+  result[0] = sre;
+  result[1] = sim;
+  result[2] = (double)npts;
+  result[3] = (double)ndom;
+  result[4] = ssc;
+  return st;
+}

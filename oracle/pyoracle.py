@@ -87,6 +87,9 @@ class Oracle:
                                    C.POINTER(Warper), C.c_int, C.c_int, _U32, _U32, C.c_int, C.c_uint32, C.c_int64,
                                    C.c_int, C.c_int, _D]
         L.or_compare_3way.argtypes = [C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int]
+        L.or_integrate_binned.argtypes = [C.POINTER(Model), C.POINTER(GfIndex), C.POINTER(GfIndex), C.c_double,
+                                          C.POINTER(Warper), C.c_int, C.c_int, _U32, _U32, C.c_int, C.c_uint32,
+                                          C.c_int64, C.c_int, C.c_double, C.c_double, _D, _D, _D, _D]
 
     # --- Sobol -------------------------------------------------------------
     def sobol_matrices(self, dim, m=32):
@@ -218,6 +221,24 @@ class Oracle:
                                    seed + 1, nr_steps, rank, world, _dp(res))
         assert st == 0
         return complex(res[0], res[1]), int(res[2]), int(res[3]), res[4]
+
+    def integrate_binned(self, model, A, B, chain, order, nr_steps, nbins, xmin, xmax, seed=0, cutoff=0.0,
+                         do_shift=False, do_scramble=False, seed_shift=0):
+        """integrator<binner_t<1>, integrand_g_direct_time>::run: (sum f*J, n_points, n_in_domain,
+        sum of scales, bins complex[nbins], counts[nbins], dropped)."""
+        Csr, shfr = self.sobol_setup(order, 31, do_shift, do_scramble, seed_shift)
+        arr = chain_array(chain)
+        res = np.zeros(5)
+        bins = np.zeros(2 * nbins)
+        counts = np.zeros(nbins)
+        dropped = np.zeros(1)
+        st = self.lib.or_integrate_binned(C.byref(model), C.byref(GfIndex(*A)), C.byref(GfIndex(*B)), cutoff, arr,
+                                          len(chain), order, Csr.ctypes.data_as(_U32), shfr.ctypes.data_as(_U32), 31,
+                                          seed + 1, nr_steps, nbins, xmin, xmax, _dp(res), _dp(bins), _dp(counts),
+                                          _dp(dropped))
+        assert st == 0
+        return (complex(res[0], res[1]), int(res[2]), int(res[3]), res[4], bins.view(np.complex128),
+                counts.astype(np.int64), int(dropped[0]))
 
     def compare_3way(self, a, b):
         return self.lib.or_compare_3way(a[0], a[1], a[2], b[0], b[1], b[2])

@@ -119,3 +119,49 @@ def test_horvatic_zlatic_series(ctx, keldy_tests, run):
         q = -1j * i_n[n % 4] * s / npts
         tol = cfg["rtol"][0] if n < 5 else cfg["rtol"][1]
         assert abs(q - hz[n]) <= tol * abs(hz[n]), (n, q, hz[n])
+
+
+def test_flat_band_orders_1_4_full_size_vs_oracle(ctx, oracle):
+    """Orders 1..4 with 2^16 Sobol points each on the flat-band dot at beta = 50, t = 10,
+    g0 on 10,001 points (10,000 raised to odd), with the product-1D 1/t ("identity on
+    [0, t]") warper and with the plasma + exponential chain, against the CPU oracle."""
+    from keldy_b200.g0_tables import flatband
+    _, le, gr = flatband(1.0, 0.0, 0.0, 50.0, 10.0, 10001)
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    for chain in (UNIFORM, PLASMA_EXP):
+        for n in (1, 2, 3, 4):
+            (s, npts, nd, _), = capi.integrate(ctx, [_item(gm, ctx.sobol(n), chain, n, 1 << 16)])
+            w, onp, ond, sc = oracle.integrate(om, CHARGE[0], CHARGE[1], chain, n, 1 << 16)
+            assert (npts, nd) == (onp, ond)
+            assert abs(s - w) <= 1e-12 * sc, (n, abs(s - w) / sc)
+
+
+def test_biased_dot_high_orders_vs_oracle(ctx, oracle):
+    """The biased dot (V = 1, eps_d = 0.5, beta = 100, t_max = 50, 100,001 mesh points, GPU
+    builder), charge at t = 50, orders 6..12: integrate against the oracle on the same
+    table and Sobol points."""
+    gm, = capi.flatband_models(ctx, [(1.0, 0.5, 1.0, 100.0)], 50.0, 100001)
+    le, gr = gm.table()
+    om = oracle.model(50.0, le, gr)
+    chain = [(capi.WARPER_PLASMA_UV, 50.0, 0.0), (capi.WARPER_EXPONENTIAL, 50.0, 1.0)]
+    A, B = (50.0, 0, 0, 0, 0), (50.0, 0, 1, 0, 0)
+    for n, npts in ((6, 256), (8, 64), (10, 12), (12, 3)):
+        (s, np_, nd, _), = capi.integrate(ctx, [_item(gm, ctx.sobol(n), chain, n, npts, A=A, B=B)])
+        w, onp, ond, sc = oracle.integrate(om, A, B, chain, n, npts)
+        assert (np_, nd) == (onp, ond)
+        assert abs(s - w) <= 1e-12 * sc, (n, abs(s - w) / sc)
+
+
+def test_model_sweep_batched_equals_separate(ctx):
+    """Many models with their own GPU-built tables and uneven orders in one launch give the
+    same sums as one call per model."""
+    params = [(1.0, e, v, b) for b in (10.0, 200.0) for v in (0.0, 1.3) for e in (-1.0, 0.2, 0.9)]
+    models = capi.flatband_models(ctx, params, 20.0, 20001)
+    chain = [(capi.WARPER_PLASMA_UV, 20.0, 0.0), (capi.WARPER_EXPONENTIAL, 20.0, 1.0)]
+    rngs = {n: ctx.sobol(n) for n in range(2, 11)}
+    items = [_item(m, rngs[2 + i % 9], chain, 2 + i % 9, 1500 - 60 * (i % 9), A=(20.0, 0, 0, 0, 0),
+                   B=(20.0, 0, 1, 0, 0)) for i, m in enumerate(models)]
+    batched = capi.integrate(ctx, items)
+    for it, b in zip(items, batched):
+        assert capi.integrate(ctx, [it])[0] == b
