@@ -215,6 +215,23 @@ typedef struct {
 int kb_integrate_binned(kb_context *ctx, const kb_work *work, int n_work, int algo, const kb_time_bins *bins,
                         kb_accum *acc, double *bin_sums, uint64_t *bin_counts, uint64_t *dropped);
 
+/* The kernel method (integrand_g_kernel, impurity_oneband/wick_kernel.cpp:42-138, with
+ * first_row_expansion, det_expansion.hpp:44-74; compute_gf_kernel, compute_obs.hpp:105-117):
+ * the fixed point X = work[i].f.A (f.B and the cutoff are not used). For every Keldysh
+ * configuration a, the first-row cofactors x of s1 (X first, then the vertices picked by
+ * a; keldy's zeroed entry (n, n) kept) times (-1)^|a| det(s2_a); vertex i's term goes to
+ * the bin of (its time, a_i) of binner_t<1, 1>(xmin, xmax, nbins) x {forward, backward}.
+ * bin_sums[n_work][nbins][2] (interleaved complex), bin_counts[n_work][nbins][2] (values
+ * added), dropped[n_work]: added to; acc: the sum of all terms and the point counts.
+ * Orders 1..10; no learned flows. */
+int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const kb_time_bins *bins, kb_accum *acc,
+                        double *bin_sums, uint64_t *bin_counts, uint64_t *dropped);
+/* integrand_g_kernel::operator()(times, keep_u_hypercube) for count points of `order` vertex
+ * times: out[count][order][2] (interleaved complex) = the point's terms summed per (vertex i,
+ * Keldysh index k), the sums of the pairs keldy's wick_kernel_test compares; in_domain. */
+int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_index *X, int order, int64_t count,
+                             const double *times, int keep_u_hypercube, double *out, int *in_domain);
+
 /* Integrate without allocating device memory. No counterpart in keldy: this entry point
  * is for callers that cannot call cudaMalloc (a host application whose own allocator
  * owns the device's memory, or a latency-bound loop that must not pay cudaMalloc's

@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <memory>
 #include <mutex>
+#include <array>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -584,6 +585,136 @@ class integrator_g_direct_time : public integrator_g_direct {
     r *= dcomplex(1.0 / double(reduce_nr_points_run()));
     return r;
   }
+};
+
+// keldy::binner::binner_t<1, 1> of the kernel method: [xmin, xmax] in nr_bins time bins x
+// the Keldysh index (forward, backward).
+class binner_2d {
+  double xmin_ = 0.0, xmax_ = 1.0, bin_size_ = 1.0;
+  std::vector<dcomplex> data_; // [bin][k]
+  std::vector<long> nr_values_added_;
+
+ public:
+  long nr_values_dropped = 0;
+  binner_2d(double xmin, double xmax, long nr_bins) : xmin_(xmin), xmax_(xmax) {
+    if (xmin >= xmax)
+      throw std::runtime_error("Boundaries of binning range are in wrong order (" + std::to_string(xmin) +
+                               " >= " + std::to_string(xmax) + ")");
+    if (nr_bins < 1 || nr_bins > 4096) throw std::runtime_error("the number of time bins must be in [1, 4096]");
+    bin_size_ = (xmax - xmin) / double(nr_bins);
+    data_.assign(2 * (size_t)nr_bins, dcomplex(0.0));
+    nr_values_added_.assign(2 * (size_t)nr_bins, 0);
+  }
+  std::vector<dcomplex> const &get_data_flat() const { return data_; }
+  std::vector<long> const &get_nr_values_added_flat() const { return nr_values_added_; }
+  long get_nr_values_dropped() const { return nr_values_dropped; }
+  int get_nr_bins() const { return (int)(data_.size() / 2); }
+  double get_bin_size() const { return bin_size_; }
+  double get_xmin() const { return xmin_; }
+  double get_xmax() const { return xmax_; }
+  std::vector<double> get_bin_coord() const {
+    std::vector<double> c(data_.size() / 2);
+    for (size_t i = 0; i < c.size(); ++i) c[i] = xmin_ + (double(i) + 0.5) * bin_size_;
+    return c;
+  }
+  binner_2d &operator*=(dcomplex s) {
+    for (auto &v : data_) v *= s;
+    return *this;
+  }
+  void add(const double *sums, const uint64_t *counts, uint64_t dropped) {
+    for (size_t b = 0; b < data_.size(); ++b) {
+      data_[b] += dcomplex(sums[2 * b], sums[2 * b + 1]);
+      nr_values_added_[b] += (long)counts[b];
+    }
+    nr_values_dropped += (long)dropped;
+  }
+};
+
+// integrand_g_kernel (wick_kernel.cpp:42-138): fixed point X; operator() returns, per
+// vertex i and Keldysh index k, the sum of the terms keldy accumulates at (u_i, k).
+class integrand_g_kernel {
+  g0_keldysh_contour_t g0_;
+  gf_index_t X_;
+
+ public:
+  integrand_g_kernel(g0_keldysh_contour_t g0, gf_index_t X) : g0_(std::move(g0)), X_(X) {}
+  std::pair<std::vector<std::array<dcomplex, 2>>, int> operator()(std::vector<double> const &times,
+                                                                    bool keep_u_hypercube = true) const {
+    const int n = (int)times.size();
+    std::vector<double> out(4 * (size_t)n);
+    int dom = 0;
+    kb_gf_index x = X_.abi();
+    keldy_b200::check(kb_integrand_kernel_eval(keldy_b200::default_context(), g0_.model.handle(), &x, n, 1,
+                                               times.data(), keep_u_hypercube, out.data(), &dom));
+    std::vector<std::array<dcomplex, 2>> r((size_t)n);
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 2; ++k) r[(size_t)i][(size_t)k] = dcomplex(out[4 * i + 2 * k], out[4 * i + 2 * k + 1]);
+    return {r, dom};
+  }
+  g0_keldysh_contour_t const &get_g0() const { return g0_; }
+  gf_index_t const &get_X() const { return X_; }
+};
+
+// integrator<binner_t<1, 1>, integrand_g_kernel> + compute_gf_kernel (compute_obs.hpp:105-117):
+// G(t) by the kernel method, binned over [0, t] x Keldysh index.
+class compute_gf_kernel {
+  int dimension = 1;
+  binner_2d bins_;
+  uint64_t n_points = 0;
+  uint64_t n_integrand_evals_in_domain = 0;
+  integrand_g_kernel integrand;
+  sobol rng_;
+
+ public:
+  warpers::warper_train_t warper{};
+
+  compute_gf_kernel(g0_model model, double time, int order, int nr_bins = 100)
+     : dimension(order), bins_(0.0, time, nr_bins),
+       integrand(g0_keldysh_contour_t{std::move(model)}, gf_index_t{time, up, forward}),
+       rng_(order > 0 ? order : 1, 0) {
+    if (dimension <= 0) throw std::runtime_error("Dimension of the integration space must be > 0.");
+  }
+
+  void run(int nr_steps) {
+    if (nr_steps <= 0) return;
+    if ((uint64_t)rng_.state() + (uint64_t)nr_steps > (1ull << 31))
+      throw std::runtime_error("More sample points requested then generator can hold.");
+    auto const &chain = warper.chain();
+    kb_gf_index x = integrand.get_X().abi();
+    kb_work w{integrand.get_g0().model.handle(), rng_.handle(), chain.data(), (int)chain.size(),
+              kb_integrand{x, x, 0.0}, dimension, rng_.state() + 1, nr_steps};
+    kb_time_bins tb{bins_.get_nr_bins(), bins_.get_xmin(), bins_.get_xmax()};
+    std::vector<double> sums(4 * (size_t)tb.nbins, 0.0);
+    std::vector<uint64_t> counts(2 * (size_t)tb.nbins, 0);
+    uint64_t dropped = 0;
+    kb_accum acc{};
+    keldy_b200::check(kb_integrate_kernel(keldy_b200::default_context(), &w, 1, &tb, &acc, sums.data(),
+                                          counts.data(), &dropped));
+    rng_.discard(nr_steps);
+    bins_.add(sums.data(), counts.data(), dropped);
+    n_points += acc.n_points;
+    n_integrand_evals_in_domain += acc.n_in_domain;
+  }
+
+  void reset_rng(std::string rng_name, int rng_state_seed, bool do_shift = false, bool do_scramble = false,
+                 int rng_seed_shift = 0) {
+    if (rng_name == "sobol_unshifted")
+      rng_ = sobol(dimension, rng_state_seed);
+    else if (rng_name == "sobol")
+      rng_ = sobol(dimension, rng_state_seed, do_shift, do_scramble, rng_seed_shift);
+    else
+      throw std::runtime_error("rng '" + rng_name + "' has no device form; use sobol_unshifted or sobol");
+  }
+
+  binner_2d reduce_result() const {
+    binner_2d r = bins_;
+    r *= dcomplex(1.0 / double(n_points));
+    return r;
+  }
+  uint64_t reduce_nr_points_run() const { return n_points; }
+  uint64_t reduce_nr_points_in_domain() const { return n_integrand_evals_in_domain; }
+  integrand_g_kernel get_integrand() const { return integrand; }
+  warpers::warper_train_t get_warper() const { return warper; }
 };
 
 // compute_obs.hpp:85-101: charge G^<_{up,up}(t, t) binned over [0, t] in nr_time_slices.

@@ -36,6 +36,7 @@ EXPORTS = [
     "kb_plan_result", "kb_plan_set_k_first", "kb_context_set_launch", "kb_context_get_launch",
     "kb_flow_create", "kb_flow_destroy", "kb_flow_dim", "kb_flow_get_params", "kb_flow_set_params", "kb_flow_map",
     "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
+    "kb_integrate_kernel", "kb_integrand_kernel_eval",
 ]
 FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
 FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
@@ -126,6 +127,9 @@ def load():
     L.kb_evaluate_warped.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, C.c_int, C.c_int,
                                      C.c_int64, _D, C.c_int, C.c_int, _D, _D, _I]
     L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
+    L.kb_integrate_kernel.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(TimeBins), C.POINTER(Accum), _D,
+                                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.kb_integrand_kernel_eval.argtypes = [_VP, _VP, C.POINTER(GfIndex), C.c_int, C.c_int64, _D, C.c_int, _D, _I]
     L.kb_integrate_binned.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(TimeBins), C.POINTER(Accum),
                                       _D, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.kb_fp64_peak.argtypes = [_VP, C.c_int, _D]
@@ -375,6 +379,17 @@ class Model:
                                            _dp(sc)))
         return (out, dom, sc) if want_scale else (out, dom)
 
+    def integrand_kernel(self, X, times, keep_u_hypercube=True):
+        """integrand_g_kernel for fixed point X: (sums [count][order][2] complex per (vertex,
+        Keldysh index), in_domain)."""
+        times = np.ascontiguousarray(np.atleast_2d(times), dtype=np.float64)
+        count, n = times.shape
+        out = np.empty((count, n, 2), dtype=np.complex128)
+        dom = np.empty(count, dtype=np.int32)
+        check(self.ctx.L.kb_integrand_kernel_eval(self.ctx.h, self.h, C.byref(gf_index(X)), n, count, _dp(times),
+                                                  int(keep_u_hypercube), _dp(out.view(np.float64)), _ip(dom)))
+        return out, dom
+
     def integrand_no_det(self, A, B, times, cutoff=0.0, keep_u_hypercube=True):
         times = np.ascontiguousarray(np.atleast_2d(times), dtype=np.float64)
         count, n = times.shape
@@ -479,6 +494,23 @@ def integrate_binned(ctx, items, nbins, xmin, xmax, algo=ALGO_AUTO):
                                     acc, _dp(sums.view(np.float64)), counts.ctypes.data_as(U),
                                     dropped.ctypes.data_as(U)))
     return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback, sums[i], counts[i].astype(np.int64),
+             int(dropped[i])) for i, a in enumerate(acc[:n])]
+
+
+def integrate_kernel(ctx, items, nbins, xmin, xmax):
+    """kb_integrate_kernel (keldy's kernel method, fixed point X = item["A"]): per item (sum,
+    n_points, n_in_domain, bins complex[nbins][2], counts[nbins][2], dropped)."""
+    items = [dict(it, B=it.get("B", it["A"])) for it in items]
+    works, keep = _works(items)
+    n = len(items)
+    acc = (Accum * max(1, n))()
+    sums = np.zeros((max(1, n), nbins, 2), dtype=np.complex128)
+    counts = np.zeros((max(1, n), nbins, 2), dtype=np.uint64)
+    dropped = np.zeros(max(1, n), dtype=np.uint64)
+    U = C.POINTER(C.c_uint64)
+    check(ctx.L.kb_integrate_kernel(ctx.h, works, n, C.byref(TimeBins(int(nbins), float(xmin), float(xmax))), acc,
+                                    _dp(sums.view(np.float64)), counts.ctypes.data_as(U), dropped.ctypes.data_as(U)))
+    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, sums[i], counts[i].astype(np.int64),
              int(dropped[i])) for i, a in enumerate(acc[:n])]
 
 

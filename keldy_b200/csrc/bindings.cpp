@@ -216,4 +216,27 @@ PYBIND11_MODULE(_keldy, m) {
                  .def(py::init<g0_model, double, int, int, double>(), py::arg("model"), py::arg("time"),
                       py::arg("order"), py::arg("nr_time_slices"), py::arg("cutoff_integrand"));
   integrator_methods<compute_charge_Q_direct_time>(cqt);
+  py::class_<binner_2d>(m, "BinnerT11")
+      .def(py::init<double, double, long>(), py::arg("xmin"), py::arg("xmax"), py::arg("nr_bins"))
+      .def("get_data_flat", &binner_2d::get_data_flat)
+      .def("get_nr_values_added_flat", &binner_2d::get_nr_values_added_flat)
+      .def("get_nr_values_dropped", &binner_2d::get_nr_values_dropped)
+      .def("get_nr_bins", &binner_2d::get_nr_bins)
+      .def("get_bin_size", &binner_2d::get_bin_size)
+      .def("get_bin_coord", &binner_2d::get_bin_coord);
+  py::class_<integrand_g_kernel>(m, "IntegrandGKernel")
+      .def(py::init<g0_keldysh_contour_t, gf_index_t>(), py::arg("g0"), py::arg("g_idx_X"))
+      .def("__call__", &integrand_g_kernel::operator(), py::arg("times"), py::arg("keep_u_hypercube") = true);
+  py::class_<compute_gf_kernel>(m, "ComputeGfKernel")
+      .def(py::init<g0_model, double, int, int>(), py::arg("model"), py::arg("time"), py::arg("order"),
+           py::arg("nr_bins") = 100)
+      .def_readwrite("warper", &compute_gf_kernel::warper)
+      .def("run", &compute_gf_kernel::run, py::arg("nr_steps"), py::call_guard<py::gil_scoped_release>())
+      .def("reset_rng", &compute_gf_kernel::reset_rng, py::arg("rng_name"), py::arg("rng_state_seed"),
+           py::arg("do_shift") = false, py::arg("do_scramble") = false, py::arg("rng_seed_shift") = 0)
+      .def("reduce_result", &compute_gf_kernel::reduce_result)
+      .def("reduce_nr_points_run", &compute_gf_kernel::reduce_nr_points_run)
+      .def("reduce_nr_points_in_domain", &compute_gf_kernel::reduce_nr_points_in_domain)
+      .def("get_integrand", &compute_gf_kernel::get_integrand)
+      .def("get_warper", &compute_gf_kernel::get_warper);
 }

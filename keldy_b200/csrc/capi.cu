@@ -768,6 +768,7 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
       KB_CUDA(doc.alloc(sorted.size() * nb * sizeof(unsigned long long), st));
       KB_CUDA(dod.alloc(sorted.size() * sizeof(unsigned long long), st));
       L.nbins = bins->nbins;
+      L.bin_cols = 1;
       L.bin_xmin = bins->xmin;
       L.bin_xmax = bins->xmax;
       L.bin_size = (bins->xmax - bins->xmin) / bins->nbins;
@@ -894,6 +895,152 @@ int kb_integrate_binned(kb_context *ctx, const kb_work *work, int n_work, int al
                                   " >= " + std::to_string(bins->xmax) + ")");
   TimeBins tb{bins->nbins, bins->xmin, bins->xmax, bin_sums, bin_counts, dropped};
   return integrate_impl(ctx, work, n_work, algo, acc, &tb);
+}
+
+int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const kb_time_bins *bins, kb_accum *acc,
+                        double *bin_sums, uint64_t *bin_counts, uint64_t *dropped) {
+  KB_CHECK(ctx && bins && (n_work == 0 || (work && acc && bin_sums && bin_counts && dropped)),
+           "kb_integrate_kernel: null argument");
+  KB_CHECK(bins->nbins >= 1 && bins->nbins <= 4096, "the number of time bins must be in [1, 4096]");
+  if (!(bins->xmin < bins->xmax))
+    return fail(KB_E_INVALID, "Boundaries of binning range are in wrong order (" + std::to_string(bins->xmin) +
+                                  " >= " + std::to_string(bins->xmax) + ")");
+  if (n_work == 0) return KB_OK;
+  std::vector<ItemDev> items((size_t)n_work);
+  std::vector<long long> offs(1, 0);
+  for (int i = 0; i < n_work; ++i) {
+    int tree = 0;
+    kb_work w = work[i];
+    w.f.B = w.f.A; // the fixed point X (integrand_g_kernel has one external point and no cutoff)
+    w.f.cutoff = 0.0;
+    int st = work_item(ctx, w, KB_ALGO_AUTO, items[(size_t)i], tree);
+    if (st) return st;
+    KB_CHECK(work[i].order <= KM_MAX_ORDER, "the kernel method runs orders 1..10");
+    KB_CHECK(!work[i].flow, "the kernel method does not take a learned flow");
+    items[(size_t)i].chunk_points = 16; // a CTA evaluates its chunk's points one after another
+    offs.push_back(offs.back() + (items[(size_t)i].n_points + 15) / 16);
+  }
+  const long long nchunks = offs.back();
+  if (nchunks > INT32_MAX) return fail(KB_E_INVALID, "too many points in one call");
+  if (nchunks == 0) return KB_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const size_t nb = 2 * (size_t)bins->nbins;
+  DevBuf ditems, doff, dcnt, dpart, dacc, dbs, dbc, dbd, dos, doc, dod;
+  KB_CUDA(ditems.alloc(items.size() * sizeof(ItemDev), st));
+  KB_CUDA(doff.alloc(offs.size() * sizeof(long long), st));
+  KB_CUDA(dcnt.alloc(sizeof(int), st));
+  KB_CUDA(dpart.alloc((size_t)nchunks * sizeof(ChunkPartial), st));
+  KB_CUDA(dacc.alloc(items.size() * sizeof(kb_accum), st));
+  KB_CUDA(dbs.alloc((size_t)nchunks * nb * sizeof(double2), st));
+  KB_CUDA(dbc.alloc((size_t)nchunks * nb * sizeof(unsigned), st));
+  KB_CUDA(dbd.alloc((size_t)nchunks * sizeof(unsigned), st));
+  KB_CUDA(dos.alloc(items.size() * nb * sizeof(double2), st));
+  KB_CUDA(doc.alloc(items.size() * nb * sizeof(unsigned long long), st));
+  KB_CUDA(dod.alloc(items.size() * sizeof(unsigned long long), st));
+  KB_CUDA(cudaMemcpyAsync(ditems.p, items.data(), items.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(doff.p, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(int), st));
+  KB_CUDA(cudaMemsetAsync(dacc.p, 0, items.size() * sizeof(kb_accum), st));
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.items = ditems.as<ItemDev>();
+  L.n_items = n_work;
+  L.chunk_offsets = doff.as<long long>();
+  L.n_chunks = (int)nchunks;
+  L.chunk_counter = dcnt.as<int>();
+  L.mode = IN_SOBOL;
+  L.partials = dpart.as<ChunkPartial>();
+  L.nbins = bins->nbins;
+  L.bin_cols = 2;
+  L.bin_xmin = bins->xmin;
+  L.bin_xmax = bins->xmax;
+  L.bin_size = (bins->xmax - bins->xmin) / bins->nbins;
+  L.bin_sums = dbs.as<double2>();
+  L.bin_counts = dbc.as<unsigned>();
+  L.bin_dropped = dbd.as<unsigned>();
+  L.err = ctx->d_err;
+  KB_CUDA(launch_kernel_method(L, (int)std::min<long long>(nchunks, (long long)ctx->sm_count * 4), st));
+  KB_CUDA(launch_reduce(L, dacc.as<kb_accum>(), st));
+  KB_CUDA(launch_reduce_bins(L, dos.as<double2>(), doc.as<unsigned long long>(), dod.as<unsigned long long>(), st));
+  std::vector<kb_accum> part(items.size());
+  std::vector<double> hbs(items.size() * nb * 2);
+  std::vector<unsigned long long> hbc(items.size() * nb), hbd(items.size());
+  KB_CUDA(cudaMemcpyAsync(part.data(), dacc.p, part.size() * sizeof(kb_accum), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(hbs.data(), dos.p, hbs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(hbc.data(), doc.p, hbc.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(hbd.data(), dod.p, hbd.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  for (int w = 0; w < n_work; ++w) {
+    acc[w].sum_re += part[(size_t)w].sum_re;
+    acc[w].sum_im += part[(size_t)w].sum_im;
+    acc[w].n_points += part[(size_t)w].n_points;
+    acc[w].n_in_domain += part[(size_t)w].n_in_domain;
+    for (size_t b = 0; b < nb; ++b) {
+      bin_sums[2 * ((size_t)w * nb + b)] += hbs[2 * ((size_t)w * nb + b)];
+      bin_sums[2 * ((size_t)w * nb + b) + 1] += hbs[2 * ((size_t)w * nb + b) + 1];
+      bin_counts[(size_t)w * nb + b] += hbc[(size_t)w * nb + b];
+    }
+    dropped[w] += hbd[(size_t)w];
+  }
+  return KB_OK;
+}
+
+int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_index *X, int order, int64_t count,
+                             const double *times, int keep_u_hypercube, double *out, int *in_domain) {
+  KB_CHECK(ctx && m && X, "kb_integrand_kernel_eval: null argument");
+  KB_CHECK(order >= 1 && order <= KM_MAX_ORDER, "the kernel method runs orders 1..10");
+  KB_CHECK(count >= 0 && (count == 0 || (times && out)), "kb_integrand_kernel_eval: null buffer");
+  kb_integrand f{*X, *X, 0.0};
+  int st = check_integrand(m, &f, order);
+  if (st) return st;
+  if (count == 0) return KB_OK;
+  ItemDev it = make_item(m, &f, order);
+  it.n_points = count;
+  it.chunk_points = 16;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t s = ctx->stream;
+  const long long nchunks = (count + 15) / 16;
+  long long offs[2] = {0, nchunks};
+  DevBuf ditem, doff, dcnt, din, dout, ddom;
+  KB_CUDA(ditem.alloc(sizeof(ItemDev), s));
+  KB_CUDA(doff.alloc(sizeof(offs), s));
+  KB_CUDA(dcnt.alloc(sizeof(int), s));
+  KB_CUDA(din.alloc((size_t)count * order * sizeof(double), s));
+  KB_CUDA(dout.alloc((size_t)count * 2 * order * sizeof(double2), s));
+  KB_CUDA(ddom.alloc((size_t)count * sizeof(int), s));
+  KB_CUDA(cudaMemcpyAsync(ditem.p, &it, sizeof(ItemDev), cudaMemcpyHostToDevice, s));
+  KB_CUDA(cudaMemcpyAsync(doff.p, offs, sizeof(offs), cudaMemcpyHostToDevice, s));
+  KB_CUDA(cudaMemcpyAsync(din.p, times, (size_t)count * order * sizeof(double), cudaMemcpyHostToDevice, s));
+  KB_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(int), s));
+  KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+  Launch L;
+  memset(&L, 0, sizeof(L));
+  L.items = ditem.as<ItemDev>();
+  L.n_items = 1;
+  L.chunk_offsets = doff.as<long long>();
+  L.n_chunks = (int)nchunks;
+  L.chunk_counter = dcnt.as<int>();
+  L.mode = IN_TIMES;
+  L.keep_u_hypercube = keep_u_hypercube;
+  L.in = din.as<double>();
+  L.out_kvals = dout.as<double2>();
+  L.out_dom = ddom.as<int>();
+  L.err = ctx->d_err;
+  KB_CUDA(launch_kernel_method(L, (int)std::min<long long>(nchunks, (long long)ctx->sm_count * 4), s));
+  int err = 0;
+  KB_CUDA(cudaMemcpyAsync(out, dout.p, (size_t)count * 2 * order * sizeof(double2), cudaMemcpyDeviceToHost, s));
+  if (in_domain) KB_CUDA(cudaMemcpyAsync(in_domain, ddom.p, (size_t)count * sizeof(int), cudaMemcpyDeviceToHost, s));
+  KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  KB_CUDA(cudaStreamSynchronize(s));
+  if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
+  return KB_OK;
 }
 
 } // extern "C"

@@ -51,7 +51,9 @@ struct Launch {
   // IN_SOBOL with time bins (integrand_g_direct_time): every point's f*J also goes to the
   // bin of its earliest vertex time; per chunk: sums [n_chunks][nbins], counts, dropped
   int nbins; // 0: no bins
+  int bin_cols; // values per time bin: 1 (time-binned direct integrand), 2 (kernel method: Keldysh index)
   double bin_xmin, bin_xmax, bin_size;
+  double2 *out_kvals; // kernel method, IN_TIMES: per point the 2n sums (vertex i, Keldysh index k) at [2i + k]
   double2 *bin_sums;
   unsigned *bin_counts;
   unsigned *bin_dropped; // [n_chunks]
@@ -70,6 +72,10 @@ cudaError_t launch_fallback(const Launch &L, int grid, cudaStream_t st);
 cudaError_t launch_reduce(const Launch &L, kb_accum *acc_dev, cudaStream_t st);
 // per item: bin sums [n_items][nbins], counts [n_items][nbins], dropped [n_items] summed
 // over the item's chunks in chunk order (written, not added)
+// keldy's kernel-method integrand (integrand_g_kernel): IN_SOBOL with time bins of 2
+// columns, or IN_TIMES into out_kvals. Orders 1..KM_MAX_ORDER.
+constexpr int KM_MAX_ORDER = 10;
+cudaError_t launch_kernel_method(const Launch &L, int grid, cudaStream_t st);
 cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long long *counts,
                                unsigned long long *dropped, cudaStream_t st);
 

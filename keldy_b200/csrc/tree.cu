@@ -915,20 +915,241 @@ __global__ void __launch_bounds__(NT) reduce_kernel(Launch L, kb_accum *acc) {
   }
 }
 
+// ------------------------------------------------------------ kernel method
+// keldy's integrand_g_kernel (impurity_oneband/wick_kernel.cpp:42-138): with the fixed
+// point X in the external slot, for every Keldysh configuration a the matrix s1 (X first,
+// then the vertex copies picked by a; keldy zeroes its entry (n, n)) is factored with
+// partial pivoting and the first row of its cofactor matrix is found by solving
+// s1 x = det(s1) e_0 (first_row_expansion, det_expansion.hpp:44-74). Vertex i's term is
+// x_{i+1} (-1)^|a| det(s2_a), accumulated at (vertex time, a_i). Here the terms of a point
+// are summed per (vertex i, Keldysh index k) in configuration order (2n sums), then
+// binned; keldy accumulates them one by one into the same bins.
+struct KernelShared {
+  double2 G1[(2 * KM_MAX_ORDER + 1) * (2 * KM_MAX_ORDER + 1)];
+  double2 G2[(2 * KM_MAX_ORDER) * (2 * KM_MAX_ORDER)];
+  double u[KM_MAX_ORDER];
+  double jac[1];
+  int flag[1];
+  double2 X[NT][KM_MAX_ORDER];
+  double2 S[2 * KM_MAX_ORDER];
+};
+
+// LU with partial pivoting (first maximum of |re|+|im|) of the m x m matrix a, then the
+// solve a x = det(a) e_0 (row interchanges, unit-lower then upper substitution).
+__device__ void first_row_cofactors(double2 *a, int m, double2 *x) {
+  int piv[KM_MAX_ORDER + 1];
+  double2 det = c2(1.0, 0.0);
+  bool neg = false;
+  for (int k = 0; k < m; ++k) {
+    int p = k;
+    double best = cabs1(a[k * m + k]);
+    for (int i = k + 1; i < m; ++i) {
+      const double v = cabs1(a[i * m + k]);
+      if (v > best) {
+        best = v;
+        p = i;
+      }
+    }
+    piv[k] = p;
+    if (p != k) {
+      for (int j = 0; j < m; ++j) {
+        const double2 t = a[k * m + j];
+        a[k * m + j] = a[p * m + j];
+        a[p * m + j] = t;
+      }
+      neg = !neg;
+    }
+    const double2 pv = a[k * m + k];
+    det = cmul(det, pv);
+    if (best == 0.0) continue;
+    const double2 inv = crcp(pv);
+    for (int i = k + 1; i < m; ++i) {
+      const double2 l = cmul(a[i * m + k], inv);
+      a[i * m + k] = l;
+      for (int j = k + 1; j < m; ++j) a[i * m + j] = cfms(a[i * m + j], l, a[k * m + j]);
+    }
+  }
+  if (neg) det = c2(-det.x, -det.y);
+  for (int i = 0; i < m; ++i) x[i] = c2(0.0, 0.0);
+  x[0] = det;
+  for (int k = 0; k < m; ++k)
+    if (piv[k] != k) {
+      const double2 t = x[k];
+      x[k] = x[piv[k]];
+      x[piv[k]] = t;
+    }
+  for (int i = 1; i < m; ++i)
+    for (int j = 0; j < i; ++j) x[i] = cfms(x[i], a[i * m + j], x[j]);
+  for (int i = m - 1; i >= 0; --i) {
+    for (int j = i + 1; j < m; ++j) x[i] = cfms(x[i], a[i * m + j], x[j]);
+    x[i] = cmul(x[i], crcp(a[i * m + i]));
+  }
+}
+
+// The 2n sums of one point (inputs in K.u, K.flag): thread t < 2n returns sum (i = t/2, k = t%2).
+__device__ double2 kernel_point(KernelShared &K, const ItemDev &it, int N, int *bad) {
+  const int tid = threadIdx.x;
+  const kb_gf_index X = it.f.A;
+  const int spin = X.spin;
+  const int M1 = 2 * N + 1, M2 = 2 * N;
+  for (int e = tid; e < M1 * M1 + M2 * M2; e += blockDim.x) {
+    const bool first = e < M1 * M1;
+    const int q = first ? e : e - M1 * M1, M = first ? M1 : M2;
+    const int r = q / M, c = q - r * M;
+    kb_gf_index a, b;
+    const int sp = first ? spin : 1 - spin;
+    if (first && r == 2 * N) {
+      a = X;
+      a.timesplit = N;
+    } else {
+      a.time = K.u[r % N];
+      a.spin = sp;
+      a.k_idx = r >= N ? 1 : 0;
+      a.timesplit = r % N;
+      a.orbital = 0;
+    }
+    if (first && c == 2 * N) {
+      b = X;
+      b.timesplit = N;
+    } else {
+      b.time = K.u[c % N];
+      b.spin = sp;
+      b.k_idx = c >= N ? 1 : 0;
+      b.timesplit = c % N;
+      b.orbital = 0;
+    }
+    const double2 g = g0_contour(it.model, a, b, (first && r == 2 * N && c == 2 * N) ? 0 : 1, bad);
+    if (first)
+      K.G1[q] = g;
+    else
+      K.G2[q] = g;
+  }
+  __syncthreads();
+  const unsigned nconf = 1u << N;
+  const int ti = tid >> 1, tk = tid & 1;
+  double2 acc = c2(0.0, 0.0);
+  for (unsigned base = 0; base < nconf; base += blockDim.x) {
+    const unsigned cfg = base + tid;
+    if (cfg < nconf) {
+      double2 m1[(KM_MAX_ORDER + 1) * (KM_MAX_ORDER + 1)], m2[KM_MAX_ORDER * KM_MAX_ORDER];
+      double2 x[KM_MAX_ORDER + 1];
+      int pick[KM_MAX_ORDER + 1];
+      pick[0] = 2 * N;
+      for (int i = 0; i < N; ++i) pick[i + 1] = i + (int)((cfg >> i) & 1u) * N;
+      for (int r = 0; r <= N; ++r)
+        for (int c = 0; c <= N; ++c) m1[r * (N + 1) + c] = K.G1[pick[r] * M1 + pick[c]];
+      m1[N * (N + 1) + N] = c2(0.0, 0.0);
+      for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c) m2[r * N + c] = K.G2[pick[r + 1] * M2 + pick[c + 1]];
+      first_row_cofactors(m1, N + 1, x);
+      double2 d2 = lu_det(m2, N);
+      if (__popc(cfg) & 1) d2 = c2(-d2.x, -d2.y);
+      for (int i = 0; i < N; ++i) K.X[tid][i] = cmul(x[i + 1], d2);
+    }
+    __syncthreads();
+    if (tid < 2 * N) {
+      const unsigned cnt = min((unsigned)blockDim.x, nconf - base);
+      for (unsigned c = 0; c < cnt; ++c)
+        if ((int)(((base + c) >> ti) & 1u) == tk) acc = cadd(acc, K.X[c][ti]);
+    }
+    __syncthreads();
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(NT) kernel_method_kernel(Launch L) {
+  __shared__ KernelShared K;
+  __shared__ int s_chunk;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_bad = 0;
+  const bool eval = L.mode != IN_SOBOL;
+  const int nb = L.nbins * L.bin_cols;
+  for (;;) {
+    if (tid == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
+    __syncthreads();
+    const int c = s_chunk;
+    if (c >= L.n_chunks) break;
+    const int item = find_item(L.chunk_offsets, L.n_items, c);
+    const ItemDev &it = L.items[item];
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * it.chunk_points;
+    const long long total = eval ? it.n_points : it.n_points;
+    const int ccount = (int)min((long long)it.chunk_points, total - cfirst);
+    const int N = it.order;
+    if (!eval) {
+      for (int b = tid; b < nb; b += blockDim.x) {
+        L.bin_sums[(size_t)c * nb + b] = c2(0.0, 0.0);
+        L.bin_counts[(size_t)c * nb + b] = 0u;
+      }
+      if (tid == 0) L.bin_dropped[c] = 0u;
+    }
+    double2 csum = c2(0.0, 0.0);
+    unsigned long long cdom = 0;
+    for (int p = 0; p < ccount; ++p) {
+      const long long gp = cfirst + p;
+      load_points(L, it, N, 1, gp, K.u, K.jac, K.flag, L.mode == IN_SOBOL ? true : (L.keep_u_hypercube != 0));
+      __syncthreads();
+      const bool dom = !(K.flag[0] & 1);
+      double2 v = c2(0.0, 0.0);
+      if (dom) v = kernel_point(K, it, N, &s_bad);
+      if (tid < 2 * N) K.S[tid] = v;
+      __syncthreads();
+      if (tid == 0) {
+        const double j = K.jac[0];
+        if (eval) {
+          for (int q = 0; q < 2 * N; ++q)
+            L.out_kvals[gp * 2 * N + q] = dom ? c2(K.S[q].x * j, K.S[q].y * j) : c2(0.0, 0.0);
+          if (L.out_jac) L.out_jac[gp] = j;
+          if (L.out_dom) L.out_dom[gp] = dom ? 1 : 0;
+        } else if (dom) {
+          cdom++;
+          const unsigned half = 1u << (N - 1);
+          for (int i = 0; i < N; ++i) {
+            const int bin = time_bin(L, K.u + i, 1, 1);
+            for (int k = 0; k < 2; ++k) {
+              const double2 s = K.S[2 * i + k];
+              csum = c2(csum.x + s.x * j, csum.y + s.y * j);
+              if (bin < 0) {
+                L.bin_dropped[c] += half;
+              } else {
+                double2 &bs = L.bin_sums[(size_t)c * nb + 2 * bin + k];
+                bs = c2(bs.x + s.x * j, bs.y + s.y * j);
+                L.bin_counts[(size_t)c * nb + 2 * bin + k] += half;
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (!eval && tid == 0) {
+      ChunkPartial pr;
+      pr.sum_re = csum.x;
+      pr.sum_im = csum.y;
+      pr.n_in_domain = cdom;
+      pr.n_fallback = 0;
+      pr.fb_mask[0] = pr.fb_mask[1] = 0;
+      L.partials[c] = pr;
+    }
+  }
+  if (tid == 0 && s_bad) atomicOr(L.err, 1);
+}
+
 // Thread t of block `item` sums bins t, t + NT, ... over the item's chunks in chunk order.
 __global__ void __launch_bounds__(NT) reduce_bins_kernel(Launch L, double2 *sums, unsigned long long *counts,
                                                          unsigned long long *dropped) {
   const int item = blockIdx.x;
   const long long c0 = L.chunk_offsets[item], c1 = L.chunk_offsets[item + 1];
-  for (int b = threadIdx.x; b < L.nbins; b += blockDim.x) {
+  const int nb = L.nbins * max(1, L.bin_cols);
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
     double2 s = c2(0.0, 0.0);
     unsigned long long n = 0;
     for (long long c = c0; c < c1; ++c) {
-      s = cadd(s, L.bin_sums[(size_t)c * L.nbins + b]);
-      n += L.bin_counts[(size_t)c * L.nbins + b];
+      s = cadd(s, L.bin_sums[(size_t)c * nb + b]);
+      n += L.bin_counts[(size_t)c * nb + b];
     }
-    sums[(size_t)item * L.nbins + b] = s;
-    counts[(size_t)item * L.nbins + b] = n;
+    sums[(size_t)item * nb + b] = s;
+    counts[(size_t)item * nb + b] = n;
   }
   if (threadIdx.x == 0) {
     unsigned long long d = 0;
@@ -938,6 +1159,11 @@ __global__ void __launch_bounds__(NT) reduce_bins_kernel(Launch L, double2 *sums
 }
 
 } // namespace
+
+cudaError_t launch_kernel_method(const Launch &L, int grid, cudaStream_t st) {
+  kernel_method_kernel<<<grid, NT, 0, st>>>(L);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long long *counts,
                                unsigned long long *dropped, cudaStream_t st) {

@@ -13,7 +13,8 @@ import warnings
 import numpy as np
 
 from . import g0_tables
-from ._keldy import (BinnerT1, ComputeChargeQDirect as _ComputeChargeQDirect,  # noqa: F401
+from ._keldy import (BinnerT1, BinnerT11, ComputeGfKernel as _ComputeGfKernel, IntegrandGKernel,  # noqa: F401
+                     ComputeChargeQDirect as _ComputeChargeQDirect,
                      ComputeChargeQDirectTime as _ComputeChargeQDirectTime,
                      ComputeCurrentJDirect as _ComputeCurrentJDirect, G0KeldyshContourT, G0ModelTables, GfIndexT,
                      IntegrandGDirect)
@@ -131,6 +132,20 @@ def ComputeChargeQDirectTime(model, time, order, nr_time_slices, cutoff_integran
                                      float(cutoff_integrand))
 
 
+def ComputeGfKernel(model, time, order, nr_bins=100):
+    """compute_gf_kernel(model or params, time, order, nr_bins) (compute_obs.hpp:105-117): G(t)
+    by the kernel method, binned over [0, time] x Keldysh index; reduce_result() returns the
+    binner (BinnerT11; get_data() gives the [nr_bins][2] array)."""
+    return _ComputeGfKernel(_model(model, False), float(time), int(order), int(nr_bins))
+
+
+def binner_data(b):
+    """The [nr_bins][2] data of a BinnerT11 (or [nr_bins] of a BinnerT1) as a numpy array."""
+    if isinstance(b, BinnerT11):
+        return np.array(b.get_data_flat()).reshape(b.get_nr_bins(), 2)
+    return np.array(b.get_data())
+
+
 def ComputeCurrentJDirect(model, time, order, cutoff_integrand):
     """compute_current_J_direct(model or params, time, order, cutoff) (compute_obs.hpp:66-80)."""
     m = _model(model, True)
@@ -140,4 +155,5 @@ def ComputeCurrentJDirect(model, time, order, cutoff_integrand):
 
 
 __all__ = ["GfIndexT", "G0Model", "G0KeldyshContourT", "IntegrandGDirect", "ComputeChargeQDirect",
-           "ComputeChargeQDirectTime", "BinnerT1", "ComputeCurrentJDirect", "model_param_t", "MODEL_PARAM_DEFAULTS"]
+           "ComputeChargeQDirectTime", "BinnerT1", "BinnerT11", "ComputeGfKernel", "IntegrandGKernel", "binner_data",
+           "ComputeCurrentJDirect", "model_param_t", "MODEL_PARAM_DEFAULTS"]

@@ -758,3 +758,180 @@ int or_integrate_binned(const or_model *mdl, const or_gf_index *A, const or_gf_i
   result[4] = ssc;
   return st;
 }
+
+/* first_row_expansion (det_expansion.hpp:44-74): LU with partial pivoting (zgetrf: pivot =
+ * first maximum of |re|+|im|, multipliers from the pivot's reciprocal), det(a) from the
+ * diagonal and the interchanges, then zgetrs on b = det(a) e_0: row interchanges, unit
+ * lower and upper triangular solves. x = the first row of a's cofactor matrix. */
+static void or_first_row_expansion(cplx *a, int m, cplx *x) {
+  int piv[64];
+  cplx det = c_make(1.0, 0.0);
+  int neg = 0;
+  for (int k = 0; k < m; ++k) {
+    int p = k;
+    double best = c_abs1(a[k * m + k]);
+    for (int i = k + 1; i < m; ++i)
+      if (c_abs1(a[i * m + k]) > best) {
+        best = c_abs1(a[i * m + k]);
+        p = i;
+      }
+    piv[k] = p;
+    if (p != k) {
+      for (int j = 0; j < m; ++j) {
+        cplx t = a[k * m + j];
+        a[k * m + j] = a[p * m + j];
+        a[p * m + j] = t;
+      }
+      neg = !neg;
+    }
+    det = c_mul(det, a[k * m + k]);
+    if (best == 0.0) continue;
+    cplx inv = c_div(c_make(1.0, 0.0), a[k * m + k]);
+    for (int i = k + 1; i < m; ++i) {
+      cplx l = c_mul(a[i * m + k], inv);
+      a[i * m + k] = l;
+      for (int j = k + 1; j < m; ++j) a[i * m + j] = c_sub(a[i * m + j], c_mul(l, a[k * m + j]));
+    }
+  }
+  if (neg) det = c_scale(det, -1.0);
+  for (int i = 0; i < m; ++i) x[i] = c_make(0.0, 0.0);
+  x[0] = det;
+  for (int k = 0; k < m; ++k)
+    if (piv[k] != k) {
+      cplx t = x[k];
+      x[k] = x[piv[k]];
+      x[piv[k]] = t;
+    }
+  for (int i = 1; i < m; ++i)
+    for (int j = 0; j < i; ++j) x[i] = c_sub(x[i], c_mul(a[i * m + j], x[j]));
+  for (int i = m - 1; i >= 0; --i) {
+    for (int j = i + 1; j < m; ++j) x[i] = c_sub(x[i], c_mul(a[i * m + j], x[j]));
+    x[i] = c_div(x[i], a[i * m + i]);
+  }
+}
+
+/* integrand_g_kernel::operator() (impurity_oneband/wick_kernel.cpp:42-138) for one point:
+ * out[2 * (2 i + k)], out[2 * (2 i + k) + 1] = the sum over the Keldysh configurations with
+ * a_i = k of vertex i's term x_{i+1} (-1)^|a| det(s2_a) (keldy accumulates each term at
+ * (u_i, a_i)); *scale = sum of the terms' moduli. X's timesplit is set to n. */
+int or_integrand_kernel(const or_model *mdl, const or_gf_index *X, int n, const double *times, int keep_u_hypercube,
+                        double *out, int *in_domain, double *scale) {
+  int err = 0;
+  for (int q = 0; q < 4 * n; ++q) out[q] = 0.0;
+  *scale = 0.0;
+  *in_domain = 0;
+  if (keep_u_hypercube)
+    for (int i = 0; i < n; ++i)
+      if (times[i] < 0.0) return 0;
+  or_gf_index a = *X;
+  a.timesplit = n;
+  int N1 = 2 * n + 1, N2 = 2 * n;
+  cplx *s1 = (cplx *)malloc(sizeof(cplx) * (size_t)(N1 * N1));
+  cplx *s2 = (cplx *)malloc(sizeof(cplx) * (size_t)(N2 * N2));
+  cplx *t1 = (cplx *)malloc(sizeof(cplx) * (size_t)((n + 1) * (n + 1)));
+  cplx *t2 = (cplx *)malloc(sizeof(cplx) * (size_t)(n * n));
+  cplx *x = (cplx *)malloc(sizeof(cplx) * (size_t)(n + 1));
+  or_gf_index *c1 = (or_gf_index *)malloc(sizeof(or_gf_index) * (size_t)N2);
+  or_gf_index *c2 = (or_gf_index *)malloc(sizeof(or_gf_index) * (size_t)N2);
+  for (int i = 0; i < n; ++i) {
+    or_gf_index p = {times[i], a.spin, 0, i, 0};
+    c1[i] = p;
+    p.k_idx = 1;
+    c1[i + n] = p;
+    or_gf_index q = {times[i], 1 - a.spin, 0, i, 0};
+    c2[i] = q;
+    q.k_idx = 1;
+    c2[i + n] = q;
+  }
+  int ext = 2 * n;
+  s1[ext * N1 + ext] = or_g0c(mdl, &a, &a, 0, &err);
+  for (int i = 0; i < N2; ++i) {
+    s1[ext * N1 + i] = or_g0c(mdl, &a, &c1[i], 1, &err);
+    s1[i * N1 + ext] = or_g0c(mdl, &c1[i], &a, 1, &err);
+    for (int j = 0; j < N2; ++j) {
+      s1[i * N1 + j] = or_g0c(mdl, &c1[i], &c1[j], 1, &err);
+      s2[i * N2 + j] = or_g0c(mdl, &c2[i], &c2[j], 1, &err);
+    }
+  }
+  int pick[65];
+  uint64_t nconf = (uint64_t)1 << n;
+  for (uint64_t kel = 0; kel < nconf; ++kel) {
+    pick[0] = ext;
+    for (int i = 0; i < n; ++i) pick[i + 1] = i + (int)((kel >> i) & 1u) * n;
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) t2[i * n + j] = s2[pick[i + 1] * N2 + pick[j + 1]];
+    for (int i = 0; i <= n; ++i)
+      for (int j = 0; j <= n; ++j) t1[i * (n + 1) + j] = s1[pick[i] * N1 + pick[j]];
+    t1[n * (n + 1) + n] = c_make(0.0, 0.0); /* wick_kernel.cpp:121 */
+    or_first_row_expansion(t1, n + 1, x);
+    cplx d2 = or_det(t2, n);
+    if (__builtin_parityll(kel)) d2 = c_scale(d2, -1.0);
+    for (int i = 0; i < n; ++i) {
+      cplx v = c_mul(x[i + 1], d2);
+      int k = (int)((kel >> i) & 1u);
+      out[2 * (2 * i + k)] += v.re;
+      out[2 * (2 * i + k) + 1] += v.im;
+      *scale += c_abs(v);
+    }
+  }
+  free(s1);
+  free(s2);
+  free(t1);
+  free(t2);
+  free(x);
+  free(c1);
+  free(c2);
+  *in_domain = 1;
+  return err ? -1 : 0;
+}
+
+/* integrator<binner_t<1, 1>, integrand_g_kernel>::run (integrator.hpp:81-95): Sobol points
+ * k_first.., chain, per point the terms times the Jacobian into bins[nbins][2] (complex,
+ * (time bin, Keldysh index)), counts[nbins][2] (values added, 2^(n-1) per (vertex, index)),
+ * *dropped; result[0..1] = sum of all terms, [2] points, [3] in domain, [4] sum of moduli. */
+int or_integrate_kernel(const or_model *mdl, const or_gf_index *X, const or_warper *chain, int len, int n,
+                        const uint32_t *Csr, const uint32_t *shfr, int m, uint32_t k_first, int64_t nr_steps, int nbins,
+                        double xmin, double xmax, double *result, double *bins, double *counts, double *dropped) {
+  double li[64], ui[64], out[256], jac, sc;
+  int dom;
+  const double bin_size = (xmax - xmin) / nbins;
+  double sre = 0.0, sim = 0.0, ssc = 0.0;
+  uint64_t npts = 0, ndom = 0;
+  int st = 0;
+  for (int64_t s = 0; s < nr_steps; ++s) {
+    or_sobol_points(n, m, Csr, shfr, k_first + (uint32_t)s, 1, li);
+    jac = 1.0;
+    or_map_reverse(chain, len, len, 0, n, li, ui, &jac);
+    if (or_integrand_kernel(mdl, X, n, ui, 1, out, &dom, &sc) != 0) st = -1;
+    npts++;
+    if (!dom) continue;
+    ndom++;
+    ssc += sc * fabs(jac);
+    for (int i = 0; i < n; ++i) {
+      double t = ui[i];
+      int b = -1;
+      if (xmin <= t && t <= xmax) {
+        b = (t == xmax) ? nbins - 1 : (int)((t - xmin) / bin_size);
+        if (b > nbins - 1) b = nbins - 1;
+      }
+      for (int k = 0; k < 2; ++k) {
+        double vr = out[2 * (2 * i + k)] * jac, vi = out[2 * (2 * i + k) + 1] * jac;
+        sre += vr;
+        sim += vi;
+        if (b < 0) {
+          *dropped += (double)((uint64_t)1 << (n - 1));
+        } else {
+          bins[2 * (2 * b + k)] += vr;
+          bins[2 * (2 * b + k) + 1] += vi;
+          counts[2 * b + k] += (double)((uint64_t)1 << (n - 1));
+        }
+      }
+    }
+  }
+  result[0] = sre;
+  result[1] = sim;
+  result[2] = (double)npts;
+  result[3] = (double)ndom;
+  result[4] = ssc;
+  return st;
+}

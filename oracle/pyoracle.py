@@ -87,6 +87,10 @@ class Oracle:
                                    C.POINTER(Warper), C.c_int, C.c_int, _U32, _U32, C.c_int, C.c_uint32, C.c_int64,
                                    C.c_int, C.c_int, _D]
         L.or_compare_3way.argtypes = [C.c_double, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int]
+        L.or_integrand_kernel.argtypes = [C.POINTER(Model), C.POINTER(GfIndex), C.c_int, _D, C.c_int, _D, _I, _D]
+        L.or_integrate_kernel.argtypes = [C.POINTER(Model), C.POINTER(GfIndex), C.POINTER(Warper), C.c_int, C.c_int,
+                                          _U32, _U32, C.c_int, C.c_uint32, C.c_int64, C.c_int, C.c_double, C.c_double,
+                                          _D, _D, _D, _D]
         L.or_integrate_binned.argtypes = [C.POINTER(Model), C.POINTER(GfIndex), C.POINTER(GfIndex), C.c_double,
                                           C.POINTER(Warper), C.c_int, C.c_int, _U32, _U32, C.c_int, C.c_uint32,
                                           C.c_int64, C.c_int, C.c_double, C.c_double, _D, _D, _D, _D]
@@ -239,6 +243,43 @@ class Oracle:
         assert st == 0
         return (complex(res[0], res[1]), int(res[2]), int(res[3]), res[4], bins.view(np.complex128),
                 counts.astype(np.int64), int(dropped[0]))
+
+    def integrand_kernel(self, model, X, times, keep_u_hypercube=True):
+        """integrand_g_kernel per point: (sums [count][n][2] complex per (vertex, Keldysh index),
+        in_domain, scale)."""
+        times = np.ascontiguousarray(np.atleast_2d(times), dtype=np.float64)
+        count, n = times.shape
+        vals = np.zeros((count, n, 2), dtype=np.complex128)
+        dom = np.zeros(count, dtype=np.int32)
+        sc = np.zeros(count)
+        out = np.zeros(4 * n)
+        d = C.c_int()
+        s = C.c_double()
+        gX = GfIndex(*X)
+        for p in range(count):
+            assert self.lib.or_integrand_kernel(C.byref(model), C.byref(gX), n, _dp(times[p]), int(keep_u_hypercube),
+                                                _dp(out), C.byref(d), C.byref(s)) == 0
+            vals[p] = out.view(np.complex128).reshape(n, 2)
+            dom[p] = d.value
+            sc[p] = s.value
+        return vals, dom, sc
+
+    def integrate_kernel(self, model, X, chain, order, nr_steps, nbins, xmin, xmax, seed=0, do_shift=False,
+                         do_scramble=False, seed_shift=0):
+        """integrator<binner_t<1,1>, integrand_g_kernel>::run: (sum, n_points, n_in_domain, sum of
+        moduli, bins complex[nbins][2], counts[nbins][2], dropped)."""
+        Csr, shfr = self.sobol_setup(order, 31, do_shift, do_scramble, seed_shift)
+        arr = chain_array(chain)
+        res = np.zeros(5)
+        bins = np.zeros(4 * nbins)
+        counts = np.zeros(2 * nbins)
+        dropped = np.zeros(1)
+        st = self.lib.or_integrate_kernel(C.byref(model), C.byref(GfIndex(*X)), arr, len(chain), order,
+                                          Csr.ctypes.data_as(_U32), shfr.ctypes.data_as(_U32), 31, seed + 1, nr_steps,
+                                          nbins, xmin, xmax, _dp(res), _dp(bins), _dp(counts), _dp(dropped))
+        assert st == 0
+        return (complex(res[0], res[1]), int(res[2]), int(res[3]), res[4], bins.view(np.complex128).reshape(nbins, 2),
+                counts.reshape(nbins, 2).astype(np.int64), int(dropped[0]))
 
     def compare_3way(self, a, b):
         return self.lib.or_compare_3way(a[0], a[1], a[2], b[0], b[1], b[2])

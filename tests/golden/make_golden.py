@@ -11,7 +11,8 @@ built oracle/_ref (``make -C oracle``):
   eval_no_det values and the integrator's sums.
 * keldy_tests.json: known answers read from keldy's test files: the Horvatic-Zlatic
   charge series and its parameters and the order-1 current
-  (test/c++/impurity_oneband/compute_obs_test.cpp), the plasma-warper vectors
+  (test/c++/impurity_oneband/compute_obs_test.cpp), the order-2 kernel-method G(t) bins
+  (compute_obs_kernel_test.cpp), the plasma-warper vectors
   (test/c++/warpers/warper_plasma_uv_test.cpp), and g0 values of the semicircular and
   flat-band models (model_semicircle_test.cpp, model_flatband_test.cpp).
 
@@ -73,11 +74,11 @@ def keldy_test_values():
         ui = [float(x) for x in re.search(r"ui_times = \{([^}]*)\}", block).group(1).split(",")]
         vi = [float(x) for x in re.search(r"vi_result = \{([^}]*)\}", block).group(1).split(",")]
         vecs.append({"t_max": t_max, "ui": ui, "vi": vi})
-    def params_of(block):
+    def params_of(block, names=None):
         out = {}
         for k, v in re.findall(r"params\.(\w+) = ([^;]+);", block):
             v = v.strip()
-            out[k] = v.strip('"') if v.startswith('"') else float(v)
+            out[k] = v.strip('"') if v.startswith('"') else (names[v] if names and v in names else float(v))
         return out
 
     def test_block(text, name):
@@ -110,8 +111,21 @@ def keldy_test_values():
         p.update(params_of(blk.split("g0_model g0_fft")[1]))  # the contour run's parameters
         flat.append({"params": p, "values": [{"re": float(a), "im": float(b), "t": float(t), "tol": float(tol)}
                                              for a, b, t, tol in vals]})
+    kt = open(os.path.join(KELDY_SRC, "test/c++/impurity_oneband/compute_obs_kernel_test.cpp")).read()
+    kb = test_block(kt, r"ComputeObs, ValueKernel")
+    kvals = re.findall(r"\{([-\d.e]+) ([+-]) ([\d.e-]+)i, ([-\d.e]+) ([+-]) ([\d.e-]+)i\}", kb)
+    ktmax = float(re.search(r"double const tmax = ([\d.]+);", kb).group(1))
+    kernel = {"params": params_of(kb, {"tmax": ktmax}),
+              "t_max": ktmax,
+              "order": int(re.search(r"compute_gf_kernel computer\(g0, tmax, (\d+), nr_bins\)", kb).group(1)),
+              "nr_bins": int(re.search(r"int const nr_bins = (\d+);", kb).group(1)),
+              "n_points": int(float(re.search(r"computer\.run\(([\de.]+)\)", kb).group(1))),
+              "tol": float(re.search(r"EXPECT_LT\(max_element\(abs\(result - expected_result\)\), ([\de.-]+)\)",
+                                     kb).group(1)),
+              "expected": [[[float(a), float(b + c)], [float(d), float(e + f)]] for a, b, c, d, e, f in kvals]}
     return {
         "source": "keldy test/c++/impurity_oneband/compute_obs_test.cpp:93-206, "
+                  "test/c++/impurity_oneband/compute_obs_kernel_test.cpp:12-60, "
                   "test/c++/warpers/warper_plasma_uv_test.cpp:15-43, "
                   "test/c++/impurity_oneband/model_semicircle_test.cpp:30-86, "
                   "test/c++/impurity_oneband/model_flatband_test.cpp:154-220",
@@ -125,13 +139,15 @@ def keldy_test_values():
                       "runs": [{"warper": "inverse_square", "w": 1.0, "n_points": 10000, "rtol": [1e-3, 1e-2]},
                                {"warper": "exponential", "w": 2.0, "n_points": 50000, "rtol": [1e-2, 1e-2]}]},
         "plasma_vectors": vecs,
+        "kernel_kat": kernel,
     }
 
 
 def main():
     if "--json-only" in sys.argv:
+        values = keldy_test_values()
         with open(os.path.join(HERE, "keldy_tests.json"), "w") as f:
-            json.dump(keldy_test_values(), f, indent=1)
+            json.dump(values, f, indent=1)
         return
     ref = Reference()
     rng = np.random.default_rng(20240601)

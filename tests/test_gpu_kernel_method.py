@@ -1,0 +1,77 @@
+"""keldy's kernel method (integrand_g_kernel, compute_gf_kernel; wick_kernel.cpp:42-138,
+compute_obs.hpp:105-117) on the GPU: point values and binned integration against the
+oracle (pinned to keldy's closed forms in test_kernel_method_oracle.py), and keldy's
+order-2 value test (compute_obs_kernel_test.cpp:12-60)."""
+import numpy as np
+import pytest
+
+from keldy_b200 import capi, impurity_oneband as io, warpers
+
+pytestmark = pytest.mark.gpu
+
+X = (7.0, 0, 0, 0, 0)
+PLASMA_EXP = [(capi.WARPER_PLASMA_UV, 10.0, 0.0), (capi.WARPER_EXPONENTIAL, 10.0, 1.0)]
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 7])
+def test_point_values_vs_oracle(ctx, oracle, golden, n):
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr, 0.3)
+    om = oracle.model(10.0, le, gr, 0.3)
+    t = np.random.default_rng(n).random((12, n)) * 10.0
+    t[1, 0] = -0.5               # out of the domain
+    if n >= 2:
+        t[2, 1] = t[2, 0]        # equal vertex times
+    t[3, 0] = X[0]               # a vertex at the fixed point's time
+    got, dom = gm.integrand_kernel(X, t)
+    want, odom, sc = oracle.integrand_kernel(om, X, t)
+    assert np.array_equal(dom, odom)
+    for p in range(len(t)):
+        assert np.abs(got[p] - want[p]).max() <= 1e-12 * max(sc[p], 1e-300), (p, np.abs(got[p] - want[p]).max(), sc[p])
+
+
+@pytest.mark.parametrize("n", [1, 2, 4])
+def test_binned_integration_vs_oracle(ctx, oracle, golden, n):
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    npts = 1024
+    item = dict(model=gm, rng=ctx.sobol(n), chain=PLASMA_EXP, A=X, order=n, k_first=1, n_points=npts)
+    s, npt, nd, bins, counts, dropped = capi.integrate_kernel(ctx, [item], 8, 0.0, 10.0)[0]
+    ws, onp, ond, sc, obins, ocounts, odropped = oracle.integrate_kernel(om, X, PLASMA_EXP, n, npts, 8, 0.0, 10.0)
+    assert (npt, nd) == (onp, ond)
+    assert np.array_equal(counts, ocounts) and dropped == odropped
+    assert np.abs(bins - obins).max() <= 1e-12 * sc
+    assert abs(s - ws) <= 1e-12 * sc
+    assert abs(bins.sum() - s) <= 1e-12 * sc  # nothing dropped on [0, t]
+
+
+def test_keldy_order_2_kernel_values(keldy_tests):
+    """compute_obs_kernel_test.cpp:12-60: semicircular bath at zero temperature, alpha = 0.5,
+    G(t) bins of the order-2 kernel method against keldy's stored result (keldy's tolerance
+    1e-6, its own QMC accuracy 2e-8). keldy integrated 1e6 points through an interpolated
+    hybrid warper; here 2^22 Sobol points through plasma_uv + the 1/(v + 1) product warper
+    (the same integral; g0 decays as 1/t at zero temperature, so a 1/v^3 warper would
+    undersample the early time bins). The lesser column is the conjugate of the greater one."""
+    k = keldy_tests["kernel_kat"]
+    p = dict(k["params"])
+    p["nr_time_points_gf"] = int(p["nr_time_points_gf"])
+    model = io.G0Model(p, False)
+    comp = io.ComputeGfKernel(model, k["t_max"], k["order"], k["nr_bins"])
+    comp.warper.emplace_back(warpers.WarperPlasmaUvT(k["t_max"]))
+    comp.warper.emplace_back(warpers.make_product_1d_simple_inverse(k["t_max"], 1.0))
+    comp.run(1 << 22)
+    res = comp.reduce_result()
+    data = io.binner_data(res) / res.get_bin_size()
+    want = np.array([[complex(*c) for c in row] for row in k["expected"]])
+    assert np.abs(data[:, 0] - np.conj(data[:, 1])).max() < 1e-12
+    assert np.abs(data - want).max() < k["tol"], np.abs(data - want).max()
+
+
+def test_kernel_method_errors(ctx, golden):
+    gm = ctx.model(10.0, golden["table_beta20_lesser"], golden["table_beta20_greater"])
+    item = dict(model=gm, rng=ctx.sobol(11), chain=PLASMA_EXP, A=X, order=11, k_first=1, n_points=10)
+    with pytest.raises(capi.KbError, match="orders 1..10"):
+        capi.integrate_kernel(ctx, [item], 8, 0.0, 10.0)
+    with pytest.raises(capi.KbError, match="wrong order"):
+        capi.integrate_kernel(ctx, [dict(item, order=2, rng=ctx.sobol(2))], 8, 3.0, 1.0)
