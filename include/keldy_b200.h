@@ -79,6 +79,7 @@ int kb_sobol_points_dev(kb_context *ctx, const kb_sobol *s, uint32_t k_first, in
 #define KB_WARPER_INVERSE_SQUARE 4 /* make_product_1d_simple_inverse_square(u_max, w) (:594-608) */
 #define KB_WARPER_INVERSE_POWER 5  /* make_product_1d_simple_inverse_power(power, u_max, w) (:610-630) */
 #define KB_WARPER_UNIFORM 6        /* warper_product_1d_simple_t with f1 = 1/u_max (product_1d_simple_test.cpp:10-23) */
+#define KB_WARPER_TABLE 7          /* tabulated product warper: kb_warper_table (see below) */
 #define KB_MAX_CHAIN 8
 
 typedef struct {
@@ -86,7 +87,23 @@ typedef struct {
   int power;    /* KB_WARPER_INVERSE_POWER only */
   double u_max; /* domain_u_max, or t_max for the plasma warper */
   double w;     /* w_scale of the product makers */
+  const struct kb_warper_table *table; /* KB_WARPER_TABLE only */
 } kb_warper;
+
+/* Tabulated product-1D warpers: warper_product_1d_simple_interp_nearest_t
+ * (product_1d_simple.hpp:174-330; ndims = 1, the same table for every coordinate) and
+ * warper_product_1d_interp_nearest_t (product_1d.hpp:164-211; one table per coordinate,
+ * ndims = the order). Table d has npts[d] >= 3 points u (u[0] = 0, strictly increasing,
+ * the last one the domain's u_max) with values f1 >= 0 there; the arrays of all tables are
+ * concatenated. As keldy's integrate_and_inverse (product_1d_simple.hpp:219-253): F is
+ * f1's trapezoid integral from u_max, normalised to 1; u = F^-1(l) and the Jacobian
+ * 1/f1(u) use linear interpolation on the points (f1 on an interval: the mean of its ends).
+ * Errors as keldy: "Model function is flat zero.", fewer than 3 points, u[0] != 0. */
+typedef struct kb_warper_table kb_warper_table;
+int kb_warper_table_create(kb_context *ctx, int ndims, const int *npts, const double *u_pts, const double *f1_pts,
+                           kb_warper_table **out);
+int kb_warper_table_destroy(kb_warper_table *t);
+
 
 /* warper_train_t::map_reverse(li, start, end) (warpers.hpp:72-85; direction 0) or
  * map_forward(ui, start, end) (warpers.hpp:88-101; direction 1) on count points of n
@@ -166,6 +183,17 @@ int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integr
 int kb_evaluate_warped(kb_context *ctx, const kb_model *m, const kb_integrand *f, const kb_warper *chain,
                        int chain_len, int start_domain_nr, int order, int64_t count, const double *li,
                        int keep_u_hypercube, int algo, double *out, double *jac, int *in_domain);
+
+/* make_warper_from_proj (warpers/make_warper_from_proj.hpp:100-153): the projections of
+ * |f J| (integrand f on model m through `chain`, Sobol points 1..nr_samples of dimension
+ * order, unshifted) on num_bins bins of each axis of [0,1]^order, averaged per bin,
+ * smoothed by a local linear fit of their logarithm with a Gaussian kernel of width sigma
+ * (kernel_smoothing, :40-66), turned into f1 points (f1[0] = 0, f1[i+1] = 2 s_i - f1[i])
+ * of one table per axis. The table maps the Sobol point before `chain` (append it to the
+ * chain's end). */
+int kb_warper_table_from_projection(kb_context *ctx, const kb_model *m, const kb_integrand *f,
+                                    const kb_warper *chain, int chain_len, int order, int num_bins, int nr_samples,
+                                    double sigma, int keep_u_hypercube, kb_warper_table **out);
 
 /* ------------------------------------------------------------- integrator --- */
 /* Running sums of integrator::run (integrator.hpp:50-52). */

@@ -24,6 +24,7 @@
 #include <memory>
 #include <mutex>
 #include <array>
+#include <functional>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -169,9 +170,11 @@ inline std::pair<std::vector<double>, double> apply(std::vector<kb_warper> const
 class warper_base {
  protected:
   kb_warper desc_{};
+  std::shared_ptr<kb_warper_table> table_; // tabulated warpers: keeps the device tables alive
 
  public:
   const kb_warper &desc() const { return desc_; }
+  std::shared_ptr<kb_warper_table> const &table() const { return table_; }
   std::pair<std::vector<double>, double> map_reverse(std::vector<double> const &li_vec) const {
     return detail::apply({desc_}, KB_REVERSE, 1, 0, li_vec);
   }
@@ -228,18 +231,102 @@ inline warper_product_1d_simple_t make_product_1d_simple_uniform(double domain_u
   return warper_product_1d_simple_t(kb_warper{KB_WARPER_UNIFORM, 0, domain_u_max, 0.0});
 }
 
+namespace detail {
+inline std::shared_ptr<kb_warper_table> make_table(std::vector<int> const &npts, std::vector<double> const &u,
+                                                   std::vector<double> const &f1) {
+  kb_warper_table *t = nullptr;
+  keldy_b200::check(kb_warper_table_create(keldy_b200::default_context(), (int)npts.size(), npts.data(), u.data(),
+                                           f1.data(), &t));
+  return std::shared_ptr<kb_warper_table>(t, [](kb_warper_table *p) { kb_warper_table_destroy(p); });
+}
+} // namespace detail
+
+// product_1d_simple.hpp:174-330: f1 tabulated on points u (u[0] = 0, increasing), linear
+// interpolation of its integral and of the inverse, the same table for every coordinate.
+class warper_product_1d_simple_interp_nearest_t : public warper_base {
+  std::vector<double> u_, f1_;
+
+  void build() {
+    table_ = detail::make_table({(int)u_.size()}, u_, f1_);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, u_.back(), 0.0, table_.get()};
+  }
+
+ public:
+  warper_product_1d_simple_interp_nearest_t(std::vector<double> times_u_pts, std::vector<double> f1_pts)
+     : u_(std::move(times_u_pts)), f1_(std::move(f1_pts)) {
+    if (f1_.size() != u_.size()) throw std::runtime_error("times_u_pts and f1_pts should have the same length.");
+    build();
+  }
+  // f1 sampled on nr_sample_points equidistant points of [0, domain_u_max] (:295-318)
+  warper_product_1d_simple_interp_nearest_t(std::function<double(double)> const &f1, double domain_u_max,
+                                            int nr_sample_points) {
+    if (!(nr_sample_points >= 3))
+      throw std::runtime_error("Expect nr_sample_points to be >= 3. Given was " + std::to_string(nr_sample_points));
+    u_.resize((size_t)nr_sample_points);
+    f1_.resize((size_t)nr_sample_points);
+    for (int i = 0; i < nr_sample_points; ++i)
+      u_[(size_t)i] = 0.0 + static_cast<double>(i) / (nr_sample_points - 1) * (domain_u_max - 0.0);
+    u_.back() = domain_u_max;
+    for (int i = 0; i < nr_sample_points; ++i) f1_[(size_t)i] = f1(u_[(size_t)i]);
+    build();
+  }
+  std::vector<double> const &get_times_u_pts() const { return u_; }
+  std::vector<double> const &get_f1_pts() const { return f1_; }
+};
+
+// product_1d.hpp:164-211: one tabulated warper per coordinate.
+class warper_product_1d_interp_nearest_t : public warper_base {
+  std::vector<warper_product_1d_simple_interp_nearest_t> dims_;
+
+  void rebuild() {
+    std::vector<int> npts;
+    std::vector<double> u, f1;
+    for (auto const &d : dims_) {
+      npts.push_back((int)d.get_times_u_pts().size());
+      u.insert(u.end(), d.get_times_u_pts().begin(), d.get_times_u_pts().end());
+      f1.insert(f1.end(), d.get_f1_pts().begin(), d.get_f1_pts().end());
+    }
+    table_ = detail::make_table(npts, u, f1);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, u[(size_t)npts[0] - 1], 0.0, table_.get()};
+  }
+
+ public:
+  warper_product_1d_interp_nearest_t() = default;
+  // an already built table with one table per coordinate (make_warper_from_proj)
+  explicit warper_product_1d_interp_nearest_t(std::shared_ptr<kb_warper_table> t) {
+    table_ = std::move(t);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, 1.0, 0.0, table_.get()};
+  }
+  void reserve(size_t n) { dims_.reserve(n); }
+  int size() const { return (int)dims_.size(); }
+  void emplace_back(warper_product_1d_simple_interp_nearest_t const &w) {
+    dims_.push_back(w);
+    rebuild();
+  }
+  warper_product_1d_simple_interp_nearest_t get_1d_warper(int axis) const {
+    if (axis < 0 || axis >= (int)dims_.size()) throw std::runtime_error("out of range axis");
+    return dims_[(size_t)axis];
+  }
+};
+
 // warpers.hpp:45-137: a chain, applied last to first by map_reverse.
 class warper_train_t {
   std::vector<kb_warper> chain_;
+  std::vector<std::shared_ptr<kb_warper_table>> keep_; // device tables of tabulated warpers
 
  public:
   warper_train_t() = default;
   void emplace_back(warper_base const &w) {
     if (chain_.size() >= KB_MAX_CHAIN) throw std::runtime_error("warper train longer than KB_MAX_CHAIN");
+    if (w.desc().kind == KB_WARPER_TABLE && !w.table()) throw std::runtime_error("empty tabulated warper");
     chain_.push_back(w.desc());
+    keep_.push_back(w.table());
   }
   void reserve(size_t n) { chain_.reserve(n); }
-  void clear() { chain_.clear(); }
+  void clear() {
+    chain_.clear();
+    keep_.clear();
+  }
   size_t size() const { return chain_.size(); }
   std::vector<kb_warper> const &chain() const { return chain_; }
 
@@ -728,4 +815,24 @@ class compute_charge_Q_direct_time : public integrator_g_direct_time {
 };
 
 } // namespace impurity_oneband
+
+namespace warpers {
+// make_warper_from_proj (make_warper_from_proj.hpp:100-153) for the integrand of
+// `computer` through its current warper train: one tabulated warper per axis, built from
+// the smoothed projections of |f J| on nr_samples Sobol points; append it to the train.
+inline warper_product_1d_interp_nearest_t make_warper_from_proj(impurity_oneband::integrator_g_direct const &computer,
+                                                                int order, int num_bins, int nr_samples,
+                                                                double sigma, bool keep_u_hypercube = true) {
+  auto const train = computer.get_warper(); // a copy: its chain must outlive the call below
+  auto const &chain = train.chain();
+  kb_integrand f = computer.get_integrand().abi();
+  kb_warper_table *t = nullptr;
+  keldy_b200::check(kb_warper_table_from_projection(keldy_b200::default_context(),
+                                                    computer.get_integrand().get_g0().model.handle(), &f,
+                                                    chain.data(), (int)chain.size(), order, num_bins, nr_samples,
+                                                    sigma, keep_u_hypercube, &t));
+  return warper_product_1d_interp_nearest_t(
+      std::shared_ptr<kb_warper_table>(t, [](kb_warper_table *p) { kb_warper_table_destroy(p); }));
+}
+} // namespace warpers
 } // namespace keldy

@@ -21,6 +21,7 @@ KB_E_INVALID, KB_E_CUDA, KB_E_NOMEM, KB_E_RANGE, KB_E_EXHAUSTED, KB_E_NODEVICE =
 
 WARPER_IDENTITY, WARPER_PLASMA_UV, WARPER_EXPONENTIAL, WARPER_INVERSE = 0, 1, 2, 3
 WARPER_INVERSE_SQUARE, WARPER_INVERSE_POWER, WARPER_UNIFORM = 4, 5, 6
+WARPER_TABLE = 7
 MAX_CHAIN = 8
 REVERSE, FORWARD = 0, 1
 ALGO_AUTO, ALGO_TREE, ALGO_DIRECT = 0, 1, 2
@@ -36,7 +37,8 @@ EXPORTS = [
     "kb_plan_result", "kb_plan_set_k_first", "kb_context_set_launch", "kb_context_get_launch",
     "kb_flow_create", "kb_flow_destroy", "kb_flow_dim", "kb_flow_get_params", "kb_flow_set_params", "kb_flow_map",
     "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
-    "kb_integrate_kernel", "kb_integrand_kernel_eval",
+    "kb_integrate_kernel", "kb_integrand_kernel_eval", "kb_warper_table_create", "kb_warper_table_destroy",
+    "kb_warper_table_from_projection",
 ]
 FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
 FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
@@ -50,7 +52,8 @@ class KbError(RuntimeError):
 
 
 class Warper(C.Structure):
-    _fields_ = [("kind", C.c_int), ("power", C.c_int), ("u_max", C.c_double), ("w", C.c_double)]
+    _fields_ = [("kind", C.c_int), ("power", C.c_int), ("u_max", C.c_double), ("w", C.c_double),
+                ("table", C.c_void_p)]
 
 
 class GfIndex(C.Structure):
@@ -127,6 +130,10 @@ def load():
     L.kb_evaluate_warped.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, C.c_int, C.c_int,
                                      C.c_int64, _D, C.c_int, C.c_int, _D, _D, _I]
     L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
+    L.kb_warper_table_create.argtypes = [_VP, C.c_int, _I, _D, _D, C.POINTER(_VP)]
+    L.kb_warper_table_destroy.argtypes = [_VP]
+    L.kb_warper_table_from_projection.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, C.c_int,
+                                                  C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(_VP)]
     L.kb_integrate_kernel.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(TimeBins), C.POINTER(Accum), _D,
                                       C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.kb_integrand_kernel_eval.argtypes = [_VP, _VP, C.POINTER(GfIndex), C.c_int, C.c_int64, _D, C.c_int, _D, _I]
@@ -182,11 +189,60 @@ def _ip(a):
 
 
 def chain_array(chain):
-    """chain: list of (kind, u_max, w[, power]) -> (ctypes array, length)."""
+    """chain: list of (kind, u_max, w[, power]) or (WARPER_TABLE, WarperTable) -> (ctypes array,
+    length)."""
     arr = (Warper * MAX_CHAIN)()
     for i, c in enumerate(chain):
-        arr[i] = Warper(int(c[0]), int(c[3]) if len(c) > 3 else 0, float(c[1]), float(c[2]))
+        if int(c[0]) == WARPER_TABLE:
+            arr[i] = Warper(WARPER_TABLE, 0, 0.0, 0.0, c[1].h.value)
+        else:
+            arr[i] = Warper(int(c[0]), int(c[3]) if len(c) > 3 else 0, float(c[1]), float(c[2]), None)
     return arr, len(chain)
+
+
+class WarperTable:
+    """Tabulated product warper (kb_warper_table): one table for every coordinate or one per
+    coordinate. tables: list of (u_points, f1_values); use in a chain as (WARPER_TABLE, self)."""
+
+    def __init__(self, ctx, tables=None, _handle=None):
+        self.ctx = ctx
+        if _handle is not None:
+            self.h = _handle
+        else:
+            npts = np.array([len(u) for u, _ in tables], dtype=np.int32)
+            u = np.ascontiguousarray(np.concatenate([np.asarray(u, dtype=np.float64) for u, _ in tables]))
+            f1 = np.ascontiguousarray(np.concatenate([np.asarray(f, dtype=np.float64) for _, f in tables]))
+            h = _VP()
+            check(ctx.L.kb_warper_table_create(ctx.h, len(tables), npts.ctypes.data_as(_I), _dp(u), _dp(f1),
+                                               C.byref(h)))
+            self.h = h
+        ctx._deps.add(self)
+
+    @classmethod
+    def from_projection(cls, ctx, model, A, B, chain, order, num_bins, nr_samples, sigma, keep_u_hypercube=True,
+                        cutoff=0.0):
+        """make_warper_from_proj: one table per axis from the projections of |f J|."""
+        arr, L = chain_array(chain)
+        f = Integrand(gf_index(A), gf_index(B), float(cutoff))
+        h = _VP()
+        check(ctx.L.kb_warper_table_from_projection(ctx.h, model.h, C.byref(f), arr, L, int(order), int(num_bins),
+                                                    int(nr_samples), float(sigma), int(keep_u_hypercube),
+                                                    C.byref(h)))
+        return cls(ctx, _handle=h)
+
+    def entry(self):
+        return (WARPER_TABLE, self)
+
+    def close(self):
+        if self.h:
+            self.ctx.L.kb_warper_table_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def gf_index(x):

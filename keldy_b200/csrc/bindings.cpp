@@ -1,6 +1,7 @@
 // Python bindings of the C++ host classes (include/keldy_b200.hpp) under keldy's Python
 // names (python/keldy/common_desc.py, warpers_desc.py, impurity_oneband_desc.py).
 #include <pybind11/complex.h>
+#include <pybind11/functional.h>
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
@@ -107,6 +108,20 @@ PYBIND11_MODULE(_keldy, m) {
   m.def("make_product_1d_simple_inverse_power", &make_product_1d_simple_inverse_power, py::arg("power"),
         py::arg("domain_u_max"), py::arg("w_scale"));
   m.def("make_product_1d_simple_uniform", &make_product_1d_simple_uniform, py::arg("domain_u_max"));
+  auto wtn = py::class_<warper_product_1d_simple_interp_nearest_t>(m, "WarperProduct1dSimpleInterpNearestT")
+                 .def(py::init<std::vector<double>, std::vector<double>>(), py::arg("times_u_pts"), py::arg("f1_pts"))
+                 .def(py::init<std::function<double(double)> const &, double, int>(), py::arg("f1_"),
+                      py::arg("domain_u_max_"), py::arg("nr_sample_points_"))
+                 .def("get_times_u_pts", &warper_product_1d_simple_interp_nearest_t::get_times_u_pts)
+                 .def("get_f1_pts", &warper_product_1d_simple_interp_nearest_t::get_f1_pts);
+  warper_methods<warper_product_1d_simple_interp_nearest_t>(wtn);
+  auto wpn = py::class_<warper_product_1d_interp_nearest_t>(m, "WarperProduct1dInterpNearestT")
+                 .def(py::init<>())
+                 .def("reserve", &warper_product_1d_interp_nearest_t::reserve, py::arg("new_cap"))
+                 .def("size", &warper_product_1d_interp_nearest_t::size)
+                 .def("emplace_back", &warper_product_1d_interp_nearest_t::emplace_back, py::arg("w"))
+                 .def("get_1d_warper", &warper_product_1d_interp_nearest_t::get_1d_warper, py::arg("axis"));
+  warper_methods<warper_product_1d_interp_nearest_t>(wpn);
   m.def("vi_from_ui", &vi_from_ui, py::arg("t_max"), py::arg("u_times"));
   m.def("ui_from_vi", &ui_from_vi, py::arg("t_max"), py::arg("v_times"));
 
@@ -115,6 +130,11 @@ PYBIND11_MODULE(_keldy, m) {
       .def("emplace_back", [](warper_train_t &t, warper_identity_t const &w) { t.emplace_back(w); }, py::arg("w"))
       .def("emplace_back", [](warper_train_t &t, warper_plasma_uv_t const &w) { t.emplace_back(w); }, py::arg("w"))
       .def("emplace_back", [](warper_train_t &t, warper_product_1d_simple_t const &w) { t.emplace_back(w); },
+           py::arg("w"))
+      .def("emplace_back",
+           [](warper_train_t &t, warper_product_1d_simple_interp_nearest_t const &w) { t.emplace_back(w); },
+           py::arg("w"))
+      .def("emplace_back", [](warper_train_t &t, warper_product_1d_interp_nearest_t const &w) { t.emplace_back(w); },
            py::arg("w"))
       .def("reserve", &warper_train_t::reserve, py::arg("new_cap"))
       .def("clear", &warper_train_t::clear)
@@ -216,6 +236,13 @@ PYBIND11_MODULE(_keldy, m) {
                  .def(py::init<g0_model, double, int, int, double>(), py::arg("model"), py::arg("time"),
                       py::arg("order"), py::arg("nr_time_slices"), py::arg("cutoff_integrand"));
   integrator_methods<compute_charge_Q_direct_time>(cqt);
+  m.def(
+      "make_warper_from_proj",
+      [](compute_charge_Q_direct const &c, int order, int num_bins, int nr_samples, double sigma, bool keep) {
+        return keldy::warpers::make_warper_from_proj(c, order, num_bins, nr_samples, sigma, keep);
+      },
+      py::arg("computer"), py::arg("order"), py::arg("num_bins"), py::arg("nr_samples"), py::arg("sigma"),
+      py::arg("keep_u_hypercube") = true);
   py::class_<binner_2d>(m, "BinnerT11")
       .def(py::init<double, double, long>(), py::arg("xmin"), py::arg("xmax"), py::arg("nr_bins"))
       .def("get_data_flat", &binner_2d::get_data_flat)

@@ -261,9 +261,25 @@ static int make_warper_dev(const kb_warper &w, WarperDev &d) {
     d.c[2] = static_cast<double>(std::pow(w.w / (u_max + w.w), p - 1) - 1);
     return KB_OK;
   }
+  case KB_WARPER_TABLE:
+    if (!w.table) return fail(KB_E_INVALID, "tabulated warper without a table");
+    d.tab = w.table->d_dims;
+    d.ntab = w.table->ndims;
+    d.u_max = w.table->u_max;
+    return KB_OK;
   default:
     return fail(KB_E_INVALID, "unknown warper kind " + std::to_string(w.kind));
   }
+}
+
+// A tabulated warper with one table per coordinate needs as many coordinates as tables.
+static int check_chain_dims(const kb_warper *chain, int len, int n) {
+  for (int i = 0; i < len; ++i)
+    if (chain[i].kind == KB_WARPER_TABLE && chain[i].table && chain[i].table->ndims != 1 &&
+        chain[i].table->ndims != n)
+      return fail(KB_E_INVALID, "the tabulated warper has " + std::to_string(chain[i].table->ndims) +
+                                    " tables for " + std::to_string(n) + " coordinates");
+  return KB_OK;
 }
 
 static int make_chain(const kb_warper *chain, int len, WarperDev *out) {
@@ -280,6 +296,10 @@ static int make_chain(const kb_warper *chain, int len, WarperDev *out) {
 int kb_warp(kb_context *ctx, const kb_warper *chain, int chain_len, int direction, int start, int end, int n,
             int64_t count, const double *in, double *out, double *jac) {
   KB_CHECK(ctx, "null context");
+  if (chain_len > 0 && chain) {
+    int cd = check_chain_dims(chain, chain_len, n);
+    if (cd) return cd;
+  }
   KB_CHECK(n >= 0 && n <= MAX_ORDER, "number of coordinates must be in [0, 16]");
   KB_CHECK(count >= 0 && (count == 0 || (in && out)), "kb_warp: null buffer");
   KB_CHECK(direction == KB_REVERSE || direction == KB_FORWARD, "direction must be KB_REVERSE or KB_FORWARD");
@@ -670,6 +690,8 @@ int kb_evaluate_warped(kb_context *ctx, const kb_model *m, const kb_integrand *f
   ItemDev it = make_item(m, f, order);
   st = make_chain(chain, chain_len, it.chain);
   if (st) return st;
+  st = check_chain_dims(chain, chain_len, order);
+  if (st) return st;
   it.chain_len = chain_len;
   it.chain_start = start_domain_nr;
   return run_eval(ctx, it, IN_LI, count, li, keep_u_hypercube, algo, out, jac, in_domain, nullptr);
@@ -864,6 +886,8 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
   }
   it = make_item(w.m, &w.f, w.order);
   st = make_chain(w.chain, w.chain_len, it.chain);
+  if (st) return st;
+  st = check_chain_dims(w.chain, w.chain_len, w.order);
   if (st) return st;
   it.chain_len = w.chain_len;
   it.chain_start = w.chain_len;
@@ -1499,6 +1523,8 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     ItemDev &it = items[i];
     it = make_item(w.m, &w.f, w.order);
     st = make_chain(w.chain, w.chain_len, it.chain);
+    if (st) return st;
+    st = check_chain_dims(w.chain, w.chain_len, w.order);
     if (st) return st;
     it.chain_len = w.chain_len;
     it.chain_start = w.chain_len;

@@ -5,6 +5,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <math_constants.h>
+
 #include "kb_types.h"
 
 namespace kb {
@@ -151,10 +153,63 @@ __device__ __forceinline__ double warper_Finv(const WarperDev &w, double l) {
   }
 }
 
+// Interval i of the increasing points a[lo..hi] holding v: a[i] <= v < a[i+1], i in
+// [lo, hi-1] (GSL's bisection: the last point falls in the last interval).
+__device__ __forceinline__ int table_interval(const double *a, int lo, int hi, double v) {
+  while (hi > lo + 1) {
+    const int m = (lo + hi) >> 1;
+    if (a[m] > v)
+      hi = m;
+    else
+      lo = m;
+  }
+  return lo;
+}
+
+// Linear interpolation y(x) on the interval [x0, x1] (GSL's linear spline: y0 when the
+// interval is empty).
+__device__ __forceinline__ double table_lerp(double x, double x0, double x1, double y0, double y1) {
+  const double dx = x1 - x0;
+  return dx > 0.0 ? y0 + (x - x0) / dx * (y1 - y0) : y0;
+}
+
+// warper_product_1d_simple_interp_nearest_t (product_1d_simple.hpp:174-330) on one
+// coordinate: reverse u = F^-1(l), Jacobian 1/f1(u); forward l = F(u), Jacobian f1(u).
+// Outside the table's range the value is NaN (GSL's spline evaluation fails there).
+__device__ inline double table_reverse(const TableDimDev &t, double l, double &u) {
+  const double y = -l;
+  if (!(t.F[0] <= y && y <= t.F[t.cut])) {
+    u = CUDART_NAN;
+    return CUDART_NAN;
+  }
+  const int i = table_interval(t.F, 0, t.cut, y);
+  u = table_lerp(y, t.F[i], t.F[i + 1], t.u[i], t.u[i + 1]);
+  if (!(t.u[0] <= u && u <= t.u[t.n - 1])) return CUDART_NAN;
+  return 1.0 / t.fm[table_interval(t.u, 0, t.n - 1, u)];
+}
+__device__ inline double table_forward(const TableDimDev &t, double u, double &l) {
+  if (!(t.u[0] <= u && u <= t.u[t.n - 1])) {
+    l = CUDART_NAN;
+    return CUDART_NAN;
+  }
+  const int i = table_interval(t.u, 0, t.n - 1, u);
+  l = -table_lerp(u, t.u[i], t.u[i + 1], t.F[i], t.F[i + 1]);
+  return t.fm[i];
+}
+
 // One warper's map_reverse on x[0..n) (identity.hpp:34-48, plasma_uv.hpp:46-51,
 // product_1d_simple.hpp:109-117); returns its Jacobian.
 __device__ inline double warp_reverse_one(const WarperDev &w, int n, double *x, int stride) {
   if (w.kind == KB_WARPER_IDENTITY) return 1.0;
+  if (w.kind == KB_WARPER_TABLE) {
+    double jac = 1.0;
+    for (int i = 0; i < n; ++i) {
+      double u;
+      jac *= table_reverse(w.tab[w.ntab == 1 ? 0 : i], x[i * stride], u);
+      x[i * stride] = u;
+    }
+    return jac;
+  }
   if (w.kind == KB_WARPER_PLASMA_UV) {
     if (n > 0) {
       double u = w.u_max - x[0];
@@ -178,6 +233,15 @@ __device__ inline double warp_reverse_one(const WarperDev &w, int n, double *x, 
 // One warper's map_forward (plasma_uv.hpp:35-44, product_1d_simple.hpp:119-127).
 __device__ inline double warp_forward_one(const WarperDev &w, int n, double *x, int stride) {
   if (w.kind == KB_WARPER_IDENTITY) return 1.0;
+  if (w.kind == KB_WARPER_TABLE) {
+    double jac = 1.0;
+    for (int i = 0; i < n; ++i) {
+      double l;
+      jac *= table_forward(w.tab[w.ntab == 1 ? 0 : i], x[i * stride], l);
+      x[i * stride] = l;
+    }
+    return jac;
+  }
   if (w.kind == KB_WARPER_PLASMA_UV) {
     if (n > 0) {
       // sort descending (insertion sort; n <= MAX_ORDER), then consecutive differences

@@ -94,6 +94,17 @@ SobolDev sobol_dev(const kb_sobol *s);
 int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count);
 } // namespace kb
 
+// Tabulated product warper: per table the device arrays u, F, fm and the TableDimDev
+// descriptors (device) that the warper chain points at.
+struct kb_warper_table {
+  kb_context *ctx = nullptr;
+  int device = 0;
+  int ndims = 0;
+  double u_max = 0.0;
+  kb::TableDimDev *d_dims = nullptr; // [ndims]
+  double *d_data = nullptr;          // all tables' u, F, fm
+};
+
 // Learned coupling-flow warper: fp32 master weights and Adam moments in the internal
 // order [matrix][in][out], bf16 images for the tensor cores.
 struct kb_flow {

@@ -24,12 +24,26 @@ struct ModelDev {
   double pivot_floor; // |re|+|im| below which a tree pivot hands the point to the pivoted-LU kernel
 };
 
+// One tabulated 1D warper (warper_product_1d_simple_interp_nearest_t): the points u[n]
+// (u[0] = 0, increasing), F[n] the normalised integral of f1 from u to u_max, negated
+// (F[0] = -1 ... F[n-1] = 0), fm[n-1] = f1 on each interval (the mean of its ends), and
+// the last point `cut` before F's trailing zeros (the inverse interpolates F[0..cut]).
+struct TableDimDev {
+  const double *u;
+  const double *F;
+  const double *fm;
+  int n;
+  int cut;
+};
+
 struct WarperDev {
   int kind;
   int power;
   double u_max;
   double w;
-  double c[3]; // constants of the product makers, computed on the host (see make_warper_dev)
+  double c[3];             // constants of the product makers, computed on the host (see make_warper_dev)
+  const TableDimDev *tab;  // KB_WARPER_TABLE: ntab tables (1: every coordinate; n: one per coordinate)
+  int ntab;
 };
 
 struct SobolDev {
