@@ -79,7 +79,7 @@ int kb_sobol_points_dev(kb_context *ctx, const kb_sobol *s, uint32_t k_first, in
 #define KB_WARPER_INVERSE_SQUARE 4 /* make_product_1d_simple_inverse_square(u_max, w) (:594-608) */
 #define KB_WARPER_INVERSE_POWER 5  /* make_product_1d_simple_inverse_power(power, u_max, w) (:610-630) */
 #define KB_WARPER_UNIFORM 6        /* warper_product_1d_simple_t with f1 = 1/u_max (product_1d_simple_test.cpp:10-23) */
-#define KB_WARPER_TABLE 7          /* tabulated product warper: kb_warper_table (see below) */
+#define KB_WARPER_TABLE 7          /* device-resident product warper: kb_warper_table (see below) */
 #define KB_MAX_CHAIN 8
 
 typedef struct {
@@ -90,20 +90,68 @@ typedef struct {
   const struct kb_warper_table *table; /* KB_WARPER_TABLE only */
 } kb_warper;
 
-/* Tabulated product-1D warpers: warper_product_1d_simple_interp_nearest_t
- * (product_1d_simple.hpp:174-330; ndims = 1, the same table for every coordinate) and
- * warper_product_1d_interp_nearest_t (product_1d.hpp:164-211; one table per coordinate,
- * ndims = the order). Table d has npts[d] >= 3 points u (u[0] = 0, strictly increasing,
- * the last one the domain's u_max) with values f1 >= 0 there; the arrays of all tables are
- * concatenated. As keldy's integrate_and_inverse (product_1d_simple.hpp:219-253): F is
- * f1's trapezoid integral from u_max, normalised to 1; u = F^-1(l) and the Jacobian
- * 1/f1(u) use linear interpolation on the points (f1 on an interval: the mean of its ends).
- * Errors as keldy: "Model function is flat zero.", fewer than 3 points, u[0] != 0. */
+/* Device-resident product warpers, used in a chain as {KB_WARPER_TABLE, .table = t}. A
+ * table object holds one 1D warper per coordinate (ndims = the order) or one for every
+ * coordinate (ndims = 1). Its type:
+ * KB_TABLE_NEAREST: warper_product_1d_simple_interp_nearest_t (product_1d_simple.hpp:
+ *   174-330; ndims = 1) and warper_product_1d_interp_nearest_t (product_1d.hpp:164-211).
+ *   kb_warper_table_create: table d has npts[d] >= 3 points u (u[0] = 0, strictly
+ *   increasing, the last one the domain's u_max) with values f1 >= 0 there; the arrays of
+ *   all tables are concatenated. As keldy's integrate_and_inverse (:219-253): F is f1's
+ *   trapezoid integral from u_max, normalised to 1; u = F^-1(l) and the Jacobian 1/f1(u)
+ *   use linear interpolation on the points (f1 on an interval: the mean of its ends).
+ *   Errors as keldy: "Model function is flat zero.", fewer than 3 points, u[0] != 0.
+ * KB_TABLE_PROJECTION: warper_projection_t (projection.hpp:176-382), see below.
+ * KB_TABLE_ANALYTIC: warper_product_1d_t (product_1d.hpp:110-160): dims[d] one of the
+ *   product makers (KB_WARPER_EXPONENTIAL .. KB_WARPER_UNIFORM) for coordinate d
+ *   (make_product_1d_inverse_cube_alternate, :253-266).
+ * KB_TABLE_HYBRID: warper_product_1d_simple_interp_hybrid_t (product_1d_simple.hpp:
+ *   381-554) per coordinate: f1[d].kind names the closed form of f1 up to a factor
+ *   (EXPONENTIAL exp(-u/w), INVERSE w/(w+u), INVERSE_SQUARE (w/(w+u))^2, INVERSE_POWER
+ *   (w/(w+u))^power, UNIFORM 1), f1[d].u_max the domain, npts[d] >= 3 equidistant points;
+ *   F by Simpson's rule, Steffen splines of F and of its inverse, Jacobian from the closed
+ *   form (make_product_1d_inverse_cube_alternate_interp_hybrid, product_1d.hpp:290-309). */
+#define KB_TABLE_NEAREST 0
+#define KB_TABLE_PROJECTION 1
+#define KB_TABLE_ANALYTIC 2
+#define KB_TABLE_HYBRID 3
 typedef struct kb_warper_table kb_warper_table;
 int kb_warper_table_create(kb_context *ctx, int ndims, const int *npts, const double *u_pts, const double *f1_pts,
                            kb_warper_table **out);
+int kb_warper_table_analytic(kb_context *ctx, int ndims, const kb_warper *dims, kb_warper_table **out);
+int kb_warper_table_hybrid(kb_context *ctx, int ndims, const kb_warper *f1, const int *npts, kb_warper_table **out);
 int kb_warper_table_destroy(kb_warper_table *t);
+/* type, number of coordinates and (npts, optional, [ndims]) the points of each one's table */
+int kb_warper_table_info(const kb_warper_table *t, int *type, int *ndims, int *npts);
+/* KB_TABLE_NEAREST: the points u and the f1 values (as given, before normalisation) of
+ * coordinate d's table (npts[d] each). */
+int kb_warper_table_points(const kb_warper_table *t, int d, double *u, double *f1);
 
+/* make_warper_from_proj (warpers/make_warper_from_proj.hpp:118-153) from samples the
+ * caller computed: li [n][order] (keldy uses Sobol points 1..n of dimension order,
+ * unshifted) and values[n] = |f J| there. Per axis the mean value in each of num_bins
+ * bins of [0, 1], smoothed by a local linear fit of its logarithm with a Gaussian kernel
+ * of width sigma (kernel_smoothing, :40-66), turned into f1 points (f1[0] = 0,
+ * f1[i+1] = 2 s_i - f1[i]) of a KB_TABLE_NEAREST table per axis. */
+int kb_warper_table_from_samples(kb_context *ctx, int order, int num_bins, int64_t n, const double *li,
+                                 const double *values, double sigma, kb_warper_table **out);
+
+/* warper_projection_t(warped_integrand, order, num_bins, nr_samples, sigma, optimize_sigma)
+ * (projection.hpp:225-332) from samples li [n][order] with values |f J|: per axis the
+ * mean value in num_bins bins centred on the points i/(num_bins-1), smoothed with width
+ * sigma or, with optimize_sigma, the width (>= 0.3 bins) minimising the leave-one-out
+ * error (optimize_sigma, :82-128); fn = the smoothed projection on num_bins mesh points,
+ * its normalised integral, and the integral's inverse (Akima interpolation) on
+ * 1 + 5 (num_bins - 1) points. Reverse map u = inverse(l) with Jacobian norm / fn(u),
+ * forward l = integral(u) with Jacobian fn(u), all linearly interpolated on the meshes.
+ * num_bins >= 5. */
+int kb_warper_projection_create(kb_context *ctx, int order, int num_bins, int64_t n, const double *li,
+                                const double *values, double sigma, int optimize_sigma, kb_warper_table **out);
+/* One axis of a projection warper: its smoothing width (natural units), the binned mean
+ * |f J| and counts (num_bins each; get_xi) and fn on the mesh (num_bins; get_fi). Any
+ * output may be null. */
+int kb_warper_projection_axis(const kb_warper_table *t, int axis, double *sigma, double *xi, uint64_t *xi_count,
+                              double *fn);
 
 /* warper_train_t::map_reverse(li, start, end) (warpers.hpp:72-85; direction 0) or
  * map_forward(ui, start, end) (warpers.hpp:88-101; direction 1) on count points of n
@@ -184,16 +232,19 @@ int kb_evaluate_warped(kb_context *ctx, const kb_model *m, const kb_integrand *f
                        int chain_len, int start_domain_nr, int order, int64_t count, const double *li,
                        int keep_u_hypercube, int algo, double *out, double *jac, int *in_domain);
 
-/* make_warper_from_proj (warpers/make_warper_from_proj.hpp:100-153): the projections of
- * |f J| (integrand f on model m through `chain`, Sobol points 1..nr_samples of dimension
- * order, unshifted) on num_bins bins of each axis of [0,1]^order, averaged per bin,
- * smoothed by a local linear fit of their logarithm with a Gaussian kernel of width sigma
- * (kernel_smoothing, :40-66), turned into f1 points (f1[0] = 0, f1[i+1] = 2 s_i - f1[i])
- * of one table per axis. The table maps the Sobol point before `chain` (append it to the
- * chain's end). */
+/* make_warper_from_proj (warpers/make_warper_from_proj.hpp:118-153) for the integrand f
+ * on model m through `chain`: |f J| at Sobol points 1..nr_samples of dimension order
+ * (unshifted), evaluated on the GPU, then as kb_warper_table_from_samples. The table maps
+ * the Sobol point before `chain` (append it to the chain's end). */
 int kb_warper_table_from_projection(kb_context *ctx, const kb_model *m, const kb_integrand *f,
                                     const kb_warper *chain, int chain_len, int order, int num_bins, int nr_samples,
                                     double sigma, int keep_u_hypercube, kb_warper_table **out);
+/* warper_projection_t for the integrand f on model m through `chain` (Sobol points
+ * 1..nr_samples, unshifted, evaluated on the GPU). */
+int kb_warper_projection_from_integrand(kb_context *ctx, const kb_model *m, const kb_integrand *f,
+                                        const kb_warper *chain, int chain_len, int order, int num_bins,
+                                        int nr_samples, double sigma, int optimize_sigma, int keep_u_hypercube,
+                                        kb_warper_table **out);
 
 /* ------------------------------------------------------------- integrator --- */
 /* Running sums of integrator::run (integrator.hpp:50-52). */

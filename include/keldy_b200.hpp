@@ -232,6 +232,14 @@ inline warper_product_1d_simple_t make_product_1d_simple_uniform(double domain_u
 }
 
 namespace detail {
+inline std::shared_ptr<kb_warper_table> own_table(kb_warper_table *t) {
+  return std::shared_ptr<kb_warper_table>(t, [](kb_warper_table *p) { kb_warper_table_destroy(p); });
+}
+inline int table_dims(kb_warper_table const *t) {
+  int n = 0;
+  keldy_b200::check(kb_warper_table_info(t, nullptr, &n, nullptr));
+  return n;
+}
 inline std::shared_ptr<kb_warper_table> make_table(std::vector<int> const &npts, std::vector<double> const &u,
                                                    std::vector<double> const &f1) {
   kb_warper_table *t = nullptr;
@@ -298,14 +306,221 @@ class warper_product_1d_interp_nearest_t : public warper_base {
     desc_ = kb_warper{KB_WARPER_TABLE, 0, 1.0, 0.0, table_.get()};
   }
   void reserve(size_t n) { dims_.reserve(n); }
-  int size() const { return (int)dims_.size(); }
+  int size() const { return (dims_.empty() && table_) ? detail::table_dims(table_.get()) : (int)dims_.size(); }
   void emplace_back(warper_product_1d_simple_interp_nearest_t const &w) {
     dims_.push_back(w);
     rebuild();
   }
   warper_product_1d_simple_interp_nearest_t get_1d_warper(int axis) const {
-    if (axis < 0 || axis >= (int)dims_.size()) throw std::runtime_error("out of range axis");
+    if (axis < 0 || axis >= size()) throw std::runtime_error("out of range axis");
+    if (dims_.empty()) { // built by make_warper_from_proj: read its points back
+      std::vector<int> npts((size_t)size());
+      keldy_b200::check(kb_warper_table_info(table_.get(), nullptr, nullptr, npts.data()));
+      std::vector<double> u((size_t)npts[(size_t)axis]), f1(u.size());
+      keldy_b200::check(kb_warper_table_points(table_.get(), axis, u.data(), f1.data()));
+      return warper_product_1d_simple_interp_nearest_t(u, f1);
+    }
     return dims_[(size_t)axis];
+  }
+};
+
+namespace detail {
+// Sobol points 1..nr_samples of dimension order (keldy's sobol(order, 0), qrng.hpp:69-109)
+// and |warped_integrand| there, on the host (the caller's function).
+inline void sample_host(std::function<dcomplex(std::vector<double>)> const &warped_integrand, int order,
+                        int nr_samples, std::vector<double> &li, std::vector<double> &values) {
+  if (order < 1 || nr_samples < 1) throw std::runtime_error("need order >= 1 and nr_samples >= 1");
+  kb_sobol *g = nullptr;
+  keldy_b200::check(kb_sobol_create(keldy_b200::default_context(), order, 31, 0, 0, 0, &g));
+  li.assign((size_t)nr_samples * order, 0.0);
+  int st = kb_sobol_points(keldy_b200::default_context(), g, 1, nr_samples, li.data());
+  kb_sobol_destroy(g);
+  keldy_b200::check(st);
+  values.resize((size_t)nr_samples);
+  for (int p = 0; p < nr_samples; ++p)
+    values[(size_t)p] = std::abs(warped_integrand(std::vector<double>(li.begin() + (long)p * order,
+                                                                      li.begin() + (long)(p + 1) * order)));
+}
+} // namespace detail
+
+// product_1d.hpp:110-160: one analytic product maker per coordinate.
+class warper_product_1d_t : public warper_base {
+  std::vector<warper_product_1d_simple_t> dims_;
+
+ public:
+  warper_product_1d_t() = default;
+  void reserve(size_t n) { dims_.reserve(n); }
+  int size() const { return (int)dims_.size(); }
+  void emplace_back(warper_product_1d_simple_t const &w) {
+    dims_.push_back(w);
+    std::vector<kb_warper> d;
+    for (auto const &x : dims_) d.push_back(x.desc());
+    kb_warper_table *t = nullptr;
+    keldy_b200::check(kb_warper_table_analytic(keldy_b200::default_context(), (int)d.size(), d.data(), &t));
+    table_ = detail::own_table(t);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, d[0].u_max, 0.0, table_.get()};
+  }
+  warper_product_1d_simple_t get_1d_warper(int axis) const {
+    if (axis < 0 || axis >= size()) throw std::runtime_error("out of range axis");
+    return dims_[(size_t)axis];
+  }
+};
+
+// product_1d.hpp:253-266
+inline warper_product_1d_t make_product_1d_inverse_cube_alternate(int order, double time, double warper_scale) {
+  warper_product_1d_t result{};
+  result.reserve((size_t)order);
+  for (int n = 1; n <= order; ++n)
+    result.emplace_back(n % 2 == 0 ? make_product_1d_simple_inverse_power(3, time, warper_scale)
+                                   : make_product_1d_simple_inverse(time, warper_scale));
+  return result;
+}
+
+// product_1d.hpp:268-288: the same f1 shapes, tabulated on nr_sample_points points.
+inline warper_product_1d_interp_nearest_t make_product_1d_inverse_cube_alternate_interp_nearest(
+    int order, double time, double warper_scale, int nr_sample_points_warper) {
+  warper_product_1d_interp_nearest_t result{};
+  result.reserve((size_t)order);
+  auto f1 = [warper_scale](double t) -> double { return warper_scale / (warper_scale + t); };
+  auto f2 = [warper_scale](double t) -> double {
+    return warper_scale * warper_scale * warper_scale / ((warper_scale + t) * (warper_scale + t) * (warper_scale + t));
+  };
+  for (int n = 1; n <= order; ++n)
+    result.emplace_back(n % 2 == 0 ? warper_product_1d_simple_interp_nearest_t(f2, time, nr_sample_points_warper)
+                                   : warper_product_1d_simple_interp_nearest_t(f1, time, nr_sample_points_warper));
+  return result;
+}
+
+// product_1d_simple.hpp:381-554: f1 in closed form (f1_shape.kind: KB_WARPER_EXPONENTIAL
+// exp(-u/w), INVERSE w/(w+u), INVERSE_SQUARE (w/(w+u))^2, INVERSE_POWER (w/(w+u))^power,
+// UNIFORM 1; f1_shape.u_max the domain), Simpson integral on nr_sample_points points and
+// Steffen splines of the integral and of its inverse. keldy takes f1 as any function; the
+// device needs one of these closed forms.
+class warper_product_1d_simple_interp_hybrid_t : public warper_base {
+  kb_warper shape_{};
+  int npts_ = 0;
+
+ public:
+  warper_product_1d_simple_interp_hybrid_t(kb_warper const &f1_shape, int nr_sample_points)
+     : shape_(f1_shape), npts_(nr_sample_points) {
+    kb_warper_table *t = nullptr;
+    keldy_b200::check(kb_warper_table_hybrid(keldy_b200::default_context(), 1, &shape_, &npts_, &t));
+    table_ = detail::own_table(t);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, shape_.u_max, 0.0, table_.get()};
+  }
+  kb_warper const &get_f1_shape() const { return shape_; }
+  int get_nr_sample_points() const { return npts_; }
+};
+
+// product_1d.hpp:213-251: one hybrid warper per coordinate.
+class warper_product_1d_interp_hybrid_t : public warper_base {
+  std::vector<warper_product_1d_simple_interp_hybrid_t> dims_;
+
+ public:
+  warper_product_1d_interp_hybrid_t() = default;
+  void reserve(size_t n) { dims_.reserve(n); }
+  int size() const { return (int)dims_.size(); }
+  void emplace_back(warper_product_1d_simple_interp_hybrid_t const &w) {
+    dims_.push_back(w);
+    std::vector<kb_warper> shapes;
+    std::vector<int> npts;
+    for (auto const &x : dims_) {
+      shapes.push_back(x.get_f1_shape());
+      npts.push_back(x.get_nr_sample_points());
+    }
+    kb_warper_table *t = nullptr;
+    keldy_b200::check(
+        kb_warper_table_hybrid(keldy_b200::default_context(), (int)shapes.size(), shapes.data(), npts.data(), &t));
+    table_ = detail::own_table(t);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, shapes[0].u_max, 0.0, table_.get()};
+  }
+  warper_product_1d_simple_interp_hybrid_t get_1d_warper(int axis) const {
+    if (axis < 0 || axis >= size()) throw std::runtime_error("out of range axis");
+    return dims_[(size_t)axis];
+  }
+};
+
+// product_1d.hpp:290-309
+inline warper_product_1d_interp_hybrid_t make_product_1d_inverse_cube_alternate_interp_hybrid(
+    int order, double time, double warper_scale, int nr_sample_points_warper) {
+  warper_product_1d_interp_hybrid_t result{};
+  result.reserve((size_t)order);
+  for (int n = 1; n <= order; ++n)
+    result.emplace_back(warper_product_1d_simple_interp_hybrid_t(
+        n % 2 == 0 ? kb_warper{KB_WARPER_INVERSE_POWER, 3, time, warper_scale}
+                   : kb_warper{KB_WARPER_INVERSE, 0, time, warper_scale},
+        nr_sample_points_warper));
+  return result;
+}
+
+// The binned projection of one axis of a projection warper (binner_t<1, 0, double>):
+// mean |f J| and counts per bin.
+struct projection_bins {
+  double xmin = 0.0, xmax = 1.0;
+  std::vector<double> data;
+  std::vector<uint64_t> nr_values_added;
+  std::vector<double> const &get_data() const { return data; }
+  std::vector<uint64_t> const &get_nr_values_added() const { return nr_values_added; }
+  int get_nr_bins() const { return (int)data.size(); }
+  double get_bin_size() const { return (xmax - xmin) / double(data.size()); }
+  std::vector<double> get_bin_coord() const {
+    std::vector<double> c(data.size());
+    for (size_t i = 0; i < c.size(); ++i) c[i] = xmin + (double(i) + 0.5) * get_bin_size();
+    return c;
+  }
+};
+
+// projection.hpp:176-382: per axis the binned |f J| of nr_samples Sobol points, smoothed
+// (width sigma, or optimised), its normalised integral and the integral's inverse.
+class warper_projection_t : public warper_base {
+  int order_ = 0, num_bins_ = 0;
+
+  void adopt(kb_warper_table *t, int order, int num_bins) {
+    table_ = detail::own_table(t);
+    desc_ = kb_warper{KB_WARPER_TABLE, 0, 1.0, 0.0, table_.get()};
+    order_ = order;
+    num_bins_ = num_bins;
+  }
+
+ public:
+  warper_projection_t(std::function<dcomplex(std::vector<double>)> const &warped_integrand, int order, int num_bins,
+                      int nr_samples, double sigma, bool optimize_sigma = true) {
+    std::vector<double> li, values;
+    detail::sample_host(warped_integrand, order, nr_samples, li, values);
+    kb_warper_table *t = nullptr;
+    keldy_b200::check(kb_warper_projection_create(keldy_b200::default_context(), order, num_bins, nr_samples,
+                                                  li.data(), values.data(), sigma, optimize_sigma, &t));
+    adopt(t, order, num_bins);
+  }
+  // an already built projection warper (see make_projection_warper below)
+  explicit warper_projection_t(kb_warper_table *t) {
+    int n = detail::table_dims(t);
+    std::vector<int> npts((size_t)n);
+    keldy_b200::check(kb_warper_table_info(t, nullptr, nullptr, npts.data()));
+    adopt(t, n, npts[0]);
+  }
+  std::vector<double> get_sigmas() const {
+    std::vector<double> out((size_t)order_);
+    for (int a = 0; a < order_; ++a)
+      keldy_b200::check(kb_warper_projection_axis(table_.get(), a, &out[(size_t)a], nullptr, nullptr, nullptr));
+    return out;
+  }
+  // fn on the uniform mesh of [0, 1] with num_bins points
+  std::vector<double> get_fi(int axis) const {
+    std::vector<double> fn((size_t)num_bins_);
+    keldy_b200::check(kb_warper_projection_axis(table_.get(), axis, nullptr, nullptr, nullptr, fn.data()));
+    return fn;
+  }
+  projection_bins get_xi(int axis) const {
+    projection_bins b;
+    const double delta = 1.0 / (num_bins_ - 1.0);
+    b.xmin = -delta / 2;
+    b.xmax = 1 + delta / 2;
+    b.data.resize((size_t)num_bins_);
+    b.nr_values_added.resize((size_t)num_bins_);
+    keldy_b200::check(
+        kb_warper_projection_axis(table_.get(), axis, nullptr, b.data.data(), b.nr_values_added.data(), nullptr));
+    return b;
   }
 };
 
@@ -817,7 +1032,36 @@ class compute_charge_Q_direct_time : public integrator_g_direct_time {
 } // namespace impurity_oneband
 
 namespace warpers {
-// make_warper_from_proj (make_warper_from_proj.hpp:100-153) for the integrand of
+// make_warper_from_proj (make_warper_from_proj.hpp:118-153) for any warped integrand (the
+// caller's function, evaluated on the host at Sobol points 1..nr_samples).
+inline warper_product_1d_interp_nearest_t make_warper_from_proj(
+    std::function<dcomplex(std::vector<double>)> const &warped_integrand, int order, int num_bins, int nr_samples,
+    double sigma) {
+  std::vector<double> li, values;
+  detail::sample_host(warped_integrand, order, nr_samples, li, values);
+  kb_warper_table *t = nullptr;
+  keldy_b200::check(kb_warper_table_from_samples(keldy_b200::default_context(), order, num_bins, nr_samples,
+                                                 li.data(), values.data(), sigma, &t));
+  return warper_product_1d_interp_nearest_t(detail::own_table(t));
+}
+
+// warper_projection_t for the integrand of `computer` through its current warper train,
+// sampled on the GPU (the same tables as warper_projection_t(warped_integrand, ...) with
+// warped_integrand = computer.evaluate_warped_integrand(l, train size, keep_u_hypercube)).
+inline warper_projection_t make_projection_warper(impurity_oneband::integrator_g_direct const &computer, int order,
+                                                  int num_bins, int nr_samples, double sigma,
+                                                  bool optimize_sigma = true, bool keep_u_hypercube = true) {
+  auto const train = computer.get_warper();
+  auto const &chain = train.chain();
+  kb_integrand f = computer.get_integrand().abi();
+  kb_warper_table *t = nullptr;
+  keldy_b200::check(kb_warper_projection_from_integrand(
+      keldy_b200::default_context(), computer.get_integrand().get_g0().model.handle(), &f, chain.data(),
+      (int)chain.size(), order, num_bins, nr_samples, sigma, optimize_sigma, keep_u_hypercube, &t));
+  return warper_projection_t(t);
+}
+
+// make_warper_from_proj (make_warper_from_proj.hpp:118-153) for the integrand of
 // `computer` through its current warper train: one tabulated warper per axis, built from
 // the smoothed projections of |f J| on nr_samples Sobol points; append it to the train.
 inline warper_product_1d_interp_nearest_t make_warper_from_proj(impurity_oneband::integrator_g_direct const &computer,
@@ -831,8 +1075,7 @@ inline warper_product_1d_interp_nearest_t make_warper_from_proj(impurity_oneband
                                                     computer.get_integrand().get_g0().model.handle(), &f,
                                                     chain.data(), (int)chain.size(), order, num_bins, nr_samples,
                                                     sigma, keep_u_hypercube, &t));
-  return warper_product_1d_interp_nearest_t(
-      std::shared_ptr<kb_warper_table>(t, [](kb_warper_table *p) { kb_warper_table_destroy(p); }));
+  return warper_product_1d_interp_nearest_t(detail::own_table(t));
 }
 } // namespace warpers
 } // namespace keldy

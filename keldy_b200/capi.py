@@ -38,7 +38,10 @@ EXPORTS = [
     "kb_flow_create", "kb_flow_destroy", "kb_flow_dim", "kb_flow_get_params", "kb_flow_set_params", "kb_flow_map",
     "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
     "kb_integrate_kernel", "kb_integrand_kernel_eval", "kb_warper_table_create", "kb_warper_table_destroy",
-    "kb_warper_table_from_projection",
+    "kb_warper_table_from_projection", "kb_warper_table_analytic", "kb_warper_table_hybrid", "kb_warper_table_info",
+    "kb_warper_table_points",
+    "kb_warper_table_from_samples", "kb_warper_projection_create", "kb_warper_projection_axis",
+    "kb_warper_projection_from_integrand",
 ]
 FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
 FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
@@ -132,6 +135,17 @@ def load():
     L.kb_integrate.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(Accum)]
     L.kb_warper_table_create.argtypes = [_VP, C.c_int, _I, _D, _D, C.POINTER(_VP)]
     L.kb_warper_table_destroy.argtypes = [_VP]
+    L.kb_warper_table_analytic.argtypes = [_VP, C.c_int, C.POINTER(Warper), C.POINTER(_VP)]
+    L.kb_warper_table_hybrid.argtypes = [_VP, C.c_int, C.POINTER(Warper), _I, C.POINTER(_VP)]
+    L.kb_warper_table_info.argtypes = [_VP, _I, _I, _I]
+    L.kb_warper_table_points.argtypes = [_VP, C.c_int, _D, _D]
+    L.kb_warper_table_from_samples.argtypes = [_VP, C.c_int, C.c_int, C.c_int64, _D, _D, C.c_double, C.POINTER(_VP)]
+    L.kb_warper_projection_create.argtypes = [_VP, C.c_int, C.c_int, C.c_int64, _D, _D, C.c_double, C.c_int,
+                                              C.POINTER(_VP)]
+    L.kb_warper_projection_axis.argtypes = [_VP, C.c_int, _D, _D, C.POINTER(C.c_uint64), _D]
+    L.kb_warper_projection_from_integrand.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int,
+                                                      C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                                      C.POINTER(_VP)]
     L.kb_warper_table_from_projection.argtypes = [_VP, _VP, C.POINTER(Integrand), C.POINTER(Warper), C.c_int, C.c_int,
                                                   C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(_VP)]
     L.kb_integrate_kernel.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(TimeBins), C.POINTER(Accum), _D,
@@ -200,9 +214,22 @@ def chain_array(chain):
     return arr, len(chain)
 
 
+TABLE_NEAREST, TABLE_PROJECTION, TABLE_ANALYTIC, TABLE_HYBRID = 0, 1, 2, 3
+
+
+def _samples(li, values):
+    li = np.ascontiguousarray(np.atleast_2d(li), dtype=np.float64)
+    values = np.ascontiguousarray(values, dtype=np.float64)
+    if len(values) != len(li):
+        raise ValueError("one value per sample point")
+    return li, values
+
+
 class WarperTable:
-    """Tabulated product warper (kb_warper_table): one table for every coordinate or one per
-    coordinate. tables: list of (u_points, f1_values); use in a chain as (WARPER_TABLE, self)."""
+    """Device-resident product warper (kb_warper_table): one 1D warper for every
+    coordinate or one per coordinate; use in a chain as (WARPER_TABLE, self).
+    WarperTable(ctx, tables): interp-nearest tables from a list of (u_points, f1_values);
+    the classmethods build the other kinds."""
 
     def __init__(self, ctx, tables=None, _handle=None):
         self.ctx = ctx
@@ -229,6 +256,77 @@ class WarperTable:
                                                     int(nr_samples), float(sigma), int(keep_u_hypercube),
                                                     C.byref(h)))
         return cls(ctx, _handle=h)
+
+    @classmethod
+    def analytic(cls, ctx, dims):
+        """warper_product_1d_t: dims = [(kind, u_max, w[, power])] per coordinate."""
+        arr = (Warper * len(dims))()
+        for i, c in enumerate(dims):
+            arr[i] = Warper(int(c[0]), int(c[3]) if len(c) > 3 else 0, float(c[1]), float(c[2]), None)
+        h = _VP()
+        check(ctx.L.kb_warper_table_analytic(ctx.h, len(dims), arr, C.byref(h)))
+        return cls(ctx, _handle=h)
+
+    @classmethod
+    def hybrid(cls, ctx, shapes, npts):
+        """warper_product_1d_simple_interp_hybrid_t per coordinate: shapes = [(kind, u_max,
+        w[, power])], the closed form of f1 (up to a factor) and the domain; npts points each."""
+        arr = (Warper * len(shapes))()
+        for i, c in enumerate(shapes):
+            arr[i] = Warper(int(c[0]), int(c[3]) if len(c) > 3 else 0, float(c[1]), float(c[2]), None)
+        n = np.ascontiguousarray(np.broadcast_to(np.asarray(npts, dtype=np.int32), (len(shapes),)))
+        h = _VP()
+        check(ctx.L.kb_warper_table_hybrid(ctx.h, len(shapes), arr, n.ctypes.data_as(_I), C.byref(h)))
+        return cls(ctx, _handle=h)
+
+    @classmethod
+    def from_samples(cls, ctx, li, values, num_bins, sigma):
+        """make_warper_from_proj from samples li [n, order] with values |f J|."""
+        li, values = _samples(li, values)
+        h = _VP()
+        check(ctx.L.kb_warper_table_from_samples(ctx.h, li.shape[1], int(num_bins), len(li), _dp(li), _dp(values),
+                                                 float(sigma), C.byref(h)))
+        return cls(ctx, _handle=h)
+
+    @classmethod
+    def projection(cls, ctx, li, values, num_bins, sigma, optimize_sigma=True):
+        """warper_projection_t from samples li [n, order] with values |f J|."""
+        li, values = _samples(li, values)
+        h = _VP()
+        check(ctx.L.kb_warper_projection_create(ctx.h, li.shape[1], int(num_bins), len(li), _dp(li), _dp(values),
+                                                float(sigma), int(bool(optimize_sigma)), C.byref(h)))
+        return cls(ctx, _handle=h)
+
+    @classmethod
+    def projection_from_integrand(cls, ctx, model, A, B, chain, order, num_bins, nr_samples, sigma,
+                                  optimize_sigma=True, keep_u_hypercube=True, cutoff=0.0):
+        """warper_projection_t for the integrand through `chain`, sampled on the GPU."""
+        arr, L = chain_array(chain)
+        f = Integrand(gf_index(A), gf_index(B), float(cutoff))
+        h = _VP()
+        check(ctx.L.kb_warper_projection_from_integrand(ctx.h, model.h, C.byref(f), arr, L, int(order),
+                                                        int(num_bins), int(nr_samples), float(sigma),
+                                                        int(bool(optimize_sigma)), int(keep_u_hypercube),
+                                                        C.byref(h)))
+        return cls(ctx, _handle=h)
+
+    def info(self):
+        """(type, ndims, points of each coordinate's first table)."""
+        t, n = C.c_int(), C.c_int()
+        check(self.ctx.L.kb_warper_table_info(self.h, C.byref(t), C.byref(n), None))
+        pts = np.zeros(n.value, dtype=np.int32)
+        check(self.ctx.L.kb_warper_table_info(self.h, None, None, pts.ctypes.data_as(_I)))
+        return t.value, n.value, pts
+
+    def projection_axis(self, axis):
+        """Projection warper: (sigma, xi means, xi counts, fn) of one axis."""
+        nb = int(self.info()[2][axis])
+        s = C.c_double()
+        xi, fn = np.zeros(nb), np.zeros(nb)
+        cnt = np.zeros(nb, dtype=np.uint64)
+        check(self.ctx.L.kb_warper_projection_axis(self.h, int(axis), C.byref(s), _dp(xi),
+                                                   cnt.ctypes.data_as(C.POINTER(C.c_uint64)), _dp(fn)))
+        return s.value, xi, cnt, fn
 
     def entry(self):
         return (WARPER_TABLE, self)

@@ -122,6 +122,61 @@ PYBIND11_MODULE(_keldy, m) {
                  .def("emplace_back", &warper_product_1d_interp_nearest_t::emplace_back, py::arg("w"))
                  .def("get_1d_warper", &warper_product_1d_interp_nearest_t::get_1d_warper, py::arg("axis"));
   warper_methods<warper_product_1d_interp_nearest_t>(wpn);
+  auto wpa = py::class_<warper_product_1d_t>(m, "WarperProduct1dT")
+                 .def(py::init<>())
+                 .def("reserve", &warper_product_1d_t::reserve, py::arg("new_cap"))
+                 .def("size", &warper_product_1d_t::size)
+                 .def("emplace_back", &warper_product_1d_t::emplace_back, py::arg("w"))
+                 .def("get_1d_warper", &warper_product_1d_t::get_1d_warper, py::arg("axis"));
+  warper_methods<warper_product_1d_t>(wpa);
+  m.def("make_product_1d_inverse_cube_alternate", &make_product_1d_inverse_cube_alternate, py::arg("order"),
+        py::arg("time"), py::arg("warper_scale"));
+  m.def("make_product_1d_inverse_cube_alternate_interp_nearest", &make_product_1d_inverse_cube_alternate_interp_nearest,
+        py::arg("order"), py::arg("time"), py::arg("warper_scale"), py::arg("nr_sample_points_warper"));
+  // f1_: the closed form of f1 by name (the device has no Python); w_scale, power its parameters
+  auto wth =
+      py::class_<warper_product_1d_simple_interp_hybrid_t>(m, "WarperProduct1dSimpleInterpHybridT")
+          .def(py::init([](py::object f1, double domain_u_max, int n, double w_scale, int power) {
+                 if (!py::isinstance<py::str>(f1))
+                   throw std::runtime_error("WarperProduct1dSimpleInterpHybridT needs f1 in closed form on the GPU: "
+                                            "'exponential', 'inverse', 'inverse_square', 'inverse_power' or "
+                                            "'uniform' (with w_scale, power)");
+                 const std::string name = f1.cast<std::string>();
+                 int kind = name == "exponential"      ? KB_WARPER_EXPONENTIAL
+                            : name == "inverse"        ? KB_WARPER_INVERSE
+                            : name == "inverse_square" ? KB_WARPER_INVERSE_SQUARE
+                            : name == "inverse_power"  ? KB_WARPER_INVERSE_POWER
+                            : name == "uniform"        ? KB_WARPER_UNIFORM
+                                                       : -1;
+                 if (kind < 0) throw std::runtime_error("unknown f1 closed form '" + name + "'");
+                 return warper_product_1d_simple_interp_hybrid_t(kb_warper{kind, power, domain_u_max, w_scale}, n);
+               }),
+               py::arg("f1_"), py::arg("domain_u_max_"), py::arg("nr_sample_points_"), py::arg("w_scale") = 1.0,
+               py::arg("power") = 1);
+  warper_methods<warper_product_1d_simple_interp_hybrid_t>(wth);
+  auto wph = py::class_<warper_product_1d_interp_hybrid_t>(m, "WarperProduct1dInterpHybridT")
+                 .def(py::init<>())
+                 .def("reserve", &warper_product_1d_interp_hybrid_t::reserve, py::arg("new_cap"))
+                 .def("size", &warper_product_1d_interp_hybrid_t::size)
+                 .def("emplace_back", &warper_product_1d_interp_hybrid_t::emplace_back, py::arg("w"))
+                 .def("get_1d_warper", &warper_product_1d_interp_hybrid_t::get_1d_warper, py::arg("axis"));
+  warper_methods<warper_product_1d_interp_hybrid_t>(wph);
+  m.def("make_product_1d_inverse_cube_alternate_interp_hybrid", &make_product_1d_inverse_cube_alternate_interp_hybrid,
+        py::arg("order"), py::arg("time"), py::arg("warper_scale"), py::arg("nr_sample_points_warper"));
+  py::class_<projection_bins>(m, "ProjectionBins")
+      .def("get_data", &projection_bins::get_data)
+      .def("get_nr_values_added", &projection_bins::get_nr_values_added)
+      .def("get_nr_bins", &projection_bins::get_nr_bins)
+      .def("get_bin_size", &projection_bins::get_bin_size)
+      .def("get_bin_coord", &projection_bins::get_bin_coord);
+  auto wpr = py::class_<warper_projection_t>(m, "WarperProjectionT")
+                 .def(py::init<std::function<dcomplex(std::vector<double>)> const &, int, int, int, double, bool>(),
+                      py::arg("warped_integrand"), py::arg("order"), py::arg("num_bins"), py::arg("nr_samples"),
+                      py::arg("sigma"), py::arg("optimize_sigma") = true)
+                 .def("get_xi", &warper_projection_t::get_xi, py::arg("axis"))
+                 .def("get_sigmas", &warper_projection_t::get_sigmas)
+                 .def("get_fi", &warper_projection_t::get_fi, py::arg("axis"));
+  warper_methods<warper_projection_t>(wpr);
   m.def("vi_from_ui", &vi_from_ui, py::arg("t_max"), py::arg("u_times"));
   m.def("ui_from_vi", &ui_from_vi, py::arg("t_max"), py::arg("v_times"));
 
@@ -136,6 +191,13 @@ PYBIND11_MODULE(_keldy, m) {
            py::arg("w"))
       .def("emplace_back", [](warper_train_t &t, warper_product_1d_interp_nearest_t const &w) { t.emplace_back(w); },
            py::arg("w"))
+      .def("emplace_back", [](warper_train_t &t, warper_product_1d_t const &w) { t.emplace_back(w); }, py::arg("w"))
+      .def("emplace_back",
+           [](warper_train_t &t, warper_product_1d_simple_interp_hybrid_t const &w) { t.emplace_back(w); },
+           py::arg("w"))
+      .def("emplace_back", [](warper_train_t &t, warper_product_1d_interp_hybrid_t const &w) { t.emplace_back(w); },
+           py::arg("w"))
+      .def("emplace_back", [](warper_train_t &t, warper_projection_t const &w) { t.emplace_back(w); }, py::arg("w"))
       .def("reserve", &warper_train_t::reserve, py::arg("new_cap"))
       .def("clear", &warper_train_t::clear)
       .def("size", &warper_train_t::size)
@@ -243,6 +305,19 @@ PYBIND11_MODULE(_keldy, m) {
       },
       py::arg("computer"), py::arg("order"), py::arg("num_bins"), py::arg("nr_samples"), py::arg("sigma"),
       py::arg("keep_u_hypercube") = true);
+  m.def(
+      "make_warper_from_proj",
+      [](std::function<dcomplex(std::vector<double>)> const &f, int order, int num_bins, int nr_samples,
+         double sigma) { return keldy::warpers::make_warper_from_proj(f, order, num_bins, nr_samples, sigma); },
+      py::arg("warped_integrand"), py::arg("order"), py::arg("num_bins"), py::arg("nr_samples"), py::arg("sigma"));
+  m.def(
+      "make_projection_warper",
+      [](compute_charge_Q_direct const &c, int order, int num_bins, int nr_samples, double sigma, bool optimize,
+         bool keep) {
+        return keldy::warpers::make_projection_warper(c, order, num_bins, nr_samples, sigma, optimize, keep);
+      },
+      py::arg("computer"), py::arg("order"), py::arg("num_bins"), py::arg("nr_samples"), py::arg("sigma"),
+      py::arg("optimize_sigma") = true, py::arg("keep_u_hypercube") = true);
   py::class_<binner_2d>(m, "BinnerT11")
       .def(py::init<double, double, long>(), py::arg("xmin"), py::arg("xmax"), py::arg("nr_bins"))
       .def("get_data_flat", &binner_2d::get_data_flat)

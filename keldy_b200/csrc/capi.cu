@@ -272,11 +272,32 @@ static int make_warper_dev(const kb_warper &w, WarperDev &d) {
   }
 }
 
-// A tabulated warper with one table per coordinate needs as many coordinates as tables.
+} // extern "C"
+
+namespace kb {
+int simple_dev(const kb_warper &w, SimpleDev &out) {
+  WarperDev d;
+  int st = make_warper_dev(w, d);
+  if (st) return st;
+  out.kind = d.kind;
+  out.power = d.power;
+  out.u_max = d.u_max;
+  out.w = d.w;
+  for (int i = 0; i < 3; ++i) out.c[i] = d.c[i];
+  return KB_OK;
+}
+} // namespace kb
+
+extern "C" {
+
+// A product warper with one 1D warper per coordinate maps coordinate i with warper i
+// (keldy's ui_from_li enumerates the point's coordinates, product_1d.hpp and
+// projection.hpp:330-344): it needs at least as many warpers as coordinates; one 1D
+// warper maps every coordinate.
 static int check_chain_dims(const kb_warper *chain, int len, int n) {
   for (int i = 0; i < len; ++i)
     if (chain[i].kind == KB_WARPER_TABLE && chain[i].table && chain[i].table->ndims != 1 &&
-        chain[i].table->ndims != n)
+        chain[i].table->ndims < n)
       return fail(KB_E_INVALID, "the tabulated warper has " + std::to_string(chain[i].table->ndims) +
                                     " tables for " + std::to_string(n) + " coordinates");
   return KB_OK;

@@ -115,8 +115,10 @@ __device__ __forceinline__ double sobol_coord(const SobolDev &s, uint32_t k, int
 // ---------------------------------------------------------------- warpers
 // f1, f1_integrated and f1_integrated_inverse of the analytic product makers
 // (product_1d_simple.hpp:560-630). The constants c[] are the makers' normalisations,
-// evaluated once on the host in long double and rounded to double.
-__device__ __forceinline__ double warper_f1(const WarperDev &w, double t) {
+// evaluated once on the host in long double and rounded to double. W is WarperDev or
+// SimpleDev (the same fields).
+template <class W>
+__device__ __forceinline__ double warper_f1(const W &w, double t) {
   switch (w.kind) {
   case KB_WARPER_EXPONENTIAL: return exp(-t / w.w) / w.c[1];
   case KB_WARPER_INVERSE: return 1.0 / (w.c[0] * (w.w + t));
@@ -127,7 +129,8 @@ __device__ __forceinline__ double warper_f1(const WarperDev &w, double t) {
   }
 }
 
-__device__ __forceinline__ double warper_F(const WarperDev &w, double t) {
+template <class W>
+__device__ __forceinline__ double warper_F(const W &w, double t) {
   switch (w.kind) {
   case KB_WARPER_EXPONENTIAL: return expm1((w.u_max - t) / w.w) / w.c[0];
   case KB_WARPER_INVERSE: return log1p(t / w.w) / w.c[0];
@@ -139,7 +142,8 @@ __device__ __forceinline__ double warper_F(const WarperDev &w, double t) {
   }
 }
 
-__device__ __forceinline__ double warper_Finv(const WarperDev &w, double l) {
+template <class W>
+__device__ __forceinline__ double warper_Finv(const W &w, double l) {
   switch (w.kind) {
   case KB_WARPER_EXPONENTIAL: return w.u_max - w.w * log1p(w.c[0] * l);
   case KB_WARPER_INVERSE: return w.w * expm1(l * w.c[0]);
@@ -150,6 +154,26 @@ __device__ __forceinline__ double warper_Finv(const WarperDev &w, double l) {
   }
   case KB_WARPER_UNIFORM: return w.u_max * l;
   default: return l;
+  }
+}
+
+// The unnormalised f1 shapes of the hybrid warpers (make_product_1d_inverse_cube_alternate_
+// interp_hybrid, product_1d.hpp:293-300): exp(-t/w), w/(w+t), (w/(w+t))^2, w^p/(w+t)^p
+// (products in keldy's order), 1.
+__device__ __forceinline__ double hybrid_f1(const SimpleDev &f, double t) {
+  switch (f.kind) {
+  case KB_WARPER_EXPONENTIAL: return exp(-t / f.w);
+  case KB_WARPER_INVERSE: return f.w / (f.w + t);
+  case KB_WARPER_INVERSE_SQUARE: return f.w * f.w / ((f.w + t) * (f.w + t));
+  case KB_WARPER_INVERSE_POWER: {
+    double num = f.w, den = f.w + t;
+    for (int k = 1; k < f.power; ++k) {
+      num *= f.w;
+      den *= f.w + t;
+    }
+    return num / den;
+  }
+  default: return 1.0;
   }
 }
 
@@ -173,28 +197,91 @@ __device__ __forceinline__ double table_lerp(double x, double x0, double x1, dou
   return dx > 0.0 ? y0 + (x - x0) / dx * (y1 - y0) : y0;
 }
 
-// warper_product_1d_simple_interp_nearest_t (product_1d_simple.hpp:174-330) on one
-// coordinate: reverse u = F^-1(l), Jacobian 1/f1(u); forward l = F(u), Jacobian f1(u).
-// Outside the table's range the value is NaN (GSL's spline evaluation fails there).
-__device__ inline double table_reverse(const TableDimDev &t, double l, double &u) {
-  const double y = -l;
-  if (!(t.F[0] <= y && y <= t.F[t.cut])) {
-    u = CUDART_NAN;
-    return CUDART_NAN;
-  }
-  const int i = table_interval(t.F, 0, t.cut, y);
-  u = table_lerp(y, t.F[i], t.F[i + 1], t.u[i], t.u[i + 1]);
-  if (!(t.u[0] <= u && u <= t.u[t.n - 1])) return CUDART_NAN;
-  return 1.0 / t.fm[table_interval(t.u, 0, t.n - 1, u)];
+// Cubic Hermite interpolation on [x0, x1] from the end values y0, y1 and slopes d0, d1
+// (the form of GSL's Steffen spline between two knots).
+__device__ __forceinline__ double table_hermite(double x, double x0, double x1, double y0, double y1, double d0,
+                                                double d1) {
+  const double h = x1 - x0;
+  const double s = (y1 - y0) / h;
+  const double c2 = (3.0 * s - 2.0 * d0 - d1) / h;
+  const double c3 = (d0 + d1 - 2.0 * s) / (h * h);
+  const double dx = x - x0;
+  return y0 + dx * (d0 + dx * (c2 + dx * c3));
 }
-__device__ inline double table_forward(const TableDimDev &t, double u, double &l) {
-  if (!(t.u[0] <= u && u <= t.u[t.n - 1])) {
-    l = CUDART_NAN;
-    return CUDART_NAN;
+
+// A real function on the uniform mesh of [0, 1] with n points, linearly interpolated
+// (TRIQS gf<retime> evaluation): NaN outside the mesh (out of window).
+__device__ __forceinline__ double mesh_eval(const double *g, int n, double x) {
+  const double delta_inv = 1.0 / (1.0 / (n - 1));
+  const double a = x * delta_inv;
+  double fi = floor(a);
+  double w = a - fi;
+  long i = (long)fi;
+  if (i == n - 1 && fabs(w) < 1e-14) {
+    i = n - 2;
+    w = 1.0;
   }
-  const int i = table_interval(t.u, 0, t.n - 1, u);
-  l = -table_lerp(u, t.u[i], t.u[i + 1], t.F[i], t.F[i + 1]);
-  return t.fm[i];
+  if (!(i >= 0 && i < n - 1) || !(x == x)) return CUDART_NAN;
+  return (1.0 - w) * g[i] + w * g[i + 1];
+}
+
+// One coordinate of a device-resident product warper. reverse: u from l and the Jacobian
+// of u(l); forward: l from u and the Jacobian of l(u). Outside a table's range the values
+// are NaN (GSL's and TRIQS's evaluations fail there).
+__device__ inline double table_reverse(const TableDimDev &t, double l, double &u) {
+  switch (t.type) {
+  case TAB_NEAREST: { // product_1d_simple.hpp:206-217, 270-278
+    const double y = -l;
+    if (!(t.p1[0] <= y && y <= t.p1[t.cut])) break;
+    const int i = table_interval(t.p1, 0, t.cut, y);
+    u = table_lerp(y, t.p1[i], t.p1[i + 1], t.p0[i], t.p0[i + 1]);
+    if (!(t.p0[0] <= u && u <= t.p0[t.n - 1])) return CUDART_NAN;
+    return 1.0 / t.p2[table_interval(t.p0, 0, t.n - 1, u)];
+  }
+  case TAB_PROJECTION: // projection.hpp:330-344, 361-363
+    u = mesh_eval(t.p2, t.m, l);
+    return t.norm / mesh_eval(t.p0, t.n, u);
+  case TAB_ANALYTIC:
+    u = warper_Finv(t.f, l);
+    return 1.0 / warper_f1(t.f, u);
+  case TAB_HYBRID: { // product_1d_simple.hpp:411-415, 484-492
+    const double y = -l;
+    if (!(t.p1[0] <= y && y <= t.p1[t.cut])) break;
+    const int i = table_interval(t.p1, 0, t.cut, y);
+    u = table_hermite(y, t.p1[i], t.p1[i + 1], t.p0[i], t.p0[i + 1], t.p3[i], t.p3[i + 1]);
+    return 1.0 / (hybrid_f1(t.f, u) / t.norm);
+  }
+  }
+  u = CUDART_NAN;
+  return CUDART_NAN;
+}
+
+__device__ inline double table_forward(const TableDimDev &t, double u, double &l) {
+  switch (t.type) {
+  case TAB_NEAREST: {
+    if (!(t.p0[0] <= u && u <= t.p0[t.n - 1])) break;
+    const int i = table_interval(t.p0, 0, t.n - 1, u);
+    l = -table_lerp(u, t.p0[i], t.p0[i + 1], t.p1[i], t.p1[i + 1]);
+    return t.p2[i];
+  }
+  case TAB_PROJECTION: // projection.hpp:338-345, 352-358
+    l = mesh_eval(t.p1, t.n, u);
+    return mesh_eval(t.p0, t.n, u);
+  case TAB_ANALYTIC: {
+    const double f = warper_f1(t.f, u);
+    l = warper_F(t.f, u);
+    return f;
+  }
+  case TAB_HYBRID: {
+    if (!(t.p0[0] <= u && u <= t.p0[t.n - 1])) break;
+    const int i = table_interval(t.p0, 0, t.n - 1, u);
+    const double f = hybrid_f1(t.f, u) / t.norm;
+    l = -table_hermite(u, t.p0[i], t.p0[i + 1], t.p1[i], t.p1[i + 1], t.p2[i], t.p2[i + 1]);
+    return f;
+  }
+  }
+  l = CUDART_NAN;
+  return CUDART_NAN;
 }
 
 // One warper's map_reverse on x[0..n) (identity.hpp:34-48, plasma_uv.hpp:46-51,

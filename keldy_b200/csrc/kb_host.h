@@ -7,6 +7,7 @@
 
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "kb_flow.h"
 #include "kb_launch.h"
@@ -94,16 +95,29 @@ SobolDev sobol_dev(const kb_sobol *s);
 int check_sobol_range(const kb_sobol *s, uint32_t k_first, int64_t count);
 } // namespace kb
 
-// Tabulated product warper: per table the device arrays u, F, fm and the TableDimDev
-// descriptors (device) that the warper chain points at.
+// Device-resident product warper (tabulated, projection, hybrid or per-coordinate
+// analytic): the per-coordinate descriptors and their arrays on the device, and what the
+// projection warper reports back (its widths, binned projections and smoothed fn).
 struct kb_warper_table {
   kb_context *ctx = nullptr;
   int device = 0;
   int ndims = 0;
+  int type = KB_TABLE_NEAREST;
   double u_max = 0.0;
   kb::TableDimDev *d_dims = nullptr; // [ndims]
-  double *d_data = nullptr;          // all tables' u, F, fm
+  double *d_data = nullptr;          // all coordinates' arrays
+  std::vector<int> npts;             // points of each coordinate's first table
+  std::vector<std::vector<double>> pts_u, pts_f1; // nearest tables: the points and f1 as given
+  std::vector<double> sigmas;        // projection: smoothing width per axis (natural units)
+  std::vector<std::vector<double>> xi;
+  std::vector<std::vector<uint64_t>> xi_count;
+  std::vector<std::vector<double>> fn;
 };
+
+namespace kb {
+// The device form of one analytic product maker (the constants of make_warper_dev).
+int simple_dev(const kb_warper &w, SimpleDev &out);
+} // namespace kb
 
 // Learned coupling-flow warper: fp32 master weights and Adam moments in the internal
 // order [matrix][in][out], bf16 images for the tensor cores.

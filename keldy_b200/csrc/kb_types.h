@@ -24,16 +24,49 @@ struct ModelDev {
   double pivot_floor; // |re|+|im| below which a tree pivot hands the point to the pivoted-LU kernel
 };
 
-// One tabulated 1D warper (warper_product_1d_simple_interp_nearest_t): the points u[n]
-// (u[0] = 0, increasing), F[n] the normalised integral of f1 from u to u_max, negated
-// (F[0] = -1 ... F[n-1] = 0), fm[n-1] = f1 on each interval (the mean of its ends), and
-// the last point `cut` before F's trailing zeros (the inverse interpolates F[0..cut]).
+// One analytic 1D warper of the product makers (product_1d_simple.hpp:560-630): kind
+// (KB_WARPER_*), power, u_max, w and the constants c[] computed on the host.
+struct SimpleDev {
+  int kind;
+  int power;
+  double u_max;
+  double w;
+  double c[3];
+};
+
+// What one coordinate of a device-resident product warper (kb_warper_table) holds.
+enum TableType : int {
+  // warper_product_1d_simple_interp_nearest_t (product_1d_simple.hpp:174-330): p0 = the
+  // points u[n] (u[0] = 0, increasing), p1 = F[n], the normalised integral of f1 from u to
+  // u_max, negated (F[0] = -1 ... F[n-1] = 0), p2 = f1 on each of the n-1 intervals (the
+  // mean of its ends); the inverse interpolates F[0..cut] (cut: the last point before F's
+  // trailing zeros).
+  TAB_NEAREST = 0,
+  // warper_projection_t (projection.hpp:176-382): uniform meshes of [0, 1]: p0 = fn[n],
+  // p1 = its normalised integral fint[n], p2 = the inverse of fint on m points; norm = the
+  // integral before normalisation.
+  TAB_PROJECTION = 1,
+  // one analytic warper_product_1d_simple_t per coordinate (warper_product_1d_t,
+  // product_1d.hpp:110-160): f.
+  TAB_ANALYTIC = 2,
+  // warper_product_1d_simple_interp_hybrid_t (product_1d_simple.hpp:381-554): p0 = u[n],
+  // p1 = F[n] (Simpson's rule), p2 = Steffen slopes dF/du at the n points, p3 = Steffen
+  // slopes du/dF of the inverse at F[0..cut]; the Jacobian uses the closed form f.kind of
+  // f1 divided by norm.
+  TAB_HYBRID = 3,
+};
+
 struct TableDimDev {
-  const double *u;
-  const double *F;
-  const double *fm;
+  int type;
   int n;
+  int m;
   int cut;
+  const double *p0;
+  const double *p1;
+  const double *p2;
+  const double *p3;
+  double norm;
+  SimpleDev f;
 };
 
 struct WarperDev {

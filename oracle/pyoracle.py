@@ -320,10 +320,23 @@ class Reference:
         L.ref_integrate.argtypes = [C.c_void_p, C.POINTER(GfIndex), C.POINTER(GfIndex), C.c_double,
                                     C.POINTER(Warper), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                     C.c_long, C.c_int, C.c_int, _D]
+        L.ref_interp_nearest.argtypes = [C.c_int, _D, _D, C.c_int, C.c_int, C.c_long, _D, _D, _D]
 
     def _check(self, st):
         if st != 0:
             raise RuntimeError(self.lib.ref_last_error().decode())
+
+    def interp_nearest(self, u, f1, x, direction="reverse"):
+        """keldy's warper_product_1d_simple_interp_nearest_t(u, f1).map_reverse / map_forward
+        on the rows of x."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        f1 = np.ascontiguousarray(f1, dtype=np.float64)
+        x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
+        out = np.zeros_like(x)
+        jac = np.zeros(len(x))
+        self._check(self.lib.ref_interp_nearest(len(u), _dp(u), _dp(f1), 0 if direction == "reverse" else 1,
+                                                x.shape[1], len(x), _dp(x), _dp(out), _dp(jac)))
+        return out, jac
 
     def sobol_matrices(self, dim, m=32):
         out = np.zeros(dim * m, dtype=np.uint32)

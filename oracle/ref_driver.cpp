@@ -176,6 +176,30 @@ int ref_warp(ref_warper_desc const *chain, int len, int direction, int start, in
   return 0;
 }
 
+// keldy's warper_product_1d_simple_interp_nearest_t(times_u_pts, f1_pts) on count points
+// of n coordinates: direction 0 map_reverse, 1 map_forward.
+int ref_interp_nearest(int npts, double const *u, double const *f1, int direction, int n, long count,
+                       double const *in, double *out, double *jac) {
+  try {
+    triqs::arrays::vector<double> tu(npts), tf(npts);
+    for (int i = 0; i < npts; ++i) {
+      tu[i] = u[i];
+      tf[i] = f1[i];
+    }
+    warper_product_1d_simple_interp_nearest_t w(tu, tf);
+    for (long p = 0; p < count; ++p) {
+      std::vector<double> x(in + p * n, in + (p + 1) * n);
+      auto r = direction == 0 ? w.map_reverse(x) : w.map_forward(x);
+      std::memcpy(out + p * n, r.first.data(), sizeof(double) * static_cast<size_t>(n));
+      jac[p] = r.second;
+    }
+  } catch (std::exception const &e) {
+    g_err = e.what();
+    return -1;
+  }
+  return 0;
+}
+
 // A g0 model whose lesser/greater tables (interleaved complex, orbital (0,0), on the
 // mesh [-time_max, time_max] with npts points) are given; spin down = spin up.
 void *ref_model_create(int npts, double time_max, double alpha, double const *lesser, double const *greater) {

@@ -7,12 +7,13 @@ built oracle/_ref (``make -C oracle``):
 
 * golden.npz: outputs of keldy's own code (digitalseq_b2g.hpp, the warper headers and
   wick_direct.cpp, compiled by oracle/Makefile) on seeded inputs: Sobol points, warper
-  chains, integrand values (two g0 tables, several external-point pairs, orders 0-6),
+  chains, tabulated (interp-nearest) warpers, integrand values (two g0 tables, several external-point pairs, orders 0-6),
   eval_no_det values and the integrator's sums.
 * keldy_tests.json: known answers read from keldy's test files: the Horvatic-Zlatic
   charge series and its parameters and the order-1 current
   (test/c++/impurity_oneband/compute_obs_test.cpp), the order-2 kernel-method G(t) bins
-  (compute_obs_kernel_test.cpp), the plasma-warper vectors
+  (compute_obs_kernel_test.cpp), the projection warper's values
+  (test/c++/warpers/projection_test.cpp), the plasma-warper vectors
   (test/c++/warpers/warper_plasma_uv_test.cpp), and g0 values of the semicircular and
   flat-band models (model_semicircle_test.cpp, model_flatband_test.cpp).
 
@@ -123,12 +124,27 @@ def keldy_test_values():
               "tol": float(re.search(r"EXPECT_LT\(max_element\(abs\(result - expected_result\)\), ([\de.-]+)\)",
                                      kb).group(1)),
               "expected": [[[float(a), float(b + c)], [float(d), float(e + f)]] for a, b, c, d, e, f in kvals]}
+    pt = open(os.path.join(KELDY_SRC, "test/c++/warpers/projection_test.cpp")).read()
+    pb = test_block(pt, r"ProjectionWarper, Values")
+    pargs = re.search(r"warper_projection_t\(warped_integrand, (\d+), int\(([\de.]+)\), int\(([\de.]+)\), "
+                      r"([\d.]+), (true|false)\)", pb)
+    projection = {
+        "t_max": float(re.search(r"double const tmax = ([\d.]+);", pb).group(1)),
+        "tol": float(re.search(r"double const tol = ([\de.-]+);", pb).group(1)),
+        "interp_points": int(re.search(r"warper = \{cst, tmax, (\d+)\}", pb).group(1)),
+        "order": int(pargs.group(1)), "num_bins": int(float(pargs.group(2))),
+        "nr_samples": int(float(pargs.group(3))), "sigma": float(pargs.group(4)),
+        "optimize_sigma": pargs.group(5) == "true",
+        "values": [{"method": m, "x": float(x), "value": float(v)} for m, x, v in
+                   re.findall(r"EXPECT_NEAR\(proj_warper\.(\w+)\(\{([\d.]+)\}\)(?:\[0\])?, ([\d.]+), tol\)", pb)],
+    }
     return {
         "source": "keldy test/c++/impurity_oneband/compute_obs_test.cpp:93-206, "
                   "test/c++/impurity_oneband/compute_obs_kernel_test.cpp:12-60, "
                   "test/c++/warpers/warper_plasma_uv_test.cpp:15-43, "
                   "test/c++/impurity_oneband/model_semicircle_test.cpp:30-86, "
-                  "test/c++/impurity_oneband/model_flatband_test.cpp:154-220",
+                  "test/c++/impurity_oneband/model_flatband_test.cpp:154-220, "
+                  "test/c++/warpers/projection_test.cpp:70-103",
         "current_kat": current,
         "semicircle_kat": semi,
         "flatband_kat": flat,
@@ -140,6 +156,7 @@ def keldy_test_values():
                                {"warper": "exponential", "w": 2.0, "n_points": 50000, "rtol": [1e-2, 1e-2]}]},
         "plasma_vectors": vecs,
         "kernel_kat": kernel,
+        "projection_kat": projection,
     }
 
 
@@ -202,6 +219,28 @@ def main():
                 else [(W_UNIFORM, 10.0, 0.0)]
             s, npts, ndom = ref.integrate(model, EXTERNALS[0][1], EXTERNALS[0][2], chain, n, 4096)
             out[f"integrate_{cname}_n{n}"] = np.array([s.real, s.imag, npts, ndom])
+    # tabulated warpers (warper_product_1d_simple_interp_nearest_t): random positive f1,
+    # f1 with a zero tail (the inverse's cut), keldy's f1 = exp(-u/2) on 1000 points
+    tables = []
+    for k in range(3):
+        n = int(rng.integers(5, 40))
+        u = np.concatenate([[0.0], np.cumsum(rng.random(n - 1) + 0.05)])
+        f1 = rng.random(n) + 0.1
+        if k == 1:
+            f1[-4:] = 0.0
+        tables.append((u, f1))
+    u = np.array([i / 999 * 5.0 for i in range(1000)])
+    u[-1] = 5.0
+    tables.append((u, np.exp(-u / 2.0)))
+    for k, (u, f1) in enumerate(tables):
+        x = rng.random((48, 3))
+        x[0] = [0.0, 1.0, 0.5]
+        ur, jr = ref.interp_nearest(u, f1, x, "reverse")
+        y = np.clip(ur, u[0], u[-1])
+        lf, jf = ref.interp_nearest(u, f1, y, "forward")
+        for key, val in (("u", u), ("f1", f1), ("li", x), ("ui", ur), ("jr", jr), ("fin", y), ("fout", lf),
+                         ("jf", jf)):
+            out[f"interp_{k}_{key}"] = val
     np.savez_compressed(os.path.join(HERE, "golden.npz"), **out)
     with open(os.path.join(HERE, "keldy_tests.json"), "w") as f:
         json.dump(keldy_test_values(), f, indent=1)
