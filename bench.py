@@ -274,14 +274,30 @@ def measure_sweep(ctx):
 def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8)):
     """Learned flow vs the plain chain per order: training time, per-point variance gain,
     RQMC standard errors at a fixed 2^24-evaluation budget (16 shifts x 2^20 points) and
-    wall time to a 1e-3 relative standard error (16 shifts, points doubled from 2^8)."""
-    from keldy_b200 import learned, rqmc
+    wall time to a 1e-3 relative standard error (16 shifts, points doubled from 2^8).
+    The adaptive plain warper (make_warper_from_proj: 100 bins per axis, 2^14 samples,
+    sigma 0.05, appended to the chain) is measured beside them as the stronger plain
+    baseline."""
+    from keldy_b200 import capi, learned, rqmc
     out = {}
     for n in orders:
         flow, fit_s, loss = learned.fit(ctx, model, A, B, chain, n, 1 << 18, seed=n)
         budget = learned.compare(ctx, model, A, B, chain, n, flow, 1 << 20, 16)
         tp = rqmc.time_to_relative_error(ctx, model, A, B, chain, n, 1e-3, 16, start_points=1 << 8)
         tl = rqmc.time_to_relative_error(ctx, model, A, B, chain, n, 1e-3, 16, start_points=1 << 8, flow=flow)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        table = capi.WarperTable.from_projection(ctx, model, A, B, chain, n, 100, 1 << 14, 0.05)
+        build_s = time.perf_counter() - t0
+        achain = chain + [table.entry()]
+        ma, ea, _ = rqmc.estimate(ctx, model, A, B, achain, n, 1 << 20, 16)
+        ta = rqmc.time_to_relative_error(ctx, model, A, B, achain, n, 1e-3, 16, start_points=1 << 8)
+        mp = budget["plain"]["mean"]
+        adaptive = {"build_s": build_s, "budget_2e24_stderr": ea, "budget_2e24_rel": ea / abs(ma),
+                    "stderr_ratio_plain_over_adaptive": budget["plain"]["stderr"] / ea,
+                    "diff_in_combined_sigma": abs(ma - mp) / math.hypot(ea, budget["plain"]["stderr"]),
+                    "time_to_1e-3_s": ta["seconds"], "time_to_1e-3_points_per_shift": ta["points_per_replica"]}
+        table.close()
         out[str(n)] = {
             "fit_s": fit_s, "fit_loss": loss,
             "per_point_variance_gain": learned.variance_gain(ctx, model, A, B, chain, flow),
@@ -294,6 +310,7 @@ def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8)):
                              "learned_s": tl["seconds"], "learned_points_per_shift": tl["points_per_replica"],
                              "learned_incl_training_s": tl["seconds"] + fit_s,
                              "speedup_plain_over_learned": tp["seconds"] / tl["seconds"]},
+            "adaptive_plain": adaptive,
         }
         flow.close()
     return out
