@@ -33,8 +33,8 @@ if ROOT not in sys.path:
 
 GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
 # DRAM bytes (read + write) of one tree_kernel launch of this workload (2^20 points,
-# order 8), from an ncu capture of that launch
-TREE_LAUNCH_DRAM_BYTES = 1_870_000
+# order 8), from an ncu capture of that launch (profiles/tree_kernel_order8_2e20pts_dram.md)
+TREE_LAUNCH_DRAM_BYTES = 1_799_680
 
 
 def flop_lu(m):
@@ -447,9 +447,9 @@ def run_ours(args, rank, world, local_rank):
             "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": TREE_LAUNCH_DRAM_BYTES if order == 8 and N == 1 << 20 else None,
                          "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-point order-8 "
-                                           "tree_kernel launch (ncu, profiles/tree_kernel_order8_65536pts.md): the "
-                                           "g0 table and chunk partials; the 17,440 B per evaluation of table "
-                                           "gathers are served by L2/L1",
+                                           "tree_kernel launch (ncu, profiles/tree_kernel_order8_2e20pts_dram.md): "
+                                           "the g0 table, generator and set-up data; the 17,440 B per evaluation "
+                                           "of table gathers are served by L2/L1",
                          "numerator": f"reference-equivalent: {reference_flops(order)} FLOP per evaluation "
                                       f"(keldy's 2^n LU pairs); the tree executes ~{tree_flops(order)}",
                          "peak_source": "FP64 FMA rate measured in this run (kb_fp64_peak, 8 independent "
