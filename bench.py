@@ -239,6 +239,29 @@ def measure_biased_dot(ctx):
             "fallback_points": sum(r[3] for r in res)}
 
 
+def measure_semicircle_build(ctx):
+    """Tables of the dot with semicircular leads (D = 2, Gamma = 1, eps_d = 0.3, V = 0.5,
+    beta = 20, t in [-50, 50], 100,001 points, dot and dot-lead blocks): the band
+    quadrature's Fourier sums on the GPU (kb_model_set_fourier) and the same sums on the
+    host in numpy (g0_tables.semicircle)."""
+    from keldy_b200 import capi, g0_tables
+    args = (1.0, 0.3, 0.5, 20.0, 2.0, 50.0, 100001)
+    capi.semicircle_model(ctx, *args, dot_lead=True).close()  # warm-up
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    m = capi.semicircle_model(ctx, *args, dot_lead=True)
+    ctx.synchronize()
+    gpu_s = time.perf_counter() - t0
+    m.close()
+    t0 = time.perf_counter()
+    g0_tables.semicircle(*args, dot_lead=True)
+    host_s = time.perf_counter() - t0
+    nodes = len(g0_tables.semicircle_nodes(*args[:6])[0])
+    return {"workload": "semicircular bath D=2 Gamma=1 eps_d=0.3 V=0.5 beta=20, 100,001 points on [-50,50], "
+                        f"dot + dot-lead blocks, {nodes} quadrature nodes",
+            "gpu_ms": gpu_s * 1e3, "host_numpy_s": host_s}
+
+
 def measure_sweep(ctx):
     """256 models (V in [0,2] x eps_d in [-1,1] x beta in {10,50,200}, Gamma = 1), each with
     its own 20,001-point g0 table built on the GPU in one launch; model i integrates order
@@ -468,6 +491,7 @@ def run_ours(args, rank, world, local_rank):
         if not args.no_extras:
             line["biased_dot_orders_6_12"] = measure_biased_dot(ctx)
             line["sweep_256_models"] = measure_sweep(ctx)
+            line["semicircle_g0_build"] = measure_semicircle_build(ctx)
             line["learned_vs_plain"] = measure_learned(ctx, model, A, B, chain)
         if cpu is not None:
             line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}

@@ -187,6 +187,20 @@ int kb_model_get_table(kb_model *m, int spin, int o1, int o2, double *lesser, do
  * temperature; mu_left = -V/2, mu_right = +V/2). All models share one context and one
  * time mesh (odd npts). */
 int kb_models_set_flatband(int n, kb_model *const *models, const double *params);
+/* Fourier sums by quadrature, the GPU form of keldy's finite-contour construction
+ * (make_g0_by_finite_contour, model.cpp:220-319, which integrates g^{</>}(w) e^{-iwt}/2pi
+ * over the band by adaptive quadrature) with the nodes and weights chosen by the caller:
+ * block (o1, o2) of model m (used for both spins) gets
+ *   g^<(t) = sum_k cl[k] e^{-i w[k] t},   g^>(t) = sum_k cg[k] e^{-i w[k] t}
+ * at every mesh point (cl, cg: n_nodes interleaved complex, the quadrature weights and
+ * 1/2pi included). KB_FT_SYMMETRIC: only t >= 0 is summed (t = 0 exactly at the middle
+ * point; odd npts) and g(-t) = -conj(g(t)) fills the rest (the dot block, model.cpp:302-310).
+ * KB_FT_MIRROR: block (o2, o1) is also set, to -conj(g_{o1 o2}(-t)) (model.cpp:311-313).
+ * KB_E_INVALID if a value is not finite. */
+#define KB_FT_SYMMETRIC 1
+#define KB_FT_MIRROR 2
+int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double *w, const double *cl,
+                         const double *cg, int flags);
 
 /* A point of the Keldysh contour with spin and orbital: keldy's gf_index_t (model.hpp:55-78). */
 typedef struct {

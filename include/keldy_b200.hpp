@@ -635,6 +635,40 @@ class g0_model {
     return g;
   }
 
+  // A model with no tables yet (npts points on [-time_max, time_max]); fill its blocks with
+  // set_table or set_fourier.
+  static g0_model empty(double time_max, int npts, double alpha = 0.0) {
+    g0_model g;
+    kb_model *m = nullptr;
+    keldy_b200::check(kb_model_create(keldy_b200::default_context(), npts, time_max, alpha, &m));
+    g.m_ = std::shared_ptr<kb_model>(m, kb_model_destroy);
+    g.time_max_ = time_max;
+    g.npts_ = npts;
+    g.alpha_ = alpha;
+    g.param.time_max = time_max;
+    g.param.nr_time_points_gf = npts;
+    g.param.alpha = alpha;
+    return g;
+  }
+
+  // Block (o1, o2) built on the GPU from quadrature nodes w and weights cl, cg
+  // (kb_model_set_fourier: g(t) = sum_k c_k e^{-i w_k t}; flags KB_FT_SYMMETRIC, KB_FT_MIRROR).
+  void set_fourier(int o1, int o2, std::vector<double> const &w, std::vector<dcomplex> const &cl,
+                   std::vector<dcomplex> const &cg, int flags) {
+    if (cl.size() != w.size() || cg.size() != w.size()) throw std::runtime_error("one weight per node");
+    keldy_b200::check(kb_model_set_fourier(m_.get(), o1, o2, (int)w.size(), w.data(),
+                                           reinterpret_cast<const double *>(cl.data()),
+                                           reinterpret_cast<const double *>(cg.data()), flags));
+  }
+
+  // keldy's public g0_lesser / g0_greater data of one block (model.hpp:184-188)
+  std::pair<std::vector<dcomplex>, std::vector<dcomplex>> get_table(int spin, int o1, int o2) const {
+    std::vector<dcomplex> l((size_t)npts_), g((size_t)npts_);
+    keldy_b200::check(kb_model_get_table(m_.get(), spin, o1, o2, reinterpret_cast<double *>(l.data()),
+                                         reinterpret_cast<double *>(g.data())));
+    return {l, g};
+  }
+
   void set_table(int spin, int o1, int o2, std::vector<dcomplex> const &lesser, std::vector<dcomplex> const &greater) {
     if ((int)lesser.size() != npts_ || (int)greater.size() != npts_)
       throw std::runtime_error("table length differs from the model's mesh");

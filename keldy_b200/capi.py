@@ -39,7 +39,7 @@ EXPORTS = [
     "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
     "kb_integrate_kernel", "kb_integrand_kernel_eval", "kb_warper_table_create", "kb_warper_table_destroy",
     "kb_warper_table_from_projection", "kb_warper_table_analytic", "kb_warper_table_hybrid", "kb_warper_table_info",
-    "kb_warper_table_points",
+    "kb_warper_table_points", "kb_model_set_fourier",
     "kb_warper_table_from_samples", "kb_warper_projection_create", "kb_warper_projection_axis",
     "kb_warper_projection_from_integrand",
 ]
@@ -137,6 +137,7 @@ def load():
     L.kb_warper_table_destroy.argtypes = [_VP]
     L.kb_warper_table_analytic.argtypes = [_VP, C.c_int, C.POINTER(Warper), C.POINTER(_VP)]
     L.kb_warper_table_hybrid.argtypes = [_VP, C.c_int, C.POINTER(Warper), _I, C.POINTER(_VP)]
+    L.kb_model_set_fourier.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D, _D, C.c_int]
     L.kb_warper_table_info.argtypes = [_VP, _I, _I, _I]
     L.kb_warper_table_points.argtypes = [_VP, C.c_int, _D, _D]
     L.kb_warper_table_from_samples.argtypes = [_VP, C.c_int, C.c_int, C.c_int64, _D, _D, C.c_double, C.POINTER(_VP)]
@@ -489,6 +490,15 @@ class Model:
         assert le.size == 2 * self.npts and gr.size == 2 * self.npts
         check(self.ctx.L.kb_model_set_table(self.h, spin, o1, o2, _dp(le), _dp(gr)))
 
+    def set_fourier(self, o1, o2, w, cl, cg, flags=0):
+        """Block (o1, o2) as the Fourier sums g(t) = sum_k c_k e^{-i w_k t} on the GPU
+        (kb_model_set_fourier; flags FT_SYMMETRIC, FT_MIRROR)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        cl = np.ascontiguousarray(cl, dtype=np.complex128).view(np.float64)
+        cg = np.ascontiguousarray(cg, dtype=np.complex128).view(np.float64)
+        assert cl.size == 2 * w.size and cg.size == 2 * w.size
+        check(self.ctx.L.kb_model_set_fourier(self.h, int(o1), int(o2), w.size, _dp(w), _dp(cl), _dp(cg), int(flags)))
+
     def table(self, spin=0, o1=0, o2=0):
         """(lesser, greater) complex arrays of one block, read back from the device."""
         le = np.empty(self.npts, dtype=np.complex128)
@@ -576,6 +586,23 @@ def flatband_models(ctx, params, time_max, npts, alpha=0.0):
     hs = (_VP * max(1, len(models)))(*[m.h for m in models])
     check(ctx.L.kb_models_set_flatband(len(models), hs, _dp(params)))
     return models
+
+
+FT_SYMMETRIC, FT_MIRROR = 1, 2
+
+
+def semicircle_model(ctx, gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, alpha=0.0, dot_lead=False,
+                     nodes=None):
+    """A model of the dot with semicircular leads, its tables built on the GPU: the band
+    quadrature of g0_tables.semicircle_nodes summed by kb_model_set_fourier (the dot block
+    on t >= 0 and mirrored; with dot_lead the (1,0) block and its mirror (0,1))."""
+    from .g0_tables import semicircle_nodes
+    w, f_less, f_great, f_l10, f_g10 = semicircle_nodes(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, nodes)
+    m = Model(ctx, time_max, None, None, alpha, npts=npts)
+    m.set_fourier(0, 0, w, f_less, f_great, FT_SYMMETRIC)
+    if dot_lead:
+        m.set_fourier(1, 0, w, f_l10, f_g10, FT_MIRROR)
+    return m
 
 
 def _works(items):

@@ -230,6 +230,8 @@ PYBIND11_MODULE(_keldy, m) {
           "spin", [](gf_index_t const &g) { return int(g.spin); }, [](gf_index_t &g, int s) { g.spin = spin_t(s); })
       .def_readwrite("orbital", &gf_index_t::orbital);
 
+  m.attr("FT_SYMMETRIC") = KB_FT_SYMMETRIC;
+  m.attr("FT_MIRROR") = KB_FT_MIRROR;
   py::class_<g0_model>(m, "G0ModelTables", py::dynamic_attr(),
                        "g0 tables on the device (spin up, orbital (0,0) plus optional blocks)")
       .def_static(
@@ -242,6 +244,27 @@ PYBIND11_MODULE(_keldy, m) {
           [](g0_model &g, int spin, int o1, int o2, py::array_t<std::complex<double>> lesser,
              py::array_t<std::complex<double>> greater) { g.set_table(spin, o1, o2, to_cvec(lesser), to_cvec(greater)); },
           py::arg("spin"), py::arg("o1"), py::arg("o2"), py::arg("lesser"), py::arg("greater"))
+      .def_static("empty", &g0_model::empty, py::arg("time_max"), py::arg("npts"), py::arg("alpha") = 0.0)
+      .def(
+          "set_fourier",
+          [](g0_model &g, int o1, int o2, py::array_t<double> w, py::array_t<std::complex<double>> cl,
+             py::array_t<std::complex<double>> cg, int flags) {
+            auto wr = w.unchecked<1>();
+            std::vector<double> wv((size_t)wr.shape(0));
+            for (py::ssize_t k = 0; k < wr.shape(0); ++k) wv[(size_t)k] = wr(k);
+            g.set_fourier(o1, o2, wv, to_cvec(cl), to_cvec(cg), flags);
+          },
+          py::arg("o1"), py::arg("o2"), py::arg("w"), py::arg("cl"), py::arg("cg"), py::arg("flags"))
+      .def(
+          "get_table",
+          [](g0_model const &g, int spin, int o1, int o2) {
+            auto t = g.get_table(spin, o1, o2);
+            py::array_t<std::complex<double>> l((py::ssize_t)t.first.size()), r((py::ssize_t)t.second.size());
+            std::copy(t.first.begin(), t.first.end(), l.mutable_data());
+            std::copy(t.second.begin(), t.second.end(), r.mutable_data());
+            return py::make_tuple(l, r);
+          },
+          py::arg("spin"), py::arg("o1"), py::arg("o2"))
       .def_readwrite("make_dot_lead", &g0_model::make_dot_lead)
       .def_property_readonly("time_max", &g0_model::time_max)
       .def_property_readonly("npts", &g0_model::npts)

@@ -519,6 +519,59 @@ int kb_models_set_flatband(int n, kb_model *const *models, const double *params)
   return KB_OK;
 }
 
+int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double *w, const double *cl,
+                         const double *cg, int flags) {
+  KB_CHECK(m && w && cl && cg, "kb_model_set_fourier: null argument");
+  KB_CHECK(o1 >= 0 && o1 < 2 && o2 >= 0 && o2 < 2, "orbital index out of range");
+  KB_CHECK(n_nodes >= 1 && n_nodes <= (1 << 24), "n_nodes must be in [1, 2^24]");
+  KB_CHECK(!(flags & KB_FT_SYMMETRIC) || (m->npts % 2 == 1 && m->npts >= 3),
+           "a symmetric block needs an odd number of mesh points (t = 0 on the mesh)");
+  KB_CHECK(!(flags & KB_FT_MIRROR) || o1 != o2, "KB_FT_MIRROR needs an off-diagonal block");
+  for (int k = 0; k < n_nodes; ++k)
+    KB_CHECK(std::isfinite(w[k]) && std::isfinite(cl[2 * k]) && std::isfinite(cl[2 * k + 1]) &&
+                 std::isfinite(cg[2 * k]) && std::isfinite(cg[2 * k + 1]),
+             "quadrature nodes and weights must be finite");
+  kb_context *ctx = m->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const size_t n = (size_t)m->npts;
+  const bool mirror = (flags & KB_FT_MIRROR) != 0;
+  if (!m->tab[0][o1][o2]) KB_CUDA(cudaMalloc(&m->tab[0][o1][o2], n * 2 * sizeof(double2)));
+  if (mirror && !m->tab[0][o2][o1]) KB_CUDA(cudaMalloc(&m->tab[0][o2][o1], n * 2 * sizeof(double2)));
+  DevBuf dw, dl, dg, dbad, dmax;
+  KB_CUDA(dw.alloc((size_t)n_nodes * sizeof(double), st));
+  KB_CUDA(dl.alloc((size_t)n_nodes * sizeof(double2), st));
+  KB_CUDA(dg.alloc((size_t)n_nodes * sizeof(double2), st));
+  KB_CUDA(dbad.alloc(sizeof(int), st));
+  KB_CUDA(dmax.alloc(2 * sizeof(double), st));
+  KB_CUDA(cudaMemcpyAsync(dw.p, w, (size_t)n_nodes * sizeof(double), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dl.p, cl, (size_t)n_nodes * sizeof(double2), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dg.p, cg, (size_t)n_nodes * sizeof(double2), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemsetAsync(dbad.p, 0, sizeof(int), st));
+  KB_CUDA(launch_fourier_table(dw.as<double>(), dl.as<double2>(), dg.as<double2>(), n_nodes, m->tab[0][o1][o2],
+                               m->npts, m->tmax, (flags & KB_FT_SYMMETRIC) ? 1 : 0, dbad.as<int>(), st));
+  KB_CUDA(launch_table_max(m->tab[0][o1][o2], m->npts, dmax.as<double>(), st));
+  if (mirror) KB_CUDA(launch_mirror_block(m->tab[0][o1][o2], m->tab[0][o2][o1], m->npts, st));
+  int bad = 0;
+  double mx = 0.0;
+  KB_CUDA(cudaMemcpyAsync(&bad, dbad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(&mx, dmax.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (bad) return fail(KB_E_INVALID, "g0 table contains non-finite values");
+  // spin down uses the spin-up blocks (model.cpp:209-211): drop any spin-down copy
+  const int blocks[2][2] = {{o1, o2}, {o2, o1}};
+  for (int k = 0; k < (mirror ? 2 : 1); ++k) {
+    const int a = blocks[k][0], b = blocks[k][1];
+    cudaFree(m->tab[1][a][b]);
+    m->tab[1][a][b] = nullptr;
+    m->hash[0][a][b] = 0;
+    m->hash[1][a][b] = 0;
+  }
+  m->tabmax = std::max(m->tabmax, mx);
+  return KB_OK;
+}
+
 // Device view of a model. A spin whose (o1,o2) block was never uploaded uses the
 // other spin's block (keldy's models are spin symmetric, model.cpp:209-211).
 static ModelDev model_dev(const kb_model *m, bool *spin_symmetric) {

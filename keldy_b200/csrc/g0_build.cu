@@ -172,7 +172,81 @@ __global__ void flatband_kernel(const FlatbandParams *params, double2 *const *ta
   }
 }
 
+// Fourier sums by quadrature: keldy's finite-contour construction (model.cpp:220-319,
+// qagp over the band of the semicircular bath) with the nodes and weights chosen by the
+// caller: per mesh point t, g^<(t) = sum_k cl_k e^{-i w_k t}, g^>(t) = sum_k cg_k e^{-i w_k t}.
+// symmetric: the dot block, summed on t >= 0 only (t = 0 exactly at the middle point) with
+// g(-t) = -conj(g(t)) (model.cpp:302-310); otherwise every mesh point. One thread per
+// summed point; the nodes are staged through shared memory in tiles of FT_TILE.
+constexpr int FT_TILE = 256;
+
+__global__ void fourier_kernel(const double *w, const double2 *cl, const double2 *cg, int n_nodes, double2 *tab,
+                               int npts, double tmax, int symmetric, int *bad) {
+  __shared__ double sw[FT_TILE];
+  __shared__ double2 sl[FT_TILE], sg[FT_TILE];
+  const int mid = npts / 2;
+  const double delta = (tmax - (-tmax)) / (double)(npts - 1);
+  const int count = symmetric ? npts - mid : npts;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = idx < count;
+  const int i = symmetric ? mid + idx : idx;
+  const double t = (symmetric && idx == 0) ? 0.0 : -tmax + i * delta;
+  double2 gl = c2(0.0, 0.0), gg = c2(0.0, 0.0);
+  for (int base = 0; base < n_nodes; base += FT_TILE) {
+    const int nt = min(FT_TILE, n_nodes - base);
+    __syncthreads();
+    for (int k = threadIdx.x; k < nt; k += blockDim.x) {
+      sw[k] = w[base + k];
+      sl[k] = cl[base + k];
+      sg[k] = cg[base + k];
+    }
+    __syncthreads();
+    if (active) {
+      for (int k = 0; k < nt; ++k) {
+        double sn, cs;
+        sincos(t * sw[k], &sn, &cs);
+        // c e^{-i theta} = (c.x cos + c.y sin) + i (c.y cos - c.x sin)
+        gl.x += sl[k].x * cs + sl[k].y * sn;
+        gl.y += sl[k].y * cs - sl[k].x * sn;
+        gg.x += sg[k].x * cs + sg[k].y * sn;
+        gg.y += sg[k].y * cs - sg[k].x * sn;
+      }
+    }
+  }
+  if (!active) return;
+  if (!isfinite(gl.x) || !isfinite(gl.y) || !isfinite(gg.x) || !isfinite(gg.y)) atomicOr(bad, 1);
+  tab[2 * i] = gl;
+  tab[2 * i + 1] = gg;
+  if (symmetric && idx > 0) {
+    const int j = npts - 1 - i; // mirror point of -t
+    tab[2 * j] = c2(-gl.x, gl.y);
+    tab[2 * j + 1] = c2(-gg.x, gg.y);
+  }
+}
+
+// Block (o2, o1) from block (o1, o2): g_{o2 o1}(t) = -conj(g_{o1 o2}(-t)) (model.cpp:311-313).
+__global__ void mirror_block_kernel(const double2 *src, double2 *dst, int npts) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
+    const int j = npts - 1 - i;
+    const double2 l = src[2 * j], g = src[2 * j + 1];
+    dst[2 * i] = c2(-l.x, l.y);
+    dst[2 * i + 1] = c2(-g.x, g.y);
+  }
+}
+
 } // namespace
+
+cudaError_t launch_fourier_table(const double *w, const double2 *cl, const double2 *cg, int n_nodes, double2 *tab,
+                                 int npts, double tmax, int symmetric, int *bad, cudaStream_t st) {
+  const int count = symmetric ? npts - npts / 2 : npts;
+  fourier_kernel<<<(count + 127) / 128, 128, 0, st>>>(w, cl, cg, n_nodes, tab, npts, tmax, symmetric, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mirror_block(const double2 *src, double2 *dst, int npts, cudaStream_t st) {
+  mirror_block_kernel<<<(npts + 255) / 256, 256, 0, st>>>(src, dst, npts);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_flatband_tables(int n_models, const double *params_dev, double2 *const *tabs_dev, int npts,
                                    double tmax, const double *nodes_dev, const double *weights_dev, int n_nodes,

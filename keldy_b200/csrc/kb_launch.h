@@ -90,6 +90,9 @@ cudaError_t launch_table_max(const double2 *tab, int npts, double *out, cudaStre
 cudaError_t launch_fp64_peak(int iters, double *sink, int grid, int block, cudaStream_t st);
 // Flat-band dot g0 tables of n models ({Gamma, eps_d, V, beta} each) on the mesh of
 // npts points over [-tmax, tmax] (g0_build.cu); Gauss-Legendre rule on [-1, 1].
+cudaError_t launch_fourier_table(const double *w, const double2 *cl, const double2 *cg, int n_nodes, double2 *tab,
+                                 int npts, double tmax, int symmetric, int *bad, cudaStream_t st);
+cudaError_t launch_mirror_block(const double2 *src, double2 *dst, int npts, cudaStream_t st);
 cudaError_t launch_flatband_tables(int n_models, const double *params_dev, double2 *const *tabs_dev, int npts,
                                    double tmax, const double *nodes_dev, const double *weights_dev, int n_nodes,
                                    cudaStream_t st);

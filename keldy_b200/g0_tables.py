@@ -123,17 +123,14 @@ def _fermi(x, beta):
     return 0.5 * (1.0 - np.tanh(0.5 * beta * x))
 
 
-def semicircle(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_lead=False, nodes=None):
-    """Dot coupled to two semicircular leads of half-bandwidth D (model.cpp:92-105):
+def semicircle_nodes(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, nodes=None):
+    """Quadrature of the semicircular-bath Fourier integrals (model.cpp:92-105, 220-319):
     Delta^R(w) = Gamma/(2D) (w - i sqrt(D^2 - w^2)) per lead inside the band. As keldy's
-    finite-contour method (model.cpp:220-319), the Fourier integrals run over the band
-    [-D, D]; here in theta with w = -D cos(theta), which removes the square-root edges,
-    by Gauss-Legendre panels split at the chemical potentials.
-
-    Returns (t, lesser, greater) for the dot, and with dot_lead=True also the
-    (lead, dot) and (dot, lead) blocks: (t, lesser, greater, lesser_10, greater_10,
-    lesser_01, greater_01) (right lead, model.hpp:94-99)."""
-    t = time_mesh(time_max, npts)
+    finite-contour method, the integrals run over the band [-D, D]; here in theta with
+    w = -D cos(theta), which removes the square-root edges, by Gauss-Legendre panels split
+    at the chemical potentials. Returns (w, f_less, f_great, f_l10, f_g10): the nodes and
+    the weights of g(t) = sum_k f_k e^{-i w_k t} for the dot's lesser and greater functions
+    and for the (right lead, dot) block (model.hpp:94-99)."""
     D = float(half_bandwidth)
     mus = (-bias_V / 2.0, bias_V / 2.0)
     breaks = sorted({0.0, np.pi} | {float(np.arccos(-mu / D)) for mu in mus if abs(mu) < D})
@@ -154,9 +151,25 @@ def semicircle(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_l
     nl = [_fermi(w - mu, beta) for mu in mus]
     less_w = 1j * c * (nl[0] + nl[1]) * np.abs(gR) ** 2
     great_w = -1j * c * ((1 - nl[0]) + (1 - nl[1])) * np.abs(gR) ** 2
+    # right lead - dot (model.hpp:94-99): -s n_R^(s) (Delta^R - Delta^A)_R g^A + Delta^R_R g_dot^(s)
+    gA = np.conj(gR)
+    l10_w = -(nl[1]) * (-1j * c) * gA + delta_r * less_w
+    g10_w = (1 - nl[1]) * (-1j * c) * gA + delta_r * great_w
+    k = wq * jac / (2 * np.pi)
+    return w, k * less_w, k * great_w, k * l10_w, k * g10_w
 
-    def ft(gw, times):
-        f = wq * jac * gw / (2 * np.pi)
+
+def semicircle(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_lead=False, nodes=None):
+    """Dot coupled to two semicircular leads of half-bandwidth D (model.cpp:92-105), the
+    Fourier sums of semicircle_nodes on the host.
+
+    Returns (t, lesser, greater) for the dot, and with dot_lead=True also the
+    (lead, dot) and (dot, lead) blocks: (t, lesser, greater, lesser_10, greater_10,
+    lesser_01, greater_01) (right lead, model.hpp:94-99)."""
+    t = time_mesh(time_max, npts)
+    w, f_less, f_great, f_l10, f_g10 = semicircle_nodes(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, nodes)
+
+    def ft(f, times):
         out = np.empty(len(times), dtype=np.complex128)
         for s in range(0, len(times), 8192):
             out[s:s + 8192] = np.exp(-1j * np.outer(times[s:s + 8192], w)) @ f
@@ -164,22 +177,18 @@ def semicircle(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_l
 
     mid = len(t) // 2
 
-    def dot_block(gw):
-        pos = ft(gw, t[mid + 1:])
+    def dot_block(f):
+        pos = ft(f, t[mid + 1:])
         g = np.empty(len(t), dtype=np.complex128)
         g[mid + 1:] = pos
-        g[mid] = ft(gw, np.zeros(1))[0]
+        g[mid] = ft(f, np.zeros(1))[0]
         g[:mid] = -np.conj(pos[::-1])
         return g
 
-    gl, gg = dot_block(less_w), dot_block(great_w)
+    gl, gg = dot_block(f_less), dot_block(f_great)
     if not dot_lead:
         return t, gl, gg
-    # right lead - dot (model.hpp:94-99): -s n_R^(s) (Delta^R - Delta^A)_R g^A + Delta^R_R g_dot^(s)
-    gA = np.conj(gR)
-    l10_w = -(nl[1]) * (-1j * c) * gA + delta_r * less_w
-    g10_w = (1 - nl[1]) * (-1j * c) * gA + delta_r * great_w
-    l10, g10 = ft(l10_w, t), ft(g10_w, t)
+    l10, g10 = ft(f_l10, t), ft(f_g10, t)
     l01 = -np.conj(l10[::-1])
     g01 = -np.conj(g10[::-1])
     return t, gl, gg, l10, g10, l01, g01

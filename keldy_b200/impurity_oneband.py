@@ -16,8 +16,8 @@ from . import g0_tables
 from ._keldy import (BinnerT1, BinnerT11, ComputeGfKernel as _ComputeGfKernel, IntegrandGKernel,  # noqa: F401
                      ComputeChargeQDirect as _ComputeChargeQDirect,
                      ComputeChargeQDirectTime as _ComputeChargeQDirectTime,
-                     ComputeCurrentJDirect as _ComputeCurrentJDirect, G0KeldyshContourT, G0ModelTables, GfIndexT,
-                     IntegrandGDirect)
+                     ComputeCurrentJDirect as _ComputeCurrentJDirect, FT_MIRROR, FT_SYMMETRIC, G0KeldyshContourT,
+                     G0ModelTables, GfIndexT, IntegrandGDirect)
 
 MODEL_PARAM_DEFAULTS = {
     "beta": 1.0,
@@ -82,11 +82,17 @@ def G0Model(params=None, make_dot_lead=False, **kw):
     elif bath == "semicircle":
         if ft == "analytic":
             raise RuntimeError("analytic ft only works for flatband")
-        out = g0_tables.semicircle(p["Gamma"], p["eps_d"], p["bias_V"], beta, p["half_bandwidth"], p["time_max"],
-                                   npts, dot_lead=make_dot_lead)
-        le, gr = out[1], out[2]
+        # the band quadrature's nodes on the host, its Fourier sums on the GPU
+        w, f_less, f_great, f_l10, f_g10 = g0_tables.semicircle_nodes(p["Gamma"], p["eps_d"], p["bias_V"], beta,
+                                                                      p["half_bandwidth"], p["time_max"])
+        g = G0ModelTables.empty(float(p["time_max"]), npts, float(p["alpha"]))
+        g.set_fourier(0, 0, w, f_less, f_great, FT_SYMMETRIC)
         if make_dot_lead:
-            blocks = {(1, 0): (out[3], out[4]), (0, 1): (out[5], out[6])}
+            g.set_fourier(1, 0, w, f_l10, f_g10, FT_MIRROR)
+        g.make_dot_lead = bool(make_dot_lead)
+        g.param = dict(p)
+        g.g0_lesser, g.g0_greater = g.get_table(0, 0, 0)
+        return g
     else:
         raise NotImplementedError("lorentzian bath: no table builder in keldy_b200; use G0Model.from_tables")
     return from_tables(p["time_max"], le, gr, p["alpha"], blocks=blocks, make_dot_lead=make_dot_lead, param=p)
