@@ -230,13 +230,25 @@ def measure_biased_dot(ctx):
     ms = ctx.last_timing()[0]
     plan.close()
     ref = sum(reference_flops(n) << 22 for n in orders)
-    return {"workload": "biased dot V=1 eps_d=0.5 beta=100, charge G^<(t=50), g0 100,001 points on [-50,50] "
-                        "(GPU-built, linear interpolation), chain [plasma_uv(50), exponential(50,1)], "
-                        "orders 6..12 x 2^22 Sobol points, one graph launch",
-            "ms": ms, "evals_per_s": len(orders) * (1 << 22) / (ms * 1e-3),
-            "reference_equivalent_tflops": ref / (ms * 1e-3) / 1e12, "g0_build_s": build_s,
-            "charge_by_order": {str(n): [r[0].real / r[1], r[0].imag / r[1]] for n, r in zip(orders, res)},
-            "fallback_points": sum(r[3] for r in res)}
+    out = {"workload": "biased dot V=1 eps_d=0.5 beta=100, charge G^<(t=50), g0 100,001 points on [-50,50] "
+                       "(GPU-built, linear interpolation), chain [plasma_uv(50), exponential(50,1)], "
+                       "orders 6..12 x 2^22 Sobol points, one graph launch",
+           "ms": ms, "evals_per_s": len(orders) * (1 << 22) / (ms * 1e-3),
+           "reference_equivalent_tflops": ref / (ms * 1e-3) / 1e12, "g0_build_s": build_s,
+           "charge_by_order": {str(n): [r[0].real / r[1], r[0].imag / r[1]] for n, r in zip(orders, res)},
+           "fallback_points": sum(r[3] for r in res)}
+    # the same with cubic g0 interpolation (the workload's own setting; no keldy counterpart)
+    model.set_interpolation(3)
+    plan = capi.Plan(ctx, items)
+    plan.run()
+    res_c = plan.run()
+    ms_c = ctx.last_timing()[0]
+    plan.close()
+    out["cubic_interpolation"] = {
+        "ms": ms_c, "evals_per_s": len(orders) * (1 << 22) / (ms_c * 1e-3),
+        "charge_by_order": {str(n): [r[0].real / r[1], r[0].imag / r[1]] for n, r in zip(orders, res_c)},
+        "max_abs_diff_vs_linear": max(abs(a[0] / a[1] - b[0] / b[1]) for a, b in zip(res, res_c))}
+    return out
 
 
 def measure_semicircle_build(ctx):

@@ -187,6 +187,14 @@ int kb_model_get_table(kb_model *m, int spin, int o1, int o2, double *lesser, do
  * temperature; mu_left = -V/2, mu_right = +V/2). All models share one context and one
  * time mesh (odd npts). */
 int kb_models_set_flatband(int n, kb_model *const *models, const double *params);
+/* Interpolation of the tables between mesh points: KB_INTERP_LINEAR (keldy's, TRIQS
+ * gf<retime> evaluation; the default) or KB_INTERP_CUBIC, an extension with no keldy
+ * counterpart: Lagrange interpolation through the 4 mesh points around the interval (the
+ * window moved inside the mesh at its ends). Needs npts >= 4 for cubic. */
+#define KB_INTERP_LINEAR 1
+#define KB_INTERP_CUBIC 3
+int kb_model_set_interpolation(kb_model *m, int order);
+
 /* Fourier sums by quadrature, the GPU form of keldy's finite-contour construction
  * (make_g0_by_finite_contour, model.cpp:220-319, which integrates g^{</>}(w) e^{-iwt}/2pi
  * over the band by adaptive quadrature) with the nodes and weights chosen by the caller:

@@ -661,6 +661,9 @@ class g0_model {
                                            reinterpret_cast<const double *>(cg.data()), flags));
   }
 
+  // KB_INTERP_LINEAR (keldy's) or KB_INTERP_CUBIC (an extension) between mesh points
+  void set_interpolation(int order) { keldy_b200::check(kb_model_set_interpolation(m_.get(), order)); }
+
   // keldy's public g0_lesser / g0_greater data of one block (model.hpp:184-188)
   std::pair<std::vector<dcomplex>, std::vector<dcomplex>> get_table(int spin, int o1, int o2) const {
     std::vector<dcomplex> l((size_t)npts_), g((size_t)npts_);

@@ -39,7 +39,7 @@ EXPORTS = [
     "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
     "kb_integrate_kernel", "kb_integrand_kernel_eval", "kb_warper_table_create", "kb_warper_table_destroy",
     "kb_warper_table_from_projection", "kb_warper_table_analytic", "kb_warper_table_hybrid", "kb_warper_table_info",
-    "kb_warper_table_points", "kb_model_set_fourier",
+    "kb_warper_table_points", "kb_model_set_fourier", "kb_model_set_interpolation",
     "kb_warper_table_from_samples", "kb_warper_projection_create", "kb_warper_projection_axis",
     "kb_warper_projection_from_integrand",
 ]
@@ -138,6 +138,7 @@ def load():
     L.kb_warper_table_analytic.argtypes = [_VP, C.c_int, C.POINTER(Warper), C.POINTER(_VP)]
     L.kb_warper_table_hybrid.argtypes = [_VP, C.c_int, C.POINTER(Warper), _I, C.POINTER(_VP)]
     L.kb_model_set_fourier.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D, _D, C.c_int]
+    L.kb_model_set_interpolation.argtypes = [_VP, C.c_int]
     L.kb_warper_table_info.argtypes = [_VP, _I, _I, _I]
     L.kb_warper_table_points.argtypes = [_VP, C.c_int, _D, _D]
     L.kb_warper_table_from_samples.argtypes = [_VP, C.c_int, C.c_int, C.c_int64, _D, _D, C.c_double, C.POINTER(_VP)]
@@ -489,6 +490,10 @@ class Model:
         gr = np.ascontiguousarray(greater, dtype=np.complex128).view(np.float64)
         assert le.size == 2 * self.npts and gr.size == 2 * self.npts
         check(self.ctx.L.kb_model_set_table(self.h, spin, o1, o2, _dp(le), _dp(gr)))
+
+    def set_interpolation(self, order):
+        """1: linear (keldy's); 3: cubic Lagrange through 4 mesh points (an extension)."""
+        check(self.ctx.L.kb_model_set_interpolation(self.h, int(order)))
 
     def set_fourier(self, o1, o2, w, cl, cg, flags=0):
         """Block (o1, o2) as the Fourier sums g(t) = sum_k c_k e^{-i w_k t} on the GPU

@@ -245,6 +245,7 @@ PYBIND11_MODULE(_keldy, m) {
              py::array_t<std::complex<double>> greater) { g.set_table(spin, o1, o2, to_cvec(lesser), to_cvec(greater)); },
           py::arg("spin"), py::arg("o1"), py::arg("o2"), py::arg("lesser"), py::arg("greater"))
       .def_static("empty", &g0_model::empty, py::arg("time_max"), py::arg("npts"), py::arg("alpha") = 0.0)
+      .def("set_interpolation", &g0_model::set_interpolation, py::arg("order"))
       .def(
           "set_fourier",
           [](g0_model &g, int o1, int o2, py::array_t<double> w, py::array_t<std::complex<double>> cl,

@@ -519,6 +519,14 @@ int kb_models_set_flatband(int n, kb_model *const *models, const double *params)
   return KB_OK;
 }
 
+int kb_model_set_interpolation(kb_model *m, int order) {
+  KB_CHECK(m, "null model");
+  KB_CHECK(order == KB_INTERP_LINEAR || order == KB_INTERP_CUBIC, "interpolation order must be 1 or 3");
+  KB_CHECK(order == KB_INTERP_LINEAR || m->npts >= 4, "cubic interpolation needs at least 4 mesh points");
+  m->interp = order;
+  return KB_OK;
+}
+
 int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double *w, const double *cl,
                          const double *cg, int flags) {
   KB_CHECK(m && w && cl && cg, "kb_model_set_fourier: null argument");
@@ -591,6 +599,7 @@ static ModelDev model_dev(const kb_model *m, bool *spin_symmetric) {
   d.delta = (m->tmax - d.xmin) / (double)(m->npts - 1);
   d.alpha = m->alpha;
   d.pivot_floor = 1e-8 * (m->tabmax > 0 ? m->tabmax : 1.0);
+  d.interp = m->interp;
   if (spin_symmetric) *spin_symmetric = sym;
   return d;
 }

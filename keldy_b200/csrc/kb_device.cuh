@@ -52,6 +52,37 @@ __device__ __forceinline__ void interp_pair(const double2 *tab, int i, double w,
   gg = c2(__dadd_rn(__dmul_rn(v, g0.x), __dmul_rn(w, g1.x)), __dadd_rn(__dmul_rn(v, g0.y), __dmul_rn(w, g1.y)));
 }
 
+// Cubic Lagrange interpolation (an extension: keldy interpolates linearly) through the 4
+// mesh points s0..s0+3 around the interval [i, i+1] (s0 = i-1, moved inside the mesh at
+// its ends) at u = i + w - s0; every operation rounded separately, as the CPU oracle.
+__device__ __forceinline__ void interp_pair_cubic(const double2 *tab, int npts, int i, double w, double2 &gl,
+                                                  double2 &gg) {
+  const int s0 = max(0, min(i - 1, npts - 4));
+  const double u = __dadd_rn((double)(i - s0), w);
+  const double am = __dsub_rn(u, 1.0), bm = __dsub_rn(u, 2.0), cm = __dsub_rn(u, 3.0);
+  double L[4];
+  L[0] = -__ddiv_rn(__dmul_rn(__dmul_rn(am, bm), cm), 6.0);
+  L[1] = __ddiv_rn(__dmul_rn(__dmul_rn(u, bm), cm), 2.0);
+  L[2] = -__ddiv_rn(__dmul_rn(__dmul_rn(u, am), cm), 2.0);
+  L[3] = __ddiv_rn(__dmul_rn(__dmul_rn(u, am), bm), 6.0);
+  gl = gg = c2(0.0, 0.0);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double2 l = __ldg(tab + 2 * (s0 + k)), g = __ldg(tab + 2 * (s0 + k) + 1);
+    gl = c2(__dadd_rn(gl.x, __dmul_rn(L[k], l.x)), __dadd_rn(gl.y, __dmul_rn(L[k], l.y)));
+    gg = c2(__dadd_rn(gg.x, __dmul_rn(L[k], g.x)), __dadd_rn(gg.y, __dmul_rn(L[k], g.y)));
+  }
+}
+
+// The model's interpolation of both tables at mesh interval i, weight w.
+__device__ __forceinline__ void interp_model(const ModelDev &m, const double2 *tab, int i, double w, double2 &gl,
+                                             double2 &gg) {
+  if (m.interp == 3)
+    interp_pair_cubic(tab, m.npts, i, w, gl, gg);
+  else
+    interp_pair(tab, i, w, gl, gg);
+}
+
 // Both tables at x; zero when the block is absent. Sets *bad outside the window.
 __device__ __forceinline__ void g0_pair(const ModelDev &m, const double2 *tab, double x, double2 &gl, double2 &gg,
                                         int *bad) {
@@ -66,7 +97,7 @@ __device__ __forceinline__ void g0_pair(const ModelDev &m, const double2 *tab, d
     i = 0;
     w = 0.0;
   }
-  interp_pair(tab, i, w, gl, gg);
+  interp_model(m, tab, i, w, gl, gg);
 }
 
 // keldy::compare_3way (common.cpp:47-57) on (time, keldysh index, timesplit).

@@ -79,6 +79,7 @@ struct kb_model {
   double2 *tab[2][2][2] = {};
   uint64_t hash[2][2][2] = {}; // 0 = unknown (device upload)
   double tabmax = 0;
+  int interp = 1; // 1 linear, 3 cubic
 };
 
 struct kb_sobol {

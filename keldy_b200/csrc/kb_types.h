@@ -22,6 +22,7 @@ struct ModelDev {
   double delta;
   double alpha;
   double pivot_floor; // |re|+|im| below which a tree pivot hands the point to the pivoted-LU kernel
+  int interp;         // 1: linear (keldy, TRIQS gf<retime>); 3: cubic Lagrange through 4 mesh points
 };
 
 // One analytic 1D warper of the product makers (product_1d_simple.hpp:560-630): kind

@@ -188,7 +188,7 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
 #pragma unroll
     for (int k = 0; k < GK; ++k) {
       if (tb[k])
-        interp_pair(tb[k], ix[k], wt[k], gl[k], gg[k]);
+        interp_model(m, tb[k], ix[k], wt[k], gl[k], gg[k]);
       else
         gl[k] = gg[k] = c2(0.0, 0.0);
     }

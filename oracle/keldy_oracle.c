@@ -417,6 +417,7 @@ typedef struct {
   double time_max;
   double alpha;
   const double *tab[2][2][2][2];
+  int interp; /* 3: cubic (4-point Lagrange, an extension with no keldy counterpart); else linear */
 } or_model;
 
 typedef struct {
@@ -436,7 +437,8 @@ int or_compare_3way(double ta, int ka, int sa, double tb, int kb, int sb) {
   return (1 - 2 * ka) * (sa - sb);
 }
 
-/* Linear interpolation on the uniform mesh. Returns -1 outside [-time_max, time_max]. */
+/* Linear (or, interp = 3, cubic) interpolation on the uniform mesh. Returns -1 outside
+ * [-time_max, time_max]. */
 static int or_interp(const or_model *mdl, const double *tab, double x, cplx *out) {
   if (!tab) {
     *out = c_make(0.0, 0.0);
@@ -450,6 +452,27 @@ static int or_interp(const or_model *mdl, const double *tab, double x, cplx *out
   if (i == mdl->npts - 1) i = mdl->npts - 2;
   if (i < 0 || i > mdl->npts - 2) return -1;
   double w = a - (double)i;
+  if (mdl->interp == 3) {
+    /* cubic Lagrange interpolation through the 4 mesh points s0..s0+3 around the interval
+     * [i, i+1] (s0 = i-1, moved inside the mesh at its ends), evaluated at u = x/delta - s0 */
+    long s0 = i - 1;
+    if (s0 < 0) s0 = 0;
+    if (s0 > mdl->npts - 4) s0 = mdl->npts - 4;
+    double u = (double)(i - s0) + w;
+    double am = u - 1.0, bm = u - 2.0, cm = u - 3.0;
+    double L[4];
+    L[0] = -((am * bm) * cm) / 6.0;
+    L[1] = ((u * bm) * cm) / 2.0;
+    L[2] = -((u * am) * cm) / 2.0;
+    L[3] = ((u * am) * bm) / 6.0;
+    double re = 0.0, im = 0.0;
+    for (int k = 0; k < 4; ++k) {
+      re = re + L[k] * tab[2 * (s0 + k)];
+      im = im + L[k] * tab[2 * (s0 + k) + 1];
+    }
+    *out = c_make(re, im);
+    return 0;
+  }
   cplx g0 = c_make(tab[2 * i], tab[2 * i + 1]);
   cplx g1 = c_make(tab[2 * i + 2], tab[2 * i + 3]);
   *out = c_add(c_scale(g0, 1.0 - w), c_scale(g1, w));

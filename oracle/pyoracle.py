@@ -35,7 +35,7 @@ class GfIndex(C.Structure):
 
 class Model(C.Structure):
     _fields_ = [("npts", C.c_int), ("time_max", C.c_double), ("alpha", C.c_double),
-                ("tab", C.c_void_p * 16)]
+                ("tab", C.c_void_p * 16), ("interp", C.c_int)]
 
 
 _D = C.POINTER(C.c_double)
@@ -141,13 +141,15 @@ class Oracle:
         return out, jac
 
     # --- Model / integrand -------------------------------------------------
-    def model(self, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None):
-        """Tables: complex arrays on the uniform mesh [-time_max, time_max], orbital (0,0)."""
+    def model(self, time_max, lesser, greater, alpha=0.0, lesser_down=None, greater_down=None, interp=1):
+        """Tables: complex arrays on the uniform mesh [-time_max, time_max], orbital (0,0).
+        interp 3: cubic interpolation (an extension; keldy interpolates linearly)."""
         m = Model()
         npts = len(lesser)
         m.npts = npts
         m.time_max = time_max
         m.alpha = alpha
+        m.interp = int(interp)
         keep = []
         def ptr(a):
             a = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).view(np.float64))

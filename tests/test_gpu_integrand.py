@@ -147,3 +147,37 @@ def test_pivot_guard_falls_back_to_lu(ctx, oracle):
     v, d = gm.integrand(A, B, x)
     w, dw, sc = oracle.integrand(om, A, B, x)
     _check(v, w, sc)
+
+
+# ------------------------------------------------------------------ cubic g0 interpolation
+def test_cubic_interpolation_vs_oracle(ctx, oracle, golden):
+    """The cubic-interpolation option (an extension with no keldy counterpart) against the
+    oracle's: g0 lookups bit-exact across the window (ends included), the integrand of
+    orders 1-8 on both algorithms and the fused integration within the usual tolerances."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr, 0.3)
+    gm.set_interpolation(3)
+    om = oracle.model(10.0, le, gr, 0.3, interp=3)
+    x = np.concatenate([np.random.default_rng(5).uniform(-10, 10, 300), [-10.0, -9.999, 9.999, 10.0, 0.0]])
+    a = [(v, 0, 0, 0, 0) for v in x]
+    b = [(0.0, 0, 1, 0, 0)] * len(x)
+    got = gm.g0(a, b)
+    want = np.array([oracle.g0(om, p, q) for p, q in zip(a, b)])
+    np.testing.assert_array_equal(got, want)
+    lin = ctx.model(10.0, le, gr, 0.3)
+    assert np.abs(lin.g0(a, b) - got).max() > 0  # the option changes the values
+    rng = np.random.default_rng(9)
+    A, B = EXTERNALS[0][1], EXTERNALS[0][2]
+    for n in range(1, 9):
+        t = rng.random((8, n)) * 10.0
+        want, dw, sc = oracle.integrand(om, A, B, t)
+        for algo in (capi.ALGO_TREE, capi.ALGO_DIRECT):
+            v, d = gm.integrand(A, B, t, algo=algo)
+            np.testing.assert_array_equal(d, dw)
+            _check(v, want, sc)
+    chain = [(capi.WARPER_PLASMA_UV, 10.0, 0.0), (capi.WARPER_EXPONENTIAL, 10.0, 1.0)]
+    for n in (2, 4, 6):
+        s_o, np_o, nd_o, scale = oracle.integrate(om, A, B, chain, n, 4096)
+        (s_g, np_g, nd_g, _), = capi.integrate(ctx, [dict(model=gm, rng=ctx.sobol(n), chain=chain, A=A, B=B,
+                                                          order=n, n_points=4096)])
+        assert (np_g, nd_g) == (np_o, nd_o) and abs(s_g - s_o) <= 1e-12 * scale
