@@ -698,6 +698,7 @@ static int run_eval(kb_context *ctx, ItemDev it, int mode, int64_t count, const 
   memset(&L, 0, sizeof(L));
   L.items = ditem.as<ItemDev>();
   L.n_items = 1;
+  L.any_cubic = items_any_cubic(&it, 1);
   L.chunk_offsets = doff.as<long long>();
   L.n_chunks = (int)nchunks;
   L.chunk_counter = dcnt.as<int>();
@@ -857,6 +858,7 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
     memset(&L, 0, sizeof(L));
     L.items = ditems.as<ItemDev>();
     L.n_items = (int)sorted.size();
+    L.any_cubic = items_any_cubic(sorted.data(), sorted.size());
     L.chunk_offsets = doff.as<long long>();
     L.n_chunks = (int)nchunks;
     L.chunk_counter = dcnt.as<int>();
@@ -1069,9 +1071,13 @@ int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const 
   L.bin_counts = dbc.as<unsigned>();
   L.bin_dropped = dbd.as<unsigned>();
   L.err = ctx->d_err;
+  if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
   KB_CUDA(launch_kernel_method(L, (int)std::min<long long>(nchunks, (long long)ctx->sm_count * 4), st));
+  if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[1], st));
   KB_CUDA(launch_reduce(L, dacc.as<kb_accum>(), st));
   KB_CUDA(launch_reduce_bins(L, dos.as<double2>(), doc.as<unsigned long long>(), dod.as<unsigned long long>(), st));
+  if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[2], st));
+  ctx->last_launches = 3;
   std::vector<kb_accum> part(items.size());
   std::vector<double> hbs(items.size() * nb * 2);
   std::vector<unsigned long long> hbc(items.size() * nb), hbd(items.size());
@@ -1082,6 +1088,14 @@ int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const 
   int err = 0;
   KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   KB_CUDA(cudaStreamSynchronize(st));
+  if (ctx->timing) {
+    float a = 0, c = 0;
+    KB_CUDA(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
+    KB_CUDA(cudaEventElapsedTime(&c, ctx->ev[1], ctx->ev[2]));
+    ctx->last_ms[0] = a;
+    ctx->last_ms[1] = 0.0;
+    ctx->last_ms[2] = c;
+  }
   if (err & 1) return fail(KB_E_RANGE, "g0 evaluated outside its tabulated time window");
   for (int w = 0; w < n_work; ++w) {
     acc[w].sum_re += part[(size_t)w].sum_re;
@@ -1131,6 +1145,7 @@ int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_ind
   memset(&L, 0, sizeof(L));
   L.items = ditem.as<ItemDev>();
   L.n_items = 1;
+  L.any_cubic = items_any_cubic(&it, 1);
   L.chunk_offsets = doff.as<long long>();
   L.n_chunks = (int)nchunks;
   L.chunk_counter = dcnt.as<int>();
@@ -1393,6 +1408,7 @@ static int plan_enqueue(kb_context *ctx, kb_plan *p, cudaStream_t st) {
     memset(&L, 0, sizeof(L));
     L.items = g.d_items;
     L.n_items = g.n_items;
+    L.any_cubic = items_any_cubic(g.items.data(), g.items.size());
     L.chunk_offsets = g.d_offs;
     L.n_chunks = (int)g.n_chunks;
     L.chunk_counter = g.d_cnt;
@@ -1663,6 +1679,7 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     memset(&L, 0, sizeof(L));
     L.items = d_items;
     L.n_items = nids[g];
+    L.any_cubic = items_any_cubic(sorted, (size_t)nids[g]);
     L.chunk_offsets = d_offs;
     L.n_chunks = (int)offs[nids[g]];
     L.chunk_counter = d_cnt;

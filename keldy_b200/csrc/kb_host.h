@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <string.h>
 
 #include <mutex>
 #include <string>
@@ -34,11 +35,24 @@ struct DevBuf {
   template <typename T> T *as() const { return static_cast<T *>(p); }
 };
 
+// Content hash of a table (equality test of spin blocks): four independent lanes of
+// 64-bit words, each an FNV-1a step on the word followed by a xor-shift, then the lanes
+// and the tail bytes combined.
 inline uint64_t fnv1a(const void *data, size_t n) {
   const unsigned char *c = static_cast<const unsigned char *>(data);
-  uint64_t h = 1469598103934665603ULL;
-  for (size_t i = 0; i < n; ++i) h = (h ^ c[i]) * 1099511628211ULL;
-  return h;
+  const uint64_t P = 1099511628211ULL;
+  uint64_t h[4] = {1469598103934665603ULL, 0x9E3779B97F4A7C15ULL, 0xC2B2AE3D27D4EB4FULL, 0x165667B19E3779F9ULL};
+  size_t i = 0;
+  for (; i + 32 <= n; i += 32)
+    for (int k = 0; k < 4; ++k) {
+      uint64_t w;
+      memcpy(&w, c + i + 8 * k, 8);
+      h[k] = (h[k] ^ w) * P;
+      h[k] ^= h[k] >> 29;
+    }
+  uint64_t r = h[0] ^ (h[1] * 3) ^ (h[2] * 5) ^ (h[3] * 7);
+  for (; i < n; ++i) r = (r ^ c[i]) * P;
+  return r ^ n;
 }
 
 } // namespace kb

@@ -59,7 +59,17 @@ struct Launch {
   unsigned *bin_dropped; // [n_chunks]
   // errors
   int *err; // bit 0: g0 evaluated outside its window
+  // some item's model interpolates its tables cubically: the tree kernel's instantiation
+  // that carries both interpolations (the default one has the linear lookup only)
+  int any_cubic;
 };
+
+// any_cubic of a launch over items[0..n)
+inline int items_any_cubic(const ItemDev *items, size_t n) {
+  for (size_t i = 0; i < n; ++i)
+    if (items[i].model.interp == 3) return 1;
+  return 0;
+}
 
 size_t tree_smem_bytes();
 // sets the kernels' shared-memory attributes (before any stream capture)

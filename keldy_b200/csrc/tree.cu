@@ -125,6 +125,7 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
 // external-column entries (one table lookup each: g^< and g^> at one time difference),
 // the N diagonal blocks (g(0)) and the corner. Each thread computes the lookup positions
 // of GK items before issuing their loads, so that GK L2 round trips overlap.
+template <bool CUBIC>
 __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
                         int spin, int *bad) {
   constexpr int GK = 4;
@@ -187,8 +188,10 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
     double2 gl[GK], gg[GK];
 #pragma unroll
     for (int k = 0; k < GK; ++k) {
-      if (tb[k])
-        interp_model(m, tb[k], ix[k], wt[k], gl[k], gg[k]);
+      if (tb[k] && CUBIC)
+        interp_pair_cubic(tb[k], m.npts, ix[k], wt[k], gl[k], gg[k]);
+      else if (tb[k])
+        interp_pair(tb[k], ix[k], wt[k], gl[k], gg[k]);
       else
         gl[k] = gg[k] = c2(0.0, 0.0);
     }
@@ -252,6 +255,17 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
       }
     }
   }
+}
+
+// build_G with the model's interpolation chosen once per call; ANY_CUBIC = false compiles
+// the linear lookup only (launches whose models all interpolate linearly).
+template <bool ANY_CUBIC>
+__device__ void build_G_any(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
+                            int spin, int *bad) {
+  if (ANY_CUBIC && it.model.interp == 3)
+    build_G<true>(it, N, np, u, flag, buf, spin, bad);
+  else
+    build_G<false>(it, N, np, u, flag, buf, spin, bad);
 }
 
 // One breadth-first level, both children of a node from one read of its rows: thread r
@@ -434,6 +448,7 @@ __device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, dou
 
 // Integrand of np points whose inputs are loaded (S.u, S.flag): S.fval, S.fscale, and
 // flag bit 1 where a pivot fell below the guard.
+template <bool ANY_CUBIC>
 __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad) {
   const int tid = threadIdx.x;
   if (tid < np) {
@@ -458,7 +473,7 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   const double floor_ = it.model.pivot_floor;
   const int spin = it.f.A.spin;
   for (int sub = 0; sub < (1 << K0); ++sub) {
-    build_G(it, N, np, S.u, S.flag, S.buf[0], spin, bad);
+    build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, S.buf[0], spin, bad);
     if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
     __syncthreads();
     int m = 2 * N + 1, cur = 0;
@@ -536,7 +551,7 @@ __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
   if (threadIdx.x == 0) L.bin_dropped[c] = 0u;
 }
 
-template <bool EVAL>
+template <bool EVAL, bool ANY_CUBIC>
 __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
@@ -571,7 +586,7 @@ __global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
         S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
       }
       __syncthreads();
-      tree_points(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
+      tree_points<ANY_CUBIC>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
       if (EVAL) {
         if (tid < np) {
           long long o = cfirst + sb + tid;
@@ -705,10 +720,10 @@ __device__ __forceinline__ void direct_point(DirectShared &D, const ItemDev &it,
   }
   const int M = 2 * N + 1;
   const int spin = it.f.A.spin;
-  build_G(it, N, 1, D.u, D.flag, D.G1, spin, bad);
+  build_G_any<true>(it, N, 1, D.u, D.flag, D.G1, spin, bad);
   const double2 *G2 = D.G1;
   if (!it.spin_symmetric) {
-    build_G(it, N, 1, D.u, D.flag, D.G2, 1 - spin, bad);
+    build_G_any<true>(it, N, 1, D.u, D.flag, D.G2, 1 - spin, bad);
     G2 = D.G2;
   }
   __syncthreads();
@@ -1174,11 +1189,20 @@ cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long lon
 
 size_t tree_smem_bytes() { return sizeof(TreeShared); }
 
-cudaError_t configure_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(tree_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(TreeShared));
+// Shared-memory limit of the four tree-kernel instantiations.
+static cudaError_t configure_tree(int smem) {
+  cudaError_t e = cudaFuncSetAttribute(tree_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TreeShared));
+    e = cudaFuncSetAttribute(tree_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tree_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tree_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
+}
+
+cudaError_t configure_kernels() {
+  cudaError_t e = configure_tree((int)sizeof(TreeShared));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirectShared));
   if (e == cudaSuccess)
@@ -1192,16 +1216,21 @@ cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
   static bool configured = false;
   size_t smem = tree_smem_bytes();
   if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(tree_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(tree_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = configure_tree((int)smem);
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  if (L.mode == IN_SOBOL)
-    tree_kernel<false><<<grid, NT, smem, st>>>(L);
-  else
-    tree_kernel<true><<<grid, NT, smem, st>>>(L);
+  if (L.mode == IN_SOBOL) {
+    if (L.any_cubic)
+      tree_kernel<false, true><<<grid, NT, smem, st>>>(L);
+    else
+      tree_kernel<false, false><<<grid, NT, smem, st>>>(L);
+  } else {
+    if (L.any_cubic)
+      tree_kernel<true, true><<<grid, NT, smem, st>>>(L);
+    else
+      tree_kernel<true, false><<<grid, NT, smem, st>>>(L);
+  }
   return cudaGetLastError();
 }
 
