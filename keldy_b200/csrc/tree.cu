@@ -32,6 +32,9 @@ namespace kb {
 namespace {
 
 constexpr int NT = CTA_THREADS;
+// Threads of a tree-kernel CTA: four per 7x7 node of the last breadth-first level (64
+// nodes per sub-batch at every order).
+constexpr int TREE_THREADS = 2 * CTA_THREADS;
 
 struct TreeShared {
   double2 buf[2][FRONTIER];
@@ -42,8 +45,8 @@ struct TreeShared {
   double2 fval[NT];
   double fscale[NT];
   int flag[NT];      // bit 0: out of domain, bit 1: needs the pivoted-LU kernel
-  double2 wsum[NT / 32]; // per-warp partial sums of the per-point reduction
-  double wscale[NT / 32];
+  double2 wsum[TREE_THREADS / 32]; // per-warp partial sums of the per-point reduction
+  double wscale[TREE_THREADS / 32];
 };
 
 __device__ __forceinline__ int find_item(const long long *off, int n_items, long long c) {
@@ -390,7 +393,56 @@ __device__ __forceinline__ void tree_bottom7(const double2 *S, double2 D, int b,
   tree_bottom5r(t, Db, parity ^ b, floor_, want_scale, sum, scale, guard);
 }
 
-// Sums (v, sc) over aligned groups of G consecutive threads (G a power of two <= NT)
+// Grandchild (b, bp) of a 7x7 node (shared memory; rows 0,1: vertex k, 2,3: vertex k+1,
+// 4,5: vertex k+2, 6: external) in registers: eliminate row b, then row 2 + bp of the
+// child, leaving the 3x3 Schur complement T over rows {4, 5, 6}; then its two leaves,
+// each (-1)^|a| det(s2)^2 T_cc (T_cc T_ee - T_ce T_ec). Only the child's entries that T
+// needs are formed (rows and columns 2 + bp, 4, 5, 6), each as the two-level scheme forms it.
+__device__ __forceinline__ void tree_bottom7q(const double2 *S, double2 D, int b, int bp, int parity, double floor_,
+                                              bool want_scale, double2 &sum, double &scale, bool &guard) {
+  const double2 p1 = S[b * 8];
+  if (!(cabs1(p1) >= floor_)) guard = true;
+  const double2 i1 = crcp(p1);
+  const int c0 = 2 + bp;
+  // child row c0 at columns c0, 4, 5, 6
+  double2 a0[4];
+  {
+    const double2 Lf = cmul(S[c0 * 7 + b], i1);
+    a0[0] = cfms(S[c0 * 7 + c0], Lf, S[b * 7 + c0]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) a0[j + 1] = cfms(S[c0 * 7 + 4 + j], Lf, S[b * 7 + 4 + j]);
+  }
+  const double2 p2 = a0[0];
+  if (!(cabs1(p2) >= floor_)) guard = true;
+  const double2 i2 = crcp(p2);
+  double2 T[9];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int ri = 4 + r;
+    const double2 Lf = cmul(S[ri * 7 + b], i1);
+    const double2 ar0 = cfms(S[ri * 7 + c0], Lf, S[b * 7 + c0]);
+    const double2 L2 = cmul(ar0, i2);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) T[r * 3 + j] = cfms(cfms(S[ri * 7 + 4 + j], Lf, S[b * 7 + 4 + j]), L2, a0[j + 1]);
+  }
+  const double2 Db = cmul(cmul(D, p1), p2);
+  const double2 Db2 = cmul(Db, Db);
+  sum = c2(0.0, 0.0);
+  scale = 0.0;
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    const double2 q = cmul(T[c * 4], cfms(cmul(T[c * 4], T[8]), T[c * 3 + 2], T[6 + c]));
+    const double2 term = cmul(Db2, q);
+    if ((b ^ bp ^ c) & 1)
+      sum = c2(sum.x - term.x, sum.y - term.y);
+    else
+      sum = cadd(sum, term);
+    if (want_scale) scale += cabs(term);
+  }
+  if (parity & 1) sum = c2(-sum.x, -sum.y);
+}
+
+// Sums (v, sc) over aligned groups of G consecutive threads (G a power of two <= TREE_THREADS)
 // and adds group g's sum to fval[g], fscale[g] for g < ngroups. Fixed shuffle pattern:
 // deterministic. Every thread of the CTA calls it.
 __device__ void group_sum(double2 v, double sc, int G, int ngroups, double2 *fval, double *fscale, double2 *wsum,
@@ -495,13 +547,13 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
     double sc = 0.0;
     bool guard = false;
     int G, p = 0;
-    if (m == 7) { // two threads per 7x7 node, one per child
-      G = 2 << lg;
-      if (tid < 2 * nodes) {
-        const int node = tid >> 1, b = tid & 1;
+    if (m == 7) { // four threads per 7x7 node, one per grandchild
+      G = 4 << lg;
+      if (tid < 4 * nodes) {
+        const int node = tid >> 2, b = (tid >> 1) & 1, bp = tid & 1;
         p = node >> lg;
         const int parity = __popc(node & ((1 << lg) - 1)) + __popc(sub);
-        tree_bottom7(S.buf[cur] + node * 49, S.D[cur][node], b, parity, floor_, want_scale, v, sc, guard);
+        tree_bottom7q(S.buf[cur] + node * 49, S.D[cur][node], b, bp, parity, floor_, want_scale, v, sc, guard);
       }
     } else if (m == 5) { // order 2: the root itself
       G = 1;
@@ -552,7 +604,7 @@ __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
 }
 
 template <bool EVAL, bool ANY_CUBIC>
-__global__ void __launch_bounds__(NT, 2) tree_kernel(Launch L) {
+__global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
   __shared__ int s_chunk;
@@ -1222,14 +1274,14 @@ cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
   }
   if (L.mode == IN_SOBOL) {
     if (L.any_cubic)
-      tree_kernel<false, true><<<grid, NT, smem, st>>>(L);
+      tree_kernel<false, true><<<grid, TREE_THREADS, smem, st>>>(L);
     else
-      tree_kernel<false, false><<<grid, NT, smem, st>>>(L);
+      tree_kernel<false, false><<<grid, TREE_THREADS, smem, st>>>(L);
   } else {
     if (L.any_cubic)
-      tree_kernel<true, true><<<grid, NT, smem, st>>>(L);
+      tree_kernel<true, true><<<grid, TREE_THREADS, smem, st>>>(L);
     else
-      tree_kernel<true, false><<<grid, NT, smem, st>>>(L);
+      tree_kernel<true, false><<<grid, TREE_THREADS, smem, st>>>(L);
   }
   return cudaGetLastError();
 }
