@@ -127,11 +127,12 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
 // Items per point: the N(N-1) ordered vertex pairs, the N external-row and N
 // external-column entries (one table lookup each: g^< and g^> at one time difference),
 // the N diagonal blocks (g(0)) and the corner. Each thread computes the lookup positions
-// of GK items before issuing their loads, so that GK L2 round trips overlap.
+// of GK items before issuing their loads, so that GK L2 round trips overlap (GK = 2: more
+// would cost registers that the 256-thread CTAs do not have).
 template <bool CUBIC>
 __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
                         int spin, int *bad) {
-  constexpr int GK = 4;
+  constexpr int GK = 2;
   const ModelDev &m = it.model;
   const int M = 2 * N + 1;
   const int npair = N * (N - 1), nlook = npair + 2 * N, per = nlook + N + 1;
@@ -287,9 +288,9 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
   const unsigned rows = (unsigned)(nodes * mc);
   const unsigned magic = 0xFFFFFFFFu / (unsigned)mc + 1u; // r / mc == umulhi(r, magic) for r < 2^20, mc <= 31
-  // split rows into column segments while the CTA has idle threads
+  // split rows into column segments of at least 5 columns while the CTA has idle threads
   int lgseg = 0;
-  while ((rows << (lgseg + 1)) <= blockDim.x && (mc >> (lgseg + 1)) >= 3) ++lgseg;
+  while ((rows << (lgseg + 1)) <= blockDim.x && (mc >> (lgseg + 1)) >= 5) ++lgseg;
   const int seglen = (mc + (1 << lgseg) - 1) >> lgseg;
   const unsigned items = rows << lgseg;
   for (unsigned t = threadIdx.x; t < items; t += blockDim.x) {
