@@ -1203,6 +1203,382 @@ __global__ void __launch_bounds__(NT) kernel_method_kernel(Launch L) {
   if (tid == 0 && s_bad) atomicOr(L.err, 1);
 }
 
+// ------------------------------------------------------------ kernel method, tree form
+// For spin-symmetric models det(s2_a) = det(V_a), V_a the vertex block of G picked by a,
+// and keldy's s1_a = [[g_XX, r], [c, W_a]] with W_a = V_a except its last vertex's
+// diagonal entry set to 0. The first-row cofactors of s1_a are x_0 = det(W_a) and
+// x_{i+1} = -det(W_a) (W_a^-1 c)_i (block inverse), so only the vertex block and the X
+// column enter. Gauss-Jordan elimination of the vertices in order 0..n-1, pivoting on the
+// diagonal entry of the chosen copy and carrying the X column, visits the 2^n
+// configurations as the leaves of a binary tree that shares its prefixes, as the direct
+// integrand's tree does; a node after j eliminations holds the j eliminated rows (pivot
+// rows normalised by their pivots), both copies' rows of the remaining vertices, and the
+// columns of the remaining copies plus the X column. At a leaf (copy b of the last
+// vertex), with D the product of the earlier pivots, p the last pivot and p_W = p minus
+// that copy's original diagonal entry (the Schur complement is affine in it with
+// coefficient 1), c_b the carried X entry of the last row and (e_j, f_j) an eliminated
+// row's last-copy and X entries:
+//   x_n = -D c_b,  x_{j+1} = -D (p_W f_j - e_j c_b),  det(V_a) = D p,
+// with no division by p_W (W_a may be singular, as for n = 1). Cost O(2^n n) per point
+// after the shared levels, instead of 2^n pivoted LU pairs. A point whose pivot falls
+// below the guard (or a model whose spins differ) takes keldy's pivoted-LU path,
+// kernel_point above, with the same per-(vertex, index) sums.
+
+struct KMTreeShared {
+  union {
+    double2 buf[2][FRONTIER];
+    KernelShared K; // the pivoted-LU path of a guarded point (after the tree pass)
+  };
+  double2 D[2][NT];
+  double2 inv[NT];
+  double u[256];      // vertex times, u[j * np + p]
+  double jac[NT];
+  int flag[NT];       // bit 0: out of domain, bit 1: a guarded pivot
+  double2 gd[NT][2];  // original diagonal entries of the last vertex's two copies, per point
+  double2 S[256];     // per point the 2n sums, S[p * 2n + 2i + k]
+  double2 red[NT / 32][2 * KM_MAX_ORDER];
+};
+
+// Points per pass of the tree form: 2^(n-1) threads per point (one per configuration of
+// the first n-1 vertices; two for n = 1) up to the CTA's 128; orders 9 and 10 walk their first 2 and 3
+// levels one path at a time so that the widest level fits a frontier buffer.
+__host__ __device__ inline int km_points_per_pass(int n) { return n == 1 ? 64 : n <= 8 ? (128 >> (n - 1)) : 1; }
+__host__ __device__ inline int km_path_levels(int n) { return n <= 8 ? 0 : n - 7; }
+
+// One elimination level: vertex j of every node (rows 2n - j, columns 2(n - j) + 1,
+// stride `cs` elements per node) into its children (rows 2n - j - 1, columns
+// 2(n - j) - 1). bsel < 0: both children (child 2 par + b pivots on copy b); otherwise
+// the single child on copy bsel. inv and Dn get the children's pivot reciprocals and
+// prefix determinants.
+__device__ void km_level(const double2 *cur, int cs, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *inv,
+                         int *flag, int nodes, int lg_npp, int j, int n, int bsel, double floor_) {
+  const int R = 2 * n - j, C = 2 * (n - j) + 1;
+  const int R1 = R - 1, C1 = C - 2;
+  const int nch = bsel < 0 ? 2 : 1;
+  for (int c = threadIdx.x; c < nodes * nch; c += blockDim.x) {
+    const int par = c / nch, b = bsel < 0 ? (c & 1) : bsel;
+    const double2 piv = cur[par * cs + (j + b) * C + b];
+    if (!(cabs1(piv) >= floor_)) flag[par >> lg_npp] |= 2;
+    inv[c] = crcp(piv);
+    Dn[c] = cmul(Dc[par], piv);
+  }
+  __syncthreads();
+  // rows split into column segments of at least 4 columns while the CTA has idle threads
+  const int rows = nodes * R1;
+  int lgseg = 0;
+  while ((rows << (lgseg + 1)) <= (int)blockDim.x && (C1 >> (lgseg + 1)) >= 4) ++lgseg;
+  const int seglen = (C1 + (1 << lgseg) - 1) >> lgseg;
+  for (int t = threadIdx.x; t < (rows << lgseg); t += blockDim.x) {
+    const int r = t >> lgseg;
+    const int q0 = (t & ((1 << lgseg) - 1)) * seglen, q1 = min(C1, q0 + seglen);
+    const int par = r / R1, ri = r - par * R1;
+    const double2 *S = cur + par * cs;
+    for (int k = 0; k < nch; ++k) {
+      const int b = bsel < 0 ? k : bsel;
+      const int ci = par * nch + k;
+      const double2 *prow = S + (j + b) * C + 2;
+      double2 *o = nxt + (size_t)ci * (R1 * C1) + ri * C1;
+      const double2 iv = inv[ci];
+      if (ri == j) {
+        for (int q = q0; q < q1; ++q) o[q] = cmul(prow[q], iv);
+      } else {
+        const int old = ri < j ? ri : ri + 1;
+        const double2 *srow = S + old * C;
+        const double2 Lf = cmul(srow[b], iv);
+#pragma unroll 4
+        for (int q = q0; q < q1; ++q) o[q] = cfms(srow[q + 2], Lf, prow[q]);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// The leaves under a node after n-2 eliminations (rows: n-2 eliminated, then vertex
+// n-2's two copies, then vertex n-1's; columns: the four copies, then X), on thread b
+// (copy of vertex n-2): the last elimination in registers, then both leaves. Adds the
+// terms into v[2i + k] (vertex i, Keldysh index k). path: the copies of vertices
+// 0..n-3 (bit n-3-i for vertex i), parity their count.
+template <int n>
+__device__ __forceinline__ void km_leaves2(const double2 *S, double2 D, const double2 *gd, int b, unsigned path,
+                                           int parity, double floor_, bool &guard, double2 (&v)[2 * n]) {
+  const int C = 5;
+  const double2 p1 = S[(n - 2 + b) * C + b];
+  if (!(cabs1(p1) >= floor_)) guard = true;
+  const double2 i1 = crcp(p1);
+  const double2 D1 = cmul(D, p1);
+  double2 prow[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) prow[q] = cmul(S[(n - 2 + b) * C + 2 + q], i1);
+  // rows of vertex n-1's copies after the elimination: pivot, X entry, W pivot
+  double2 p[2], cb[2], pw[2], e[2];
+#pragma unroll
+  for (int bp = 0; bp < 2; ++bp) {
+    const double2 *r = S + (n + bp) * C;
+    const double2 Lf = r[b]; // prow is normalised by the pivot already
+    p[bp] = cfms(r[2 + bp], Lf, prow[bp]);
+    cb[bp] = cfms(r[4], Lf, prow[2]);
+    pw[bp] = c2(p[bp].x - gd[bp].x, p[bp].y - gd[bp].y);
+    if (!(cabs1(p[bp]) >= floor_)) guard = true;
+  }
+  // coefficient of each leaf: -D1 * det(V) * sign = -D1^2 p (-1)^(parity + b + bp)
+  double2 coef[2];
+#pragma unroll
+  for (int bp = 0; bp < 2; ++bp) {
+    double2 t = cmul(cmul(D1, D1), p[bp]);
+    if ((parity + b + bp) & 1) t = c2(-t.x, -t.y);
+    coef[bp] = c2(-t.x, -t.y);
+  }
+  // vertex n-1: x_n = -D1 c_b (the D1 factor is in coef)
+#pragma unroll
+  for (int bp = 0; bp < 2; ++bp) {
+    const double2 t = cmul(coef[bp], cb[bp]);
+    v[2 * (n - 1) + bp] = cadd(v[2 * (n - 1) + bp], t);
+  }
+  // eliminated rows: vertices 0..n-3 (rows 0..n-3), then vertex n-2 (the pivot row)
+#pragma unroll
+  for (int i = 0; i <= n - 2; ++i) {
+    double2 r0, r1, rx; // the child's row i at vertex n-1's copies and X
+    if (i == n - 2) {
+      r0 = prow[0];
+      r1 = prow[1];
+      rx = prow[2];
+    } else {
+      const double2 *r = S + i * C;
+      const double2 Lf = r[b];
+      r0 = cfms(r[2], Lf, prow[0]);
+      r1 = cfms(r[3], Lf, prow[1]);
+      rx = cfms(r[4], Lf, prow[2]);
+    }
+    const int k = (i == n - 2) ? b : (int)((path >> (n - 3 - i)) & 1u);
+    double2 acc = c2(0.0, 0.0);
+#pragma unroll
+    for (int bp = 0; bp < 2; ++bp) {
+      // x_{i+1} / D1 = p_W f - e c_b
+      const double2 x = cfms(cmul(pw[bp], rx), bp ? r1 : r0, cb[bp]);
+      acc = cadd(acc, cmul(coef[bp], x));
+    }
+    // to (i, k), written without a dynamic index so that v stays in registers
+    v[2 * i] = cadd(v[2 * i], k ? c2(0.0, 0.0) : acc);
+    v[2 * i + 1] = cadd(v[2 * i + 1], k ? acc : c2(0.0, 0.0));
+  }
+}
+
+// Sums the 2n values v[] over aligned groups of G consecutive threads (G a power of two)
+// into S[g * 2n + q] for group g < ngroups; fixed shuffle pattern (deterministic).
+template <int n2>
+__device__ void km_group_sum(double2 (&v)[n2], int G, int ngroups, double2 *S, double2 (*red)[2 * KM_MAX_ORDER]) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gw = G < 32 ? G : 32;
+#pragma unroll
+  for (int q = 0; q < n2; ++q)
+    for (int off = 1; off < gw; off <<= 1) {
+      v[q].x += __shfl_xor_sync(0xffffffffu, v[q].x, off);
+      v[q].y += __shfl_xor_sync(0xffffffffu, v[q].y, off);
+    }
+  if (G <= 32) {
+    const int g = tid / G;
+    if ((lane & (G - 1)) == 0 && g < ngroups)
+#pragma unroll
+      for (int q = 0; q < n2; ++q) S[g * n2 + q] = cadd(S[g * n2 + q], v[q]);
+    __syncthreads();
+  } else {
+    if (lane == 0)
+#pragma unroll
+      for (int q = 0; q < n2; ++q) red[warp][q] = v[q];
+    __syncthreads();
+    const int wpg = G / 32;
+    for (int e = tid; e < ngroups * n2; e += blockDim.x) {
+      const int g = e / n2, q = e - g * n2;
+      double2 s = S[e];
+      for (int w = g * wpg; w < (g + 1) * wpg; ++w) s = cadd(s, red[w][q]);
+      S[e] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// Per-point sums S of np points whose inputs are in K.u, K.flag (tree form; flag bit 1
+// marks points to redo on the pivoted-LU path).
+template <int N>
+__device__ void km_tree_points(KMTreeShared &K, const ItemDev &it, int np, int *bad) {
+  const int tid = threadIdx.x;
+  const int n2 = 2 * N;
+  for (int e = tid; e < np * n2; e += blockDim.x) K.S[e] = c2(0.0, 0.0);
+  __syncthreads();
+  const double floor_ = it.model.pivot_floor;
+  const int spin = it.f.A.spin;
+  const int K0 = km_path_levels(N);
+  const int M = 2 * N + 1;
+  for (int sub = 0; sub < (1 << K0); ++sub) {
+    build_G_any<true>(it, N, np, K.u, K.flag, K.buf[0], spin, bad);
+    __syncthreads();
+    for (int p = tid; p < np; p += blockDim.x) {
+      K.D[0][p] = c2(1.0, 0.0);
+      const double2 *G = K.buf[0] + (size_t)p * M * M;
+      K.gd[p][0] = G[(2 * N - 2) * M + 2 * N - 2];
+      K.gd[p][1] = G[(2 * N - 1) * M + 2 * N - 1];
+    }
+    __syncthreads();
+    double2 v[2 * N];
+#pragma unroll
+    for (int q = 0; q < 2 * N; ++q) v[q] = c2(0.0, 0.0);
+    if (N == 1) {
+      // the leaves of the root itself: x_1 = -c_b, det(V) = p
+      if (tid < 2 * np) {
+        const int p = tid >> 1, b = tid & 1;
+        const double2 *G = K.buf[0] + (size_t)p * M * M;
+        const double2 piv = G[b * M + b], cb = G[b * M + 2];
+        double2 t = cmul(piv, cb);
+        if (!b) t = c2(-t.x, -t.y); // -(-1)^b p c_b
+        v[0] = b ? c2(0.0, 0.0) : t;
+        v[1] = b ? t : c2(0.0, 0.0);
+      }
+      km_group_sum<2 * N>(v, 2, np, K.S, K.red);
+      continue;
+    }
+    int cur = 0, cs = M * M, nodes = np, lg = 0;
+    for (int j = 0; j < N - 2; ++j) {
+      const int bsel = j < K0 ? (int)((sub >> (K0 - 1 - j)) & 1u) : -1;
+      km_level(K.buf[cur], cs, K.buf[cur ^ 1], K.D[cur], K.D[cur ^ 1], K.inv, K.flag, nodes, lg, j, N, bsel, floor_);
+      if (bsel < 0) {
+        nodes *= 2;
+        lg += 1;
+      }
+      cur ^= 1;
+      cs = (2 * N - j - 1) * (2 * (N - j) - 1);
+    }
+    // nodes after N-2 eliminations: 2 threads each
+    bool guard = false;
+    int p = 0;
+    if (tid < 2 * nodes) {
+      const int node = tid >> 1, b = tid & 1;
+      p = node >> lg;
+      const unsigned pathbits = ((unsigned)sub << lg) | (unsigned)(node & ((1 << lg) - 1));
+      if constexpr (N >= 2)
+        km_leaves2<N>(K.buf[cur] + (size_t)node * cs, K.D[cur][node], K.gd[p], b, pathbits, __popc(pathbits), floor_,
+                      guard, v);
+    }
+    if (guard) K.flag[p] |= 2;
+    km_group_sum<2 * N>(v, 2 << lg, np, K.S, K.red);
+  }
+}
+
+__device__ void km_tree_points_any(KMTreeShared &K, const ItemDev &it, int N, int np, int *bad) {
+  switch (N) {
+  case 1: km_tree_points<1>(K, it, np, bad); break;
+  case 2: km_tree_points<2>(K, it, np, bad); break;
+  case 3: km_tree_points<3>(K, it, np, bad); break;
+  case 4: km_tree_points<4>(K, it, np, bad); break;
+  case 5: km_tree_points<5>(K, it, np, bad); break;
+  case 6: km_tree_points<6>(K, it, np, bad); break;
+  case 7: km_tree_points<7>(K, it, np, bad); break;
+  case 8: km_tree_points<8>(K, it, np, bad); break;
+  case 9: km_tree_points<9>(K, it, np, bad); break;
+  default: km_tree_points<10>(K, it, np, bad); break;
+  }
+}
+
+__global__ void __launch_bounds__(NT) km_tree_kernel(Launch L) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  KMTreeShared &K = *reinterpret_cast<KMTreeShared *>(smem_raw);
+  __shared__ int s_chunk;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  if (tid == 0) s_bad = 0;
+  const bool eval = L.mode != IN_SOBOL;
+  const int nb = L.nbins * L.bin_cols;
+  for (;;) {
+    if (tid == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
+    __syncthreads();
+    const int c = s_chunk;
+    if (c >= L.n_chunks) break;
+    const int item = find_item(L.chunk_offsets, L.n_items, c);
+    const ItemDev &it = L.items[item];
+    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * it.chunk_points;
+    const int ccount = (int)min((long long)it.chunk_points, it.n_points - cfirst);
+    const int N = it.order;
+    const int n2 = 2 * N;
+    const bool keep = L.mode == IN_SOBOL ? true : (L.keep_u_hypercube != 0);
+    if (!eval) {
+      for (int b = tid; b < nb; b += blockDim.x) {
+        L.bin_sums[(size_t)c * nb + b] = c2(0.0, 0.0);
+        L.bin_counts[(size_t)c * nb + b] = 0u;
+      }
+      if (tid == 0) L.bin_dropped[c] = 0u;
+    }
+    double2 csum = c2(0.0, 0.0);
+    unsigned long long cdom = 0;
+    const int P = it.spin_symmetric ? km_points_per_pass(N) : 1;
+    for (int sb = 0; sb < ccount; sb += P) {
+      const int np = min(P, ccount - sb);
+      load_points(L, it, N, np, cfirst + sb, K.u, K.jac, K.flag, keep);
+      __syncthreads();
+      if (it.spin_symmetric) {
+        km_tree_points_any(K, it, N, np, &s_bad);
+      } else {
+        for (int e = tid; e < np * n2; e += blockDim.x) K.S[e] = c2(0.0, 0.0);
+        if (tid < np) K.flag[tid] |= (K.flag[tid] & 1) ? 0 : 2;
+        __syncthreads();
+      }
+      // guarded points (and the spin-asymmetric ones): keldy's pivoted-LU path, one by one
+      for (int p = 0; p < np; ++p) {
+        if ((K.flag[p] & 3) != 2) continue;
+        double ut[KM_MAX_ORDER];
+        for (int j = 0; j < N; ++j) ut[j] = K.u[j * np + p];
+        __syncthreads();
+        if (tid < N) K.K.u[tid] = ut[tid];
+        if (tid == 0) K.K.flag[0] = 0;
+        __syncthreads();
+        const double2 s = kernel_point(K.K, it, N, &s_bad);
+        if (tid < n2) K.S[p * n2 + tid] = s;
+        __syncthreads();
+      }
+      if (tid == 0) {
+        for (int p = 0; p < np; ++p) {
+          const long long gp = cfirst + sb + p;
+          const bool dom = !(K.flag[p] & 1);
+          const double j = K.jac[p];
+          const double2 *Sp = K.S + p * n2;
+          if (eval) {
+            for (int q = 0; q < n2; ++q)
+              L.out_kvals[gp * n2 + q] = dom ? c2(Sp[q].x * j, Sp[q].y * j) : c2(0.0, 0.0);
+            if (L.out_jac) L.out_jac[gp] = j;
+            if (L.out_dom) L.out_dom[gp] = dom ? 1 : 0;
+          } else if (dom) {
+            cdom++;
+            const unsigned half = 1u << (N - 1);
+            for (int i = 0; i < N; ++i) {
+              const int bin = time_bin(L, K.u + i * np + p, 1, 1);
+              for (int k = 0; k < 2; ++k) {
+                const double2 s = Sp[2 * i + k];
+                csum = c2(csum.x + s.x * j, csum.y + s.y * j);
+                if (bin < 0) {
+                  L.bin_dropped[c] += half;
+                } else {
+                  double2 &bs = L.bin_sums[(size_t)c * nb + 2 * bin + k];
+                  bs = c2(bs.x + s.x * j, bs.y + s.y * j);
+                  L.bin_counts[(size_t)c * nb + 2 * bin + k] += half;
+                }
+              }
+            }
+          }
+        }
+      }
+      __syncthreads();
+    }
+    if (!eval && tid == 0) {
+      ChunkPartial pr;
+      pr.sum_re = csum.x;
+      pr.sum_im = csum.y;
+      pr.n_in_domain = cdom;
+      pr.n_fallback = 0;
+      pr.fb_mask[0] = pr.fb_mask[1] = 0;
+      L.partials[c] = pr;
+    }
+  }
+  if (tid == 0 && s_bad) atomicOr(L.err, 1);
+}
+
 // Thread t of block `item` sums bins t, t + NT, ... over the item's chunks in chunk order.
 __global__ void __launch_bounds__(NT) reduce_bins_kernel(Launch L, double2 *sums, unsigned long long *counts,
                                                          unsigned long long *dropped) {
@@ -1229,7 +1605,14 @@ __global__ void __launch_bounds__(NT) reduce_bins_kernel(Launch L, double2 *sums
 } // namespace
 
 cudaError_t launch_kernel_method(const Launch &L, int grid, cudaStream_t st) {
-  kernel_method_kernel<<<grid, NT, 0, st>>>(L);
+  static bool configured = false;
+  const int smem = (int)sizeof(KMTreeShared);
+  if (!configured) {
+    cudaError_t e = cudaFuncSetAttribute(km_tree_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  km_tree_kernel<<<grid, NT, smem, st>>>(L);
   return cudaGetLastError();
 }
 
@@ -1260,6 +1643,8 @@ cudaError_t configure_kernels() {
     e = cudaFuncSetAttribute(direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirectShared));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(DirectShared));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(km_tree_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(KMTreeShared));
   return e;
 }
 

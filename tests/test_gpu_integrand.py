@@ -181,3 +181,39 @@ def test_cubic_interpolation_vs_oracle(ctx, oracle, golden):
         (s_g, np_g, nd_g, _), = capi.integrate(ctx, [dict(model=gm, rng=ctx.sobol(n), chain=chain, A=A, B=B,
                                                           order=n, n_points=4096)])
         assert (np_g, nd_g) == (np_o, nd_o) and abs(s_g - s_o) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("n", [13, 14, 15, 16])
+def test_integrand_maximum_orders_vs_oracle(ctx, oracle, golden, n):
+    """The largest orders (up to the library's 16): the tree walks its first n - 9 levels one
+    path at a time; one point each against the oracle's 2^n LU pairs."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr, 0.3)
+    om = oracle.model(10.0, le, gr, 0.3)
+    t = np.random.default_rng(300 + n).random((1, n)) * 10.0
+    A, B = EXTERNALS[0][1], EXTERNALS[0][2]
+    want, dw, sc = oracle.integrand(om, A, B, t)
+    for algo in (capi.ALGO_TREE, capi.ALGO_AUTO):
+        v, d = gm.integrand(A, B, t, algo=algo)
+        np.testing.assert_array_equal(d, dw)
+        _check(v, want, sc)
+
+
+def test_empty_and_ragged_inputs(ctx, golden):
+    """No points: empty results, no launch error; a work list mixing empty items and orders
+    of uneven cost sums each item as it would alone; order 17 is refused."""
+    gm = ctx.model(10.0, golden["table_beta20_lesser"], golden["table_beta20_greater"])
+    A, B = EXTERNALS[0][1], EXTERNALS[0][2]
+    v, d = gm.integrand(A, B, np.zeros((0, 3)))
+    assert v.shape == (0,) and d.shape == (0,)
+    chain = [(capi.WARPER_PLASMA_UV, 10.0, 0.0), (capi.WARPER_EXPONENTIAL, 10.0, 1.0)]
+    items = [dict(model=gm, rng=ctx.sobol(n), chain=chain, A=A, B=B, order=n, n_points=p)
+             for n, p in ((3, 0), (7, 333), (1, 5), (5, 0), (2, 1000))]
+    together = capi.integrate(ctx, items)
+    for it, res in zip(items, together):
+        alone = capi.integrate(ctx, [it])[0]
+        assert res[:3] == alone[:3]
+        if it["n_points"] == 0:
+            assert res[0] == 0 and res[1] == 0
+    with pytest.raises(capi.KbError):
+        capi.integrate(ctx, [dict(items[1], order=17, rng=ctx.sobol(17))])

@@ -75,3 +75,46 @@ def test_kernel_method_errors(ctx, golden):
         capi.integrate_kernel(ctx, [item], 8, 0.0, 10.0)
     with pytest.raises(capi.KbError, match="wrong order"):
         capi.integrate_kernel(ctx, [dict(item, order=2, rng=ctx.sobol(2))], 8, 3.0, 1.0)
+
+
+@pytest.mark.parametrize("n", [8, 9, 10])
+def test_point_values_high_orders_vs_oracle(ctx, oracle, golden, n):
+    """Orders 8-10 (the tree form walks the first n - 7 levels of orders 9 and 10 one path
+    at a time)."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr, 0.3)
+    om = oracle.model(10.0, le, gr, 0.3)
+    t = np.random.default_rng(50 + n).random((3, n)) * 10.0
+    got, dom = gm.integrand_kernel(X, t)
+    want, odom, sc = oracle.integrand_kernel(om, X, t)
+    assert np.array_equal(dom, odom)
+    for p in range(len(t)):
+        assert np.abs(got[p] - want[p]).max() <= 1e-12 * max(sc[p], 1e-300), (p, np.abs(got[p] - want[p]).max(), sc[p])
+
+
+def test_spin_asymmetric_and_guarded_points(ctx, oracle, golden):
+    """Points that leave the tree form take keldy's pivoted-LU path: a model whose spin-down
+    tables differ (det(s2) is then not the tree's), and a table that vanishes at t = 0 (every
+    diagonal pivot below the guard)."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    rng = np.random.default_rng(4)
+    t = rng.random((6, 4)) * 10.0
+    # different spin-down tables
+    ld, gd = 0.7 * le, 1.3 * gr
+    gm = ctx.model(10.0, le, gr, 0.0, lesser_down=ld, greater_down=gd)
+    om = oracle.model(10.0, le, gr, 0.0, lesser_down=ld, greater_down=gd)
+    got, _ = gm.integrand_kernel(X, t)
+    want, _, sc = oracle.integrand_kernel(om, X, t)
+    for p in range(len(t)):
+        assert np.abs(got[p] - want[p]).max() <= 1e-12 * sc[p]
+    # a table zero at t = 0
+    mid = len(le) // 2
+    lz, gz = le.copy(), gr.copy()
+    lz[mid] = 0.0
+    gz[mid] = 0.0
+    gm = ctx.model(10.0, lz, gz)
+    om = oracle.model(10.0, lz, gz)
+    got, _ = gm.integrand_kernel(X, t)
+    want, _, sc = oracle.integrand_kernel(om, X, t)
+    for p in range(len(t)):
+        assert np.abs(got[p] - want[p]).max() <= 1e-12 * max(sc[p], 1e-300)
