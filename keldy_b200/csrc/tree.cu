@@ -1237,6 +1237,7 @@ struct KMTreeShared {
   double2 gd[NT][2];  // original diagonal entries of the last vertex's two copies, per point
   double2 S[256];     // per point the 2n sums, S[p * 2n + 2i + k]
   double2 red[NT / 32][2 * KM_MAX_ORDER];
+  int bidx[256];      // per (point, vertex) the time bin (-1 dropped, -2 out of domain)
 };
 
 // Points per pass of the tree form: 2^(n-1) threads per point (one per configuration of
@@ -1533,32 +1534,57 @@ __global__ void __launch_bounds__(NT) km_tree_kernel(Launch L) {
         if (tid < n2) K.S[p * n2 + tid] = s;
         __syncthreads();
       }
-      if (tid == 0) {
-        for (int p = 0; p < np; ++p) {
+      if (eval) {
+        for (int e = tid; e < np * n2; e += blockDim.x) {
+          const int p = e / n2, q = e - p * n2;
           const long long gp = cfirst + sb + p;
           const bool dom = !(K.flag[p] & 1);
           const double j = K.jac[p];
-          const double2 *Sp = K.S + p * n2;
-          if (eval) {
-            for (int q = 0; q < n2; ++q)
-              L.out_kvals[gp * n2 + q] = dom ? c2(Sp[q].x * j, Sp[q].y * j) : c2(0.0, 0.0);
+          L.out_kvals[gp * n2 + q] = dom ? c2(K.S[e].x * j, K.S[e].y * j) : c2(0.0, 0.0);
+          if (q == 0) {
             if (L.out_jac) L.out_jac[gp] = j;
             if (L.out_dom) L.out_dom[gp] = dom ? 1 : 0;
-          } else if (dom) {
+          }
+        }
+      } else {
+        // bin of every (point, vertex); then one thread per (bin, index) adds the pass's
+        // terms in point and vertex order, as one thread walking them would
+        for (int e = tid; e < np * N; e += blockDim.x) {
+          const int p = e / N, i = e - p * N;
+          K.bidx[e] = (K.flag[p] & 1) ? -2 : time_bin(L, K.u + i * np + p, 1, 1);
+        }
+        __syncthreads();
+        const unsigned half = 1u << (N - 1);
+        for (int bk = tid; bk < nb; bk += blockDim.x) {
+          const int bin = bk >> 1, k = bk & 1;
+          double2 bs = L.bin_sums[(size_t)c * nb + bk];
+          unsigned cnt = 0;
+          bool any = false;
+          for (int p = 0; p < np; ++p) {
+            const double j = K.jac[p];
+            for (int i = 0; i < N; ++i)
+              if (K.bidx[p * N + i] == bin) {
+                const double2 sv = K.S[p * n2 + 2 * i + k];
+                bs = c2(bs.x + sv.x * j, bs.y + sv.y * j);
+                cnt += half;
+                any = true;
+              }
+          }
+          if (any) {
+            L.bin_sums[(size_t)c * nb + bk] = bs;
+            L.bin_counts[(size_t)c * nb + bk] += cnt;
+          }
+        }
+        if (tid == 0) {
+          for (int p = 0; p < np; ++p) {
+            if (K.flag[p] & 1) continue;
             cdom++;
-            const unsigned half = 1u << (N - 1);
+            const double j = K.jac[p];
             for (int i = 0; i < N; ++i) {
-              const int bin = time_bin(L, K.u + i * np + p, 1, 1);
+              if (K.bidx[p * N + i] < 0) L.bin_dropped[c] += 2 * half;
               for (int k = 0; k < 2; ++k) {
-                const double2 s = Sp[2 * i + k];
-                csum = c2(csum.x + s.x * j, csum.y + s.y * j);
-                if (bin < 0) {
-                  L.bin_dropped[c] += half;
-                } else {
-                  double2 &bs = L.bin_sums[(size_t)c * nb + 2 * bin + k];
-                  bs = c2(bs.x + s.x * j, bs.y + s.y * j);
-                  L.bin_counts[(size_t)c * nb + 2 * bin + k] += half;
-                }
+                const double2 sv = K.S[p * n2 + 2 * i + k];
+                csum = c2(csum.x + sv.x * j, csum.y + sv.y * j);
               }
             }
           }
