@@ -1224,20 +1224,23 @@ __global__ void __launch_bounds__(NT) kernel_method_kernel(Launch L) {
 // below the guard (or a model whose spins differ) takes keldy's pivoted-LU path,
 // kernel_point above, with the same per-(vertex, index) sums.
 
+// Sized for two CTAs per SM: at most 64 points per pass, 64 nodes per level, 128 vertex
+// times; the per-warp partial sums of the leaves' reduction live in the frontier buffer
+// that the last level leaves free.
+constexpr int KM_MAX_PASS = 64;
 struct KMTreeShared {
   union {
     double2 buf[2][FRONTIER];
     KernelShared K; // the pivoted-LU path of a guarded point (after the tree pass)
   };
-  double2 D[2][NT];
-  double2 inv[NT];
-  double u[256];      // vertex times, u[j * np + p]
-  double jac[NT];
-  int flag[NT];       // bit 0: out of domain, bit 1: a guarded pivot
-  double2 gd[NT][2];  // original diagonal entries of the last vertex's two copies, per point
-  double2 S[256];     // per point the 2n sums, S[p * 2n + 2i + k]
-  double2 red[NT / 32][2 * KM_MAX_ORDER];
-  int bidx[256];      // per (point, vertex) the time bin (-1 dropped, -2 out of domain)
+  double2 D[2][KM_MAX_PASS];
+  double2 inv[KM_MAX_PASS];
+  double u[2 * KM_MAX_PASS];   // vertex times, u[j * np + p]
+  double jac[KM_MAX_PASS];
+  int flag[KM_MAX_PASS];       // bit 0: out of domain, bit 1: a guarded pivot
+  double2 gd[KM_MAX_PASS][2];  // original diagonal entries of the last vertex's two copies, per point
+  double2 S[256];              // per point the 2n sums, S[p * 2n + 2i + k]
+  int bidx[256];               // per (point, vertex) the time bin (-1 dropped, -2 out of domain)
 };
 
 // Points per pass of the tree form: 2^(n-1) threads per point (one per configuration of
@@ -1434,7 +1437,7 @@ __device__ void km_tree_points(KMTreeShared &K, const ItemDev &it, int np, int *
         v[0] = b ? c2(0.0, 0.0) : t;
         v[1] = b ? t : c2(0.0, 0.0);
       }
-      km_group_sum<2 * N>(v, 2, np, K.S, K.red);
+      km_group_sum<2 * N>(v, 2, np, K.S, reinterpret_cast<double2(*)[2 * KM_MAX_ORDER]>(K.buf[1]));
       continue;
     }
     int cur = 0, cs = M * M, nodes = np, lg = 0;
@@ -1460,7 +1463,7 @@ __device__ void km_tree_points(KMTreeShared &K, const ItemDev &it, int np, int *
                       guard, v);
     }
     if (guard) K.flag[p] |= 2;
-    km_group_sum<2 * N>(v, 2 << lg, np, K.S, K.red);
+    km_group_sum<2 * N>(v, 2 << lg, np, K.S, reinterpret_cast<double2(*)[2 * KM_MAX_ORDER]>(K.buf[cur ^ 1]));
   }
 }
 
