@@ -24,8 +24,10 @@ struct ChunkPartial {
 
 constexpr int CHUNK_POINTS = 128; // points per scheduling chunk (<= 128: two 64-bit masks)
 // Per-CTA slot of the tree kernel's chunk set-up: coordinates [MAX_ORDER][CHUNK_POINTS],
-// then the Jacobians and the domain flags of the chunk's points.
-constexpr int PTS_SLOT = CHUNK_POINTS * (MAX_ORDER + 2);
+// then the Jacobians and the domain flags of the chunk's points; with time bins also each
+// point's bin code (2 bin + 1 when its value is added, 2 bin when only counted, -1 when
+// dropped) and its f*J (re, im).
+constexpr int PTS_SLOT = CHUNK_POINTS * (MAX_ORDER + 5);
 
 struct Launch {
   const ItemDev *items; // device

@@ -32,6 +32,9 @@ namespace kb {
 namespace {
 
 constexpr int NT = CTA_THREADS;
+// first of the set-up slot's three rows of per-point bin data (after the coordinates,
+// the Jacobians and the flags)
+constexpr int BIN_CODE_ROW = MAX_ORDER + 2;
 // Threads of a tree-kernel CTA: four per 7x7 node of the last breadth-first level (64
 // nodes per sub-batch at every order).
 constexpr int TREE_THREADS = 2 * CTA_THREADS;
@@ -93,6 +96,17 @@ __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, l
   flag_out[p] = dom ? 0 : 1;
 }
 
+// Bin of the earliest vertex time (binner_t::in_bounds and coord2index, binner.hpp:163-176:
+// in [xmin, xmax], xmax itself in the last bin); -1: dropped. An index that rounds up to
+// nbins just below xmax goes to the last bin.
+__device__ __forceinline__ int time_bin(const Launch &L, const double *u, int stride, int N) {
+  double t = u[0];
+  for (int j = 1; j < N; ++j) t = fmin(t, u[j * stride]);
+  if (!(L.bin_xmin <= t && t <= L.bin_xmax)) return -1;
+  if (t == L.bin_xmax) return L.nbins - 1;
+  return min((int)((t - L.bin_xmin) / L.bin_size), L.nbins - 1);
+}
+
 // One point of a chunk, on one thread: Sobol coordinates (or the given inputs), the
 // warper chain, the domain flag; written to the CTA's set-up slot at column t.
 __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long long gp, bool keep, double *slot,
@@ -120,6 +134,10 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
   for (int j = 0; j < N; ++j) slot[j * CHUNK_POINTS + t] = x[j];
   slot[MAX_ORDER * CHUNK_POINTS + t] = jac;
   slot[(MAX_ORDER + 1) * CHUNK_POINTS + t] = dom ? 0.0 : 1.0;
+  if (L.nbins) { // the time bin of the earliest vertex: code 2 bin, or -1 when dropped
+    const int bin = time_bin(L, x, 1, N);
+    slot[BIN_CODE_ROW * CHUNK_POINTS + t] = bin < 0 ? -1.0 : (double)(2 * bin);
+  }
 }
 
 // G (row-major, M = 2N+1) of np points: G[p*M*M + r*M + c]. Out-of-domain points get
@@ -376,24 +394,6 @@ __device__ __forceinline__ void tree_bottom5(const double2 *R, double2 D, int pa
   tree_bottom5r(s, D, parity, floor_, want_scale, sum, scale, guard);
 }
 
-// The child on pivot b of a 7x7 node (shared memory), built in registers, then its last
-// two levels: the breadth-first level into 5x5 nodes fused with the bottom.
-__device__ __forceinline__ void tree_bottom7(const double2 *S, double2 D, int b, int parity, double floor_,
-                                             bool want_scale, double2 &sum, double &scale, bool &guard) {
-  const double2 piv = S[b * 8];
-  if (!(cabs1(piv) >= floor_)) guard = true;
-  const double2 inv = crcp(piv);
-  const double2 Db = cmul(D, piv);
-  double2 t[25];
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    const double2 Lf = cmul(S[(i + 2) * 7 + b], inv);
-#pragma unroll
-    for (int j = 0; j < 5; ++j) t[i * 5 + j] = cfms(S[(i + 2) * 7 + j + 2], Lf, S[b * 7 + j + 2]);
-  }
-  tree_bottom5r(t, Db, parity ^ b, floor_, want_scale, sum, scale, guard);
-}
-
 // Grandchild (b, bp) of a 7x7 node (shared memory; rows 0,1: vertex k, 2,3: vertex k+1,
 // 4,5: vertex k+2, 6: external) in registers: eliminate row b, then row 2 + bp of the
 // child, leaving the 3x3 Schur complement T over rows {4, 5, 6}; then its two leaves,
@@ -583,17 +583,6 @@ __device__ __forceinline__ double2 apply_cutoff(double2 f, double cutoff) {
   return (cabs(f) < cutoff) ? c2(0.0, 0.0) : f;
 }
 
-// Bin of the earliest vertex time (binner_t::in_bounds and coord2index, binner.hpp:163-176:
-// in [xmin, xmax], xmax itself in the last bin); -1: dropped. An index that rounds up to
-// nbins just below xmax goes to the last bin.
-__device__ __forceinline__ int time_bin(const Launch &L, const double *u, int stride, int N) {
-  double t = u[0];
-  for (int j = 1; j < N; ++j) t = fmin(t, u[j * stride]);
-  if (!(L.bin_xmin <= t && t <= L.bin_xmax)) return -1;
-  if (t == L.bin_xmax) return L.nbins - 1;
-  return min((int)((t - L.bin_xmin) / L.bin_size), L.nbins - 1);
-}
-
 // Zeroes chunk c's bins (all threads of the CTA; a barrier follows before their use).
 __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
   if (!L.nbins) return;
@@ -627,9 +616,9 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
     const bool keep = (L.mode == IN_SOBOL) ? true : (L.keep_u_hypercube != 0);
     double2 csum = c2(0.0, 0.0);
     unsigned long long cdom = 0, cfb = 0, mask0 = 0, mask1 = 0;
+    unsigned cdrop = 0;
     double *slot = L.pts + (size_t)blockIdx.x * PTS_SLOT;
     if (tid < ccount) prepare_point(L, it, N, cfirst + tid, keep, slot, tid);
-    if (!EVAL) clear_bins(L, c);
     __syncthreads();
     for (int sb = 0; sb < ccount; sb += P) {
       const int np = min(P, ccount - sb);
@@ -657,12 +646,10 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
         for (int p = 0; p < np; ++p) {
           int fl = S.flag[p];
           int bin = -2;
-          if (L.nbins) {
-            bin = time_bin(L, slot + sb + p, CHUNK_POINTS, N);
-            if (bin < 0)
-              L.bin_dropped[c]++;
-            else
-              L.bin_counts[(size_t)c * L.nbins + bin]++;
+          if (L.nbins) { // the code prepare_point stored: 2 bin, or -1 when dropped
+            const double code = slot[BIN_CODE_ROW * CHUNK_POINTS + sb + p];
+            bin = code < 0.0 ? -1 : (int)code >> 1;
+            if (bin < 0) cdrop++;
           }
           if (fl & 1) continue;
           cdom++;
@@ -680,12 +667,47 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
           csum.x += f.x * j;
           csum.y += f.y * j;
           if (bin >= 0) {
-            double2 &bs = L.bin_sums[(size_t)c * L.nbins + bin];
-            bs = c2(bs.x + f.x * j, bs.y + f.y * j);
+            slot[BIN_CODE_ROW * CHUNK_POINTS + sb + p] = (double)(2 * bin + 1);
+            slot[(BIN_CODE_ROW + 1) * CHUNK_POINTS + sb + p] = f.x * j;
+            slot[(BIN_CODE_ROW + 2) * CHUNK_POINTS + sb + p] = f.y * j;
           }
         }
       }
       __syncthreads();
+    }
+    if (!EVAL && L.nbins) {
+      // the chunk's bins with its points added in point order (the order of one thread
+      // walking the chunk): one thread per bin for up to 512 bins, else one thread over the
+      // points; the pivoted-LU pass adds its points later
+      const double *code = slot + BIN_CODE_ROW * CHUNK_POINTS;
+      const double *vre = code + CHUNK_POINTS, *vim = vre + CHUNK_POINTS;
+      if (L.nbins <= 512) {
+        for (int b = tid; b < L.nbins; b += blockDim.x) {
+          double2 bs = c2(0.0, 0.0);
+          unsigned cnt = 0;
+          for (int q = 0; q < ccount; ++q) {
+            if (code[q] < 0.0 || (int)code[q] >> 1 != b) continue;
+            cnt++;
+            if ((int)code[q] & 1) bs = c2(bs.x + vre[q], bs.y + vim[q]);
+          }
+          L.bin_sums[(size_t)c * L.nbins + b] = bs;
+          L.bin_counts[(size_t)c * L.nbins + b] = cnt;
+        }
+      } else {
+        clear_bins(L, c);
+        __syncthreads();
+        if (tid == 0)
+          for (int q = 0; q < ccount; ++q) {
+            if (code[q] < 0.0) continue;
+            const int b = (int)code[q] >> 1;
+            L.bin_counts[(size_t)c * L.nbins + b]++;
+            if ((int)code[q] & 1) {
+              double2 &bs = L.bin_sums[(size_t)c * L.nbins + b];
+              bs = c2(bs.x + vre[q], bs.y + vim[q]);
+            }
+          }
+      }
+      if (tid == 0) L.bin_dropped[c] = cdrop;
     }
     if (!EVAL && tid == 0) {
       ChunkPartial pr;
@@ -1125,84 +1147,6 @@ __device__ double2 kernel_point(KernelShared &K, const ItemDev &it, int N, int *
   return acc;
 }
 
-__global__ void __launch_bounds__(NT) kernel_method_kernel(Launch L) {
-  __shared__ KernelShared K;
-  __shared__ int s_chunk;
-  __shared__ int s_bad;
-  const int tid = threadIdx.x;
-  if (tid == 0) s_bad = 0;
-  const bool eval = L.mode != IN_SOBOL;
-  const int nb = L.nbins * L.bin_cols;
-  for (;;) {
-    if (tid == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
-    __syncthreads();
-    const int c = s_chunk;
-    if (c >= L.n_chunks) break;
-    const int item = find_item(L.chunk_offsets, L.n_items, c);
-    const ItemDev &it = L.items[item];
-    const long long cfirst = (long long)(c - L.chunk_offsets[item]) * it.chunk_points;
-    const long long total = eval ? it.n_points : it.n_points;
-    const int ccount = (int)min((long long)it.chunk_points, total - cfirst);
-    const int N = it.order;
-    if (!eval) {
-      for (int b = tid; b < nb; b += blockDim.x) {
-        L.bin_sums[(size_t)c * nb + b] = c2(0.0, 0.0);
-        L.bin_counts[(size_t)c * nb + b] = 0u;
-      }
-      if (tid == 0) L.bin_dropped[c] = 0u;
-    }
-    double2 csum = c2(0.0, 0.0);
-    unsigned long long cdom = 0;
-    for (int p = 0; p < ccount; ++p) {
-      const long long gp = cfirst + p;
-      load_points(L, it, N, 1, gp, K.u, K.jac, K.flag, L.mode == IN_SOBOL ? true : (L.keep_u_hypercube != 0));
-      __syncthreads();
-      const bool dom = !(K.flag[0] & 1);
-      double2 v = c2(0.0, 0.0);
-      if (dom) v = kernel_point(K, it, N, &s_bad);
-      if (tid < 2 * N) K.S[tid] = v;
-      __syncthreads();
-      if (tid == 0) {
-        const double j = K.jac[0];
-        if (eval) {
-          for (int q = 0; q < 2 * N; ++q)
-            L.out_kvals[gp * 2 * N + q] = dom ? c2(K.S[q].x * j, K.S[q].y * j) : c2(0.0, 0.0);
-          if (L.out_jac) L.out_jac[gp] = j;
-          if (L.out_dom) L.out_dom[gp] = dom ? 1 : 0;
-        } else if (dom) {
-          cdom++;
-          const unsigned half = 1u << (N - 1);
-          for (int i = 0; i < N; ++i) {
-            const int bin = time_bin(L, K.u + i, 1, 1);
-            for (int k = 0; k < 2; ++k) {
-              const double2 s = K.S[2 * i + k];
-              csum = c2(csum.x + s.x * j, csum.y + s.y * j);
-              if (bin < 0) {
-                L.bin_dropped[c] += half;
-              } else {
-                double2 &bs = L.bin_sums[(size_t)c * nb + 2 * bin + k];
-                bs = c2(bs.x + s.x * j, bs.y + s.y * j);
-                L.bin_counts[(size_t)c * nb + 2 * bin + k] += half;
-              }
-            }
-          }
-        }
-      }
-      __syncthreads();
-    }
-    if (!eval && tid == 0) {
-      ChunkPartial pr;
-      pr.sum_re = csum.x;
-      pr.sum_im = csum.y;
-      pr.n_in_domain = cdom;
-      pr.n_fallback = 0;
-      pr.fb_mask[0] = pr.fb_mask[1] = 0;
-      L.partials[c] = pr;
-    }
-  }
-  if (tid == 0 && s_bad) atomicOr(L.err, 1);
-}
-
 // ------------------------------------------------------------ kernel method, tree form
 // For spin-symmetric models det(s2_a) = det(V_a), V_a the vertex block of G picked by a,
 // and keldy's s1_a = [[g_XX, r], [c, W_a]] with W_a = V_a except its last vertex's
@@ -1314,7 +1258,7 @@ __device__ __forceinline__ void km_leaves2(const double2 *S, double2 D, const do
 #pragma unroll
   for (int q = 0; q < 3; ++q) prow[q] = cmul(S[(n - 2 + b) * C + 2 + q], i1);
   // rows of vertex n-1's copies after the elimination: pivot, X entry, W pivot
-  double2 p[2], cb[2], pw[2], e[2];
+  double2 p[2], cb[2], pw[2];
 #pragma unroll
   for (int bp = 0; bp < 2; ++bp) {
     const double2 *r = S + (n + bp) * C;

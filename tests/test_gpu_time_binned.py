@@ -20,7 +20,7 @@ def _item(model, rng, chain, order, n, A=CHARGE[0], B=CHARGE[1]):
     return dict(model=model, rng=rng, chain=chain, A=A, B=B, order=order, k_first=1, n_points=n)
 
 
-@pytest.mark.parametrize("nbins,xmin,xmax", [(10, 0.0, 10.0), (7, 1.0, 6.5), (1, 0.0, 10.0)])
+@pytest.mark.parametrize("nbins,xmin,xmax", [(10, 0.0, 10.0), (7, 1.0, 6.5), (1, 0.0, 10.0), (600, 0.0, 10.0)])
 def test_bins_vs_oracle(ctx, oracle, golden, nbins, xmin, xmax):
     le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
     gm = ctx.model(10.0, le, gr)
