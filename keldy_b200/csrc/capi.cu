@@ -60,8 +60,12 @@ int kb_context_create(int device, kb_context **out) {
     delete ctx;
     return fail(KB_E_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
   }
+  // Every upload goes through the library's stream: it does not synchronise with the
+  // legacy default stream, and a plain cudaMemcpy from pageable memory may return before
+  // its data has landed.
   e = cudaMalloc(&ctx->d_err, sizeof(int));
-  if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -128,11 +132,14 @@ int kb_sobol_create(kb_context *ctx, int dim, int log_max_points, int do_shift, 
   s->device = ctx->device;
   s->dim = dim;
   s->m = log_max_points;
+  std::lock_guard<std::mutex> lk(ctx->mu); // the upload uses the context's stream
   cudaSetDevice(ctx->device);
   cudaError_t e = cudaMalloc(&s->d_Csr, Csr.size() * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMalloc(&s->d_shfr, shfr.size() * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMemcpy(s->d_Csr, Csr.data(), Csr.size() * 4, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(s->d_shfr, shfr.data(), shfr.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_Csr, Csr.data(), Csr.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_shfr, shfr.data(), shfr.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     cudaFree(s->d_Csr);
     cudaFree(s->d_shfr);
@@ -1380,8 +1387,11 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
     if (e == cudaSuccess) e = cudaMalloc(&g.d_part, sizeof(ChunkPartial) * (size_t)g.n_chunks);
     if (e == cudaSuccess && gi == 0) e = cudaMalloc(&g.d_pts, sizeof(double) * PTS_SLOT * (size_t)g.grid);
     if (e == cudaSuccess) e = cudaMalloc(&g.d_acc, sizeof(kb_accum) * g.n_items);
-    if (e == cudaSuccess) e = cudaMemcpy(g.d_items, g.items.data(), sizeof(ItemDev) * g.n_items, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(g.d_offs, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(g.d_items, g.items.data(), sizeof(ItemDev) * g.n_items, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(g.d_offs, offs.data(), sizeof(long long) * offs.size(), cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
       plan_free(p);
       return fail(KB_E_NOMEM, std::string("kb_plan_create: ") + cudaGetErrorString(e));

@@ -81,9 +81,10 @@ int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out) {
   if (e == cudaSuccess) e = cudaMalloc(&f->adam_m, nb);
   if (e == cudaSuccess) e = cudaMalloc(&f->adam_v, nb);
   if (e == cudaSuccess) e = cudaMalloc(&f->img, (size_t)FLOW_NPARAM * sizeof(uint16_t));
-  if (e == cudaSuccess) e = cudaMemcpy(f->master, inr.data(), nb, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemset(f->adam_m, 0, nb);
-  if (e == cudaSuccess) e = cudaMemset(f->adam_v, 0, nb);
+  // on the library's stream, which does not synchronise with the legacy default stream
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f->master, inr.data(), nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_m, 0, nb, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_v, 0, nb, ctx->stream);
   if (e == cudaSuccess) e = launch_flow_pack(f->master, f->img, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {

@@ -531,8 +531,12 @@ int upload(kb_context *ctx, std::vector<HostDim> &dims, int type, double u_max, 
     t->pts_u.push_back(dims[(size_t)d].u_in);
     t->pts_f1.push_back(dims[(size_t)d].f1_in);
   }
-  if (e == cudaSuccess) e = cudaMemcpy(t->d_data, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(t->d_dims, meta.data(), meta.size() * sizeof(TableDimDev), cudaMemcpyHostToDevice);
+  // on the library's stream, which does not synchronise with the legacy default stream
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(t->d_data, host.data(), host.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(t->d_dims, meta.data(), meta.size() * sizeof(TableDimDev), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     cudaFree(t->d_data);
     cudaFree(t->d_dims);

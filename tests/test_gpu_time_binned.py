@@ -90,7 +90,7 @@ def test_bins_with_a_flow_and_pivoted_lu(ctx, golden):
     flow = capi.integrate_binned(ctx, [dict(item, flow=ctx.flow(4))], 8, 0.0, 10.0)[0]
     lu = capi.integrate_binned(ctx, [item], 8, 0.0, 10.0, algo=capi.ALGO_DIRECT)[0]
     for other in (flow, lu):
-        assert np.array_equal(other[5], base[5]) and other[6] == base[6]
+        assert np.array_equal(other[5], base[5]) and other[6] == base[6], (other[:4], other[6], base[:4], base[6])
         assert np.abs(other[4] - base[4]).max() <= 1e-12 * np.abs(base[4]).sum()
 
 
