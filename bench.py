@@ -597,7 +597,7 @@ def run_single(args):
                                         flow=flow)])
         print("single-flow", args.order, args.points, loss, res[0])
     if args.single_kernel:
-        # the kernel method at the same order: one kernel_method_kernel launch
+        # the kernel method at the same order: one km_tree_kernel launch
         res = capi.integrate_kernel(ctx, [dict(model=model, rng=ctx.sobol(args.order), chain=chain,
                                                A=(T_MAX, 0, 0, 0, 0), order=args.order, k_first=1,
                                                n_points=args.points)], 100, 0.0, T_MAX)

@@ -43,10 +43,18 @@ __device__ __forceinline__ bool interp_index(const ModelDev &m, double x, int &i
   return true;
 }
 
-// g^<(x) and g^>(x) of one table (interleaved lesser/greater per mesh point).
+// g^<(x) and g^>(x) of one table (interleaved lesser/greater per mesh point): mesh points
+// i and i + 1 as two 32-byte read-only loads (the tables are cudaMalloc'd, so 256-byte
+// aligned, and a mesh point's pair starts on a 32-byte boundary). The loads are volatile
+// so that they are never hoisted above the callers' checks of the table pointer.
 __device__ __forceinline__ void interp_pair(const double2 *tab, int i, double w, double2 &gl, double2 &gg) {
-  double2 l0 = __ldg(tab + 2 * i), g0 = __ldg(tab + 2 * i + 1);
-  double2 l1 = __ldg(tab + 2 * i + 2), g1 = __ldg(tab + 2 * i + 3);
+  double2 l0, g0, l1, g1;
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(l0.x), "=d"(l0.y), "=d"(g0.x), "=d"(g0.y)
+               : "l"(tab + 2 * i));
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(l1.x), "=d"(l1.y), "=d"(g1.x), "=d"(g1.y)
+               : "l"(tab + 2 * i + 2));
   double v = __dsub_rn(1.0, w);
   gl = c2(__dadd_rn(__dmul_rn(v, l0.x), __dmul_rn(w, l1.x)), __dadd_rn(__dmul_rn(v, l0.y), __dmul_rn(w, l1.y)));
   gg = c2(__dadd_rn(__dmul_rn(v, g0.x), __dmul_rn(w, g1.x)), __dadd_rn(__dmul_rn(v, g0.y), __dmul_rn(w, g1.y)));

@@ -483,6 +483,40 @@ __device__ void group_sum(double2 v, double sc, int G, int ngroups, double2 *fva
   }
 }
 
+// Per-point sums of the 7x7 bottom (thread q * 64 + node, 2^lg nodes per point): lane
+// groups of consecutive nodes by shuffles, then each point's groups and the four
+// grandchild slots q in a fixed order by thread p; adds to fval[p], fscale[p]. Every
+// thread calls it; scratch: 256 double2 + 256 double of free shared memory.
+__device__ void bottom_sum(double2 v, double sc, int lg, int np, double2 *fval, double *fscale, double2 *scratch) {
+  static_assert(TREE_THREADS == 256, "four grandchild slots of 64 nodes");
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int g = lg < 5 ? (1 << lg) : 32;
+  for (int off = 1; off < g; off <<= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, off);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, off);
+    sc += __shfl_xor_sync(0xffffffffu, sc, off);
+  }
+  double *sscale = reinterpret_cast<double *>(scratch + TREE_THREADS);
+  if ((lane & (g - 1)) == 0) {
+    scratch[tid] = v;
+    sscale[tid] = sc;
+  }
+  __syncthreads();
+  if (tid < np) {
+    const int per = 1 << lg;
+    double2 f = fval[tid];
+    double s2 = fscale[tid];
+    for (int q = 0; q < 4; ++q)
+      for (int nd = tid * per; nd < (tid + 1) * per; nd += g) {
+        f = cadd(f, scratch[q * 64 + nd]);
+        s2 += sscale[q * 64 + nd];
+      }
+    fval[tid] = f;
+    fscale[tid] = s2;
+  }
+  __syncthreads();
+}
+
 // Order 1: the 3x3 root's two leaves directly.
 __device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, double &scale, bool want_scale) {
   sum = c2(0.0, 0.0);
@@ -548,14 +582,18 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
     double sc = 0.0;
     bool guard = false;
     int G, p = 0;
-    if (m == 7) { // four threads per 7x7 node, one per grandchild
-      G = 4 << lg;
-      if (tid < 4 * nodes) {
-        const int node = tid >> 2, b = (tid >> 1) & 1, bp = tid & 1;
+    if (m == 7) { // four threads per 7x7 node: grandchild tid >> 6 of node tid & 63, so that a
+                  // warp's lanes read consecutive nodes (49-entry stride: no bank conflicts)
+      const int node = tid & 63, q = tid >> 6;
+      if (node < nodes) {
         p = node >> lg;
         const int parity = __popc(node & ((1 << lg) - 1)) + __popc(sub);
-        tree_bottom7q(S.buf[cur] + node * 49, S.D[cur][node], b, bp, parity, floor_, want_scale, v, sc, guard);
+        tree_bottom7q(S.buf[cur] + node * 49, S.D[cur][node], q >> 1, q & 1, parity, floor_, want_scale, v, sc,
+                      guard);
       }
+      if (guard) S.flag[p] |= 2;
+      bottom_sum(v, sc, lg, np, S.fval, S.fscale, S.buf[cur ^ 1]);
+      continue;
     } else if (m == 5) { // order 2: the root itself
       G = 1;
       if (tid < nodes) {
