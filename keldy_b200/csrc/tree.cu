@@ -1052,13 +1052,16 @@ __global__ void __launch_bounds__(NT) reduce_kernel(Launch L, kb_accum *acc) {
 // x_{i+1} (-1)^|a| det(s2_a), accumulated at (vertex time, a_i). Here the terms of a point
 // are summed per (vertex i, Keldysh index k) in configuration order (2n sums), then
 // binned; keldy accumulates them one by one into the same bins.
+// Threads of a km_tree_kernel CTA (two CTAs per SM: 16 warps); the points per pass stay
+// sized for 128 (km_points_per_pass), the extra warps hide the levels' latency.
+constexpr int KM_THREADS = 256;
 struct KernelShared {
   double2 G1[(2 * KM_MAX_ORDER + 1) * (2 * KM_MAX_ORDER + 1)];
   double2 G2[(2 * KM_MAX_ORDER) * (2 * KM_MAX_ORDER)];
   double u[KM_MAX_ORDER];
   double jac[1];
   int flag[1];
-  double2 X[NT][KM_MAX_ORDER];
+  double2 X[KM_THREADS][KM_MAX_ORDER];
   double2 S[2 * KM_MAX_ORDER];
 };
 
@@ -1464,7 +1467,7 @@ __device__ void km_tree_points_any(KMTreeShared &K, const ItemDev &it, int N, in
   }
 }
 
-__global__ void __launch_bounds__(NT) km_tree_kernel(Launch L) {
+__global__ void __launch_bounds__(KM_THREADS, 2) km_tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   KMTreeShared &K = *reinterpret_cast<KMTreeShared *>(smem_raw);
   __shared__ int s_chunk;
@@ -1623,7 +1626,7 @@ cudaError_t launch_kernel_method(const Launch &L, int grid, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  km_tree_kernel<<<grid, NT, smem, st>>>(L);
+  km_tree_kernel<<<grid, KM_THREADS, smem, st>>>(L);
   return cudaGetLastError();
 }
 
