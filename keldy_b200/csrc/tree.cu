@@ -331,6 +331,28 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
 }
 
+// Orders above TREE_MAX_SUB solve one point per sub-batch in 2^K0 passes (K0 = N -
+// TREE_MAX_SUB path steps, then the breadth-first levels), all starting from the same G.
+// That G can stay at the end of one frontier buffer across the passes when no step of a
+// pass writes that buffer far enough to reach it (step t writes buffer t & 1 from its
+// start). Returns the buffer (0 or 1), or -1 when G has to be rebuilt for every pass.
+__host__ __device__ constexpr int tree_root_buffer(int N) {
+  if (N <= TREE_MAX_SUB) return -1;
+  const int K0 = N - TREE_MAX_SUB, LB = TREE_MAX_SUB - 3, root = (2 * N + 1) * (2 * N + 1);
+  int use[2] = {0, 0};
+  int m = 2 * N + 1, nodes = 1;
+  for (int t = 1; t <= K0 + LB; ++t) {
+    m -= 2;
+    if (t > K0) nodes *= 2;
+    const int sz = nodes * m * m;
+    if (use[t & 1] < sz) use[t & 1] = sz;
+  }
+  // keep clear of the bottom's scratch at the start of the free buffer as well
+  for (int b = 0; b < 2; ++b)
+    if (use[b] + root <= FRONTIER && root + 384 <= FRONTIER) return b;
+  return -1;
+}
+
 // One step down a fixed path (single point): pivot on row b, drop rows 0 and 1.
 __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *tmp,
                                int *flag, int m, int b, double floor_) {
@@ -559,14 +581,17 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   const int LB = R >= 3 ? R - 3 : 0; // breadth-first levels down to 7x7 nodes
   const double floor_ = it.model.pivot_floor;
   const int spin = it.f.A.spin;
+  const int rb = tree_root_buffer(N); // >= 0: G built once, kept at the end of buffer rb
+  double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - (2 * N + 1) * (2 * N + 1)) : S.buf[0];
   for (int sub = 0; sub < (1 << K0); ++sub) {
-    build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, S.buf[0], spin, bad);
+    if (rb < 0 || sub == 0) build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, root, spin, bad);
     if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
     __syncthreads();
     int m = 2 * N + 1, cur = 0;
     for (int k = 0; k < K0; ++k) {
       int b = (sub >> (K0 - 1 - k)) & 1;
-      tree_path_step(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, m, b, floor_);
+      tree_path_step(k == 0 ? root : S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, m, b,
+                     floor_);
       m -= 2;
       cur ^= 1;
     }
