@@ -331,28 +331,6 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
 }
 
-// Orders above TREE_MAX_SUB solve one point per sub-batch in 2^K0 passes (K0 = N -
-// TREE_MAX_SUB path steps, then the breadth-first levels), all starting from the same G.
-// That G can stay at the end of one frontier buffer across the passes when no step of a
-// pass writes that buffer far enough to reach it (step t writes buffer t & 1 from its
-// start). Returns the buffer (0 or 1), or -1 when G has to be rebuilt for every pass.
-__host__ __device__ constexpr int tree_root_buffer(int N) {
-  if (N <= TREE_MAX_SUB) return -1;
-  const int K0 = N - TREE_MAX_SUB, LB = TREE_MAX_SUB - 3, root = (2 * N + 1) * (2 * N + 1);
-  int use[2] = {0, 0};
-  int m = 2 * N + 1, nodes = 1;
-  for (int t = 1; t <= K0 + LB; ++t) {
-    m -= 2;
-    if (t > K0) nodes *= 2;
-    const int sz = nodes * m * m;
-    if (use[t & 1] < sz) use[t & 1] = sz;
-  }
-  // keep clear of the bottom's scratch at the start of the free buffer as well
-  for (int b = 0; b < 2; ++b)
-    if (use[b] + root <= FRONTIER && root + 384 <= FRONTIER) return b;
-  return -1;
-}
-
 // One step down a fixed path (single point): pivot on row b, drop rows 0 and 1.
 __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *tmp,
                                int *flag, int m, int b, double floor_) {
@@ -558,7 +536,8 @@ __device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, dou
 // Integrand of np points whose inputs are loaded (S.u, S.flag): S.fval, S.fscale, and
 // flag bit 1 where a pivot fell below the guard.
 template <bool ANY_CUBIC>
-__device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad) {
+__device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad,
+                            double2 *groot) {
   const int tid = threadIdx.x;
   if (tid < np) {
     S.fval[tid] = c2(0.0, 0.0);
@@ -581,12 +560,20 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   const int LB = R >= 3 ? R - 3 : 0; // breadth-first levels down to 7x7 nodes
   const double floor_ = it.model.pivot_floor;
   const int spin = it.f.A.spin;
-  const int rb = tree_root_buffer(N); // >= 0: G built once, kept at the end of buffer rb
-  double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - (2 * N + 1) * (2 * N + 1)) : S.buf[0];
+  // G built once per point: kept at the end of frontier buffer rb (rb >= 0), else in the
+  // CTA's global keeper groot (L2-resident) and copied back for every later pass
+  const int rb = tree_root_buffer(N), MM = (2 * N + 1) * (2 * N + 1);
+  const bool gkeep = K0 > 0 && rb < 0 && groot != nullptr;
+  double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - MM) : S.buf[0];
   for (int sub = 0; sub < (1 << K0); ++sub) {
-    if (rb < 0 || sub == 0) build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, root, spin, bad);
+    if (gkeep && sub > 0)
+      for (int e = tid; e < MM; e += blockDim.x) root[e] = groot[e];
+    else if (rb < 0 || sub == 0)
+      build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, root, spin, bad);
     if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
     __syncthreads();
+    if (gkeep && sub == 0) // the first path step only reads buffer 0
+      for (int e = tid; e < MM; e += blockDim.x) groot[e] = root[e];
     int m = 2 * N + 1, cur = 0;
     for (int k = 0; k < K0; ++k) {
       int b = (sub >> (K0 - 1 - k)) & 1;
@@ -691,7 +678,8 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
         S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
       }
       __syncthreads();
-      tree_points<ANY_CUBIC>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
+      tree_points<ANY_CUBIC>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad,
+                             L.roots ? L.roots + (size_t)blockIdx.x * ROOT_SLOT : nullptr);
       if (EVAL) {
         if (tid < np) {
           long long o = cfirst + sb + tid;
