@@ -47,6 +47,24 @@ def test_integrate_higher_orders_vs_oracle(ctx, oracle, golden):
         assert abs(s - w) <= 1e-12 * sc, (n, abs(s - w) / sc)
 
 
+def test_kept_g_across_path_passes(ctx, oracle, golden):
+    """Orders 10-13 walk their first n - 9 levels in 2^(n-9) passes from one G per point,
+    built once (kept in shared memory at orders 10 and 11, in a global keeper above).
+    Their sums equal the oracle's, and bit for bit those of the no-alloc entry point,
+    which has no keeper and rebuilds G for every pass."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    for n, npts in ((10, 6), (11, 4), (12, 3), (13, 2)):
+        item = _item(gm, ctx.sobol(n), PLASMA_EXP, n, npts)
+        (s, np_, nd, _), = capi.integrate(ctx, [item])
+        w, onp, ond, sc = oracle.integrate(om, CHARGE[0], CHARGE[1], PLASMA_EXP, n, npts)
+        assert (np_, nd) == (onp, ond)
+        assert abs(s - w) <= 1e-12 * sc, (n, abs(s - w) / sc)
+        (s2, np2, nd2, _), = capi.integrate_noalloc(ctx, [item])
+        assert (s2, np2, nd2) == (s, np_, nd), n
+
+
 def test_batched_items_equal_separate_calls(ctx, golden):
     le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
     gm = ctx.model(10.0, le, gr)
