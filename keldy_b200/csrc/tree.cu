@@ -335,14 +335,14 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
 __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *tmp,
                                int *flag, int m, int b, double floor_) {
   const int mc = m - 2;
+  // every thread forms the pivot's reciprocal itself: no barrier before the row updates
+  const double2 piv = cur[b * m + b];
+  const double2 inv = crcp(piv);
   if (threadIdx.x == 0) {
-    double2 piv = cur[b * m + b];
     if (!(cabs1(piv) >= floor_)) flag[0] |= 2;
-    tmp[0] = crcp(piv);
     Dn[0] = cmul(Dc[0], piv);
   }
-  __syncthreads();
-  const double2 inv = tmp[0];
+  (void)tmp;
   for (int r = threadIdx.x; r < mc * mc; r += blockDim.x) {
     int i = r / mc, j = r - i * mc;
     double2 Lf = cmul(cur[(i + 2) * m + b], inv);
