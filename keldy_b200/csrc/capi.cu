@@ -823,6 +823,35 @@ int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integr
 // ------------------------------------------------------------- integrator
 } // extern "C"
 
+namespace kb {
+cudaMemPool_t kb_pool() {
+  constexpr int MAX_DEVICES = 64;
+  static std::mutex mu;
+  static cudaMemPool_t pools[MAX_DEVICES] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= MAX_DEVICES) dev = 0;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) == cudaSuccess) {
+      unsigned long long keep = KB_POOL_KEEP_BYTES;
+      cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+      cudaGetLastError();
+      cudaDeviceGetDefaultMemPool(&p, dev);
+    }
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+} // namespace kb
+
 namespace {
 // Time bins of an integration (integrand_g_direct_time) and the caller's outputs.
 struct TimeBins {

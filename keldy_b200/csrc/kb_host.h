@@ -18,6 +18,13 @@ namespace kb {
 // Records msg as the calling thread's last error (kb_last_error) and returns code.
 int fail(int code, const std::string &msg);
 
+// The current device's memory pool of the library's stream-ordered allocations: unlike the
+// device's default pool, which hands freed memory back to the driver at every
+// synchronisation (so that the next call maps it again), it keeps up to
+// KB_POOL_KEEP_BYTES of freed memory cached for the next call.
+constexpr unsigned long long KB_POOL_KEEP_BYTES = 256ull << 20;
+cudaMemPool_t kb_pool();
+
 // Stream-ordered device buffer released at scope exit (on the same stream).
 struct DevBuf {
   void *p = nullptr;
@@ -27,7 +34,7 @@ struct DevBuf {
   DevBuf &operator=(const DevBuf &) = delete;
   cudaError_t alloc(size_t bytes, cudaStream_t s) {
     st = s;
-    return cudaMallocAsync(&p, bytes ? bytes : 16, s);
+    return cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, kb_pool(), s);
   }
   ~DevBuf() {
     if (p) cudaFreeAsync(p, st);
