@@ -1247,6 +1247,24 @@ struct KMTreeShared {
 __host__ __device__ inline int km_points_per_pass(int n) { return n == 1 ? 64 : n <= 8 ? (128 >> (n - 1)) : 1; }
 __host__ __device__ inline int km_path_levels(int n) { return n <= 8 ? 0 : n - 7; }
 
+// Orders with path levels run 2^K0 passes from the same G (one point per pass). It stays
+// at the end of the frontier buffer that no level of a pass writes that far (level j
+// writes buffer (j + 1) & 1 from its start; the leaves' reduction scratch takes the first
+// 160 entries of the free buffer). Returns that buffer, or -1 (single pass, or no room).
+__host__ __device__ inline int km_root_buffer(int N) {
+  const int K0 = km_path_levels(N);
+  if (K0 == 0) return -1;
+  const int root = (2 * N + 1) * (2 * N + 1);
+  int use[2] = {0, 0}, nodes = 1;
+  for (int j = 0; j < N - 2; ++j) {
+    if (j >= K0) nodes *= 2;
+    const int sz = nodes * (2 * N - j - 1) * (2 * (N - j) - 1);
+    if (use[(j + 1) & 1] < sz) use[(j + 1) & 1] = sz;
+  }
+  const int b = use[0] <= use[1] ? 0 : 1;
+  return (use[b] + root <= FRONTIER && root + 160 <= FRONTIER) ? b : -1;
+}
+
 // One elimination level: vertex j of every node (rows 2n - j, columns 2(n - j) + 1,
 // stride `cs` elements per node) into its children (rows 2n - j - 1, columns
 // 2(n - j) - 1). bsel < 0: both children (child 2 par + b pivots on copy b); otherwise
@@ -1411,12 +1429,15 @@ __device__ void km_tree_points(KMTreeShared &K, const ItemDev &it, int np, int *
   const int spin = it.f.A.spin;
   const int K0 = km_path_levels(N);
   const int M = 2 * N + 1;
+  // G built once for all passes (one point per pass) when it fits at a buffer's end
+  const int rb = km_root_buffer(N);
+  double2 *root = rb >= 0 ? K.buf[rb] + (FRONTIER - M * M) : K.buf[0];
   for (int sub = 0; sub < (1 << K0); ++sub) {
-    build_G_any<true>(it, N, np, K.u, K.flag, K.buf[0], spin, bad);
+    if (rb < 0 || sub == 0) build_G_any<true>(it, N, np, K.u, K.flag, root, spin, bad);
     __syncthreads();
     for (int p = tid; p < np; p += blockDim.x) {
       K.D[0][p] = c2(1.0, 0.0);
-      const double2 *G = K.buf[0] + (size_t)p * M * M;
+      const double2 *G = root + (size_t)p * M * M;
       K.gd[p][0] = G[(2 * N - 2) * M + 2 * N - 2];
       K.gd[p][1] = G[(2 * N - 1) * M + 2 * N - 1];
     }
@@ -1441,7 +1462,8 @@ __device__ void km_tree_points(KMTreeShared &K, const ItemDev &it, int np, int *
     int cur = 0, cs = M * M, nodes = np, lg = 0;
     for (int j = 0; j < N - 2; ++j) {
       const int bsel = j < K0 ? (int)((sub >> (K0 - 1 - j)) & 1u) : -1;
-      km_level(K.buf[cur], cs, K.buf[cur ^ 1], K.D[cur], K.D[cur ^ 1], K.inv, K.flag, nodes, lg, j, N, bsel, floor_);
+      km_level(j == 0 ? root : K.buf[cur], cs, K.buf[cur ^ 1], K.D[cur], K.D[cur ^ 1], K.inv, K.flag, nodes, lg, j,
+               N, bsel, floor_);
       if (bsel < 0) {
         nodes *= 2;
         lg += 1;
