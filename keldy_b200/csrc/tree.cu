@@ -535,7 +535,9 @@ __device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, dou
 
 // Integrand of np points whose inputs are loaded (S.u, S.flag): S.fval, S.fscale, and
 // flag bit 1 where a pivot fell below the guard.
-template <bool ANY_CUBIC>
+// KEEP: the instantiation with the global G keeper of orders above 11 (launches that hold
+// such an order; the others compile without it, which schedules their code better).
+template <bool ANY_CUBIC, bool KEEP>
 __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad,
                             double2 *groot) {
   const int tid = threadIdx.x;
@@ -563,7 +565,7 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   // G built once per point: kept at the end of frontier buffer rb (rb >= 0), else in the
   // CTA's global keeper groot (L2-resident) and copied back for every later pass
   const int rb = tree_root_buffer(N), MM = (2 * N + 1) * (2 * N + 1);
-  const bool gkeep = K0 > 0 && rb < 0 && groot != nullptr;
+  const bool gkeep = KEEP && K0 > 0 && rb < 0 && groot != nullptr;
   double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - MM) : S.buf[0];
   for (int sub = 0; sub < (1 << K0); ++sub) {
     if (gkeep && sub > 0)
@@ -643,7 +645,7 @@ __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
   if (threadIdx.x == 0) L.bin_dropped[c] = 0u;
 }
 
-template <bool EVAL, bool ANY_CUBIC>
+template <bool EVAL, bool ANY_CUBIC, bool KEEP>
 __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
@@ -678,8 +680,8 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
         S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
       }
       __syncthreads();
-      tree_points<ANY_CUBIC>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad,
-                             L.roots ? L.roots + (size_t)blockIdx.x * ROOT_SLOT : nullptr);
+      tree_points<ANY_CUBIC, KEEP>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad,
+                                   KEEP && L.roots ? L.roots + (size_t)blockIdx.x * ROOT_SLOT : nullptr);
       if (EVAL) {
         if (tid < np) {
           long long o = cfirst + sb + tid;
@@ -1674,16 +1676,21 @@ cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long lon
 
 size_t tree_smem_bytes() { return sizeof(TreeShared); }
 
-// Shared-memory limit of the four tree-kernel instantiations.
-static cudaError_t configure_tree(int smem) {
-  cudaError_t e = cudaFuncSetAttribute(tree_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+// Shared-memory limit of the eight tree-kernel instantiations.
+template <bool KEEP> static cudaError_t configure_tree_keep(int smem) {
+  cudaError_t e =
+      cudaFuncSetAttribute(tree_kernel<true, false, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = cudaFuncSetAttribute(tree_kernel<false, false, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = cudaFuncSetAttribute(tree_kernel<true, true, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    e = cudaFuncSetAttribute(tree_kernel<false, true, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   return e;
+}
+static cudaError_t configure_tree(int smem) {
+  cudaError_t e = configure_tree_keep<false>(smem);
+  return e == cudaSuccess ? configure_tree_keep<true>(smem) : e;
 }
 
 cudaError_t configure_kernels() {
@@ -1707,16 +1714,21 @@ cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     configured = true;
   }
+  const bool keep = L.roots != nullptr;
   if (L.mode == IN_SOBOL) {
     if (L.any_cubic)
-      tree_kernel<false, true><<<grid, TREE_THREADS, smem, st>>>(L);
+      keep ? tree_kernel<false, true, true><<<grid, TREE_THREADS, smem, st>>>(L)
+           : tree_kernel<false, true, false><<<grid, TREE_THREADS, smem, st>>>(L);
     else
-      tree_kernel<false, false><<<grid, TREE_THREADS, smem, st>>>(L);
+      keep ? tree_kernel<false, false, true><<<grid, TREE_THREADS, smem, st>>>(L)
+           : tree_kernel<false, false, false><<<grid, TREE_THREADS, smem, st>>>(L);
   } else {
     if (L.any_cubic)
-      tree_kernel<true, true><<<grid, TREE_THREADS, smem, st>>>(L);
+      keep ? tree_kernel<true, true, true><<<grid, TREE_THREADS, smem, st>>>(L)
+           : tree_kernel<true, true, false><<<grid, TREE_THREADS, smem, st>>>(L);
     else
-      tree_kernel<true, false><<<grid, TREE_THREADS, smem, st>>>(L);
+      keep ? tree_kernel<true, false, true><<<grid, TREE_THREADS, smem, st>>>(L)
+           : tree_kernel<true, false, false><<<grid, TREE_THREADS, smem, st>>>(L);
   }
   return cudaGetLastError();
 }
