@@ -332,8 +332,8 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
 }
 
 // One step down a fixed path (single point): pivot on row b, drop rows 0 and 1.
-__device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *tmp,
-                               int *flag, int m, int b, double floor_) {
+__device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int m,
+                               int b, double floor_) {
   const int mc = m - 2;
   // every thread forms the pivot's reciprocal itself: no barrier before the row updates
   const double2 piv = cur[b * m + b];
@@ -342,7 +342,6 @@ __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *
     if (!(cabs1(piv) >= floor_)) flag[0] |= 2;
     Dn[0] = cmul(Dc[0], piv);
   }
-  (void)tmp;
   for (int r = threadIdx.x; r < mc * mc; r += blockDim.x) {
     int i = r / mc, j = r - i * mc;
     double2 Lf = cmul(cur[(i + 2) * m + b], inv);
@@ -579,8 +578,7 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
     int m = 2 * N + 1, cur = 0;
     for (int k = 0; k < K0; ++k) {
       int b = (sub >> (K0 - 1 - k)) & 1;
-      tree_path_step(k == 0 ? root : S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, m, b,
-                     floor_);
+      tree_path_step(k == 0 ? root : S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag, m, b, floor_);
       m -= 2;
       cur ^= 1;
     }

@@ -183,6 +183,29 @@ def test_cubic_interpolation_vs_oracle(ctx, oracle, golden):
         assert (np_g, nd_g) == (np_o, nd_o) and abs(s_g - s_o) <= 1e-12 * scale
 
 
+def test_cubic_interpolation_high_orders_vs_oracle(ctx, oracle, golden):
+    """Cubic interpolation at the orders whose G is built once for several path passes
+    (10 and 11: kept in shared memory; 12: in the global keeper, a kernel instantiation of
+    its own): evaluations and the fused integration against the oracle."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr, 0.3)
+    gm.set_interpolation(3)
+    om = oracle.model(10.0, le, gr, 0.3, interp=3)
+    A, B = EXTERNALS[0][1], EXTERNALS[0][2]
+    rng = np.random.default_rng(77)
+    chain = [(capi.WARPER_PLASMA_UV, 10.0, 0.0), (capi.WARPER_EXPONENTIAL, 10.0, 1.0)]
+    for n in (10, 11, 12):
+        t = rng.random((2, n)) * 10.0
+        want, dw, sc = oracle.integrand(om, A, B, t)
+        v, d = gm.integrand(A, B, t, algo=capi.ALGO_TREE)
+        np.testing.assert_array_equal(d, dw)
+        _check(v, want, sc)
+        s_o, np_o, nd_o, scale = oracle.integrate(om, A, B, chain, n, 3)
+        (s_g, np_g, nd_g, _), = capi.integrate(ctx, [dict(model=gm, rng=ctx.sobol(n), chain=chain, A=A, B=B,
+                                                          order=n, n_points=3)])
+        assert (np_g, nd_g) == (np_o, nd_o) and abs(s_g - s_o) <= 1e-12 * scale, n
+
+
 @pytest.mark.parametrize("n", [13, 14, 15, 16])
 def test_integrand_maximum_orders_vs_oracle(ctx, oracle, golden, n):
     """The largest orders (up to the library's 16): the tree walks its first n - 9 levels one
