@@ -306,9 +306,9 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
   const unsigned rows = (unsigned)(nodes * mc);
   const unsigned magic = 0xFFFFFFFFu / (unsigned)mc + 1u; // r / mc == umulhi(r, magic) for r < 2^20, mc <= 31
-  // split rows into column segments of at least 5 columns while the CTA has idle threads
+  // split rows into column segments of at least 4 columns while the CTA has idle threads
   int lgseg = 0;
-  while ((rows << (lgseg + 1)) <= blockDim.x && (mc >> (lgseg + 1)) >= 5) ++lgseg;
+  while ((rows << (lgseg + 1)) <= blockDim.x && (mc >> (lgseg + 1)) >= 4) ++lgseg;
   const int seglen = (mc + (1 << lgseg) - 1) >> lgseg;
   const unsigned items = rows << lgseg;
   for (unsigned t = threadIdx.x; t < items; t += blockDim.x) {
