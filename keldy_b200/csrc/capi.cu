@@ -830,7 +830,11 @@ cudaMemPool_t kb_pool() {
   static cudaMemPool_t pools[MAX_DEVICES] = {};
   int dev = 0;
   cudaGetDevice(&dev);
-  if (dev < 0 || dev >= MAX_DEVICES) dev = 0;
+  if (dev < 0 || dev >= MAX_DEVICES) { // beyond the table: that device's default pool
+    cudaMemPool_t p = nullptr;
+    cudaDeviceGetDefaultMemPool(&p, dev);
+    return p;
+  }
   std::lock_guard<std::mutex> lk(mu);
   if (!pools[dev]) {
     cudaMemPoolProps props;
