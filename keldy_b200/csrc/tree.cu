@@ -482,12 +482,84 @@ __device__ void group_sum(double2 v, double sc, int G, int ngroups, double2 *fva
   }
 }
 
-// Per-point sums of the 7x7 bottom (thread q * 64 + node, 2^lg nodes per point): lane
-// groups of consecutive nodes by shuffles, then each point's groups and the four
-// grandchild slots q in a fixed order by thread p; adds to fval[p], fscale[p]. Every
-// thread calls it; scratch: 256 double2 + 256 double of free shared memory.
+// Great-grandchild (b, bp, bq) of a 9x9 node (shared memory; rows 0,1: vertex k, 2,3:
+// vertex k+1, 4,5: vertex k+2, 6,7: vertex k+3, 8: external) in registers: the
+// eliminations of row b, then 2 + bp, then 4 + bq, every entry formed as the breadth-first
+// levels and tree_bottom7q form it (so each leaf term is the same number), leaving the
+// 3x3 Schur complement T over rows {6, 7, 8}; then its two leaves,
+// each (-1)^|a| det(s2)^2 T_cc (T_cc T_ee - T_ce T_ec).
+__device__ __forceinline__ void tree_bottom9(const double2 *S, double2 D, int b, int bp, int bq, int parity,
+                                             double floor_, bool want_scale, double2 &sum, double &scale,
+                                             bool &guard) {
+  constexpr int W = 9;
+  const int c = 2 + bp, d = 4 + bq;
+  const int cols[5] = {c, d, 6, 7, 8};
+  const double2 p1 = S[b * W + b];
+  if (!(cabs1(p1) >= floor_)) guard = true;
+  const double2 i1 = crcp(p1);
+  double2 rb[5]; // row b at the columns that remain needed
+#pragma unroll
+  for (int k = 0; k < 5; ++k) rb[k] = S[b * W + cols[k]];
+  // child row c (first elimination) at columns {c, d, 6, 7, 8}
+  double2 rc[5];
+  {
+    const double2 Lf = cmul(S[c * W + b], i1);
+#pragma unroll
+    for (int k = 0; k < 5; ++k) rc[k] = cfms(S[c * W + cols[k]], Lf, rb[k]);
+  }
+  const double2 p2 = rc[0];
+  if (!(cabs1(p2) >= floor_)) guard = true;
+  const double2 i2 = crcp(p2);
+  // grandchild row d (second elimination) at columns {d, 6, 7, 8}
+  double2 rd[4];
+  {
+    const double2 Lf = cmul(S[d * W + b], i1);
+    const double2 a = cfms(S[d * W + c], Lf, rb[0]);
+    const double2 L2 = cmul(a, i2);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) rd[k] = cfms(cfms(S[d * W + cols[k + 1]], Lf, rb[k + 1]), L2, rc[k + 1]);
+  }
+  const double2 p3 = rd[0];
+  if (!(cabs1(p3) >= floor_)) guard = true;
+  const double2 i3 = crcp(p3);
+  // T row r - 6 at columns {6, 7, 8} (third elimination)
+  double2 T[9];
+#pragma unroll
+  for (int rr = 0; rr < 3; ++rr) {
+    const int r = 6 + rr;
+    const double2 Lf = cmul(S[r * W + b], i1);
+    const double2 a0 = cfms(S[r * W + c], Lf, rb[0]);
+    const double2 L2 = cmul(a0, i2);
+    const double2 a1 = cfms(cfms(S[r * W + d], Lf, rb[1]), L2, rc[1]);
+    const double2 L3 = cmul(a1, i3);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      T[rr * 3 + j] = cfms(cfms(cfms(S[r * W + 6 + j], Lf, rb[2 + j]), L2, rc[2 + j]), L3, rd[1 + j]);
+  }
+  const double2 Db = cmul(cmul(cmul(D, p1), p2), p3);
+  const double2 Db2 = cmul(Db, Db);
+  sum = c2(0.0, 0.0);
+  scale = 0.0;
+#pragma unroll
+  for (int cc = 0; cc < 2; ++cc) {
+    const double2 q = cmul(T[cc * 4], cfms(cmul(T[cc * 4], T[8]), T[cc * 3 + 2], T[6 + cc]));
+    const double2 term = cmul(Db2, q);
+    if ((b ^ bp ^ bq ^ cc) & 1)
+      sum = c2(sum.x - term.x, sum.y - term.y);
+    else
+      sum = cadd(sum, term);
+    if (want_scale) scale += cabs(term);
+  }
+  if (parity & 1) sum = c2(-sum.x, -sum.y);
+}
+
+// Per-point sums of the fused bottom (thread q * NODES + node, 2^lg nodes per point): lane
+// groups of consecutive nodes by shuffles, then each point's groups and the
+// TREE_THREADS / NODES descendant slots q in a fixed order by thread p; adds to fval[p],
+// fscale[p]. Every thread calls it; scratch: 256 double2 + 256 double of free shared memory.
+template <int NODES>
 __device__ void bottom_sum(double2 v, double sc, int lg, int np, double2 *fval, double *fscale, double2 *scratch) {
-  static_assert(TREE_THREADS == 256, "four grandchild slots of 64 nodes");
+  static_assert(TREE_THREADS == 256 && NODES >= 32, "slots of whole warps");
   const int tid = threadIdx.x, lane = tid & 31;
   const int g = lg < 5 ? (1 << lg) : 32;
   for (int off = 1; off < g; off <<= 1) {
@@ -505,10 +577,10 @@ __device__ void bottom_sum(double2 v, double sc, int lg, int np, double2 *fval, 
     const int per = 1 << lg;
     double2 f = fval[tid];
     double s2 = fscale[tid];
-    for (int q = 0; q < 4; ++q)
+    for (int q = 0; q < TREE_THREADS / NODES; ++q)
       for (int nd = tid * per; nd < (tid + 1) * per; nd += g) {
-        f = cadd(f, scratch[q * 64 + nd]);
-        s2 += sscale[q * 64 + nd];
+        f = cadd(f, scratch[q * NODES + nd]);
+        s2 += sscale[q * NODES + nd];
       }
     fval[tid] = f;
     fscale[tid] = s2;
@@ -558,7 +630,9 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   }
   const int R = N < TREE_MAX_SUB ? N : TREE_MAX_SUB;
   const int K0 = N - R;
-  const int LB = R >= 3 ? R - 3 : 0; // breadth-first levels down to 7x7 nodes
+  // breadth-first levels down to 9x9 nodes, then the fused bottom of three eliminations;
+  // orders 3 and 4 go down to 7x7 nodes and a bottom of two (three were 4 % slower at 4)
+  const int LB = R >= 5 ? R - 4 : (R >= 3 ? R - 3 : 0);
   const double floor_ = it.model.pivot_floor;
   const int spin = it.f.A.spin;
   // G built once per point: kept at the end of frontier buffer rb (rb >= 0), else in the
@@ -604,7 +678,18 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
                       guard);
       }
       if (guard) S.flag[p] |= 2;
-      bottom_sum(v, sc, lg, np, S.fval, S.fscale, S.buf[cur ^ 1]);
+      bottom_sum<64>(v, sc, lg, np, S.fval, S.fscale, S.buf[cur ^ 1]);
+      continue;
+    } else if (m == 9) { // eight threads per 9x9 node: great-grandchild tid >> 5 of node tid & 31
+      const int node = tid & 31, q = tid >> 5;
+      if (node < nodes) {
+        p = node >> lg;
+        const int parity = __popc(node & ((1 << lg) - 1)) + __popc(sub);
+        tree_bottom9(S.buf[cur] + node * 81, S.D[cur][node], q >> 2, (q >> 1) & 1, q & 1, parity, floor_, want_scale,
+                     v, sc, guard);
+      }
+      if (guard) S.flag[p] |= 2;
+      bottom_sum<32>(v, sc, lg, np, S.fval, S.fscale, S.buf[cur ^ 1]);
       continue;
     } else if (m == 5) { // order 2: the root itself
       G = 1;
