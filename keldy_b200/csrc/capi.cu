@@ -720,13 +720,9 @@ static int run_eval(kb_context *ctx, ItemDev it, int mode, int64_t count, const 
   L.err = ctx->d_err;
   int grid = (int)std::min<long long>(nchunks, use_tree ? ctx->tree_grid : ctx->sm_count * 4);
   if (use_tree) {
-    DevBuf dpts, droots;
+    DevBuf dpts;
     KB_CUDA(dpts.alloc((size_t)grid * PTS_SLOT * sizeof(double), st));
     L.pts = dpts.as<double>();
-    if (const size_t rbytes = root_scratch_bytes(grid, &it, 1)) {
-      KB_CUDA(droots.alloc(rbytes, st));
-      L.roots = droots.as<double2>();
-    }
     KB_CUDA(launch_tree(L, grid, st));
     std::vector<int> flags((size_t)count);
     KB_CUDA(cudaMemcpyAsync(flags.data(), dflag.p, count * sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -927,15 +923,11 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
       L.bin_counts = dbc.as<unsigned>();
       L.bin_dropped = dbd.as<unsigned>();
     }
-    DevBuf dpts, droots;
+    DevBuf dpts;
     const int tgrid = (int)std::min<long long>(nchunks, (long long)ctx->sm_count * ctx->ctas_per_sm);
     if (group == 0) {
       KB_CUDA(dpts.alloc((size_t)tgrid * PTS_SLOT * sizeof(double), st));
       L.pts = dpts.as<double>();
-      if (const size_t rbytes = root_scratch_bytes(tgrid, sorted.data(), sorted.size())) {
-        KB_CUDA(droots.alloc(rbytes, st));
-        L.roots = droots.as<double2>();
-      }
     }
     if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
     if (group == 0)
@@ -1321,7 +1313,6 @@ struct kb_plan {
     int *d_cnt = nullptr;
     ChunkPartial *d_part = nullptr;
     double *d_pts = nullptr;
-    double2 *d_roots = nullptr; // G keepers of orders above 11 (null: none)
     kb_accum *d_acc = nullptr;
   } g[2];
   int n_work = 0;
@@ -1350,7 +1341,6 @@ static void plan_free(kb_plan *p) {
     cudaFree(g.d_cnt);
     cudaFree(g.d_part);
     cudaFree(g.d_pts);
-    cudaFree(g.d_roots);
     cudaFree(g.d_acc);
   }
   for (auto &f : p->fills) cudaFree(f.buf);
@@ -1429,9 +1419,6 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
     if (e == cudaSuccess) e = cudaMalloc(&g.d_cnt, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&g.d_part, sizeof(ChunkPartial) * (size_t)g.n_chunks);
     if (e == cudaSuccess && gi == 0) e = cudaMalloc(&g.d_pts, sizeof(double) * PTS_SLOT * (size_t)g.grid);
-    if (e == cudaSuccess && gi == 0)
-      if (const size_t rbytes = root_scratch_bytes(g.grid, g.items.data(), g.items.size()))
-        e = cudaMalloc(&g.d_roots, rbytes);
     if (e == cudaSuccess) e = cudaMalloc(&g.d_acc, sizeof(kb_accum) * g.n_items);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(g.d_items, g.items.data(), sizeof(ItemDev) * g.n_items, cudaMemcpyHostToDevice, ctx->stream);
@@ -1471,7 +1458,6 @@ static int plan_enqueue(kb_context *ctx, kb_plan *p, cudaStream_t st) {
     L.mode = IN_SOBOL;
     L.partials = g.d_part;
     L.pts = g.d_pts;
-    L.roots = g.d_roots;
     L.err = ctx->d_err;
     if (gi == 0) {
       KB_CUDA(launch_tree(L, g.grid, st));

@@ -48,9 +48,6 @@ struct Launch {
   int *out_flag;        // tree: 1 = point needs the pivoted-LU kernel
   // tree kernel: gridDim.x * PTS_SLOT doubles of set-up scratch
   double *pts;
-  // tree kernel, orders whose G does not stay in shared memory across their passes:
-  // gridDim.x * ROOT_SLOT complex keepers (null: G rebuilt for every pass)
-  double2 *roots;
   // IN_SOBOL
   ChunkPartial *partials; // [n_chunks]
   // IN_SOBOL with time bins (integrand_g_direct_time): every point's f*J also goes to the
@@ -77,13 +74,15 @@ inline int items_any_cubic(const ItemDev *items, size_t n) {
 }
 
 // Orders above TREE_MAX_SUB solve one point per sub-batch in 2^K0 passes (K0 = N -
-// TREE_MAX_SUB path steps, then the breadth-first levels), all starting from the same G.
-// That G can stay at the end of one frontier buffer across the passes when no step of a
-// pass writes that buffer far enough to reach it (step t writes buffer t & 1 from its
-// start). Returns the buffer (0 or 1), or -1 when G has to be rebuilt for every pass.
+// TREE_MAX_SUB path steps, then the breadth-first levels down to 9x9 nodes), all starting
+// from the same G. That G stays at the end of one frontier buffer across the passes when
+// no step of a pass writes that buffer far enough to reach it (step t writes buffer t & 1
+// from its start) and it clears the bottom's scratch at the start of the free buffer.
+// Returns the buffer (0 or 1), or -1 when G has to be rebuilt for every pass (no order up
+// to MAX_ORDER needs that).
 __host__ __device__ inline int tree_root_buffer(int N) {
   if (N <= TREE_MAX_SUB) return -1;
-  const int K0 = N - TREE_MAX_SUB, LB = TREE_MAX_SUB - 3, root = (2 * N + 1) * (2 * N + 1);
+  const int K0 = N - TREE_MAX_SUB, LB = TREE_MAX_SUB - 4, root = (2 * N + 1) * (2 * N + 1);
   int use[2] = {0, 0};
   int m = 2 * N + 1, nodes = 1;
   for (int t = 1; t <= K0 + LB; ++t) {
@@ -92,21 +91,9 @@ __host__ __device__ inline int tree_root_buffer(int N) {
     const int sz = nodes * m * m;
     if (use[t & 1] < sz) use[t & 1] = sz;
   }
-  // keep clear of the bottom's scratch at the start of the free buffer as well
   for (int b = 0; b < 2; ++b)
     if (use[b] + root <= FRONTIER && root + 384 <= FRONTIER) return b;
   return -1;
-}
-
-// Complex entries of one CTA's G keeper for the orders whose G does not fit there (kept in
-// global memory, L2-resident, instead): the G of one point at MAX_ORDER.
-constexpr int ROOT_SLOT = (2 * MAX_ORDER + 1) * (2 * MAX_ORDER + 1);
-// Bytes of G keepers that a tree launch of `grid` CTAs over items[0..n) wants (0: none).
-inline size_t root_scratch_bytes(int grid, const ItemDev *items, size_t n) {
-  for (size_t i = 0; i < n; ++i)
-    if (items[i].order > TREE_MAX_SUB && tree_root_buffer(items[i].order) < 0)
-      return (size_t)grid * ROOT_SLOT * 16;
-  return 0;
 }
 
 size_t tree_smem_bytes();

@@ -606,11 +606,8 @@ __device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, dou
 
 // Integrand of np points whose inputs are loaded (S.u, S.flag): S.fval, S.fscale, and
 // flag bit 1 where a pivot fell below the guard.
-// KEEP: the instantiation with the global G keeper of orders above 11 (launches that hold
-// such an order; the others compile without it, which schedules their code better).
-template <bool ANY_CUBIC, bool KEEP>
-__device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad,
-                            double2 *groot) {
+template <bool ANY_CUBIC>
+__device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad) {
   const int tid = threadIdx.x;
   if (tid < np) {
     S.fval[tid] = c2(0.0, 0.0);
@@ -635,20 +632,13 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
   const int LB = R >= 5 ? R - 4 : (R >= 3 ? R - 3 : 0);
   const double floor_ = it.model.pivot_floor;
   const int spin = it.f.A.spin;
-  // G built once per point: kept at the end of frontier buffer rb (rb >= 0), else in the
-  // CTA's global keeper groot (L2-resident) and copied back for every later pass
-  const int rb = tree_root_buffer(N), MM = (2 * N + 1) * (2 * N + 1);
-  const bool gkeep = KEEP && K0 > 0 && rb < 0 && groot != nullptr;
-  double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - MM) : S.buf[0];
+  // G built once per point for all path passes, kept at the end of frontier buffer rb
+  const int rb = tree_root_buffer(N);
+  double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - (2 * N + 1) * (2 * N + 1)) : S.buf[0];
   for (int sub = 0; sub < (1 << K0); ++sub) {
-    if (gkeep && sub > 0)
-      for (int e = tid; e < MM; e += blockDim.x) root[e] = groot[e];
-    else if (rb < 0 || sub == 0)
-      build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, root, spin, bad);
+    if (rb < 0 || sub == 0) build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, root, spin, bad);
     if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
     __syncthreads();
-    if (gkeep && sub == 0) // the first path step only reads buffer 0
-      for (int e = tid; e < MM; e += blockDim.x) groot[e] = root[e];
     int m = 2 * N + 1, cur = 0;
     for (int k = 0; k < K0; ++k) {
       int b = (sub >> (K0 - 1 - k)) & 1;
@@ -728,7 +718,7 @@ __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
   if (threadIdx.x == 0) L.bin_dropped[c] = 0u;
 }
 
-template <bool EVAL, bool ANY_CUBIC, bool KEEP>
+template <bool EVAL, bool ANY_CUBIC>
 __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
@@ -763,8 +753,7 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
         S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
       }
       __syncthreads();
-      tree_points<ANY_CUBIC, KEEP>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad,
-                                   KEEP && L.roots ? L.roots + (size_t)blockIdx.x * ROOT_SLOT : nullptr);
+      tree_points<ANY_CUBIC>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
       if (EVAL) {
         if (tid < np) {
           long long o = cfirst + sb + tid;
@@ -1759,21 +1748,16 @@ cudaError_t launch_reduce_bins(const Launch &L, double2 *sums, unsigned long lon
 
 size_t tree_smem_bytes() { return sizeof(TreeShared); }
 
-// Shared-memory limit of the eight tree-kernel instantiations.
-template <bool KEEP> static cudaError_t configure_tree_keep(int smem) {
-  cudaError_t e =
-      cudaFuncSetAttribute(tree_kernel<true, false, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<false, false, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<true, true, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(tree_kernel<false, true, KEEP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  return e;
-}
+// Shared-memory limit of the four tree-kernel instantiations.
 static cudaError_t configure_tree(int smem) {
-  cudaError_t e = configure_tree_keep<false>(smem);
-  return e == cudaSuccess ? configure_tree_keep<true>(smem) : e;
+  cudaError_t e = cudaFuncSetAttribute(tree_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tree_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tree_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tree_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
 }
 
 cudaError_t configure_kernels() {
@@ -1797,21 +1781,16 @@ cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     configured = true;
   }
-  const bool keep = L.roots != nullptr;
   if (L.mode == IN_SOBOL) {
     if (L.any_cubic)
-      keep ? tree_kernel<false, true, true><<<grid, TREE_THREADS, smem, st>>>(L)
-           : tree_kernel<false, true, false><<<grid, TREE_THREADS, smem, st>>>(L);
+      tree_kernel<false, true><<<grid, TREE_THREADS, smem, st>>>(L);
     else
-      keep ? tree_kernel<false, false, true><<<grid, TREE_THREADS, smem, st>>>(L)
-           : tree_kernel<false, false, false><<<grid, TREE_THREADS, smem, st>>>(L);
+      tree_kernel<false, false><<<grid, TREE_THREADS, smem, st>>>(L);
   } else {
     if (L.any_cubic)
-      keep ? tree_kernel<true, true, true><<<grid, TREE_THREADS, smem, st>>>(L)
-           : tree_kernel<true, true, false><<<grid, TREE_THREADS, smem, st>>>(L);
+      tree_kernel<true, true><<<grid, TREE_THREADS, smem, st>>>(L);
     else
-      keep ? tree_kernel<true, false, true><<<grid, TREE_THREADS, smem, st>>>(L)
-           : tree_kernel<true, false, false><<<grid, TREE_THREADS, smem, st>>>(L);
+      tree_kernel<true, false><<<grid, TREE_THREADS, smem, st>>>(L);
   }
   return cudaGetLastError();
 }

@@ -185,8 +185,8 @@ def test_cubic_interpolation_vs_oracle(ctx, oracle, golden):
 
 def test_cubic_interpolation_high_orders_vs_oracle(ctx, oracle, golden):
     """Cubic interpolation at the orders whose G is built once for several path passes
-    (10 and 11: kept in shared memory; 12: in the global keeper, a kernel instantiation of
-    its own): evaluations and the fused integration against the oracle."""
+    (kept at the end of a shared-memory frontier buffer): evaluations and the fused
+    integration against the oracle."""
     le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
     gm = ctx.model(10.0, le, gr, 0.3)
     gm.set_interpolation(3)

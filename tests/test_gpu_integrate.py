@@ -49,9 +49,9 @@ def test_integrate_higher_orders_vs_oracle(ctx, oracle, golden):
 
 def test_kept_g_across_path_passes(ctx, oracle, golden):
     """Orders 10-13 walk their first n - 9 levels in 2^(n-9) passes from one G per point,
-    built once (kept in shared memory at orders 10 and 11, in a global keeper above).
-    Their sums equal the oracle's, and bit for bit those of the no-alloc entry point,
-    which has no keeper and rebuilds G for every pass."""
+    built once and kept at the end of a shared-memory frontier buffer. Their sums equal
+    the oracle's, and bit for bit those of the no-alloc entry point (same kernel, its
+    scratch in the library's static array)."""
     le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
     gm = ctx.model(10.0, le, gr)
     om = oracle.model(10.0, le, gr)
