@@ -724,10 +724,20 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
   TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
   __shared__ int s_chunk;
   __shared__ int s_bad;
+  // the chunk's partial sums and dropped count (thread 0), in shared memory so that they
+  // hold no registers through the tree
+  __shared__ ChunkPartial s_part;
+  __shared__ unsigned s_drop;
   const int tid = threadIdx.x;
   if (tid == 0) s_bad = 0;
   for (;;) {
-    if (tid == 0) s_chunk = atomicAdd(L.chunk_counter, 1);
+    if (tid == 0) {
+      s_chunk = atomicAdd(L.chunk_counter, 1);
+      s_part.sum_re = s_part.sum_im = 0.0;
+      s_part.n_in_domain = s_part.n_fallback = 0;
+      s_part.fb_mask[0] = s_part.fb_mask[1] = 0;
+      s_drop = 0;
+    }
     __syncthreads();
     const int c = s_chunk;
     if (c >= L.n_chunks) break;
@@ -739,9 +749,6 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
     const int N = it.order;
     const int P = tree_points_per_chunk(N);
     const bool keep = (L.mode == IN_SOBOL) ? true : (L.keep_u_hypercube != 0);
-    double2 csum = c2(0.0, 0.0);
-    unsigned long long cdom = 0, cfb = 0, mask0 = 0, mask1 = 0;
-    unsigned cdrop = 0;
     double *slot = L.pts + (size_t)blockIdx.x * PTS_SLOT;
     if (tid < ccount) prepare_point(L, it, N, cfirst + tid, keep, slot, tid);
     __syncthreads();
@@ -768,6 +775,10 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
           if (L.out_flag) L.out_flag[o] = (dom && (fl & 2)) ? 1 : 0;
         }
       } else if (tid == 0) {
+        double2 csum = c2(s_part.sum_re, s_part.sum_im);
+        unsigned long long cdom = s_part.n_in_domain, cfb = s_part.n_fallback;
+        unsigned long long mask0 = s_part.fb_mask[0], mask1 = s_part.fb_mask[1];
+        unsigned cdrop = s_drop;
         for (int p = 0; p < np; ++p) {
           int fl = S.flag[p];
           int bin = -2;
@@ -797,6 +808,13 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
             slot[(BIN_CODE_ROW + 2) * CHUNK_POINTS + sb + p] = f.y * j;
           }
         }
+        s_part.sum_re = csum.x;
+        s_part.sum_im = csum.y;
+        s_part.n_in_domain = cdom;
+        s_part.n_fallback = cfb;
+        s_part.fb_mask[0] = mask0;
+        s_part.fb_mask[1] = mask1;
+        s_drop = cdrop;
       }
       __syncthreads();
     }
@@ -832,18 +850,9 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
             }
           }
       }
-      if (tid == 0) L.bin_dropped[c] = cdrop;
+      if (tid == 0) L.bin_dropped[c] = s_drop;
     }
-    if (!EVAL && tid == 0) {
-      ChunkPartial pr;
-      pr.sum_re = csum.x;
-      pr.sum_im = csum.y;
-      pr.n_in_domain = cdom;
-      pr.n_fallback = cfb;
-      pr.fb_mask[0] = mask0;
-      pr.fb_mask[1] = mask1;
-      L.partials[c] = pr;
-    }
+    if (!EVAL && tid == 0) L.partials[c] = s_part;
   }
   if (tid == 0 && s_bad) atomicOr(L.err, 1);
 }
