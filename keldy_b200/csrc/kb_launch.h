@@ -82,14 +82,22 @@ inline int items_any_cubic(const ItemDev *items, size_t n) {
 // to MAX_ORDER needs that).
 __host__ __device__ inline int tree_root_buffer(int N) {
   if (N <= TREE_MAX_SUB) return -1;
+  // the kernel's schedule: K0 path steps, then the levels in pairs (tree_level4) and a
+  // last single one, each write into the other buffer
   const int K0 = N - TREE_MAX_SUB, LB = TREE_MAX_SUB - 4, root = (2 * N + 1) * (2 * N + 1);
   int use[2] = {0, 0};
-  int m = 2 * N + 1, nodes = 1;
-  for (int t = 1; t <= K0 + LB; ++t) {
+  int m = 2 * N + 1, nodes = 1, t = 0;
+  for (int k = 0; k < K0; ++k) {
     m -= 2;
-    if (t > K0) nodes *= 2;
-    const int sz = nodes * m * m;
-    if (use[t & 1] < sz) use[t & 1] = sz;
+    ++t;
+    if (use[t & 1] < m * m) use[t & 1] = m * m;
+  }
+  for (int k = 0; k < LB; k += (k + 1 < LB) ? 2 : 1) {
+    const int step = (k + 1 < LB) ? 2 : 1;
+    m -= 2 * step;
+    nodes <<= step;
+    ++t;
+    if (use[t & 1] < nodes * m * m) use[t & 1] = nodes * m * m;
   }
   for (int b = 0; b < 2; ++b)
     if (use[b] + root <= FRONTIER && root + 384 <= FRONTIER) return b;

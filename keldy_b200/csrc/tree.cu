@@ -331,6 +331,65 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
 }
 
+// Two breadth-first levels at once: node `par` (m x m) into its four grandchildren
+// 4 par + 2 b + bp (pivot on row b, then on row bp of that child), (m-4) x (m-4) each,
+// every entry formed exactly as two tree_level2 steps form it. Each item (grandchild row
+// i of a parent, a column segment, all four grandchildren) forms the pivots and child
+// entries it needs itself, so the pair takes one barrier and never stores the children.
+__device__ void tree_level4(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int nodes,
+                            int lg_npp, int m, double floor_) {
+  const int mg = m - 4, mm = m * m, mgg = mg * mg;
+  const unsigned rows = (unsigned)(nodes * mg);
+  const unsigned magic = 0xFFFFFFFFu / (unsigned)mg + 1u; // r / mg == umulhi(r, magic) for r < 2^20, mg <= 31
+  int lgseg = 0;
+  while ((rows << (lgseg + 1)) <= blockDim.x && (mg >> (lgseg + 1)) >= 2) ++lgseg;
+  const int seglen = (mg + (1 << lgseg) - 1) >> lgseg;
+  const unsigned items = rows << lgseg;
+  for (unsigned t = threadIdx.x; t < items; t += blockDim.x) {
+    const unsigned r = t >> lgseg;
+    const int j0 = (int)(t & ((1u << lgseg) - 1)) * seglen, j1 = min(mg, j0 + seglen);
+    const unsigned par = __umulhi(r, magic);
+    const int i = (int)(r - par * (unsigned)mg);
+    const double2 *S = cur + par * mm;
+    double2 ib[2], Lp[2][2], icp[2][2], Lr[2], Lg[2][2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+      ib[b] = crcp(S[b * (m + 1)]);
+      Lr[b] = cmul(S[(i + 4) * m + b], ib[b]);
+#pragma unroll
+      for (int bp = 0; bp < 2; ++bp) {
+        Lp[b][bp] = cmul(S[(2 + bp) * m + b], ib[b]); // child row bp's factor
+        const double2 cpv = cfms(S[(2 + bp) * m + 2 + bp], Lp[b][bp], S[b * m + 2 + bp]);
+        icp[b][bp] = crcp(cpv);
+        const double2 cib = cfms(S[(i + 4) * m + 2 + bp], Lr[b], S[b * m + 2 + bp]); // child row i+2, column bp
+        Lg[b][bp] = cmul(cib, icp[b][bp]);
+        if (i == 0 && j0 == 0) {
+          const int g = 4 * par + 2 * b + bp;
+          const double2 piv = S[b * (m + 1)];
+          if (!(cabs1(piv) >= floor_) || !(cabs1(cpv) >= floor_)) flag[par >> lg_npp] |= 2;
+          Dn[g] = cmul(cmul(Dc[par], piv), cpv);
+        }
+      }
+    }
+    const double2 *sr = S + (i + 4) * m + 4, *s0 = S + 4, *s1 = S + m + 4, *s2 = S + 2 * m + 4, *s3 = S + 3 * m + 4;
+    double2 *o = nxt + (4 * par) * mgg + i * mg;
+#pragma unroll 2
+    for (int j = j0; j < j1; ++j) {
+      const double2 v = sr[j], a0 = s0[j], a1 = s1[j], a2 = s2[j], a3 = s3[j];
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const double2 pb = b ? a1 : a0;
+        const double2 cij = cfms(v, Lr[b], pb);            // child b, row i+2
+        const double2 c0 = cfms(a2, Lp[b][0], pb);         // child b, row 0 (pivot row of bp = 0)
+        const double2 c1 = cfms(a3, Lp[b][1], pb);         // child b, row 1
+        o[(2 * b) * mgg + j] = cfms(cij, Lg[b][0], c0);
+        o[(2 * b + 1) * mgg + j] = cfms(cij, Lg[b][1], c1);
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // One step down a fixed path (single point): pivot on row b, drop rows 0 and 1.
 __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int m,
                                int b, double floor_) {
@@ -647,7 +706,14 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
       cur ^= 1;
     }
     int nodes = np, lg = 0;
-    for (int k = 0; k < LB; ++k) {
+    for (int k = 0; k + 1 < LB; k += 2) { // pairs of levels, then a last single one
+      tree_level4(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag, nodes, lg, m, floor_);
+      nodes *= 4;
+      lg += 2;
+      m -= 4;
+      cur ^= 1;
+    }
+    if (LB & 1) {
       tree_level2(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, nodes, lg, m, floor_);
       nodes *= 2;
       lg += 1;
