@@ -34,7 +34,7 @@ if ROOT not in sys.path:
 GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
 # DRAM bytes (read + write) of one tree_kernel launch of this workload (2^20 points,
 # order 8), from an ncu capture of that launch (profiles/tree_kernel_order8_2e20pts_dram.md)
-TREE_LAUNCH_DRAM_BYTES = 1_802_240
+TREE_LAUNCH_DRAM_BYTES = 1_811_200
 E2E_REPEATS = 5
 
 
