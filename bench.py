@@ -33,9 +33,22 @@ if ROOT not in sys.path:
 
 GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
 # DRAM bytes (read + write) of one tree_kernel launch of this workload (2^20 points,
-# order 8), from an ncu capture of that launch (profiles/tree_kernel_order8_2e20pts_dram.md)
-TREE_LAUNCH_DRAM_BYTES = 1_811_200
+# order 8) from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
+# the hash of the kernel's sources (tree_source_hash) at the time of the capture. A build
+# whose sources hash differently reports no traffic figure until it is captured again.
+TREE_DRAM_CAPTURES = {}
+TREE_SOURCES = ("tree.cu", "kb_device.cuh", "kb_types.h", "kb_launch.h")
 E2E_REPEATS = 5
+
+
+def tree_source_hash():
+    """First 16 hex digits of the SHA-256 of the tree kernel's source files."""
+    import hashlib
+    h = hashlib.sha256()
+    for f in TREE_SOURCES:
+        with open(os.path.join(ROOT, "keldy_b200", "csrc", f), "rb") as fh:
+            h.update(fh.read())
+    return h.hexdigest()[:16]
 
 
 def flop_lu(m):
@@ -479,9 +492,7 @@ def run_ours(args, rank, world, local_rank):
     plan.close()
     # end to end through the public API with host buffers: per step, upload the g0
     # tables from pinned memory (kb_model_set_table), integrate, read the sums back. The
-    # K steps run E2E_REPEATS times; the best run is reported with all of them listed: on
-    # this shared machine a host-side CUDA call now and then stalls for up to ~1 s,
-    # outside the library's control.
+    # K steps run E2E_REPEATS times; the median run is reported with all of them listed.
     m2 = capi.Model(ctx, T_MAX, le_pin.view(np.complex128), gr_pin.view(np.complex128))
     e2e_runs = []
     for r in range(E2E_REPEATS):
@@ -492,7 +503,7 @@ def run_ours(args, rank, world, local_rank):
             allreduce(capi.integrate(ctx, [item(args.warmup + (1 + r) * args.steps + s, m2)]))
         barrier()
         e2e_runs.append(time.perf_counter() - t0)
-    e2e_s = min(e2e_runs)
+    e2e_s = statistics.median(e2e_runs)
     sampler.stop()
     clocks = sampler.summary(w0, max(w1, w0 + 1))
     clocks["e2e"] = sampler.summary(w1)
@@ -530,21 +541,27 @@ def run_ours(args, rank, world, local_rank):
             cref = CpuReference(order)
             cpu = cref.measure(cref.sample_size(10.0))
         h2d = 2 * NPTS * 16 + 8 * 1024
+        src_hash = tree_source_hash()
+        traffic = TREE_DRAM_CAPTURES.get(src_hash) if (order == 8 and N == 1 << 20) else None
+        traffic_source = (f"dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-point order-8 tree_kernel launch "
+                          f"(ncu) of the kernel sources with hash {src_hash}: the g0 table, generator and set-up data; "
+                          f"the 17,440 B per evaluation of table gathers are served by L2/L1"
+                          if traffic is not None else
+                          f"no ncu capture of the kernel sources with hash {src_hash} at this workload")
         line = {
             "metric": f"integrand evals/s at order {order}", "value": value, "unit": "evals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(order, N),
             "e2e": {"value": total_points / e2e_max, "unit": "evals/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": 40, "statistic": f"best of {E2E_REPEATS} runs of the K steps",
+                    "d2h_bytes_per_step": 40, "statistic": f"median of {E2E_REPEATS} runs of the K steps",
                     "runs_evals_per_s": [total_points / t for t in e2e_runs]},
             "gpu_launches": launches,
             "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": TREE_LAUNCH_DRAM_BYTES if order == 8 and N == 1 << 20 else None,
-                         "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-point order-8 "
-                                           "tree_kernel launch (ncu, profiles/tree_kernel_order8_2e20pts_dram.md): "
-                                           "the g0 table, generator and set-up data; the 17,440 B per evaluation "
-                                           "of table gathers are served by L2/L1",
+                         "frac": achieved / peak,
+                         "executed_frac": N * tree_flops(order) / (integ_max * 1e-3 / args.steps) / peak,
+                         "traffic": traffic,
+                         "traffic_source": traffic_source,
                          "numerator": f"reference-equivalent: {reference_flops(order)} FLOP per evaluation "
                                       f"(keldy's 2^n LU pairs); the tree executes ~{tree_flops(order)}",
                          "peak_source": "FP64 FMA rate measured in this run (kb_fp64_peak, 8 independent "

@@ -210,6 +210,20 @@ int kb_model_set_interpolation(kb_model *m, int order);
 int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double *w, const double *cl,
                          const double *cg, int flags);
 
+/* keldy's ft_method "fft" (make_g0_by_fft, model.cpp:179-212, which transforms with TRIQS's
+ * make_gf_from_fourier) on the GPU: block (o1, o2) of model m (both spins) from its values
+ * gl = g^<(w_j), gg = g^>(w_j) (npts interleaved complex each) on the frequency mesh adjoint
+ * to the model's time mesh: w_j = (j - c) dw, c = (npts - 1)/2, dw = 2 pi/(npts dt), dt the
+ * time step (npts odd). Every mesh point gets the discrete transform
+ *   g(t_k) = dw/(2 pi) sum_j g(w_j) e^{-i w_j t_k},
+ * with the functions' 1/w^2 tails beyond the mesh transformed exactly: m2 = the mean of
+ * w^2 g(w) at the mesh's two ends, g - m2/(w^2 + a^2) summed discretely (a = dw sqrt(npts)),
+ * m2 e^{-a|t|}/(2a) added (the subtraction TRIQS's real-frequency transform makes).
+ * KB_FT_MIRROR also sets block (o2, o1) = -conj(g_{o1 o2}(-t)), the transform of the
+ * frequency values -conj(g_{o1 o2}(w)) keldy gives that block (model.cpp:196-199).
+ * KB_E_INVALID if a value is not finite. */
+int kb_model_set_fft(kb_model *m, int o1, int o2, const double *gl, const double *gg, int flags);
+
 /* A point of the Keldysh contour with spin and orbital: keldy's gf_index_t (model.hpp:55-78). */
 typedef struct {
   double time;
@@ -327,6 +341,14 @@ int kb_integrate_binned(kb_context *ctx, const kb_work *work, int n_work, int al
  * Orders 1..10; no learned flows. */
 int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const kb_time_bins *bins, kb_accum *acc,
                         double *bin_sums, uint64_t *bin_counts, uint64_t *dropped);
+/* The kernel method at a single frequency (integrand_g_kernel_single_omega,
+ * impurity_oneband/wick_kernel_single_omega.cpp:42-140; compute_gf_kernel_single_omega,
+ * compute_obs.hpp:119-133): per point, the terms of kb_integrate_kernel (fixed point X =
+ * work[i].f.A; first-row cofactors of s1 times (-1)^|a| det(s2_a)) summed with the weight
+ * e^{i omega t} of their vertex's time t; acc[i] += the sum of those values times the
+ * warper Jacobian, and the point counts. Orders 1..10; no learned flows. */
+int kb_integrate_kernel_single_omega(kb_context *ctx, const kb_work *work, int n_work, double omega,
+                                     kb_accum *acc);
 /* integrand_g_kernel::operator()(times, keep_u_hypercube) for count points of `order` vertex
  * times: out[count][order][2] (interleaved complex) = the point's terms summed per (vertex i,
  * Keldysh index k), the sums of the pairs keldy's wick_kernel_test compares; in_domain. */
@@ -340,14 +362,22 @@ int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_ind
  * its scratch lives in one file-scope device array of KB_NOALLOC_SCRATCH_BYTES (held by
  * every GPU that loads the library until exit) instead of per-call allocations; the
  * model tables and Sobol matrices are the caller's existing objects. Limits: at most
- * KB_NOALLOC_MAX_ITEMS work items and KB_NOALLOC_MAX_CHUNKS * 128 points per call
- * (KB_E_INVALID beyond). All calls share the array: calls that overlap on the GPU race.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress);
- * make it before any stream capture. */
+ * KB_NOALLOC_MAX_ITEMS work items and KB_NOALLOC_MAX_CHUNKS scheduling chunks per call
+ * (8,388,608 points with the default 128-point chunks; KB_E_INVALID beyond). The chunk
+ * size and CTAs per SM are the context's launch shape (kb_context_set_launch), as in
+ * kb_integrate; the tree grid is also capped at the per-CTA slots the array holds (348,
+ * more than the 296 resident CTAs of a B200). All calls share the array: calls that overlap on
+ * the GPU race. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make it before any stream capture. */
 #define KB_NOALLOC_MAX_ITEMS 64
 #define KB_NOALLOC_MAX_CHUNKS 65536
-#define KB_NOALLOC_SCRATCH_BYTES (12u << 20)
+#define KB_NOALLOC_SCRATCH_BYTES (32u << 20)
 int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc);
+
+/* Number of device allocations (cudaMalloc and stream-ordered pool allocations) the
+ * library has made in this process. A diagnostic with no keldy counterpart: it lets a
+ * caller check that kb_integrate_noalloc allocates nothing. */
+uint64_t kb_device_allocations(void);
 
 /* ------------------------------------------------------------------ plans --- */
 /* A batched integration set up once and launched many times: the work items' descriptors

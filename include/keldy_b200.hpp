@@ -661,6 +661,14 @@ class g0_model {
                                            reinterpret_cast<const double *>(cg.data()), flags));
   }
 
+  // keldy's "fft" tables of block (o1, o2) from values on the adjoint frequency mesh
+  // (kb_model_set_fft; flags KB_FT_MIRROR)
+  void set_fft(int o1, int o2, std::vector<dcomplex> const &gl, std::vector<dcomplex> const &gg, int flags) {
+    if (gl.size() != gg.size()) throw std::runtime_error("one lesser and one greater value per frequency");
+    keldy_b200::check(kb_model_set_fft(m_.get(), o1, o2, reinterpret_cast<const double *>(gl.data()),
+                                       reinterpret_cast<const double *>(gg.data()), flags));
+  }
+
   // KB_INTERP_LINEAR (keldy's) or KB_INTERP_CUBIC (an extension) between mesh points
   void set_interpolation(int order) { keldy_b200::check(kb_model_set_interpolation(m_.get(), order)); }
 
@@ -1053,6 +1061,81 @@ class compute_gf_kernel {
   uint64_t reduce_nr_points_run() const { return n_points; }
   uint64_t reduce_nr_points_in_domain() const { return n_integrand_evals_in_domain; }
   integrand_g_kernel get_integrand() const { return integrand; }
+  warpers::warper_train_t get_warper() const { return warper; }
+};
+
+// integrand_g_kernel_single_omega (wick_kernel_single_omega.cpp:42-140): the kernel
+// method's terms of a point weighted by e^{i omega t} of their vertex's time and summed.
+class integrand_g_kernel_single_omega {
+  integrand_g_kernel kernel_;
+  double omega_;
+
+ public:
+  integrand_g_kernel_single_omega(g0_keldysh_contour_t g0, gf_index_t X, double omega)
+     : kernel_(std::move(g0), X), omega_(omega) {}
+  std::pair<dcomplex, int> operator()(std::vector<double> const &times, bool keep_u_hypercube = true) const {
+    auto [terms, dom] = kernel_(times, keep_u_hypercube);
+    if (!dom) return {dcomplex(0.0), 0};
+    dcomplex r(0.0);
+    for (size_t i = 0; i < times.size(); ++i)
+      r += (terms[i][0] + terms[i][1]) * std::exp(dcomplex(0.0, omega_ * times[i]));
+    return {r, 1};
+  }
+  g0_keldysh_contour_t const &get_g0() const { return kernel_.get_g0(); }
+  gf_index_t const &get_X() const { return kernel_.get_X(); }
+  double get_omega() const { return omega_; }
+};
+
+// integrator<dcomplex, integrand_g_kernel_single_omega> + compute_gf_kernel_single_omega
+// (compute_obs.hpp:119-133): the kernel method's G at one frequency, X = (time, up, forward).
+class compute_gf_kernel_single_omega {
+  int dimension = 1;
+  dcomplex result{0.0};
+  uint64_t n_points = 0;
+  uint64_t n_integrand_evals_in_domain = 0;
+  integrand_g_kernel_single_omega integrand;
+  sobol rng_;
+
+ public:
+  warpers::warper_train_t warper{};
+
+  compute_gf_kernel_single_omega(g0_model model, double time, double omega, int order)
+     : dimension(order), integrand(g0_keldysh_contour_t{std::move(model)}, gf_index_t{time, up, forward}, omega),
+       rng_(order > 0 ? order : 1, 0) {
+    if (dimension <= 0) throw std::runtime_error("Dimension of the integration space must be > 0.");
+  }
+
+  void run(int nr_steps) {
+    if (nr_steps <= 0) return;
+    if ((uint64_t)rng_.state() + (uint64_t)nr_steps > (1ull << 31))
+      throw std::runtime_error("More sample points requested then generator can hold.");
+    auto const &chain = warper.chain();
+    kb_gf_index x = integrand.get_X().abi();
+    kb_work w{integrand.get_g0().model.handle(), rng_.handle(), chain.data(), (int)chain.size(),
+              kb_integrand{x, x, 0.0}, dimension, rng_.state() + 1, nr_steps};
+    kb_accum acc{};
+    keldy_b200::check(kb_integrate_kernel_single_omega(keldy_b200::default_context(), &w, 1, integrand.get_omega(),
+                                                       &acc));
+    rng_.discard(nr_steps);
+    result += dcomplex(acc.sum_re, acc.sum_im);
+    n_points += acc.n_points;
+    n_integrand_evals_in_domain += acc.n_in_domain;
+  }
+
+  void reset_rng(std::string rng_name, int rng_state_seed, bool do_shift = false, bool do_scramble = false,
+                 int rng_seed_shift = 0) {
+    if (rng_name == "sobol_unshifted")
+      rng_ = sobol(dimension, rng_state_seed);
+    else if (rng_name == "sobol")
+      rng_ = sobol(dimension, rng_state_seed, do_shift, do_scramble, rng_seed_shift);
+    else
+      throw std::runtime_error("rng '" + rng_name + "' has no device form; use sobol_unshifted or sobol");
+  }
+
+  dcomplex reduce_result() const { return result / double(n_points); }
+  uint64_t reduce_nr_points_run() const { return n_points; }
+  uint64_t reduce_nr_points_in_domain() const { return n_integrand_evals_in_domain; }
+  integrand_g_kernel_single_omega get_integrand() const { return integrand; }
   warpers::warper_train_t get_warper() const { return warper; }
 };
 

@@ -39,9 +39,9 @@ EXPORTS = [
     "kb_flow_sample", "kb_flow_gradient", "kb_flow_train", "kb_flow_fit", "kb_integrate_binned",
     "kb_integrate_kernel", "kb_integrand_kernel_eval", "kb_warper_table_create", "kb_warper_table_destroy",
     "kb_warper_table_from_projection", "kb_warper_table_analytic", "kb_warper_table_hybrid", "kb_warper_table_info",
-    "kb_warper_table_points", "kb_model_set_fourier", "kb_model_set_interpolation",
+    "kb_warper_table_points", "kb_model_set_fourier", "kb_model_set_interpolation", "kb_model_set_fft",
     "kb_warper_table_from_samples", "kb_warper_projection_create", "kb_warper_projection_axis",
-    "kb_warper_projection_from_integrand",
+    "kb_warper_projection_from_integrand", "kb_device_allocations", "kb_integrate_kernel_single_omega",
 ]
 FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
 FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
@@ -138,6 +138,7 @@ def load():
     L.kb_warper_table_analytic.argtypes = [_VP, C.c_int, C.POINTER(Warper), C.POINTER(_VP)]
     L.kb_warper_table_hybrid.argtypes = [_VP, C.c_int, C.POINTER(Warper), _I, C.POINTER(_VP)]
     L.kb_model_set_fourier.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D, _D, C.c_int]
+    L.kb_model_set_fft.argtypes = [_VP, C.c_int, C.c_int, _D, _D, C.c_int]
     L.kb_model_set_interpolation.argtypes = [_VP, C.c_int]
     L.kb_warper_table_info.argtypes = [_VP, _I, _I, _I]
     L.kb_warper_table_points.argtypes = [_VP, C.c_int, _D, _D]
@@ -152,11 +153,14 @@ def load():
                                                   C.c_int, C.c_int, C.c_double, C.c_int, C.POINTER(_VP)]
     L.kb_integrate_kernel.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(TimeBins), C.POINTER(Accum), _D,
                                       C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.kb_integrate_kernel_single_omega.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_double, C.POINTER(Accum)]
     L.kb_integrand_kernel_eval.argtypes = [_VP, _VP, C.POINTER(GfIndex), C.c_int, C.c_int64, _D, C.c_int, _D, _I]
     L.kb_integrate_binned.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(TimeBins), C.POINTER(Accum),
                                       _D, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.kb_fp64_peak.argtypes = [_VP, C.c_int, _D]
     L.kb_integrate_noalloc.argtypes = [_VP, C.POINTER(Work), C.c_int, C.POINTER(Accum)]
+    L.kb_device_allocations.argtypes = []
+    L.kb_device_allocations.restype = C.c_uint64
     L.kb_plan_create.argtypes = [_VP, C.POINTER(Work), C.c_int, C.c_int, C.POINTER(_VP)]
     L.kb_plan_destroy.argtypes = [_VP]
     L.kb_plan_launch.argtypes = [_VP, _VP]
@@ -504,6 +508,15 @@ class Model:
         assert cl.size == 2 * w.size and cg.size == 2 * w.size
         check(self.ctx.L.kb_model_set_fourier(self.h, int(o1), int(o2), w.size, _dp(w), _dp(cl), _dp(cg), int(flags)))
 
+    def set_fft(self, o1, o2, gl_w, gg_w, flags=0):
+        """Block (o1, o2) as keldy's "fft" tables: the discrete transform on the GPU of the
+        values on the frequency mesh adjoint to the time mesh (kb_model_set_fft; flags
+        FT_MIRROR)."""
+        gl = np.ascontiguousarray(gl_w, dtype=np.complex128).view(np.float64)
+        gg = np.ascontiguousarray(gg_w, dtype=np.complex128).view(np.float64)
+        assert gl.size == 2 * self.npts and gg.size == 2 * self.npts
+        check(self.ctx.L.kb_model_set_fft(self.h, int(o1), int(o2), _dp(gl), _dp(gg), int(flags)))
+
     def table(self, spin=0, o1=0, o2=0):
         """(lesser, greater) complex arrays of one block, read back from the device."""
         le = np.empty(self.npts, dtype=np.complex128)
@@ -700,10 +713,26 @@ def integrate_kernel(ctx, items, nbins, xmin, xmax):
              int(dropped[i])) for i, a in enumerate(acc[:n])]
 
 
+def integrate_kernel_single_omega(ctx, items, omega):
+    """kb_integrate_kernel_single_omega (keldy's kernel method at one frequency, fixed point
+    X = item["A"]): per item (sum, n_points, n_in_domain)."""
+    items = [dict(it, B=it.get("B", it["A"])) for it in items]
+    works, keep = _works(items)
+    n = len(items)
+    acc = (Accum * max(1, n))()
+    check(ctx.L.kb_integrate_kernel_single_omega(ctx.h, works, n, float(omega), acc))
+    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain) for a in acc[:n]]
+
+
+def device_allocations():
+    """kb_device_allocations: device allocations the library has made in this process."""
+    return int(load().kb_device_allocations())
+
+
 def integrate_noalloc(ctx, items):
     """kb_integrate_noalloc: as integrate(algo=ALGO_AUTO), for callers that cannot allocate
     device memory; its scratch is a fixed device array inside the library (at most 64
-    items and 8,388,608 points per call)."""
+    items and 65,536 scheduling chunks per call: 8,388,608 points with 128-point chunks)."""
     works, keep = _works(items)
     acc = (Accum * max(1, len(items)))()
     check(ctx.L.kb_integrate_noalloc(ctx.h, works, len(items), acc))

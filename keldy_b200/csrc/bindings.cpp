@@ -257,6 +257,11 @@ PYBIND11_MODULE(_keldy, m) {
           },
           py::arg("o1"), py::arg("o2"), py::arg("w"), py::arg("cl"), py::arg("cg"), py::arg("flags"))
       .def(
+          "set_fft",
+          [](g0_model &g, int o1, int o2, py::array_t<std::complex<double>> gl, py::array_t<std::complex<double>> gg,
+             int flags) { g.set_fft(o1, o2, to_cvec(gl), to_cvec(gg), flags); },
+          py::arg("o1"), py::arg("o2"), py::arg("gl"), py::arg("gg"), py::arg("flags") = 0)
+      .def(
           "get_table",
           [](g0_model const &g, int spin, int o1, int o2) {
             auto t = g.get_table(spin, o1, o2);
@@ -365,4 +370,20 @@ PYBIND11_MODULE(_keldy, m) {
       .def("reduce_nr_points_in_domain", &compute_gf_kernel::reduce_nr_points_in_domain)
       .def("get_integrand", &compute_gf_kernel::get_integrand)
       .def("get_warper", &compute_gf_kernel::get_warper);
+  py::class_<integrand_g_kernel_single_omega>(m, "IntegrandGKernelSingleOmega")
+      .def(py::init<g0_keldysh_contour_t, gf_index_t, double>(), py::arg("g0"), py::arg("g_idx_X"), py::arg("omega"))
+      .def("__call__", &integrand_g_kernel_single_omega::operator(), py::arg("times"),
+           py::arg("keep_u_hypercube") = true);
+  py::class_<compute_gf_kernel_single_omega>(m, "ComputeGfKernelSingleOmega")
+      .def(py::init<g0_model, double, double, int>(), py::arg("model"), py::arg("time"), py::arg("omega"),
+           py::arg("order"))
+      .def_readwrite("warper", &compute_gf_kernel_single_omega::warper)
+      .def("run", &compute_gf_kernel_single_omega::run, py::arg("nr_steps"), py::call_guard<py::gil_scoped_release>())
+      .def("reset_rng", &compute_gf_kernel_single_omega::reset_rng, py::arg("rng_name"), py::arg("rng_state_seed"),
+           py::arg("do_shift") = false, py::arg("do_scramble") = false, py::arg("rng_seed_shift") = 0)
+      .def("reduce_result", &compute_gf_kernel_single_omega::reduce_result)
+      .def("reduce_nr_points_run", &compute_gf_kernel_single_omega::reduce_nr_points_run)
+      .def("reduce_nr_points_in_domain", &compute_gf_kernel_single_omega::reduce_nr_points_in_domain)
+      .def("get_integrand", &compute_gf_kernel_single_omega::get_integrand)
+      .def("get_warper", &compute_gf_kernel_single_omega::get_warper);
 }

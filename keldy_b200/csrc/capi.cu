@@ -36,6 +36,8 @@ const char *kb_last_error(void) { return g_last_error.c_str(); }
 
 int kb_version(void) { return 100; }
 
+uint64_t kb_device_allocations(void) { return device_allocations().load(); }
+
 int kb_context_create(int device, kb_context **out) {
   KB_CHECK(out, "kb_context_create: out is NULL");
   int n = 0;
@@ -63,7 +65,7 @@ int kb_context_create(int device, kb_context **out) {
   // Every upload goes through the library's stream: it does not synchronise with the
   // legacy default stream, and a plain cudaMemcpy from pageable memory may return before
   // its data has landed.
-  e = cudaMalloc(&ctx->d_err, sizeof(int));
+  e = device_malloc(&ctx->d_err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
@@ -134,8 +136,8 @@ int kb_sobol_create(kb_context *ctx, int dim, int log_max_points, int do_shift, 
   s->m = log_max_points;
   std::lock_guard<std::mutex> lk(ctx->mu); // the upload uses the context's stream
   cudaSetDevice(ctx->device);
-  cudaError_t e = cudaMalloc(&s->d_Csr, Csr.size() * sizeof(uint32_t));
-  if (e == cudaSuccess) e = cudaMalloc(&s->d_shfr, shfr.size() * sizeof(uint32_t));
+  cudaError_t e = device_malloc(&s->d_Csr, Csr.size() * sizeof(uint32_t));
+  if (e == cudaSuccess) e = device_malloc(&s->d_shfr, shfr.size() * sizeof(uint32_t));
   if (e == cudaSuccess) e = cudaMemcpyAsync(s->d_Csr, Csr.data(), Csr.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->d_shfr, shfr.data(), shfr.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
@@ -389,7 +391,7 @@ static int set_table(kb_model *m, int spin, int o1, int o2, const double *lesser
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   const size_t n = (size_t)m->npts;
-  if (!m->tab[spin][o1][o2]) KB_CUDA(cudaMalloc(&m->tab[spin][o1][o2], n * 2 * sizeof(double2)));
+  if (!m->tab[spin][o1][o2]) KB_CUDA(device_malloc(&m->tab[spin][o1][o2], n * 2 * sizeof(double2)));
   double2 *dst = m->tab[spin][o1][o2];
   // interleave lesser/greater per mesh point
   KB_CUDA(cudaMemcpy2DAsync(dst, 2 * sizeof(double2), lesser, sizeof(double2), sizeof(double2), n, kind,
@@ -499,7 +501,7 @@ int kb_models_set_flatband(int n, kb_model *const *models, const double *params)
   std::vector<double2 *> tabs((size_t)n);
   for (int i = 0; i < n; ++i) {
     kb_model *m = models[i];
-    if (!m->tab[0][0][0]) KB_CUDA(cudaMalloc(&m->tab[0][0][0], (size_t)npts * 2 * sizeof(double2)));
+    if (!m->tab[0][0][0]) KB_CUDA(device_malloc(&m->tab[0][0][0], (size_t)npts * 2 * sizeof(double2)));
     tabs[(size_t)i] = m->tab[0][0][0];
   }
   DevBuf dpar, dtab, dx, dw, dmax;
@@ -552,8 +554,8 @@ int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double 
   cudaStream_t st = ctx->stream;
   const size_t n = (size_t)m->npts;
   const bool mirror = (flags & KB_FT_MIRROR) != 0;
-  if (!m->tab[0][o1][o2]) KB_CUDA(cudaMalloc(&m->tab[0][o1][o2], n * 2 * sizeof(double2)));
-  if (mirror && !m->tab[0][o2][o1]) KB_CUDA(cudaMalloc(&m->tab[0][o2][o1], n * 2 * sizeof(double2)));
+  if (!m->tab[0][o1][o2]) KB_CUDA(device_malloc(&m->tab[0][o1][o2], n * 2 * sizeof(double2)));
+  if (mirror && !m->tab[0][o2][o1]) KB_CUDA(device_malloc(&m->tab[0][o2][o1], n * 2 * sizeof(double2)));
   DevBuf dw, dl, dg, dbad, dmax;
   KB_CUDA(dw.alloc((size_t)n_nodes * sizeof(double), st));
   KB_CUDA(dl.alloc((size_t)n_nodes * sizeof(double2), st));
@@ -577,6 +579,57 @@ int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double 
   // spin down uses the spin-up blocks (model.cpp:209-211): drop any spin-down copy
   const int blocks[2][2] = {{o1, o2}, {o2, o1}};
   for (int k = 0; k < (mirror ? 2 : 1); ++k) {
+    const int a = blocks[k][0], b = blocks[k][1];
+    cudaFree(m->tab[1][a][b]);
+    m->tab[1][a][b] = nullptr;
+    m->hash[0][a][b] = 0;
+    m->hash[1][a][b] = 0;
+  }
+  m->tabmax = std::max(m->tabmax, mx);
+  return KB_OK;
+}
+
+int kb_model_set_fft(kb_model *m, int o1, int o2, const double *gl, const double *gg, int flags) {
+  KB_CHECK(m && gl && gg, "kb_model_set_fft: null argument");
+  KB_CHECK(o1 >= 0 && o1 < 2 && o2 >= 0 && o2 < 2, "orbital index out of range");
+  KB_CHECK(m->npts % 2 == 1 && m->npts >= 3, "the fft method needs an odd number of mesh points (t = 0 on the mesh)");
+  KB_CHECK(!(flags & KB_FT_MIRROR) || o1 != o2, "KB_FT_MIRROR needs an off-diagonal block");
+  KB_CHECK((flags & ~KB_FT_MIRROR) == 0, "kb_model_set_fft takes only the KB_FT_MIRROR flag");
+  const size_t n = (size_t)m->npts;
+  for (size_t k = 0; k < 2 * n; ++k)
+    KB_CHECK(std::isfinite(gl[k]) && std::isfinite(gg[k]), "frequency values must be finite");
+  kb_context *ctx = m->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const bool mirror = (flags & KB_FT_MIRROR) != 0;
+  if (!m->tab[0][o1][o2]) KB_CUDA(device_malloc(&m->tab[0][o1][o2], n * 2 * sizeof(double2)));
+  if (mirror && !m->tab[0][o2][o1]) KB_CUDA(device_malloc(&m->tab[0][o2][o1], n * 2 * sizeof(double2)));
+  DevBuf dl, dg, dbad, dmax;
+  KB_CUDA(dl.alloc(n * sizeof(double2), st));
+  KB_CUDA(dg.alloc(n * sizeof(double2), st));
+  KB_CUDA(dbad.alloc(sizeof(int), st));
+  KB_CUDA(dmax.alloc(2 * sizeof(double), st));
+  KB_CUDA(cudaMemcpyAsync(dl.p, gl, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dg.p, gg, n * sizeof(double2), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemsetAsync(dbad.p, 0, sizeof(int), st));
+  // the 1/w^2 tail coefficient of each function: the mean of w^2 g(w) at the mesh's two ends
+  const double dt = 2.0 * m->tmax / (double)(n - 1), wmax = M_PI * (double)(n - 1) / ((double)n * dt);
+  const double w2 = wmax * wmax;
+  const double2 ml = make_double2(0.5 * w2 * (gl[0] + gl[2 * n - 2]), 0.5 * w2 * (gl[1] + gl[2 * n - 1]));
+  const double2 mg = make_double2(0.5 * w2 * (gg[0] + gg[2 * n - 2]), 0.5 * w2 * (gg[1] + gg[2 * n - 1]));
+  KB_CUDA(launch_dft_table(dl.as<double2>(), dg.as<double2>(), ml, mg, m->tab[0][o1][o2], m->npts, m->tmax,
+                           dbad.as<int>(), st));
+  KB_CUDA(launch_table_max(m->tab[0][o1][o2], m->npts, dmax.as<double>(), st));
+  if (mirror) KB_CUDA(launch_mirror_block(m->tab[0][o1][o2], m->tab[0][o2][o1], m->npts, st));
+  int bad = 0;
+  double mx = 0.0;
+  KB_CUDA(cudaMemcpyAsync(&bad, dbad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(&mx, dmax.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (bad) return fail(KB_E_INVALID, "g0 table contains non-finite values");
+  const int blocks[2][2] = {{o1, o2}, {o2, o1}};
+  for (int k = 0; k < (mirror ? 2 : 1); ++k) { // spin down uses the spin-up blocks (model.cpp:209-211)
     const int a = blocks[k][0], b = blocks[k][1];
     cudaFree(m->tab[1][a][b]);
     m->tab[1][a][b] = nullptr;
@@ -820,6 +873,11 @@ int kb_integrand_eval_no_det(kb_context *ctx, const kb_model *m, const kb_integr
 } // extern "C"
 
 namespace kb {
+std::atomic<unsigned long long> &device_allocations() {
+  static std::atomic<unsigned long long> n{0};
+  return n;
+}
+
 cudaMemPool_t kb_pool() {
   constexpr int MAX_DEVICES = 64;
   static std::mutex mu;
@@ -1046,14 +1104,15 @@ int kb_integrate_binned(kb_context *ctx, const kb_work *work, int n_work, int al
   return integrate_impl(ctx, work, n_work, algo, acc, &tb);
 }
 
-int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const kb_time_bins *bins, kb_accum *acc,
-                        double *bin_sums, uint64_t *bin_counts, uint64_t *dropped) {
-  KB_CHECK(ctx && bins && (n_work == 0 || (work && acc && bin_sums && bin_counts && dropped)),
-           "kb_integrate_kernel: null argument");
-  KB_CHECK(bins->nbins >= 1 && bins->nbins <= 4096, "the number of time bins must be in [1, 4096]");
-  if (!(bins->xmin < bins->xmax))
-    return fail(KB_E_INVALID, "Boundaries of binning range are in wrong order (" + std::to_string(bins->xmin) +
-                                  " >= " + std::to_string(bins->xmax) + ")");
+} // extern "C"
+
+namespace {
+// The kernel method's integration: binned by (vertex time, Keldysh index) (bins given,
+// compute_gf_kernel) or summed with the weight e^{i omega t} of each term's vertex (omega
+// given, compute_gf_kernel_single_omega).
+int integrate_kernel_impl(kb_context *ctx, const kb_work *work, int n_work, const kb_time_bins *bins,
+                          const double *omega, kb_accum *acc, double *bin_sums, uint64_t *bin_counts,
+                          uint64_t *dropped) {
   if (n_work == 0) return KB_OK;
   std::vector<ItemDev> items((size_t)n_work);
   std::vector<long long> offs(1, 0);
@@ -1075,19 +1134,21 @@ int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const 
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  const size_t nb = 2 * (size_t)bins->nbins;
+  const size_t nb = bins ? 2 * (size_t)bins->nbins : 0;
   DevBuf ditems, doff, dcnt, dpart, dacc, dbs, dbc, dbd, dos, doc, dod;
   KB_CUDA(ditems.alloc(items.size() * sizeof(ItemDev), st));
   KB_CUDA(doff.alloc(offs.size() * sizeof(long long), st));
   KB_CUDA(dcnt.alloc(sizeof(int), st));
   KB_CUDA(dpart.alloc((size_t)nchunks * sizeof(ChunkPartial), st));
   KB_CUDA(dacc.alloc(items.size() * sizeof(kb_accum), st));
-  KB_CUDA(dbs.alloc((size_t)nchunks * nb * sizeof(double2), st));
-  KB_CUDA(dbc.alloc((size_t)nchunks * nb * sizeof(unsigned), st));
-  KB_CUDA(dbd.alloc((size_t)nchunks * sizeof(unsigned), st));
-  KB_CUDA(dos.alloc(items.size() * nb * sizeof(double2), st));
-  KB_CUDA(doc.alloc(items.size() * nb * sizeof(unsigned long long), st));
-  KB_CUDA(dod.alloc(items.size() * sizeof(unsigned long long), st));
+  if (nb) {
+    KB_CUDA(dbs.alloc((size_t)nchunks * nb * sizeof(double2), st));
+    KB_CUDA(dbc.alloc((size_t)nchunks * nb * sizeof(unsigned), st));
+    KB_CUDA(dbd.alloc((size_t)nchunks * sizeof(unsigned), st));
+    KB_CUDA(dos.alloc(items.size() * nb * sizeof(double2), st));
+    KB_CUDA(doc.alloc(items.size() * nb * sizeof(unsigned long long), st));
+    KB_CUDA(dod.alloc(items.size() * sizeof(unsigned long long), st));
+  }
   KB_CUDA(cudaMemcpyAsync(ditems.p, items.data(), items.size() * sizeof(ItemDev), cudaMemcpyHostToDevice, st));
   KB_CUDA(cudaMemcpyAsync(doff.p, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice, st));
   KB_CUDA(cudaMemsetAsync(dcnt.p, 0, sizeof(int), st));
@@ -1102,29 +1163,37 @@ int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const 
   L.chunk_counter = dcnt.as<int>();
   L.mode = IN_SOBOL;
   L.partials = dpart.as<ChunkPartial>();
-  L.nbins = bins->nbins;
-  L.bin_cols = 2;
-  L.bin_xmin = bins->xmin;
-  L.bin_xmax = bins->xmax;
-  L.bin_size = (bins->xmax - bins->xmin) / bins->nbins;
-  L.bin_sums = dbs.as<double2>();
-  L.bin_counts = dbc.as<unsigned>();
-  L.bin_dropped = dbd.as<unsigned>();
+  if (bins) {
+    L.nbins = bins->nbins;
+    L.bin_cols = 2;
+    L.bin_xmin = bins->xmin;
+    L.bin_xmax = bins->xmax;
+    L.bin_size = (bins->xmax - bins->xmin) / bins->nbins;
+    L.bin_sums = dbs.as<double2>();
+    L.bin_counts = dbc.as<unsigned>();
+    L.bin_dropped = dbd.as<unsigned>();
+  } else {
+    L.km_fourier = 1;
+    L.km_omega = *omega;
+  }
   L.err = ctx->d_err;
   if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
   KB_CUDA(launch_kernel_method(L, (int)std::min<long long>(nchunks, (long long)ctx->sm_count * 4), st));
   if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[1], st));
   KB_CUDA(launch_reduce(L, dacc.as<kb_accum>(), st));
-  KB_CUDA(launch_reduce_bins(L, dos.as<double2>(), doc.as<unsigned long long>(), dod.as<unsigned long long>(), st));
+  if (nb)
+    KB_CUDA(launch_reduce_bins(L, dos.as<double2>(), doc.as<unsigned long long>(), dod.as<unsigned long long>(), st));
   if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[2], st));
-  ctx->last_launches = 3;
+  ctx->last_launches = nb ? 3 : 2;
   std::vector<kb_accum> part(items.size());
   std::vector<double> hbs(items.size() * nb * 2);
   std::vector<unsigned long long> hbc(items.size() * nb), hbd(items.size());
   KB_CUDA(cudaMemcpyAsync(part.data(), dacc.p, part.size() * sizeof(kb_accum), cudaMemcpyDeviceToHost, st));
-  KB_CUDA(cudaMemcpyAsync(hbs.data(), dos.p, hbs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
-  KB_CUDA(cudaMemcpyAsync(hbc.data(), doc.p, hbc.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
-  KB_CUDA(cudaMemcpyAsync(hbd.data(), dod.p, hbd.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  if (nb) {
+    KB_CUDA(cudaMemcpyAsync(hbs.data(), dos.p, hbs.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaMemcpyAsync(hbc.data(), doc.p, hbc.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaMemcpyAsync(hbd.data(), dod.p, hbd.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+  }
   int err = 0;
   KB_CUDA(cudaMemcpyAsync(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   KB_CUDA(cudaStreamSynchronize(st));
@@ -1142,6 +1211,7 @@ int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const 
     acc[w].sum_im += part[(size_t)w].sum_im;
     acc[w].n_points += part[(size_t)w].n_points;
     acc[w].n_in_domain += part[(size_t)w].n_in_domain;
+    if (!nb) continue;
     for (size_t b = 0; b < nb; ++b) {
       bin_sums[2 * ((size_t)w * nb + b)] += hbs[2 * ((size_t)w * nb + b)];
       bin_sums[2 * ((size_t)w * nb + b) + 1] += hbs[2 * ((size_t)w * nb + b) + 1];
@@ -1150,6 +1220,27 @@ int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const 
     dropped[w] += hbd[(size_t)w];
   }
   return KB_OK;
+}
+} // namespace
+
+extern "C" {
+
+int kb_integrate_kernel(kb_context *ctx, const kb_work *work, int n_work, const kb_time_bins *bins, kb_accum *acc,
+                        double *bin_sums, uint64_t *bin_counts, uint64_t *dropped) {
+  KB_CHECK(ctx && bins && (n_work == 0 || (work && acc && bin_sums && bin_counts && dropped)),
+           "kb_integrate_kernel: null argument");
+  KB_CHECK(bins->nbins >= 1 && bins->nbins <= 4096, "the number of time bins must be in [1, 4096]");
+  if (!(bins->xmin < bins->xmax))
+    return fail(KB_E_INVALID, "Boundaries of binning range are in wrong order (" + std::to_string(bins->xmin) +
+                                  " >= " + std::to_string(bins->xmax) + ")");
+  return integrate_kernel_impl(ctx, work, n_work, bins, nullptr, acc, bin_sums, bin_counts, dropped);
+}
+
+int kb_integrate_kernel_single_omega(kb_context *ctx, const kb_work *work, int n_work, double omega,
+                                     kb_accum *acc) {
+  KB_CHECK(ctx && (n_work == 0 || (work && acc)), "kb_integrate_kernel_single_omega: null argument");
+  KB_CHECK(std::isfinite(omega), "omega must be finite");
+  return integrate_kernel_impl(ctx, work, n_work, nullptr, &omega, acc, nullptr, nullptr, nullptr);
 }
 
 int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_index *X, int order, int64_t count,
@@ -1381,7 +1472,7 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
     f.order = w.order;
     f.gi = grp[(size_t)i];
     f.pos = -1;
-    cudaError_t e = cudaMalloc(&f.buf, (size_t)f.n * (size_t)(f.order + 1) * sizeof(double));
+    cudaError_t e = device_malloc(&f.buf, (size_t)f.n * (size_t)(f.order + 1) * sizeof(double));
     if (e != cudaSuccess) {
       plan_free(p);
       return fail(KB_E_NOMEM, std::string("kb_plan_create: ") + cudaGetErrorString(e));
@@ -1414,12 +1505,12 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
     }
     g.grid = (int)std::min<long long>(g.n_chunks, gi == 0 ? (long long)ctx->sm_count * ctx->ctas_per_sm
                                                           : (long long)ctx->sm_count * 4);
-    cudaError_t e = cudaMalloc(&g.d_items, sizeof(ItemDev) * g.n_items);
-    if (e == cudaSuccess) e = cudaMalloc(&g.d_offs, sizeof(long long) * offs.size());
-    if (e == cudaSuccess) e = cudaMalloc(&g.d_cnt, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&g.d_part, sizeof(ChunkPartial) * (size_t)g.n_chunks);
-    if (e == cudaSuccess && gi == 0) e = cudaMalloc(&g.d_pts, sizeof(double) * PTS_SLOT * (size_t)g.grid);
-    if (e == cudaSuccess) e = cudaMalloc(&g.d_acc, sizeof(kb_accum) * g.n_items);
+    cudaError_t e = device_malloc(&g.d_items, sizeof(ItemDev) * g.n_items);
+    if (e == cudaSuccess) e = device_malloc(&g.d_offs, sizeof(long long) * offs.size());
+    if (e == cudaSuccess) e = device_malloc(&g.d_cnt, sizeof(int));
+    if (e == cudaSuccess) e = device_malloc(&g.d_part, sizeof(ChunkPartial) * (size_t)g.n_chunks);
+    if (e == cudaSuccess && gi == 0) e = device_malloc(&g.d_pts, sizeof(double) * PTS_SLOT * (size_t)g.grid);
+    if (e == cudaSuccess) e = device_malloc(&g.d_acc, sizeof(kb_accum) * g.n_items);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(g.d_items, g.items.data(), sizeof(ItemDev) * g.n_items, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess)
@@ -1620,7 +1711,10 @@ constexpr size_t NOALLOC_PART_OFF = (NOALLOC_CNT_OFF + sizeof(int) + 255) / 256 
 constexpr size_t NOALLOC_PTS_OFF =
     (NOALLOC_PART_OFF + sizeof(ChunkPartial) * (size_t)KB_NOALLOC_MAX_CHUNKS + 255) / 256 * 256;
 constexpr size_t NOALLOC_PTS_SLOTS = (KB_NOALLOC_SCRATCH_BYTES - NOALLOC_PTS_OFF) / (PTS_SLOT * sizeof(double));
-static_assert(NOALLOC_PTS_SLOTS >= 296, "scratch too small for one set-up slot per resident CTA");
+// one set-up slot per resident tree CTA of a 148-SM B200 at the most CTAs per SM the
+// launch shape allows; a device with more SMs runs the tree with a grid capped at the slots
+constexpr size_t NOALLOC_B200_TREE_CTAS = 148 * 2;
+static_assert(NOALLOC_PTS_SLOTS >= NOALLOC_B200_TREE_CTAS, "scratch too small for one set-up slot per resident CTA");
 
 static __device__ __align__(256) unsigned char kb_noalloc_scratch[KB_NOALLOC_SCRATCH_BYTES];
 
@@ -1674,10 +1768,14 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     it.k_first = w.k_first;
     it.n_points = w.n_points;
     group_of[i] = it.spin_symmetric ? 0 : 1;
-    chunks_total += (w.n_points + CHUNK_POINTS - 1) / CHUNK_POINTS;
+    // the same scheduling chunks as kb_integrate (the context's launch shape of the order),
+    // so that the sums are added in the same order
+    it.chunk_points = ctx->chunk_points[w.order];
+    chunks_total += (w.n_points + it.chunk_points - 1) / it.chunk_points;
   }
   if (chunks_total > KB_NOALLOC_MAX_CHUNKS)
-    return fail(KB_E_INVALID, "kb_integrate_noalloc: more than KB_NOALLOC_MAX_CHUNKS*128 (8,388,608) points in one call");
+    return fail(KB_E_INVALID, "kb_integrate_noalloc: more than KB_NOALLOC_MAX_CHUNKS (65,536) scheduling chunks in "
+                              "one call (8,388,608 points with the default 128-point chunks)");
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   unsigned char *base = nullptr;
@@ -1713,7 +1811,7 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     offs[0] = 0;
     for (int j = 0; j < nids[g]; ++j) {
       sorted[j] = items[ids[g][j]];
-      offs[j + 1] = offs[j] + (sorted[j].n_points + CHUNK_POINTS - 1) / CHUNK_POINTS;
+      offs[j + 1] = offs[j] + (sorted[j].n_points + sorted[j].chunk_points - 1) / sorted[j].chunk_points;
     }
     KB_CUDA(cudaMemcpyAsync(d_items, sorted, sizeof(ItemDev) * nids[g], cudaMemcpyHostToDevice, stream));
     KB_CUDA(cudaMemcpyAsync(d_offs, offs, sizeof(long long) * (nids[g] + 1), cudaMemcpyHostToDevice, stream));
@@ -1731,8 +1829,10 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     L.pts = d_pts;
     L.err = ctx->d_err;
     if (g == 0) {
+      // the tree grid of kb_integrate, capped at the set-up slots the array holds
       const long long slots = (long long)NOALLOC_PTS_SLOTS;
-      KB_CUDA(launch_tree(L, (int)std::min<long long>(std::min<long long>(L.n_chunks, ctx->tree_grid), slots), stream));
+      const long long tgrid = std::min<long long>(L.n_chunks, (long long)ctx->sm_count * ctx->ctas_per_sm);
+      KB_CUDA(launch_tree(L, (int)std::min<long long>(tgrid, slots), stream));
       KB_CUDA(launch_fallback(L, ctx->sm_count * 4, stream));
     } else {
       KB_CUDA(launch_direct(L, (int)std::min<long long>(L.n_chunks, ctx->sm_count * 4), stream));

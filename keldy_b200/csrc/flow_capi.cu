@@ -77,10 +77,10 @@ int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out) {
   f->dim = dim;
   flow_layout(dim, f->layout);
   const size_t nb = (size_t)FLOW_NPARAM * sizeof(float);
-  cudaError_t e = cudaMalloc(&f->master, nb);
-  if (e == cudaSuccess) e = cudaMalloc(&f->adam_m, nb);
-  if (e == cudaSuccess) e = cudaMalloc(&f->adam_v, nb);
-  if (e == cudaSuccess) e = cudaMalloc(&f->img, (size_t)FLOW_NPARAM * sizeof(uint16_t));
+  cudaError_t e = device_malloc(&f->master, nb);
+  if (e == cudaSuccess) e = device_malloc(&f->adam_m, nb);
+  if (e == cudaSuccess) e = device_malloc(&f->adam_v, nb);
+  if (e == cudaSuccess) e = device_malloc(&f->img, (size_t)FLOW_NPARAM * sizeof(uint16_t));
   // on the library's stream, which does not synchronise with the legacy default stream
   if (e == cudaSuccess) e = cudaMemcpyAsync(f->master, inr.data(), nb, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_m, 0, nb, ctx->stream);

@@ -224,6 +224,67 @@ __global__ void fourier_kernel(const double *w, const double2 *cl, const double2
   }
 }
 
+// keldy's ft_method "fft" (make_g0_by_fft, model.cpp:179-212): TRIQS's make_gf_from_fourier
+// of frequency values on the mesh adjoint to the time mesh. With L mesh points (odd),
+// c = (L-1)/2, t_k = (k-c) dt and w_j = (j-c) dw, dw = 2 pi/(L dt), the discrete transform
+//   g(t_k) = dw/(2 pi) sum_j G_j e^{-i w_j t_k} = dw/(2 pi) sum_j G_j e^{-2 pi i (j-c)(k-c)/L}
+// summed directly, one thread per k, lesser and greater together. Within a tile of DFT_TILE
+// frequencies the twiddle advances by the factor e^{-2 pi i (k-c)/L}; each tile starts from
+// the exact twiddle of the integer phase (j-c)(k-c) mod L, so rounding does not build up.
+// The 1/w^2 tails beyond the mesh: m2/(w^2 + a^2) (a = dw sqrt(L), m2 per function) is
+// subtracted from G before the sum and its exact transform m2 e^{-a|t|}/(2a) added after.
+constexpr int DFT_TILE = 256;
+
+__device__ __forceinline__ double2 twiddle(long long phase, long long L) {
+  long long r = phase % L;
+  if (r < 0) r += L;
+  double s, c;
+  sincospi(-2.0 * (double)r / (double)L, &s, &c);
+  return c2(c, s);
+}
+
+struct DftTail {
+  double2 ml, mg; // 1/w^2 coefficients of the lesser and greater functions
+  double a;
+};
+
+__global__ void dft_kernel(const double2 *Gl, const double2 *Gg, double2 *tab, int L, double dw, double dt,
+                           DftTail tail, int *bad) {
+  __shared__ double2 sl[DFT_TILE], sg[DFT_TILE];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long c = (L - 1) / 2;
+  const long long kc = (long long)k - c;
+  const double2 step = twiddle(kc, L);
+  double2 al = c2(0.0, 0.0), ag = c2(0.0, 0.0);
+  for (int base = 0; base < L; base += DFT_TILE) {
+    const int nt = min(DFT_TILE, L - base);
+    __syncthreads();
+    for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+      const double w = (double)((long long)(base + j) - c) * dw;
+      const double lz = 1.0 / (w * w + tail.a * tail.a);
+      sl[j] = c2(Gl[base + j].x - tail.ml.x * lz, Gl[base + j].y - tail.ml.y * lz);
+      sg[j] = c2(Gg[base + j].x - tail.mg.x * lz, Gg[base + j].y - tail.mg.y * lz);
+    }
+    __syncthreads();
+    if (k < L) {
+      double2 w = twiddle(((long long)base - c) * kc, L);
+      for (int j = 0; j < nt; ++j) {
+        al = c2(fma(sl[j].x, w.x, fma(-sl[j].y, w.y, al.x)), fma(sl[j].x, w.y, fma(sl[j].y, w.x, al.y)));
+        ag = c2(fma(sg[j].x, w.x, fma(-sg[j].y, w.y, ag.x)), fma(sg[j].x, w.y, fma(sg[j].y, w.x, ag.y)));
+        w = cmul(w, step);
+      }
+    }
+  }
+  if (k >= L) return;
+  const double scale = dw / (2.0 * PI);
+  const double e = exp(-tail.a * fabs((double)kc * dt)) / (2.0 * tail.a);
+  al = c2(al.x * scale + tail.ml.x * e, al.y * scale + tail.ml.y * e);
+  ag = c2(ag.x * scale + tail.mg.x * e, ag.y * scale + tail.mg.y * e);
+  if (!isfinite(al.x) || !isfinite(al.y) || !isfinite(ag.x) || !isfinite(ag.y)) atomicOr(bad, 1);
+  tab[2 * k] = al;
+  tab[2 * k + 1] = ag;
+}
+
 // Block (o2, o1) from block (o1, o2): g_{o2 o1}(t) = -conj(g_{o1 o2}(-t)) (model.cpp:311-313).
 __global__ void mirror_block_kernel(const double2 *src, double2 *dst, int npts) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
@@ -240,6 +301,15 @@ cudaError_t launch_fourier_table(const double *w, const double2 *cl, const doubl
                                  int npts, double tmax, int symmetric, int *bad, cudaStream_t st) {
   const int count = symmetric ? npts - npts / 2 : npts;
   fourier_kernel<<<(count + 127) / 128, 128, 0, st>>>(w, cl, cg, n_nodes, tab, npts, tmax, symmetric, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dft_table(const double2 *gl, const double2 *gg, double2 ml, double2 mg, double2 *tab, int npts,
+                             double tmax, int *bad, cudaStream_t st) {
+  const double dt = (tmax - (-tmax)) / (double)(npts - 1);
+  const double dw = 2.0 * PI / ((double)npts * dt);
+  DftTail tail{ml, mg, dw * sqrt((double)npts)};
+  dft_kernel<<<(npts + 127) / 128, 128, 0, st>>>(gl, gg, tab, npts, dw, dt, tail, bad);
   return cudaGetLastError();
 }
 

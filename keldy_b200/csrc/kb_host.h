@@ -6,6 +6,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -25,6 +26,14 @@ int fail(int code, const std::string &msg);
 constexpr unsigned long long KB_POOL_KEEP_BYTES = 256ull << 20;
 cudaMemPool_t kb_pool();
 
+// Every device allocation of the library goes through device_malloc or DevBuf::alloc,
+// which count it (kb_device_allocations reads the count).
+std::atomic<unsigned long long> &device_allocations();
+template <typename T> cudaError_t device_malloc(T **p, size_t bytes) {
+  device_allocations().fetch_add(1, std::memory_order_relaxed);
+  return cudaMalloc(reinterpret_cast<void **>(p), bytes);
+}
+
 // Stream-ordered device buffer released at scope exit (on the same stream).
 struct DevBuf {
   void *p = nullptr;
@@ -34,6 +43,7 @@ struct DevBuf {
   DevBuf &operator=(const DevBuf &) = delete;
   cudaError_t alloc(size_t bytes, cudaStream_t s) {
     st = s;
+    device_allocations().fetch_add(1, std::memory_order_relaxed);
     return cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, kb_pool(), s);
   }
   ~DevBuf() {

@@ -23,11 +23,28 @@ struct ChunkPartial {
 };
 
 constexpr int CHUNK_POINTS = 128; // points per scheduling chunk (<= 128: two 64-bit masks)
-// Per-CTA slot of the tree kernel's chunk set-up: coordinates [MAX_ORDER][CHUNK_POINTS],
-// then the Jacobians and the domain flags of the chunk's points; with time bins also each
-// point's bin code (2 bin + 1 when its value is added, 2 bin when only counted, -1 when
-// dropped) and its f*J (re, im).
-constexpr int PTS_SLOT = CHUNK_POINTS * (MAX_ORDER + 5);
+// Per-CTA slot of the tree kernel in global memory (L2-resident): the chunk's set-up,
+// PTS_ROWS doubles (coordinates [MAX_ORDER][CHUNK_POINTS], then the Jacobians and the
+// domain flags of the chunk's points; with time bins also each point's bin code (2 bin + 1
+// when its value is added, 2 bin when only counted, -1 when dropped) and its f*J (re,
+// im)), then G_STAGE complex entries of staged G matrices (a G-batch, tree_gbatch).
+constexpr int PTS_ROWS = CHUNK_POINTS * (MAX_ORDER + 5);
+constexpr int G_STAGE = 4096;
+constexpr int PTS_SLOT = PTS_ROWS + 2 * G_STAGE;
+static_assert(PTS_ROWS % 2 == 0 && PTS_SLOT % 2 == 0, "staged G on 16-byte boundaries");
+
+// Points per G-batch of the tree kernel at order N: their (2N+1)^2 matrices G fit the
+// staging area, their coordinates the kernel's 256-entry shared array, and the count is a
+// multiple of the sub-batch size tree_points_per_chunk(N).
+__host__ __device__ inline int tree_gbatch(int N) {
+  const int P = tree_points_per_chunk(N);
+  const int M = 2 * N + 1;
+  int g = CHUNK_POINTS;
+  if (N > 0 && 256 / N < g) g = 256 / N;
+  if (G_STAGE / (M * M) < g) g = G_STAGE / (M * M);
+  g -= g % P;
+  return g > 0 ? g : P;
+}
 
 struct Launch {
   const ItemDev *items; // device
@@ -46,7 +63,7 @@ struct Launch {
   int *out_dom;
   double *out_scale;
   int *out_flag;        // tree: 1 = point needs the pivoted-LU kernel
-  // tree kernel: gridDim.x * PTS_SLOT doubles of set-up scratch
+  // tree kernel: gridDim.x * PTS_SLOT doubles of set-up and staging scratch
   double *pts;
   // IN_SOBOL
   ChunkPartial *partials; // [n_chunks]
@@ -64,6 +81,11 @@ struct Launch {
   // some item's model interpolates its tables cubically: the tree kernel's instantiation
   // that carries both interpolations (the default one has the linear lookup only)
   int any_cubic;
+  // kernel method at a single frequency (integrand_g_kernel_single_omega), IN_SOBOL with no
+  // bins: each point adds sum_i e^{i omega t_i} (its vertex i's terms of both Keldysh
+  // indices) times its Jacobian to the chunk partials
+  int km_fourier;
+  double km_omega;
 };
 
 // any_cubic of a launch over items[0..n)
@@ -78,8 +100,8 @@ inline int items_any_cubic(const ItemDev *items, size_t n) {
 // from the same G. That G stays at the end of one frontier buffer across the passes when
 // no step of a pass writes that buffer far enough to reach it (step t writes buffer t & 1
 // from its start) and it clears the bottom's scratch at the start of the free buffer.
-// Returns the buffer (0 or 1), or -1 when G has to be rebuilt for every pass (no order up
-// to MAX_ORDER needs that).
+// Returns the buffer (0 or 1), or -1 when G has to be copied from the kernel's staging
+// area again for every pass (no order up to MAX_ORDER needs that).
 __host__ __device__ inline int tree_root_buffer(int N) {
   if (N <= TREE_MAX_SUB) return -1;
   // the kernel's schedule: K0 path steps, then the levels in pairs (tree_level4) and a
@@ -136,6 +158,10 @@ cudaError_t launch_fp64_peak(int iters, double *sink, int grid, int block, cudaS
 cudaError_t launch_fourier_table(const double *w, const double2 *cl, const double2 *cg, int n_nodes, double2 *tab,
                                  int npts, double tmax, int symmetric, int *bad, cudaStream_t st);
 cudaError_t launch_mirror_block(const double2 *src, double2 *dst, int npts, cudaStream_t st);
+// keldy's "fft" tables: the discrete transform of npts frequency values on the adjoint mesh,
+// the 1/w^2 tails ml, mg beyond it transformed exactly
+cudaError_t launch_dft_table(const double2 *gl, const double2 *gg, double2 ml, double2 mg, double2 *tab, int npts,
+                             double tmax, int *bad, cudaStream_t st);
 cudaError_t launch_flatband_tables(int n_models, const double *params_dev, double2 *const *tabs_dev, int npts,
                                    double tmax, const double *nodes_dev, const double *weights_dev, int n_nodes,
                                    cudaStream_t st);

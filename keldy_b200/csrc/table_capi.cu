@@ -514,8 +514,8 @@ int upload(kb_context *ctx, std::vector<HostDim> &dims, int type, double u_max, 
   t->ndims = ndims;
   t->type = type;
   t->u_max = u_max;
-  cudaError_t e = cudaMalloc(&t->d_data, host.size() * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc(&t->d_dims, (size_t)ndims * sizeof(TableDimDev));
+  cudaError_t e = device_malloc(&t->d_data, host.size() * sizeof(double));
+  if (e == cudaSuccess) e = device_malloc(&t->d_dims, (size_t)ndims * sizeof(TableDimDev));
   std::vector<TableDimDev> meta((size_t)ndims);
   size_t pos = 0;
   for (int d = 0; d < ndims; ++d) {

@@ -145,12 +145,10 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
 // Items per point: the N(N-1) ordered vertex pairs, the N external-row and N
 // external-column entries (one table lookup each: g^< and g^> at one time difference),
 // the N diagonal blocks (g(0)) and the corner. Each thread computes the lookup positions
-// of GK items before issuing their loads, so that GK L2 round trips overlap (GK = 2: more
-// would cost registers that the 256-thread CTAs do not have).
-template <bool CUBIC>
+// of GK items before issuing their loads, so that GK L2 round trips overlap.
+template <bool CUBIC, int GK>
 __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
                         int spin, int *bad) {
-  constexpr int GK = 2;
   const ModelDev &m = it.model;
   const int M = 2 * N + 1;
   const int npair = N * (N - 1), nlook = npair + 2 * N, per = nlook + N + 1;
@@ -281,13 +279,27 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
 
 // build_G with the model's interpolation chosen once per call; ANY_CUBIC = false compiles
 // the linear lookup only (launches whose models all interpolate linearly).
-template <bool ANY_CUBIC>
+template <bool ANY_CUBIC, int GK = 2>
 __device__ void build_G_any(const ItemDev &it, int N, int np, const double *u, const int *flag, double2 *buf,
                             int spin, int *bad) {
   if (ANY_CUBIC && it.model.interp == 3)
-    build_G<true>(it, N, np, u, flag, buf, spin, bad);
+    build_G<true, GK>(it, N, np, u, flag, buf, spin, bad);
   else
-    build_G<false>(it, N, np, u, flag, buf, spin, bad);
+    build_G<false, GK>(it, N, np, u, flag, buf, spin, bad);
+}
+
+// 16-byte asynchronous copies global -> shared (the L2-only variant: the source was
+// written by this CTA moments before), and the wait for the calling thread's copies.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Copies n complex entries (the staged G of a sub-batch) into shared memory, spread over
+// the CTA's threads; completed by cp_async_wait_all and a barrier.
+__device__ __forceinline__ void copy_roots(double2 *dst, const double2 *src, int n) {
+  for (int e = threadIdx.x; e < n; e += blockDim.x) cp_async16(dst + e, src + e);
 }
 
 // One breadth-first level, both children of a node from one read of its rows: thread r
@@ -615,7 +627,8 @@ __device__ __forceinline__ void tree_bottom9(const double2 *S, double2 D, int b,
 // Per-point sums of the fused bottom (thread q * NODES + node, 2^lg nodes per point): lane
 // groups of consecutive nodes by shuffles, then each point's groups and the
 // TREE_THREADS / NODES descendant slots q in a fixed order by thread p; adds to fval[p],
-// fscale[p]. Every thread calls it; scratch: 256 double2 + 256 double of free shared memory.
+// fscale[p]. Every thread calls it; scratch: 256 double2 + 256 double of free shared memory
+// (BOTTOM_SCRATCH entries), read until the caller's next barrier.
 template <int NODES>
 __device__ void bottom_sum(double2 v, double sc, int lg, int np, double2 *fval, double *fscale, double2 *scratch) {
   static_assert(TREE_THREADS == 256 && NODES >= 32, "slots of whole warps");
@@ -644,7 +657,6 @@ __device__ void bottom_sum(double2 v, double sc, int lg, int np, double2 *fval, 
     fval[tid] = f;
     fscale[tid] = s2;
   }
-  __syncthreads();
 }
 
 // Order 1: the 3x3 root's two leaves directly.
@@ -663,17 +675,99 @@ __device__ __forceinline__ void tree_bottom3(const double2 *R, double2 &sum, dou
   }
 }
 
-// Integrand of np points whose inputs are loaded (S.u, S.flag): S.fval, S.fscale, and
-// flag bit 1 where a pivot fell below the guard.
-template <bool ANY_CUBIC>
-__device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, bool want_scale, int *bad) {
+// One sub-batch of np points (N <= TREE_MAX_SUB, or the subtree of a path pass) whose
+// root matrices sit at `root` in frontier buffer rb, with S.D[rb][node] their prefix
+// determinants: the breadth-first levels, then the fused bottom, each point's sum added
+// to fval[p] (fscale[p]) and bit 1 of flag[p] set where a pivot fell below the guard.
+// pf_n > 0: copies pf_n staged entries from pf_src to the buffer the bottom does not read
+// (at offset roff, past the bottom's scratch) while the bottom runs, for the next
+// sub-batch. Returns the buffer the bottom read. The per-point sums are read from the
+// bottom's scratch until the caller's next barrier.
+__device__ int tree_sub(TreeShared &S, int N, int np, int rb, const double2 *root, int *flag, double2 *fval,
+                        double *fscale, double floor_, bool want_scale, int parity0, const double2 *pf_src,
+                        int pf_n, int roff) {
   const int tid = threadIdx.x;
-  if (tid < np) {
-    S.fval[tid] = c2(0.0, 0.0);
-    S.fscale[tid] = 0.0;
+  // breadth-first levels down to 9x9 nodes, then the fused bottom of three eliminations;
+  // orders 3 and 4 go down to 7x7 nodes and a bottom of two (three were 4 % slower at 4)
+  const int LB = N >= 5 ? N - 4 : (N >= 3 ? N - 3 : 0);
+  int m = 2 * N + 1, cur = rb, nodes = np, lg = 0;
+  const double2 *src = root;
+  for (int k = 0; k + 1 < LB; k += 2) { // pairs of levels, then a last single one
+    tree_level4(src, S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], flag, nodes, lg, m, floor_);
+    nodes *= 4;
+    lg += 2;
+    m -= 4;
+    cur ^= 1;
+    src = S.buf[cur];
   }
+  if (LB & 1) {
+    tree_level2(src, S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, flag, nodes, lg, m, floor_);
+    nodes *= 2;
+    lg += 1;
+    m -= 2;
+    cur ^= 1;
+    src = S.buf[cur];
+  }
+  if (pf_n > 0) copy_roots(S.buf[cur ^ 1] + roff, pf_src, pf_n);
+  double2 v = c2(0.0, 0.0);
+  double sc = 0.0;
+  bool guard = false;
+  int p = 0;
+  if (m == 7) { // four threads per 7x7 node: grandchild tid >> 6 of node tid & 63, so that a
+                // warp's lanes read consecutive nodes (49-entry stride: no bank conflicts)
+    const int node = tid & 63, q = tid >> 6;
+    if (node < nodes) {
+      p = node >> lg;
+      const int parity = __popc(node & ((1 << lg) - 1)) + parity0;
+      tree_bottom7q(src + node * 49, S.D[cur][node], q >> 1, q & 1, parity, floor_, want_scale, v, sc, guard);
+    }
+    if (guard) flag[p] |= 2;
+    bottom_sum<64>(v, sc, lg, np, fval, fscale, S.buf[cur ^ 1]);
+  } else if (m == 9) { // eight threads per 9x9 node: great-grandchild tid >> 5 of node tid & 31
+    const int node = tid & 31, q = tid >> 5;
+    if (node < nodes) {
+      p = node >> lg;
+      const int parity = __popc(node & ((1 << lg) - 1)) + parity0;
+      tree_bottom9(src + node * 81, S.D[cur][node], q >> 2, (q >> 1) & 1, q & 1, parity, floor_, want_scale, v, sc,
+                   guard);
+    }
+    if (guard) flag[p] |= 2;
+    bottom_sum<32>(v, sc, lg, np, fval, fscale, S.buf[cur ^ 1]);
+  } else { // orders 1 and 2: the root itself, one thread per point
+    if (tid < nodes) {
+      p = tid;
+      if (m == 5)
+        tree_bottom5(src + tid * 25, S.D[cur][tid], parity0, floor_, want_scale, v, sc, guard);
+      else
+        tree_bottom3(src + tid * 9, v, sc, want_scale);
+    }
+    if (guard) flag[p] |= 2;
+    group_sum(v, sc, 1, np, fval, fscale, S.wsum, S.wscale);
+  }
+  return cur;
+}
+
+// Frontier entries at the start of a buffer that the fused bottom's per-point sums use.
+constexpr int BOTTOM_SCRATCH = TREE_THREADS + TREE_THREADS / 2;
+
+// Where a sub-batch's roots go when they are copied while the previous sub-batch's bottom
+// runs: past the bottom's scratch (orders 3 and up) of the buffer the bottom does not read.
+// -1: they do not fit beside it (order 3); those sub-batches copy theirs after a barrier.
+__device__ __forceinline__ int tree_prefetch_offset(int N, int P) {
+  const int off = N >= 3 ? BOTTOM_SCRATCH : 0;
+  return off + P * (2 * N + 1) * (2 * N + 1) <= FRONTIER ? off : -1;
+}
+
+// The G-batch's points (gb, staged G at gst: point p at p M^2): the integrand of each,
+// added to S.fval[p] (S.fscale[p]) with bit 1 of S.flag[p] set where a pivot fell below
+// the guard. S.D and the frontier buffers are free on entry; the caller's barrier follows.
+__device__ void tree_gbatch_points(TreeShared &S, const ItemDev &it, int N, int gb, const double2 *gst,
+                                   bool want_scale, int *bad) {
+  const int tid = threadIdx.x;
+  const int M = 2 * N + 1, MM = M * M;
+  const double floor_ = it.model.pivot_floor;
   if (N == 0) {
-    if (tid < np && !(S.flag[tid] & 1)) {
+    if (tid < gb && !(S.flag[tid] & 1)) {
       kb_gf_index a = it.f.A, b = it.f.B;
       a.timesplit = 0;
       b.timesplit = 0;
@@ -681,93 +775,61 @@ __device__ void tree_points(TreeShared &S, const ItemDev &it, int N, int np, boo
       S.fval[tid] = v;
       S.fscale[tid] = cabs(v);
     }
-    __syncthreads();
     return;
   }
-  const int R = N < TREE_MAX_SUB ? N : TREE_MAX_SUB;
-  const int K0 = N - R;
-  // breadth-first levels down to 9x9 nodes, then the fused bottom of three eliminations;
-  // orders 3 and 4 go down to 7x7 nodes and a bottom of two (three were 4 % slower at 4)
-  const int LB = R >= 5 ? R - 4 : (R >= 3 ? R - 3 : 0);
-  const double floor_ = it.model.pivot_floor;
-  const int spin = it.f.A.spin;
-  // G built once per point for all path passes, kept at the end of frontier buffer rb
-  const int rb = tree_root_buffer(N);
-  double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - (2 * N + 1) * (2 * N + 1)) : S.buf[0];
-  for (int sub = 0; sub < (1 << K0); ++sub) {
-    if (rb < 0 || sub == 0) build_G_any<ANY_CUBIC>(it, N, np, S.u, S.flag, root, spin, bad);
-    if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
+  if (N > TREE_MAX_SUB) {
+    // one point at a time in 2^K0 passes, each walking K0 levels along one root-to-subtree
+    // path, then the breadth-first levels of its subtree; the point's G is copied once and
+    // kept at the end of a frontier buffer when the passes leave it there (tree_root_buffer)
+    const int K0 = N - TREE_MAX_SUB;
+    const int rb = tree_root_buffer(N);
+    double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - MM) : S.buf[0];
+    for (int p = 0; p < gb; ++p) {
+      for (int sub = 0; sub < (1 << K0); ++sub) {
+        if (rb < 0 || sub == 0) copy_roots(root, gst + (size_t)p * MM, MM);
+        if (tid == 0) S.D[0][0] = c2(1.0, 0.0);
+        cp_async_wait_all();
+        __syncthreads();
+        int m = M, cur = 0;
+        for (int k = 0; k < K0; ++k) {
+          const int b = (sub >> (K0 - 1 - k)) & 1;
+          tree_path_step(k == 0 ? root : S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag + p, m, b,
+                         floor_);
+          m -= 2;
+          cur ^= 1;
+        }
+        tree_sub(S, TREE_MAX_SUB, 1, cur, S.buf[cur], S.flag + p, S.fval + p, S.fscale + p, floor_, want_scale,
+                 __popc(sub), nullptr, 0, 0);
+        __syncthreads();
+      }
+    }
+    return;
+  }
+  const int P = tree_points_per_chunk(N);
+  const int pf = tree_prefetch_offset(N, P);
+  int rb = 0, roff = 0;
+  for (int sb = 0; sb < gb; sb += P) {
+    const int np = min(P, gb - sb);
+    if (sb == 0 || pf < 0) { // copy this sub-batch's roots now
+      rb = 0;
+      roff = 0;
+      copy_roots(S.buf[0], gst + (size_t)sb * MM, np * MM);
+      if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
+      cp_async_wait_all();
+      __syncthreads();
+    }
+    const int nsb = sb + P, nnp = min(P, gb - nsb);
+    const bool prefetch = pf >= 0 && nnp > 0;
+    const int bot = tree_sub(S, N, np, rb, S.buf[rb] + roff, S.flag + sb, S.fval + sb, S.fscale + sb, floor_,
+                             want_scale, 0, gst + (size_t)nsb * MM, prefetch ? nnp * MM : 0, pf);
+    if (prefetch) {
+      rb = bot ^ 1;
+      roff = pf;
+      if (tid < nnp) S.D[rb][tid] = c2(1.0, 0.0);
+      cp_async_wait_all();
+    }
     __syncthreads();
-    int m = 2 * N + 1, cur = 0;
-    for (int k = 0; k < K0; ++k) {
-      int b = (sub >> (K0 - 1 - k)) & 1;
-      tree_path_step(k == 0 ? root : S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag, m, b, floor_);
-      m -= 2;
-      cur ^= 1;
-    }
-    int nodes = np, lg = 0;
-    for (int k = 0; k + 1 < LB; k += 2) { // pairs of levels, then a last single one
-      tree_level4(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag, nodes, lg, m, floor_);
-      nodes *= 4;
-      lg += 2;
-      m -= 4;
-      cur ^= 1;
-    }
-    if (LB & 1) {
-      tree_level2(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.tmp, S.flag, nodes, lg, m, floor_);
-      nodes *= 2;
-      lg += 1;
-      m -= 2;
-      cur ^= 1;
-    }
-    double2 v = c2(0.0, 0.0);
-    double sc = 0.0;
-    bool guard = false;
-    int G, p = 0;
-    if (m == 7) { // four threads per 7x7 node: grandchild tid >> 6 of node tid & 63, so that a
-                  // warp's lanes read consecutive nodes (49-entry stride: no bank conflicts)
-      const int node = tid & 63, q = tid >> 6;
-      if (node < nodes) {
-        p = node >> lg;
-        const int parity = __popc(node & ((1 << lg) - 1)) + __popc(sub);
-        tree_bottom7q(S.buf[cur] + node * 49, S.D[cur][node], q >> 1, q & 1, parity, floor_, want_scale, v, sc,
-                      guard);
-      }
-      if (guard) S.flag[p] |= 2;
-      bottom_sum<64>(v, sc, lg, np, S.fval, S.fscale, S.buf[cur ^ 1]);
-      continue;
-    } else if (m == 9) { // eight threads per 9x9 node: great-grandchild tid >> 5 of node tid & 31
-      const int node = tid & 31, q = tid >> 5;
-      if (node < nodes) {
-        p = node >> lg;
-        const int parity = __popc(node & ((1 << lg) - 1)) + __popc(sub);
-        tree_bottom9(S.buf[cur] + node * 81, S.D[cur][node], q >> 2, (q >> 1) & 1, q & 1, parity, floor_, want_scale,
-                     v, sc, guard);
-      }
-      if (guard) S.flag[p] |= 2;
-      bottom_sum<32>(v, sc, lg, np, S.fval, S.fscale, S.buf[cur ^ 1]);
-      continue;
-    } else if (m == 5) { // order 2: the root itself
-      G = 1;
-      if (tid < nodes) {
-        p = tid;
-        tree_bottom5(S.buf[cur] + tid * 25, S.D[cur][tid], __popc(sub), floor_, want_scale, v, sc, guard);
-      }
-    } else { // order 1
-      G = 1;
-      if (tid < nodes) {
-        p = tid;
-        tree_bottom3(S.buf[cur] + tid * 9, v, sc, want_scale);
-      }
-    }
-    if (guard) S.flag[p] |= 2;
-    group_sum(v, sc, G, np, S.fval, S.fscale, S.wsum, S.wscale);
   }
-  if (tid < np) {
-    double2 f = S.fval[tid];
-    if (!isfinite(f.x) || !isfinite(f.y)) S.flag[tid] |= 2;
-  }
-  __syncthreads();
 }
 
 __device__ __forceinline__ double2 apply_cutoff(double2 f, double cutoff) {
@@ -784,6 +846,12 @@ __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
   if (threadIdx.x == 0) L.bin_dropped[c] = 0u;
 }
 
+// Persistent CTAs pull chunks of up to 128 points. Per chunk: the points' set-up (Sobol
+// coordinates or given inputs, warper chain, domain flag: one thread per point) into the
+// CTA's global slot; then per G-batch of tree_gbatch(N) points: every table lookup of the
+// batch in flight at once (build_G into the slot's staging area), then the trees of its
+// sub-batches, each sub-batch's G copied into shared memory asynchronously while the
+// previous sub-batch's bottom runs; then the batch's values in point order.
 template <bool EVAL, bool ANY_CUBIC>
 __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -813,27 +881,37 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
     const long long total = EVAL ? (L.index ? (long long)L.n_index : it.n_points) : it.n_points;
     const int ccount = (int)min((long long)it.chunk_points, total - cfirst);
     const int N = it.order;
-    const int P = tree_points_per_chunk(N);
+    const int GB = tree_gbatch(N);
     const bool keep = (L.mode == IN_SOBOL) ? true : (L.keep_u_hypercube != 0);
+    const bool want_scale = EVAL && L.out_scale != nullptr;
     double *slot = L.pts + (size_t)blockIdx.x * PTS_SLOT;
+    double2 *gst = reinterpret_cast<double2 *>(slot + PTS_ROWS);
     if (tid < ccount) prepare_point(L, it, N, cfirst + tid, keep, slot, tid);
     __syncthreads();
-    for (int sb = 0; sb < ccount; sb += P) {
-      const int np = min(P, ccount - sb);
-      if (tid < np) {
-        for (int j = 0; j < N; ++j) S.u[j * np + tid] = slot[j * CHUNK_POINTS + sb + tid];
-        S.jac[tid] = slot[MAX_ORDER * CHUNK_POINTS + sb + tid];
-        S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
+    for (int g0 = 0; g0 < ccount; g0 += GB) {
+      const int gb = min(GB, ccount - g0);
+      if (tid < gb) {
+        for (int j = 0; j < N; ++j) S.u[j * gb + tid] = slot[j * CHUNK_POINTS + g0 + tid];
+        S.jac[tid] = slot[MAX_ORDER * CHUNK_POINTS + g0 + tid];
+        S.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + g0 + tid];
+        S.fval[tid] = c2(0.0, 0.0);
+        S.fscale[tid] = 0.0;
       }
       __syncthreads();
-      tree_points<ANY_CUBIC>(S, it, N, np, EVAL && L.out_scale != nullptr, &s_bad);
+      if (N > 0) {
+        build_G_any<ANY_CUBIC, 4>(it, N, gb, S.u, S.flag, gst, it.f.A.spin, &s_bad);
+        __syncthreads();
+      }
+      tree_gbatch_points(S, it, N, gb, gst, want_scale, &s_bad);
       if (EVAL) {
-        if (tid < np) {
-          long long o = cfirst + sb + tid;
+        if (tid < gb) {
+          const long long o = cfirst + g0 + tid;
           int fl = S.flag[tid];
-          bool dom = !(fl & 1);
-          double2 f = dom ? apply_cutoff(S.fval[tid], it.f.cutoff) : c2(0.0, 0.0);
-          double j = S.jac[tid];
+          const double2 fv = S.fval[tid];
+          if (!isfinite(fv.x) || !isfinite(fv.y)) fl |= 2;
+          const bool dom = !(fl & 1);
+          const double2 f = dom ? apply_cutoff(fv, it.f.cutoff) : c2(0.0, 0.0);
+          const double j = S.jac[tid];
           L.out_val[o] = c2(f.x * j, f.y * j);
           if (L.out_jac) L.out_jac[o] = j;
           if (L.out_dom) L.out_dom[o] = dom ? 1 : 0;
@@ -845,33 +923,35 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
         unsigned long long cdom = s_part.n_in_domain, cfb = s_part.n_fallback;
         unsigned long long mask0 = s_part.fb_mask[0], mask1 = s_part.fb_mask[1];
         unsigned cdrop = s_drop;
-        for (int p = 0; p < np; ++p) {
+        for (int p = 0; p < gb; ++p) {
           int fl = S.flag[p];
+          const double2 fv = S.fval[p];
+          if (!isfinite(fv.x) || !isfinite(fv.y)) fl |= 2;
+          const int q = g0 + p;
           int bin = -2;
           if (L.nbins) { // the code prepare_point stored: 2 bin, or -1 when dropped
-            const double code = slot[BIN_CODE_ROW * CHUNK_POINTS + sb + p];
+            const double code = slot[BIN_CODE_ROW * CHUNK_POINTS + q];
             bin = code < 0.0 ? -1 : (int)code >> 1;
             if (bin < 0) cdrop++;
           }
           if (fl & 1) continue;
           cdom++;
           if (fl & 2) {
-            int bit = sb + p;
-            if (bit < 64)
-              mask0 |= 1ull << bit;
+            if (q < 64)
+              mask0 |= 1ull << q;
             else
-              mask1 |= 1ull << (bit - 64);
+              mask1 |= 1ull << (q - 64);
             cfb++;
             continue;
           }
-          double2 f = apply_cutoff(S.fval[p], it.f.cutoff);
-          double j = S.jac[p];
+          const double2 f = apply_cutoff(fv, it.f.cutoff);
+          const double j = S.jac[p];
           csum.x += f.x * j;
           csum.y += f.y * j;
           if (bin >= 0) {
-            slot[BIN_CODE_ROW * CHUNK_POINTS + sb + p] = (double)(2 * bin + 1);
-            slot[(BIN_CODE_ROW + 1) * CHUNK_POINTS + sb + p] = f.x * j;
-            slot[(BIN_CODE_ROW + 2) * CHUNK_POINTS + sb + p] = f.y * j;
+            slot[BIN_CODE_ROW * CHUNK_POINTS + q] = (double)(2 * bin + 1);
+            slot[(BIN_CODE_ROW + 1) * CHUNK_POINTS + q] = f.x * j;
+            slot[(BIN_CODE_ROW + 2) * CHUNK_POINTS + q] = f.y * j;
           }
         }
         s_part.sum_re = csum.x;
@@ -1672,7 +1752,7 @@ __global__ void __launch_bounds__(KM_THREADS, 2) km_tree_kernel(Launch L) {
     const int N = it.order;
     const int n2 = 2 * N;
     const bool keep = L.mode == IN_SOBOL ? true : (L.keep_u_hypercube != 0);
-    if (!eval) {
+    if (!eval && nb) {
       for (int b = tid; b < nb; b += blockDim.x) {
         L.bin_sums[(size_t)c * nb + b] = c2(0.0, 0.0);
         L.bin_counts[(size_t)c * nb + b] = 0u;
@@ -1716,6 +1796,24 @@ __global__ void __launch_bounds__(KM_THREADS, 2) km_tree_kernel(Launch L) {
           if (q == 0) {
             if (L.out_jac) L.out_jac[gp] = j;
             if (L.out_dom) L.out_dom[gp] = dom ? 1 : 0;
+          }
+        }
+      } else if (L.km_fourier) {
+        // integrand_g_kernel_single_omega (wick_kernel_single_omega.cpp:126-135): the
+        // point's terms weighted by e^{i omega t} of their vertex, in point and vertex order
+        if (tid == 0) {
+          for (int p = 0; p < np; ++p) {
+            if (K.flag[p] & 1) continue;
+            cdom++;
+            const double j = K.jac[p];
+            double2 f = c2(0.0, 0.0);
+            for (int i = 0; i < N; ++i) {
+              double sn, cs;
+              sincos(L.km_omega * K.u[i * np + p], &sn, &cs);
+              const double2 sv = cadd(K.S[p * n2 + 2 * i], K.S[p * n2 + 2 * i + 1]);
+              f = cadd(f, cmul(sv, c2(cs, sn)));
+            }
+            csum = c2(csum.x + f.x * j, csum.y + f.y * j);
           }
         }
       } else {
@@ -1802,15 +1900,11 @@ __global__ void __launch_bounds__(NT) reduce_bins_kernel(Launch L, double2 *sums
 
 } // namespace
 
+// The launchers rely on configure_kernels() having set the kernels' shared-memory limits
+// on the launching device: kb_context_create calls it, with the context's device current,
+// for every context (the attribute belongs to each device's context, not to the process).
 cudaError_t launch_kernel_method(const Launch &L, int grid, cudaStream_t st) {
-  static bool configured = false;
-  const int smem = (int)sizeof(KMTreeShared);
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(km_tree_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  km_tree_kernel<<<grid, KM_THREADS, smem, st>>>(L);
+  km_tree_kernel<<<grid, KM_THREADS, (int)sizeof(KMTreeShared), st>>>(L);
   return cudaGetLastError();
 }
 
@@ -1849,13 +1943,7 @@ cudaError_t configure_kernels() {
 static size_t direct_smem_bytes() { return sizeof(DirectShared); }
 
 cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
-  static bool configured = false;
-  size_t smem = tree_smem_bytes();
-  if (!configured) {
-    cudaError_t e = configure_tree((int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
+  const size_t smem = tree_smem_bytes();
   if (L.mode == IN_SOBOL) {
     if (L.any_cubic)
       tree_kernel<false, true><<<grid, TREE_THREADS, smem, st>>>(L);
@@ -1871,26 +1959,12 @@ cudaError_t launch_tree(const Launch &L, int grid, cudaStream_t st) {
 }
 
 cudaError_t launch_direct(const Launch &L, int grid, cudaStream_t st) {
-  static bool configured = false;
-  size_t smem = direct_smem_bytes();
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(direct_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  direct_kernel<<<grid, NT, smem, st>>>(L);
+  direct_kernel<<<grid, NT, direct_smem_bytes(), st>>>(L);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fallback(const Launch &L, int grid, cudaStream_t st) {
-  static bool configured = false;
-  size_t smem = direct_smem_bytes();
-  if (!configured) {
-    cudaError_t e = cudaFuncSetAttribute(fallback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = true;
-  }
-  fallback_kernel<<<grid, NT, smem, st>>>(L);
+  fallback_kernel<<<grid, NT, direct_smem_bytes(), st>>>(L);
   return cudaGetLastError();
 }
 

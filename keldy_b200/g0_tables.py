@@ -192,3 +192,71 @@ def semicircle(gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_l
     l01 = -np.conj(l10[::-1])
     g01 = -np.conj(g10[::-1])
     return t, gl, gg, l10, g10, l01, g01
+
+
+# ---------------------------------------------------------------- frequency domain
+def bath_hybrid_R(bath_type, gamma, half_bandwidth, w):
+    """Retarded hybridisation of one lead at real frequencies w (model.cpp:92-119):
+    semicircle Gamma/(2D) (w - i sqrt(D^2 - w^2)) inside the band and
+    Gamma/(2D) (w - sgn(w) sqrt(w^2 - D^2)) outside; flatband -i Gamma/2; lorentzian
+    Gamma hw/2 / (w + i hw) (half_bandwidth read as the half width at half maximum)."""
+    w = np.asarray(w, dtype=np.float64)
+    g, D = float(gamma), float(half_bandwidth)
+    if bath_type == "semicircle":
+        inside = np.abs(w) < D
+        root_in = np.sqrt(np.maximum(D * D - w * w, 0.0))
+        root_out = np.sqrt(np.maximum(w * w - D * D, 0.0))
+        sgn = np.where(np.signbit(w), -1.0, 1.0)
+        return np.where(inside, 0.5 * (g / D) * (w - 1j * root_in), 0.5 * (g / D) * (w - sgn * root_out))
+    if bath_type == "flatband":
+        return np.full(w.shape, -0.5j * g, dtype=np.complex128)
+    if bath_type == "lorentzian":
+        return g * D / 2.0 / (w + 1j * D)
+    raise RuntimeError("bath_type not defined")
+
+
+def omega_functions(bath_type, gamma, eps_d, bias_V, beta, half_bandwidth, w):
+    """keldy's g0_model_omega at real frequencies w (model.hpp:94-170; both leads alike, mu_left
+    = -V/2, mu_right = +V/2): (g0_dot_lesser, g0_dot_greater, g0_rightlead_dot_lesser,
+    g0_rightlead_dot_greater). On the real axis keldy keeps only i Im of the dot functions."""
+    w = np.asarray(w, dtype=np.float64)
+    dR = bath_hybrid_R(bath_type, gamma, half_bandwidth, w)
+    dA = np.conj(dR)
+    hyb = dR - dA                               # per lead, both leads alike
+    gR = 1.0 / (w - eps_d - 2.0 * dR)
+    gA = 1.0 / (w - eps_d - 2.0 * dA)
+    mus = (-bias_V / 2.0, bias_V / 2.0)
+    out = []
+    for lesser in (True, False):
+        s = 1 if lesser else -1
+        nl = [_fermi(s * (w - mu), beta) for mu in mus]
+        dot = -s * gR * (nl[0] * hyb + nl[1] * hyb) * gA
+        out.append(1j * dot.imag)
+    dots = list(out)
+    for lesser, dot in zip((True, False), dots):
+        s = 1 if lesser else -1
+        # g0_rightlead_dot (model.hpp:94-99), with the full (complex) dot function
+        full = -s * gR * (_fermi(s * (w - mus[0]), beta) * hyb + _fermi(s * (w - mus[1]), beta) * hyb) * gA
+        out.append(-s * _fermi(s * (w - mus[1]), beta) * hyb * gA + dR * full)
+    return tuple(out)
+
+
+def adjoint_frequencies(time_max, npts):
+    """The frequency mesh adjoint to keldy's time mesh (TRIQS make_adjoint_mesh): npts points
+    w_j = (j - c) dw, c = (npts - 1)/2, dw = 2 pi / (npts dt)."""
+    t = time_mesh(time_max, npts)
+    L = len(t)
+    dt = t[1] - t[0]
+    return (np.arange(L) - (L - 1) // 2) * (2.0 * np.pi / (L * dt))
+
+
+def fft_samples(bath_type, gamma, eps_d, bias_V, beta, half_bandwidth, time_max, npts, dot_lead=False):
+    """The frequency values keldy's make_g0_by_fft transforms (model.cpp:179-212): on the
+    adjoint mesh, the dot block i Im g0_dot^{</>}(w) and, with dot_lead, the (right lead, dot)
+    block g0_rightlead_dot^{</>}(w). Returns {(o1, o2): (lesser_w, greater_w)}."""
+    w = adjoint_frequencies(time_max, npts)
+    dl, dg, ll, lg = omega_functions(bath_type, gamma, eps_d, bias_V, beta, half_bandwidth, w)
+    out = {(0, 0): (dl, dg)}
+    if dot_lead:
+        out[(1, 0)] = (ll, lg)
+    return out

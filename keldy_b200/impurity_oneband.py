@@ -14,6 +14,7 @@ import numpy as np
 
 from . import g0_tables
 from ._keldy import (BinnerT1, BinnerT11, ComputeGfKernel as _ComputeGfKernel, IntegrandGKernel,  # noqa: F401
+                     ComputeGfKernelSingleOmega as _ComputeGfKernelSingleOmega, IntegrandGKernelSingleOmega,
                      ComputeChargeQDirect as _ComputeChargeQDirect,
                      ComputeChargeQDirectTime as _ComputeChargeQDirectTime,
                      ComputeCurrentJDirect as _ComputeCurrentJDirect, FT_MIRROR, FT_SYMMETRIC, G0KeldyshContourT,
@@ -49,11 +50,13 @@ def G0Model(params=None, make_dot_lead=False, **kw):
     """g0_model{g0_model_omega{params}, make_dot_lead} (model.cpp:79-177): the lesser and
     greater tables on [-time_max, time_max], spin up = spin down.
 
-    bath_type "flatband": every ft_method gives the same closed-form tables (the
-    "analytic" method keeps keldy's zero-temperature formula and its restrictions);
-    "semicircle": the band integral of keldy's finite-contour method, with the dot-lead
-    blocks when make_dot_lead. "lorentzian" has no table builder here; build the tables
-    elsewhere and use G0Model.from_tables."""
+    ft_method "fft" (keldy's default, make_g0_by_fft, model.cpp:179-212), any bath: keldy's
+    frequency functions on the mesh adjoint to the time mesh (g0_tables.fft_samples, on the
+    host) and their discrete transform on the GPU (kb_model_set_fft), with the dot-lead
+    blocks when make_dot_lead. ft_method "contour": flatband in closed form; semicircle by
+    the band integral of keldy's finite-contour method (Fourier sums on the GPU), with the
+    dot-lead blocks when make_dot_lead; lorentzian has no contour builder here (use "fft").
+    ft_method "analytic": keldy's zero-temperature flat-band formula and its restrictions."""
     p = model_param_t(params, **kw)
     beta = float(p["beta"])
     if beta < 0:
@@ -69,6 +72,19 @@ def G0Model(params=None, make_dot_lead=False, **kw):
     if ft not in ("fft", "contour", "analytic"):
         raise RuntimeError(f"ft_method '{ft}' is not defined")
     blocks = {}
+    if bath == "flatband" and make_dot_lead:
+        raise RuntimeError("The dot-lead g0 for flatband bath is singular and not implemented accurately.")
+    if ft == "fft":
+        samples = g0_tables.fft_samples(bath, p["Gamma"], p["eps_d"], p["bias_V"], beta, p["half_bandwidth"],
+                                        p["time_max"], npts, dot_lead=make_dot_lead)
+        g = G0ModelTables.empty(float(p["time_max"]), npts, float(p["alpha"]))
+        g.set_fft(0, 0, *samples[(0, 0)])
+        if make_dot_lead:
+            g.set_fft(1, 0, *samples[(1, 0)], FT_MIRROR)
+        g.make_dot_lead = bool(make_dot_lead)
+        g.param = dict(p)
+        g.g0_lesser, g.g0_greater = g.get_table(0, 0, 0)
+        return g
     if bath == "flatband":
         if make_dot_lead:
             raise RuntimeError("The dot-lead g0 for flatband bath is singular and not implemented accurately.")
@@ -94,7 +110,10 @@ def G0Model(params=None, make_dot_lead=False, **kw):
         g.g0_lesser, g.g0_greater = g.get_table(0, 0, 0)
         return g
     else:
-        raise NotImplementedError("lorentzian bath: no table builder in keldy_b200; use G0Model.from_tables")
+        if ft == "analytic":
+            raise RuntimeError("analytic ft only works for flatband")
+        raise NotImplementedError("lorentzian bath: tables by ft_method 'fft' only (keldy's default); the complex "
+                                  "contour method (model.cpp:326-426) has no builder here")
     return from_tables(p["time_max"], le, gr, p["alpha"], blocks=blocks, make_dot_lead=make_dot_lead, param=p)
 
 
@@ -145,6 +164,13 @@ def ComputeGfKernel(model, time, order, nr_bins=100):
     return _ComputeGfKernel(_model(model, False), float(time), int(order), int(nr_bins))
 
 
+def ComputeGfKernelSingleOmega(model, time, omega, order):
+    """compute_gf_kernel_single_omega(model or params, time, omega, order)
+    (compute_obs.hpp:119-133): the kernel method's G at frequency omega; reduce_result()
+    returns the complex mean."""
+    return _ComputeGfKernelSingleOmega(_model(model, False), float(time), float(omega), int(order))
+
+
 def binner_data(b):
     """The [nr_bins][2] data of a BinnerT11 (or [nr_bins] of a BinnerT1) as a numpy array."""
     if isinstance(b, BinnerT11):
@@ -162,4 +188,5 @@ def ComputeCurrentJDirect(model, time, order, cutoff_integrand):
 
 __all__ = ["GfIndexT", "G0Model", "G0KeldyshContourT", "IntegrandGDirect", "ComputeChargeQDirect",
            "ComputeChargeQDirectTime", "BinnerT1", "BinnerT11", "ComputeGfKernel", "IntegrandGKernel", "binner_data",
+           "ComputeGfKernelSingleOmega", "IntegrandGKernelSingleOmega",
            "ComputeCurrentJDirect", "model_param_t", "MODEL_PARAM_DEFAULTS"]

@@ -1,7 +1,7 @@
 """Generates tests/golden/golden.npz and tests/golden/keldy_tests.json.
 
-Run in a checkout that has keldy's sources (KELDY_SRC, default /root/reference) and a
-built oracle/_ref (``make -C oracle``):
+Run in a checkout that has keldy's sources (KELDY_SRC, default: a checkout named
+`reference` beside the repository) and a built oracle/_ref (``make -C oracle``):
 
     python tests/golden/make_golden.py
 
@@ -36,7 +36,7 @@ from oracle.pyoracle import (Reference, W_EXPONENTIAL, W_IDENTITY, W_INVERSE, W_
                              W_INVERSE_SQUARE, W_PLASMA_UV, W_UNIFORM)
 from keldy_b200.g0_tables import flatband, flatband_analytic  # noqa: E402
 
-KELDY_SRC = os.environ.get("KELDY_SRC", "/root/reference")
+KELDY_SRC = os.environ.get("KELDY_SRC", os.path.join(os.path.dirname(ROOT), "reference"))
 
 SOBOL_CASES = [  # (dim, seed, do_shift, do_scramble, seed_shift)
     (1, 0, 0, 0, 0), (3, 0, 0, 0, 0), (8, 0, 0, 0, 0), (12, 0, 0, 0, 0), (8, 1000, 0, 0, 0),
@@ -112,6 +112,25 @@ def keldy_test_values():
         p.update(params_of(blk.split("g0_model g0_fft")[1]))  # the contour run's parameters
         flat.append({"params": p, "values": [{"re": float(a), "im": float(b), "t": float(t), "tol": float(tol)}
                                              for a, b, t, tol in vals]})
+    # the same tests' fft runs (first part of Flatband_asym_1/2, Flatband_3) and Flatband_sym
+    flat_fft = []
+    for name in ("g0_model, Flatband_asym_1", "g0_model, Flatband_asym_2", "g0_model, Flatband_3"):
+        blk = test_block(fb, name)
+        first = blk.split("g0_model g0_ctr")[0] if "g0_model g0_ctr" in blk else blk
+        first = first.split("params.bath_type = \"flatband\";\n  params.ft_method = \"contour\"")[0]
+        vals = re.findall(r"EXPECT_COMPLEX_NEAR\(([-\d.e]+) \+ ([-\d.e]+)i, g0(?:_fft)?\.g0_lesser\[up\]\(([\d.]+)\)"
+                          r"\(0, 0\), ([\d.e-]+)\)", first)
+        sym = re.findall(r"EXPECT_COMPLEX_NEAR\(g0_fft\.g0_(lesser|greater)\[up\]\(([\d.]+)\)\(0, 0\), "
+                         r"-std::conj\(g0_fft\.g0_\w+\[up\]\(-[\d.]+\)\(0, 0\)\), ([\d.e-]+)\)", first)
+        flat_fft.append({"test": name.split(", ")[1], "params": params_of(blk.split("g0_model g0_fft")[0]),
+                         "values": [{"re": float(a), "im": float(b), "t": float(t), "tol": float(tol)}
+                                    for a, b, t, tol in vals],
+                         "symmetry": [{"function": f, "t": float(t), "tol": float(tol)} for f, t, tol in sym]})
+    sb = test_block(fb, "g0_model, Flatband_sym")
+    grid = re.search(r"for \(size_t i = 0; i <= (\d+); \+\+i\) \{\s*time = ([-\d.]+) \+ i \* ([\d.]+);", sb)
+    flat_sym = {"params": params_of(sb), "n_times": int(grid.group(1)) + 1, "t0": float(grid.group(2)),
+                "dt": float(grid.group(3)),
+                "tol": float(re.search(r"g0\.g0_lesser\[up\]\(time\)\(0, 0\), ([\d.e-]+)\)", sb).group(1))}
     kt = open(os.path.join(KELDY_SRC, "test/c++/impurity_oneband/compute_obs_kernel_test.cpp")).read()
     kb = test_block(kt, r"ComputeObs, ValueKernel")
     kvals = re.findall(r"\{([-\d.e]+) ([+-]) ([\d.e-]+)i, ([-\d.e]+) ([+-]) ([\d.e-]+)i\}", kb)
@@ -143,11 +162,13 @@ def keldy_test_values():
                   "test/c++/impurity_oneband/compute_obs_kernel_test.cpp:12-60, "
                   "test/c++/warpers/warper_plasma_uv_test.cpp:15-43, "
                   "test/c++/impurity_oneband/model_semicircle_test.cpp:30-86, "
-                  "test/c++/impurity_oneband/model_flatband_test.cpp:154-220, "
+                  "test/c++/impurity_oneband/model_flatband_test.cpp:60-269, "
                   "test/c++/warpers/projection_test.cpp:70-103",
         "current_kat": current,
         "semicircle_kat": semi,
         "flatband_kat": flat,
+        "flatband_fft_kat": flat_fft,
+        "flatband_sym_kat": flat_sym,
         "hz_charge_series": hz,
         "hz_params": {"beta": "inf", "bias_V": 0.0, "eps_d": 0.0, "Gamma": 1.0, "time_max": 30.0,
                       "nr_time_points_gf": 10001, "alpha": 0.0, "bath_type": "flatband", "ft_method": "analytic",

@@ -183,3 +183,21 @@ def test_model_sweep_batched_equals_separate(ctx):
     batched = capi.integrate(ctx, items)
     for it, b in zip(items, batched):
         assert capi.integrate(ctx, [it])[0] == b
+
+
+def test_contexts_on_two_devices(oracle, golden):
+    """A context on each of two devices in one process: each sets the kernels' shared-memory
+    limits on its own device when it is created, so the tree kernel (over the 48 KB
+    default) launches on both. Skipped with fewer than two GPUs."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    om = oracle.model(10.0, le, gr)
+    w, onp, ond, sc = oracle.integrate(om, CHARGE[0], CHARGE[1], PLASMA_EXP, 8, 256)
+    for dev in (0, 1):
+        c = capi.Context(dev)
+        gm = c.model(10.0, le, gr)
+        (s, npts, nd, _), = capi.integrate(c, [_item(gm, c.sobol(8), PLASMA_EXP, 8, 256)])
+        assert (npts, nd) == (onp, ond)
+        assert abs(s - w) <= 1e-12 * sc, dev

@@ -118,3 +118,68 @@ def test_spin_asymmetric_and_guarded_points(ctx, oracle, golden):
     want, _, sc = oracle.integrand_kernel(om, X, t)
     for p in range(len(t)):
         assert np.abs(got[p] - want[p]).max() <= 1e-12 * max(sc[p], 1e-300)
+
+
+def _omega_values(oracle, om, times, omega):
+    """integrand_g_kernel_single_omega restated on the oracle's per-(vertex, index) terms
+    (wick_kernel_single_omega.cpp:126-135): sum_i e^{i omega t_i} (term_i0 + term_i1)."""
+    vals, dom, sc = oracle.integrand_kernel(om, X_OMEGA, times)
+    ph = np.exp(1j * omega * np.atleast_2d(times))
+    return (vals.sum(axis=2) * ph).sum(axis=1), dom, sc
+
+
+X_OMEGA = (5.0, 0, 0, 0, 0)
+
+
+def test_single_omega_point_values_vs_oracle(ctx, oracle):
+    """keldy's wick_kernel_single_omega_test.cpp setting (flat band, beta = 1, Gamma = 1,
+    t_max = 10, 1,000 -> 1,001 points, X = (5, up, forward), omega = 1, times {2, 0} and
+    {4.9, 4.8}), plus random points at orders 1..6, through keldy's Python name."""
+    from keldy_b200.g0_tables import flatband
+    _, le, gr = flatband(1.0, 0.0, 0.0, 1.0, 10.0, 1001)
+    model = io.G0Model.from_tables(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    integ = io.IntegrandGKernelSingleOmega(io.G0KeldyshContourT(model), io.GfIndexT(5.0, 0, 0), 1.0)
+    rng = np.random.default_rng(5)
+    cases = [np.array([[2.0, 0.0], [4.9, 4.8]])] + [rng.random((6, n)) * 10.0 for n in range(1, 7)]
+    for t in cases:
+        want, dom, sc = _omega_values(oracle, om, t, 1.0)
+        for p in range(len(t)):
+            v, d = integ(list(t[p]))
+            assert d == dom[p]
+            assert abs(v - want[p]) <= 1e-12 * max(sc[p], 1e-300), (t[p], v, want[p])
+
+
+@pytest.mark.parametrize("n,omega", [(1, 1.0), (2, -0.7), (4, 2.5), (6, 1.0)])
+def test_single_omega_integration_vs_oracle(ctx, oracle, golden, n, omega):
+    """integrator<dcomplex, integrand_g_kernel_single_omega>::run: Sobol points through the
+    chain, each point's Fourier-weighted kernel terms times its Jacobian, summed."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    gm = ctx.model(10.0, le, gr)
+    om = oracle.model(10.0, le, gr)
+    npts = 512
+    item = dict(model=gm, rng=ctx.sobol(n), chain=PLASMA_EXP, A=X_OMEGA, order=n, k_first=1, n_points=npts)
+    s, npt, nd = capi.integrate_kernel_single_omega(ctx, [item], omega)[0]
+    li = oracle.sobol_points(n, 0, npts)
+    u, jac = oracle.warp(PLASMA_EXP, li)
+    f, dom, sc = _omega_values(oracle, om, u, omega)
+    assert (npt, nd) == (npts, int(dom.sum()))
+    assert abs(s - (f * jac).sum()) <= 1e-12 * (sc * np.abs(jac)).sum()
+
+
+def test_single_omega_compute_class(ctx, oracle, golden):
+    """ComputeGfKernelSingleOmega (compute_obs.hpp:119-133): run() twice continues the Sobol
+    sequence, and reduce_result() is the mean over all points, equal to one integration."""
+    le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
+    model = io.G0Model.from_tables(10.0, le, gr)
+    comp = io.ComputeGfKernelSingleOmega(model, 7.0, 0.8, 3)
+    comp.warper.emplace_back(warpers.WarperPlasmaUvT(7.0))
+    comp.run(300)
+    comp.run(212)
+    gm = ctx.model(10.0, le, gr)
+    chain = [(capi.WARPER_PLASMA_UV, 7.0, 0.0)]
+    s, npt, nd = capi.integrate_kernel_single_omega(ctx, [dict(model=gm, rng=ctx.sobol(3), chain=chain,
+                                                               A=(7.0, 0, 0, 0, 0), order=3, k_first=1,
+                                                               n_points=512)], 0.8)[0]
+    assert comp.reduce_nr_points_run() == 512 and comp.reduce_nr_points_in_domain() == nd
+    assert abs(comp.reduce_result() - s / 512) <= 1e-12 * abs(s / 512) + 1e-15

@@ -48,11 +48,38 @@ def test_noalloc_equals_integrate_twice(ctx):
             assert abs(s - ws) <= 1e-12 * sc, (call, abs(s - ws) / sc)
 
 
+def test_noalloc_allocates_nothing(ctx):
+    """The defining property: after a first call (which looks up the array's address), a
+    call makes no device allocation at all, while kb_integrate does."""
+    items, keep = _items(ctx)
+    capi.integrate_noalloc(ctx, items)
+    before = capi.device_allocations()
+    capi.integrate_noalloc(ctx, items)
+    capi.integrate_noalloc(ctx, items)
+    assert capi.device_allocations() == before
+    capi.integrate(ctx, items[:1])
+    assert capi.device_allocations() > before
+
+
+def test_noalloc_follows_the_launch_shape(ctx):
+    """With a non-default launch shape (chunk size, CTAs per SM) both entry points split the
+    points into the same chunks and add them in the same order: equal sums."""
+    items, keep = _items(ctx)
+    saved = {n: ctx.get_launch(n) for n in range(1, 8)}
+    try:
+        ctx.set_launch(-1, 48, 1)
+        want = capi.integrate(ctx, items)
+        assert capi.integrate_noalloc(ctx, items) == want
+    finally:
+        for n, (cp, k) in saved.items():
+            ctx.set_launch(n, cp, k)
+
+
 def test_noalloc_limits(ctx):
     items, keep = _items(ctx)
     with pytest.raises(capi.KbError) as e:
         capi.integrate_noalloc(ctx, [dict(items[0], n_points=capi.NOALLOC_MAX_CHUNKS * 128 + 1)])
-    assert e.value.code == capi.KB_E_INVALID and "points in one call" in str(e.value)
+    assert e.value.code == capi.KB_E_INVALID and "scheduling chunks in" in str(e.value)
     with pytest.raises(capi.KbError) as e:
         capi.integrate_noalloc(ctx, [items[0]] * (capi.NOALLOC_MAX_ITEMS + 1))
     assert e.value.code == capi.KB_E_INVALID
