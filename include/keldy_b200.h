@@ -224,6 +224,20 @@ int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double 
  * KB_E_INVALID if a value is not finite. */
 int kb_model_set_fft(kb_model *m, int o1, int o2, const double *gl, const double *gg, int flags);
 
+/* keldy's ft_method "contour" for the baths whose hybridisation is rational (flat band,
+ * Lorentzian: make_g0_by_contour, model.cpp:326-426, integrates their Fourier transforms
+ * along a contour in the complex plane) in closed form on the GPU. The block's functions are
+ * given as sums over n_terms leads of a Fermi function times a rational function with
+ * simple poles: g^<(w) = sum_l n_F(w - mu[l]) R_l(w), g^>(w) = -sum_l (1 - n_F(w - mu[l]))
+ * R_l(w), R_l(w) = sum_k r_lk / (w - z_lk) (n_poles[l] <= 8 poles z off the real axis,
+ * residues r; poles/residues interleaved complex, term after term; R_l decaying at least as
+ * 1/w^2). Every mesh point gets g(t) = int dw/2pi e^{-iwt} g(w): the zero-temperature part
+ * through the exponential integral E1 at each pole, the finite-temperature correction by
+ * Gauss-Legendre quadrature within 36/beta of each mu (beta = INFINITY: none).
+ * KB_FT_SYMMETRIC: t >= 0 only, g(-t) = -conj(g(t)); KB_FT_MIRROR: block (o2, o1) too. */
+int kb_model_set_rational(kb_model *m, int o1, int o2, int n_terms, const double *mu, const int *n_poles,
+                          const double *poles, const double *residues, double beta, int flags);
+
 /* A point of the Keldysh contour with spin and orbital: keldy's gf_index_t (model.hpp:55-78). */
 typedef struct {
   double time;

@@ -669,6 +669,25 @@ class g0_model {
                                        reinterpret_cast<const double *>(gg.data()), flags));
   }
 
+  // block (o1, o2) of a bath with a rational hybridisation in closed form
+  // (kb_model_set_rational): per lead its mu and the poles and residues of its rational part
+  void set_rational(int o1, int o2, std::vector<double> const &mu, std::vector<std::vector<dcomplex>> const &poles,
+                    std::vector<std::vector<dcomplex>> const &residues, double beta, int flags) {
+    if (poles.size() != mu.size() || residues.size() != mu.size())
+      throw std::runtime_error("one pole list and one residue list per term");
+    std::vector<int> n;
+    std::vector<dcomplex> z, r;
+    for (size_t l = 0; l < mu.size(); ++l) {
+      if (poles[l].size() != residues[l].size()) throw std::runtime_error("one residue per pole");
+      n.push_back((int)poles[l].size());
+      z.insert(z.end(), poles[l].begin(), poles[l].end());
+      r.insert(r.end(), residues[l].begin(), residues[l].end());
+    }
+    keldy_b200::check(kb_model_set_rational(m_.get(), o1, o2, (int)mu.size(), mu.data(), n.data(),
+                                            reinterpret_cast<const double *>(z.data()),
+                                            reinterpret_cast<const double *>(r.data()), beta, flags));
+  }
+
   // KB_INTERP_LINEAR (keldy's) or KB_INTERP_CUBIC (an extension) between mesh points
   void set_interpolation(int order) { keldy_b200::check(kb_model_set_interpolation(m_.get(), order)); }
 

@@ -40,6 +40,7 @@ EXPORTS = [
     "kb_integrate_kernel", "kb_integrand_kernel_eval", "kb_warper_table_create", "kb_warper_table_destroy",
     "kb_warper_table_from_projection", "kb_warper_table_analytic", "kb_warper_table_hybrid", "kb_warper_table_info",
     "kb_warper_table_points", "kb_model_set_fourier", "kb_model_set_interpolation", "kb_model_set_fft",
+    "kb_model_set_rational",
     "kb_warper_table_from_samples", "kb_warper_projection_create", "kb_warper_projection_axis",
     "kb_warper_projection_from_integrand", "kb_device_allocations", "kb_integrate_kernel_single_omega",
 ]
@@ -139,6 +140,7 @@ def load():
     L.kb_warper_table_hybrid.argtypes = [_VP, C.c_int, C.POINTER(Warper), _I, C.POINTER(_VP)]
     L.kb_model_set_fourier.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _D, _D, C.c_int]
     L.kb_model_set_fft.argtypes = [_VP, C.c_int, C.c_int, _D, _D, C.c_int]
+    L.kb_model_set_rational.argtypes = [_VP, C.c_int, C.c_int, C.c_int, _D, _I, _D, _D, C.c_double, C.c_int]
     L.kb_model_set_interpolation.argtypes = [_VP, C.c_int]
     L.kb_warper_table_info.argtypes = [_VP, _I, _I, _I]
     L.kb_warper_table_points.argtypes = [_VP, C.c_int, _D, _D]
@@ -516,6 +518,17 @@ class Model:
         gg = np.ascontiguousarray(gg_w, dtype=np.complex128).view(np.float64)
         assert gl.size == 2 * self.npts and gg.size == 2 * self.npts
         check(self.ctx.L.kb_model_set_fft(self.h, int(o1), int(o2), _dp(gl), _dp(gg), int(flags)))
+
+    def set_rational(self, o1, o2, terms, beta, flags=0):
+        """Block (o1, o2) of a bath with a rational hybridisation in closed form
+        (kb_model_set_rational): terms = [(mu, poles, residues), ...] as from
+        g0_tables.rational_terms; flags FT_SYMMETRIC, FT_MIRROR."""
+        mu = np.array([t[0] for t in terms], dtype=np.float64)
+        npl = np.array([len(t[1]) for t in terms], dtype=np.int32)
+        z = np.ascontiguousarray(np.concatenate([np.asarray(t[1], np.complex128) for t in terms])).view(np.float64)
+        r = np.ascontiguousarray(np.concatenate([np.asarray(t[2], np.complex128) for t in terms])).view(np.float64)
+        check(self.ctx.L.kb_model_set_rational(self.h, int(o1), int(o2), len(terms), _dp(mu), _ip(npl), _dp(z),
+                                               _dp(r), float(beta), int(flags)))
 
     def table(self, spin=0, o1=0, o2=0):
         """(lesser, greater) complex arrays of one block, read back from the device."""

@@ -262,6 +262,20 @@ PYBIND11_MODULE(_keldy, m) {
              int flags) { g.set_fft(o1, o2, to_cvec(gl), to_cvec(gg), flags); },
           py::arg("o1"), py::arg("o2"), py::arg("gl"), py::arg("gg"), py::arg("flags") = 0)
       .def(
+          "set_rational",
+          [](g0_model &g, int o1, int o2, py::list terms, double beta, int flags) {
+            std::vector<double> mu;
+            std::vector<std::vector<dcomplex>> z, r;
+            for (auto item : terms) {
+              auto t = item.cast<py::tuple>();
+              mu.push_back(t[0].cast<double>());
+              z.push_back(to_cvec(t[1].cast<py::array_t<std::complex<double>>>()));
+              r.push_back(to_cvec(t[2].cast<py::array_t<std::complex<double>>>()));
+            }
+            g.set_rational(o1, o2, mu, z, r, beta, flags);
+          },
+          py::arg("o1"), py::arg("o2"), py::arg("terms"), py::arg("beta"), py::arg("flags") = 0)
+      .def(
           "get_table",
           [](g0_model const &g, int spin, int o1, int o2) {
             auto t = g.get_table(spin, o1, o2);

@@ -589,6 +589,77 @@ int kb_model_set_fourier(kb_model *m, int o1, int o2, int n_nodes, const double 
   return KB_OK;
 }
 
+int kb_model_set_rational(kb_model *m, int o1, int o2, int n_terms, const double *mu, const int *n_poles,
+                          const double *poles, const double *residues, double beta, int flags) {
+  KB_CHECK(m && mu && n_poles && poles && residues, "kb_model_set_rational: null argument");
+  KB_CHECK(o1 >= 0 && o1 < 2 && o2 >= 0 && o2 < 2, "orbital index out of range");
+  KB_CHECK(n_terms >= 1 && n_terms <= RATIONAL_MAX_TERMS, "n_terms must be in [1, 4]");
+  KB_CHECK(beta > 0.0, "beta must be > 0 (INFINITY: zero temperature)");
+  KB_CHECK(m->npts % 2 == 1 && m->npts >= 3,
+           "the rational builder needs an odd number of mesh points (t = 0 on the mesh)");
+  KB_CHECK(!(flags & KB_FT_MIRROR) || o1 != o2, "KB_FT_MIRROR needs an off-diagonal block");
+  std::vector<RationalTermDev> terms((size_t)n_terms);
+  int off = 0;
+  for (int l = 0; l < n_terms; ++l) {
+    RationalTermDev &T = terms[(size_t)l];
+    memset(&T, 0, sizeof(T));
+    KB_CHECK(n_poles[l] >= 1 && n_poles[l] <= RATIONAL_MAX_POLES, "each term has 1..8 poles");
+    KB_CHECK(std::isfinite(mu[l]), "chemical potentials must be finite");
+    T.mu = mu[l];
+    T.n = n_poles[l];
+    for (int k = 0; k < T.n; ++k, ++off) {
+      T.z[k] = make_double2(poles[2 * off], poles[2 * off + 1]);
+      T.r[k] = make_double2(residues[2 * off], residues[2 * off + 1]);
+      KB_CHECK(std::isfinite(T.z[k].x) && std::isfinite(T.z[k].y) && std::isfinite(T.r[k].x) &&
+                   std::isfinite(T.r[k].y),
+               "poles and residues must be finite");
+      KB_CHECK(T.z[k].y != 0.0, "poles must lie off the real axis");
+    }
+  }
+  constexpr int NODES = 240;
+  std::vector<double> gx(NODES), gw(NODES);
+  gauss_legendre(NODES, gx.data(), gw.data());
+  kb_context *ctx = m->ctx;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = ctx->stream;
+  const size_t n = (size_t)m->npts;
+  const bool mirror = (flags & KB_FT_MIRROR) != 0;
+  if (!m->tab[0][o1][o2]) KB_CUDA(device_malloc(&m->tab[0][o1][o2], n * 2 * sizeof(double2)));
+  if (mirror && !m->tab[0][o2][o1]) KB_CUDA(device_malloc(&m->tab[0][o2][o1], n * 2 * sizeof(double2)));
+  DevBuf dterms, dx, dw, dbad, dmax;
+  KB_CUDA(dterms.alloc(terms.size() * sizeof(RationalTermDev), st));
+  KB_CUDA(dx.alloc(NODES * sizeof(double), st));
+  KB_CUDA(dw.alloc(NODES * sizeof(double), st));
+  KB_CUDA(dbad.alloc(sizeof(int), st));
+  KB_CUDA(dmax.alloc(2 * sizeof(double), st));
+  KB_CUDA(cudaMemcpyAsync(dterms.p, terms.data(), terms.size() * sizeof(RationalTermDev), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dx.p, gx.data(), NODES * sizeof(double), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dw.p, gw.data(), NODES * sizeof(double), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemsetAsync(dbad.p, 0, sizeof(int), st));
+  KB_CUDA(launch_rational_table(dterms.as<RationalTermDev>(), n_terms, beta, dx.as<double>(), dw.as<double>(), NODES,
+                                m->tab[0][o1][o2], m->npts, m->tmax, (flags & KB_FT_SYMMETRIC) ? 1 : 0,
+                                dbad.as<int>(), st));
+  KB_CUDA(launch_table_max(m->tab[0][o1][o2], m->npts, dmax.as<double>(), st));
+  if (mirror) KB_CUDA(launch_mirror_block(m->tab[0][o1][o2], m->tab[0][o2][o1], m->npts, st));
+  int bad = 0;
+  double mx = 0.0;
+  KB_CUDA(cudaMemcpyAsync(&bad, dbad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaMemcpyAsync(&mx, dmax.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (bad) return fail(KB_E_INVALID, "g0 table contains non-finite values");
+  const int blocks[2][2] = {{o1, o2}, {o2, o1}};
+  for (int k = 0; k < (mirror ? 2 : 1); ++k) { // spin down uses the spin-up blocks (model.cpp:209-211)
+    const int a = blocks[k][0], b = blocks[k][1];
+    cudaFree(m->tab[1][a][b]);
+    m->tab[1][a][b] = nullptr;
+    m->hash[0][a][b] = 0;
+    m->hash[1][a][b] = 0;
+  }
+  m->tabmax = std::max(m->tabmax, mx);
+  return KB_OK;
+}
+
 int kb_model_set_fft(kb_model *m, int o1, int o2, const double *gl, const double *gg, int flags) {
   KB_CHECK(m && gl && gg, "kb_model_set_fft: null argument");
   KB_CHECK(o1 >= 0 && o1 < 2 && o2 >= 0 && o2 < 2, "orbital index out of range");

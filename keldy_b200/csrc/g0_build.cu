@@ -285,6 +285,129 @@ __global__ void dft_kernel(const double2 *Gl, const double2 *Gg, double2 *tab, i
   tab[2 * k + 1] = ag;
 }
 
+// Baths with a rational hybridisation (flat band, Lorentzian; model.cpp:107-118): keldy's
+// dot functions are sums over the leads of Fermi functions times rational functions R_l
+// with simple poles z_k and residues r_k (g0_tables.rational_terms):
+//   g^<(w) = sum_l n_F(w - mu_l) R_l(w),   g^>(w) = -sum_l (1 - n_F(w - mu_l)) R_l(w).
+// Their transforms g(t) = int dw/2pi e^{-iwt} g(w), the exact quantity keldy's contour
+// method integrates numerically (model.cpp:326-426), in closed form for t > 0:
+//   K_mu(t) = int_{-inf}^{mu} e^{-iwt} R dw = sum_k r_k J(z_k), J(z) = -e^{-izt} E1(i (mu - z) t)
+//     (E1 continued across its cut when Im z < 0 and mu > Re z: + 2 pi i),
+//   F(t) = int e^{-iwt} R dw = -2 pi i sum_{Im z_k < 0} r_k e^{-i z_k t},
+// the finite-temperature part C_mu(t) = int e^{-iwt} (n_F - theta)(w - mu) R dw by
+// Gauss-Legendre quadrature on [mu - 36/beta, mu + 36/beta], t = 0 by the logarithms
+// K_mu(0) = sum_k r_k (Log(mu - z_k) - i pi s_k) (s_k = +1 below the real axis, -1 above),
+// and t < 0 as the conjugate of the same formulas for the conjugate poles and residues.
+// E1 is evaluated scaled, e^v E1(v), so that e^{-izt} E1 does not overflow.
+using RationalTerm = RationalTermDev;
+
+__device__ double2 e1_scaled(double2 v) {
+  const double av = hypot(v.x, v.y);
+  const bool series = av < 1.5 || (v.x < 0.0 && fabs(v.y) < 0.6 * fabs(v.x));
+  if (series) return cmul(cexpd(v), e1_complex(v));
+  double2 b = c2(v.x + 1.0, v.y), c = c2(1e300, 0.0), d = crcp(b), h = d;
+  for (int i = 1; i < 2000; ++i) { // the continued fraction of e1_complex without its e^{-v}
+    const double an = -(double)i * (double)i;
+    b = c2(b.x + 2.0, b.y);
+    d = crcp(c2(an * d.x + b.x, an * d.y + b.y));
+    const double2 q = cdiv(c2(an, 0.0), c);
+    c = c2(b.x + q.x, b.y + q.y);
+    const double2 del = cmul(c, d);
+    h = cmul(h, del);
+    if (fabs(del.x - 1.0) + fabs(del.y) < 1e-16) break;
+  }
+  return h;
+}
+
+// K, F and C of one term at t >= 0 (poles and residues conjugated when conj).
+__device__ void rational_term(const RationalTerm &T, bool conj, double t, bool finite, double beta,
+                              const double *nodes, const double *weights, int n_nodes, double2 &K, double2 &F,
+                              double2 &C) {
+  K = F = C = c2(0.0, 0.0);
+  const double mu = T.mu;
+  for (int k = 0; k < T.n; ++k) {
+    const double2 z = conj ? c2(T.z[k].x, -T.z[k].y) : T.z[k];
+    const double2 r = conj ? c2(T.r[k].x, -T.r[k].y) : T.r[k];
+    if (t == 0.0) {
+      const double2 lg = clogd(c2(mu - z.x, -z.y));
+      const double s = z.y < 0.0 ? 1.0 : -1.0;
+      K = cadd(K, cmul(r, c2(lg.x, lg.y - PI * s)));
+      if (z.y < 0.0) F = cadd(F, cmul(r, c2(0.0, -2.0 * PI)));
+      continue;
+    }
+    const double2 v = c2(z.y * t, (mu - z.x) * t); // i (mu - z) t
+    double2 J;
+    if (z.y < 0.0 && mu == z.x) { // the path ends on E1's cut: the limit from below
+      const double2 e1 = c2(-ei_positive(-z.y * t), PI);
+      J = cmul(c2(-1.0, 0.0), cmul(cexpd(c2(z.y * t, -z.x * t)), e1));
+    } else {
+      J = cmul(c2(-1.0, 0.0), cmul(cexpd(c2(0.0, -mu * t)), e1_scaled(v)));
+      if (z.y < 0.0 && mu > z.x) // continuation across the cut: -2 pi i e^{-izt}
+        J = cadd(J, cmul(c2(0.0, -2.0 * PI), cexpd(c2(z.y * t, -z.x * t))));
+    }
+    K = cadd(K, cmul(r, J));
+    if (z.y < 0.0) F = cadd(F, cmul(cmul(r, c2(0.0, -2.0 * PI)), cexpd(c2(z.y * t, -z.x * t))));
+  }
+  if (!finite) return;
+  const double W = 36.0 / beta;
+  for (int pnl = 0; pnl < 2; ++pnl) {
+    const double a = pnl == 0 ? -W : 0.0, b = pnl == 0 ? 0.0 : W;
+    for (int q = 0; q < n_nodes; ++q) {
+      const double x = 0.5 * (b - a) * nodes[q] + 0.5 * (b + a);
+      const double wq = 0.5 * (b - a) * weights[q];
+      const double e = exp(-beta * fabs(x));
+      const double dn = (x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0)) * e / (1.0 + e); // n_F(x) - theta(-x)
+      const double w = mu + x;
+      double2 R = c2(0.0, 0.0);
+      for (int k = 0; k < T.n; ++k) {
+        const double2 z = conj ? c2(T.z[k].x, -T.z[k].y) : T.z[k];
+        const double2 r = conj ? c2(T.r[k].x, -T.r[k].y) : T.r[k];
+        R = cadd(R, cdiv(r, c2(w - z.x, -z.y)));
+      }
+      double s, c;
+      sincos(-w * t, &s, &c);
+      C = cadd(C, cmul(c2(wq * dn * R.x, wq * dn * R.y), c2(c, s)));
+    }
+  }
+}
+
+// One thread per mesh point (the t >= 0 half when symmetric, mirrored by g(-t) = -conj(g(t))).
+__global__ void rational_kernel(const RationalTerm *terms, int n_terms, double beta, const double *nodes,
+                                const double *weights, int n_nodes, double2 *tab, int npts, double tmax,
+                                int symmetric, int *bad) {
+  const int mid = npts / 2;
+  const double delta = (tmax - (-tmax)) / (double)(npts - 1);
+  const int count = symmetric ? npts - mid : npts;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= count) return;
+  const int i = symmetric ? mid + idx : idx;
+  const double t = (i == mid) ? 0.0 : -tmax + i * delta;
+  const bool neg = t < 0.0;
+  const bool finite = isfinite(beta);
+  double2 less = c2(0.0, 0.0), great = c2(0.0, 0.0);
+  for (int l = 0; l < n_terms; ++l) {
+    double2 K, F, C;
+    rational_term(terms[l], neg, fabs(t), finite, beta, nodes, weights, n_nodes, K, F, C);
+    if (neg) { // g(t) for t < 0: the conjugate of the conjugate function's value at |t|
+      K = c2(K.x, -K.y);
+      F = c2(F.x, -F.y);
+      C = c2(C.x, -C.y);
+    }
+    less = cadd(less, cadd(K, C));
+    great = c2(great.x - (F.x - K.x - C.x), great.y - (F.y - K.y - C.y));
+  }
+  const double s = 1.0 / (2.0 * PI);
+  const double2 gl = c2(less.x * s, less.y * s), gg = c2(great.x * s, great.y * s);
+  if (!isfinite(gl.x) || !isfinite(gl.y) || !isfinite(gg.x) || !isfinite(gg.y)) atomicOr(bad, 1);
+  tab[2 * i] = gl;
+  tab[2 * i + 1] = gg;
+  if (symmetric && i != mid) {
+    const int j = npts - 1 - i;
+    tab[2 * j] = c2(-gl.x, gl.y);
+    tab[2 * j + 1] = c2(-gg.x, gg.y);
+  }
+}
+
 // Block (o2, o1) from block (o1, o2): g_{o2 o1}(t) = -conj(g_{o1 o2}(-t)) (model.cpp:311-313).
 __global__ void mirror_block_kernel(const double2 *src, double2 *dst, int npts) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += gridDim.x * blockDim.x) {
@@ -310,6 +433,15 @@ cudaError_t launch_dft_table(const double2 *gl, const double2 *gg, double2 ml, d
   const double dw = 2.0 * PI / ((double)npts * dt);
   DftTail tail{ml, mg, dw * sqrt((double)npts)};
   dft_kernel<<<(npts + 127) / 128, 128, 0, st>>>(gl, gg, tab, npts, dw, dt, tail, bad);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rational_table(const RationalTermDev *terms, int n_terms, double beta, const double *nodes,
+                                  const double *weights, int n_nodes, double2 *tab, int npts, double tmax, int symmetric,
+                                  int *bad, cudaStream_t st) {
+  const int count = symmetric ? npts - npts / 2 : npts;
+  rational_kernel<<<(count + 127) / 128, 128, 0, st>>>(terms, n_terms, beta, nodes, weights, n_nodes, tab, npts, tmax,
+                                                       symmetric, bad);
   return cudaGetLastError();
 }
 

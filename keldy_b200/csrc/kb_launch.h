@@ -158,6 +158,18 @@ cudaError_t launch_fp64_peak(int iters, double *sink, int grid, int block, cudaS
 cudaError_t launch_fourier_table(const double *w, const double2 *cl, const double2 *cg, int n_nodes, double2 *tab,
                                  int npts, double tmax, int symmetric, int *bad, cudaStream_t st);
 cudaError_t launch_mirror_block(const double2 *src, double2 *dst, int npts, cudaStream_t st);
+// Tables of a bath with a rational hybridisation in closed form: n_terms terms, each a
+// chemical potential and a rational function given by its simple poles and residues.
+constexpr int RATIONAL_MAX_POLES = 8;
+constexpr int RATIONAL_MAX_TERMS = 4;
+struct RationalTermDev {
+  double mu;
+  int n;
+  double2 z[RATIONAL_MAX_POLES], r[RATIONAL_MAX_POLES];
+};
+cudaError_t launch_rational_table(const RationalTermDev *terms, int n_terms, double beta, const double *nodes,
+                                  const double *weights, int n_nodes, double2 *tab, int npts, double tmax, int symmetric,
+                                  int *bad, cudaStream_t st);
 // keldy's "fft" tables: the discrete transform of npts frequency values on the adjoint mesh,
 // the 1/w^2 tails ml, mg beyond it transformed exactly
 cudaError_t launch_dft_table(const double2 *gl, const double2 *gg, double2 ml, double2 mg, double2 *tab, int npts,

@@ -260,3 +260,75 @@ def fft_samples(bath_type, gamma, eps_d, bias_V, beta, half_bandwidth, time_max,
     if dot_lead:
         out[(1, 0)] = (ll, lg)
     return out
+
+
+# ---------------------------------------------------------------- rational baths
+def _pf(c, poles):
+    """Residues of c / prod_k (w - z_k) at its simple poles z_k."""
+    poles = np.asarray(poles, dtype=np.complex128)
+    res = np.empty(len(poles), dtype=np.complex128)
+    for k, z in enumerate(poles):
+        d = z - np.delete(poles, k)
+        if np.any(np.abs(d) < 1e-9 * (1.0 + abs(z))):
+            raise RuntimeError("the rational bath functions have a double pole at these parameters")
+        res[k] = c / np.prod(d)
+    return res
+
+
+def rational_terms(bath_type, gamma, eps_d, bias_V, half_bandwidth, dot_lead=False):
+    """keldy's dot functions for a bath with a rational hybridisation (flatband: Delta^R =
+    -i Gamma/2, lorentzian: Gamma hw/2/(w + i hw) per lead; model.cpp:107-118) as sums over
+    the leads l of Fermi functions times rational functions with simple poles:
+    g^<(w) = sum_l n_F(w - mu_l) R_l(w), g^>(w) = -sum_l (1 - n_F(w - mu_l)) R_l(w)
+    (model.hpp:94-112). R_dot = -(Delta^R - Delta^A) g^R g^A for both leads; the (right lead,
+    dot) block (model.hpp:94-99) has R_1 + R_2 at mu_R and R_2 at mu_L, R_1 = -(Delta^R -
+    Delta^A) g^A, R_2 = Delta^R R_dot. Returns {(o1, o2): [(mu, poles, residues), ...]}."""
+    mus = (-bias_V / 2.0, bias_V / 2.0)
+    g, eps, hw = float(gamma), float(eps_d), float(half_bandwidth)
+    if bath_type == "flatband":
+        # R_dot = i Gamma / ((w - eps)^2 + Gamma^2)
+        poles = np.array([eps + 1j * g, eps - 1j * g])
+        dot = (poles, _pf(1j * g, poles))
+        if dot_lead:
+            raise RuntimeError("The dot-lead g0 for flatband bath is singular and not implemented accurately.")
+        return {(0, 0): [(mus[0], *dot), (mus[1], *dot)]}
+    if bath_type != "lorentzian":
+        raise RuntimeError("rational_terms: flatband or lorentzian bath")
+    # g^R = (w + i hw) / Q(w), Q(w) = (w - eps)(w + i hw) - Gamma hw; R_dot = i Gamma hw^2 / (Q Q*)
+    q = np.roots([1.0, 1j * hw - eps, -(1j * eps * hw + g * hw)])
+    qs = np.conj(q)
+    dpoles = np.concatenate([q, qs])
+    dot = (dpoles, _pf(1j * g * hw * hw, dpoles))
+    out = {(0, 0): [(mus[0], *dot), (mus[1], *dot)]}
+    if dot_lead:
+        p1 = np.concatenate([[-1j * hw], qs])
+        r1 = _pf(1j * g * hw * hw, p1)                     # R_1 = i Gamma hw^2 / ((w + i hw) Q*)
+        p2 = np.concatenate([[-1j * hw], q, qs])
+        r2 = _pf(0.5 * g * hw * 1j * g * hw * hw, p2)      # R_2 = (Gamma hw / 2) / (w + i hw) * R_dot
+        r12 = r2.copy()
+        r12[0] += r1[0]
+        r12[3:] += r1[1:]
+        out[(1, 0)] = [(mus[1], p2, r12), (mus[0], p2, r2)]
+    return out
+
+
+def rational_reference(terms, beta, t, kind):
+    """The transform (1/2pi) int e^{-iwt} g(w) dw of rational_terms' functions by direct
+    adaptive quadrature on the real axis, |w| <= 3000 (test helper; kind 'lesser' or 'greater')."""
+    from scipy.integrate import quad
+    out = []
+    for tt in np.atleast_1d(t):
+        tot = 0j
+        for mu, poles, res in terms:
+            def f(w, mu=mu, poles=poles, res=res):
+                r = np.sum(res / (w - poles))
+                n = _fermi(w - mu, beta)
+                return (n * r) if kind == "lesser" else (-(1.0 - n) * r)
+            for part in ("real", "imag"):
+                for sgn in (1.0, -1.0):
+                    fc = (lambda w, s=sgn: getattr(f(s * w) * np.exp(-1j * s * w * tt), part))
+                    v = sum(quad(fc, a, b, limit=5000, epsabs=1e-14, epsrel=1e-12)[0]
+                            for a, b in ((0.0, 10.0), (10.0, 100.0), (100.0, 3000.0)))
+                    tot += v if part == "real" else 1j * v
+        out.append(tot / (2 * np.pi))
+    return np.array(out)

@@ -54,8 +54,9 @@ def G0Model(params=None, make_dot_lead=False, **kw):
     frequency functions on the mesh adjoint to the time mesh (g0_tables.fft_samples, on the
     host) and their discrete transform on the GPU (kb_model_set_fft), with the dot-lead
     blocks when make_dot_lead. ft_method "contour": flatband in closed form; semicircle by
-    the band integral of keldy's finite-contour method (Fourier sums on the GPU), with the
-    dot-lead blocks when make_dot_lead; lorentzian has no contour builder here (use "fft").
+    the band integral of keldy's finite-contour method (Fourier sums on the GPU);
+    lorentzian in closed form from the poles of its rational functions (on the GPU); with the
+    dot-lead blocks when make_dot_lead.
     ft_method "analytic": keldy's zero-temperature flat-band formula and its restrictions."""
     p = model_param_t(params, **kw)
     beta = float(p["beta"])
@@ -112,8 +113,18 @@ def G0Model(params=None, make_dot_lead=False, **kw):
     else:
         if ft == "analytic":
             raise RuntimeError("analytic ft only works for flatband")
-        raise NotImplementedError("lorentzian bath: tables by ft_method 'fft' only (keldy's default); the complex "
-                                  "contour method (model.cpp:326-426) has no builder here")
+        # lorentzian, "contour": the transform keldy's contour integral computes, in closed form
+        # from the poles of the bath's rational functions (kb_model_set_rational)
+        terms = g0_tables.rational_terms(bath, p["Gamma"], p["eps_d"], p["bias_V"], p["half_bandwidth"],
+                                         dot_lead=make_dot_lead)
+        g = G0ModelTables.empty(float(p["time_max"]), npts, float(p["alpha"]))
+        g.set_rational(0, 0, [tuple(t) for t in terms[(0, 0)]], beta, FT_SYMMETRIC)
+        if make_dot_lead:
+            g.set_rational(1, 0, [tuple(t) for t in terms[(1, 0)]], beta, FT_MIRROR)
+        g.make_dot_lead = bool(make_dot_lead)
+        g.param = dict(p)
+        g.g0_lesser, g.g0_greater = g.get_table(0, 0, 0)
+        return g
     return from_tables(p["time_max"], le, gr, p["alpha"], blocks=blocks, make_dot_lead=make_dot_lead, param=p)
 
 

@@ -51,3 +51,38 @@ def time_to_relative_error(ctx, model, A, B, chain, order, target=1e-3, replicas
             return dict(mean=mean, stderr=err, rel=rel, points_per_replica=n, evaluations=n * replicas, seconds=dt,
                         reached=rel <= target)
         n *= 2
+
+
+def time_to_relative_error_ladders(ctx, model, A, B, chain, order, target=1e-3, ladders=8, replicas=16,
+                                   start_points=1 << 8, max_points=1 << 22, seed_shift0=1, scramble=False, flow=None):
+    """time_to_relative_error repeated over `ladders` independent ladders (disjoint blocks of
+    random digital shifts), each on a sqrt(2) grid of points per replica (start_points *
+    2^(k/2), rounded). Per ladder: the points per replica and the wall time of the run that
+    first met stderr / |mean| <= target. Returns the medians and interquartile ranges over the
+    ladders, and the per-ladder values."""
+    grid, k = [], 0
+    while True:
+        n = int(round(start_points * 2.0 ** (k / 2.0)))
+        grid.append(min(n, max_points))
+        if n >= max_points:
+            break
+        k += 1
+    secs, pts, reached = [], [], []
+    for lad in range(ladders):
+        rngs = [ctx.sobol(order, 31, True, scramble, seed_shift0 + lad * replicas + r) for r in range(replicas)]
+        estimate(ctx, model, A, B, chain, order, grid[0], replicas, rngs=rngs, flow=flow)  # warm-up
+        for n in grid:
+            ctx.synchronize()
+            t0 = time.perf_counter()
+            mean, err, _ = estimate(ctx, model, A, B, chain, order, n, replicas, rngs=rngs, flow=flow)
+            dt = time.perf_counter() - t0
+            rel = err / abs(mean) if mean != 0 else float("inf")
+            if rel <= target or n == grid[-1]:
+                secs.append(dt)
+                pts.append(n)
+                reached.append(rel <= target)
+                break
+    q = lambda a, p: float(np.percentile(np.asarray(a, dtype=float), p))  # noqa: E731
+    return dict(seconds_median=q(secs, 50), seconds_iqr=[q(secs, 25), q(secs, 75)],
+                points_median=q(pts, 50), points_iqr=[q(pts, 25), q(pts, 75)], seconds=secs, points=pts,
+                all_reached=all(reached), ladders=ladders, replicas=replicas, target=target)

@@ -82,3 +82,40 @@ def test_lorentzian_fft_vs_quadrature():
         im = sum(quad(lambda w, s=s_: im_lesser(s * w), 0, np.inf, weight="cos", wvar=tt, limlst=200)[0]
                  for s_ in (1.0, -1.0)) / (2 * np.pi)
         assert abs(gl[i] - complex(re, im)) < 1e-4, (tt, gl[i], complex(re, im))
+
+
+def test_rational_oracle_vs_quadrature_and_flatband():
+    """The closed-form transforms of the rational baths (oracle/g0_rational_oracle.py) against
+    direct adaptive quadrature of int dw/2pi e^{-iwt} g(w) for the Lorentzian bath (dot and
+    dot-lead blocks, both signs of t, finite temperature with bias), and against the host's
+    closed-form flat-band tables (g0_tables.flatband) for the flat band's two-pole terms."""
+    from oracle import g0_rational_oracle as ro
+    terms = g0_tables.rational_terms("lorentzian", 1.0, 0.3, 0.5, 2.0, dot_lead=True)
+    for blk, tol in (((0, 0), 1e-9), ((1, 0), 1e-6)):
+        for tt in (0.0, 0.7, 5.0, -3.0):
+            a, b = ro.transform(terms[blk], 20.0, [tt])
+            assert abs(a[0] - g0_tables.rational_reference(terms[blk], 20.0, [tt], "lesser")[0]) < tol
+            assert abs(b[0] - g0_tables.rational_reference(terms[blk], 20.0, [tt], "greater")[0]) < tol
+    ft = g0_tables.rational_terms("flatband", 1.0, 0.4, 0.6, 2.0)
+    t, hl, hg = g0_tables.flatband(1.0, 0.4, 0.6, 50.0, 20.0, 401)
+    a, b = ro.transform(ft[(0, 0)], 50.0, t)
+    assert np.abs(a - hl).max() < 1e-12 and np.abs(b - hg).max() < 1e-12
+
+
+def test_rational_terms_reproduce_frequency_functions():
+    """rational_terms' poles and residues give back keldy's frequency functions
+    (omega_functions, model.hpp:94-170) on the real axis to rounding."""
+    w = np.linspace(-5, 5, 11)
+    for bath, dl in (("flatband", False), ("lorentzian", True)):
+        terms = g0_tables.rational_terms(bath, 1.0, 0.3, 0.5, 2.0, dot_lead=dl)
+        of = g0_tables.omega_functions(bath, 1.0, 0.3, 0.5, 20.0, 2.0, w)
+        for blk, idx in (((0, 0), (0, 1)), ((1, 0), (2, 3))):
+            if blk not in terms:
+                continue
+            for kind, oi in zip(("lesser", "greater"), idx):
+                v = np.zeros(len(w), complex)
+                for mu, poles, res in terms[blk]:
+                    R = np.array([np.sum(res / (x - poles)) for x in w])
+                    n = g0_tables._fermi(w - mu, 20.0)
+                    v += n * R if kind == "lesser" else -(1 - n) * R
+                assert np.abs(v - of[oi]).max() < 1e-13, (bath, blk, kind)

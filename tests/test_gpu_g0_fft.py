@@ -118,3 +118,56 @@ def test_lorentzian_bath_tables_and_charge(ctx, oracle):
                                                    k_first=1, n_points=4096)])
     w, onp, ond, sc = oracle.integrate(om, A, B, chain, 2, 4096)
     assert (npts, nd) == (onp, ond) and abs(sm - w) <= 1e-12 * sc
+
+
+@pytest.mark.parametrize("beta", [np.inf, 50.0, 5.0])
+def test_rational_builder_reproduces_flatband_closed_form(ctx, beta):
+    """kb_model_set_rational on the flat band's two-pole terms equals the host's closed-form
+    flat-band tables (g0_tables.flatband: E1 at the poles, quadrature of the Fermi correction)
+    to 1e-10 of the table's maximum, at zero and finite temperature, with bias."""
+    gamma, eps, V, tmax, L = 1.0, 0.4, 0.6, 20.0, 4001
+    terms = g0_tables.rational_terms("flatband", gamma, eps, V, 2.0)
+    m = capi.Model(ctx, tmax, None, None, npts=L)
+    m.set_rational(0, 0, terms[(0, 0)], beta, capi.FT_SYMMETRIC)
+    dl, dg = m.table()
+    _, hl, hg = g0_tables.flatband(gamma, eps, V, beta, tmax, L)
+    scale = max(np.abs(hl).max(), np.abs(hg).max())
+    assert np.abs(dl - hl).max() <= 1e-10 * scale and np.abs(dg - hg).max() <= 1e-10 * scale
+
+
+def test_lorentzian_contour_tables(ctx):
+    """bath_type "lorentzian", ft_method "contour" (model.cpp:326-426) through G0Model: the GPU's
+    closed form equals the CPU restatement (oracle/g0_rational_oracle.py, pinned to direct
+    quadrature in test_g0_fft_oracle.py) on the dot and dot-lead blocks at every mesh point to
+    1e-10 of the table maximum, agrees with keldy's default fft tables of the same model
+    within the fft's discretisation (1e-3 at dw = 0.157), satisfies the sum rule
+    g^<(0) - g^>(0) = i, and the (0, 1) block mirrors the (1, 0) block."""
+    from oracle import g0_rational_oracle
+    p = io.model_param_t(bath_type="lorentzian", ft_method="contour", Gamma=1.0, eps_d=0.3, bias_V=0.5, beta=20.0,
+                         half_bandwidth=2.0, time_max=20.0, nr_time_points_gf=801)
+    g = io.G0Model(p, True)
+    t = g0_tables.time_mesh(20.0, 801)
+    terms = g0_tables.rational_terms("lorentzian", 1.0, 0.3, 0.5, 2.0, dot_lead=True)
+    l00, g00 = g.get_table(0, 0, 0)
+    l10, g10 = g.get_table(0, 1, 0)
+    l01, _ = g.get_table(0, 0, 1)
+    for (a, b), blk in (((l00, g00), (0, 0)), ((l10, g10), (1, 0))):
+        wa, wb = g0_rational_oracle.transform(terms[blk], 20.0, t)
+        scale = max(np.abs(wa).max(), np.abs(wb).max())
+        assert np.abs(a - wa).max() <= 1e-10 * scale and np.abs(b - wb).max() <= 1e-10 * scale, blk
+    c = len(t) // 2
+    assert abs(l00[c] - g00[c] - 1j) < 1e-12
+    np.testing.assert_array_equal(l01, -np.conj(l10[::-1]))
+    gf = io.G0Model(dict(p, ft_method="fft"), True)
+    assert np.abs(gf.get_table(0, 0, 0)[0] - l00).max() < 1e-3
+    assert np.abs(gf.get_table(0, 1, 0)[0] - l10).max() < 1e-3
+
+
+def test_rational_builder_errors(ctx):
+    m = capi.Model(ctx, 5.0, None, None, npts=201)
+    with pytest.raises(capi.KbError, match="off the real axis"):
+        m.set_rational(0, 0, [(0.0, np.array([1.0 + 0j, 1j]), np.array([1.0 + 0j, -1.0 + 0j]))], 10.0)
+    with pytest.raises(capi.KbError, match="beta"):
+        m.set_rational(0, 0, [(0.0, np.array([1j, -1j]), np.array([1.0 + 0j, -1.0 + 0j]))], -1.0)
+    with pytest.raises(capi.KbError, match="1..8 poles"):
+        m.set_rational(0, 0, [(0.0, np.full(9, 1j), np.zeros(9, complex))], 10.0)
