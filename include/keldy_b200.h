@@ -434,6 +434,19 @@ int kb_context_get_launch(kb_context *ctx, int order, int *chunk_points, int *ct
 #define KB_FLOW_PARAMS (KB_FLOW_LAYERS * 3 * KB_FLOW_WIDTH * KB_FLOW_WIDTH)
 /* W1, W2 uniform in +-sqrt(6/128) from mt19937_64(seed), W3 = 0 (identity flow). */
 int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out);
+/* No counterpart in keldy: the second learned first stage, a separable spline flow. Per
+ * dimension d (1..8) a monotone rational-quadratic spline CDF F_d on [0, 1] with 16 bins
+ * (widths and heights from softmaxes of 16 logits each, at least 1e-3; knot derivatives
+ * 1e-3 + softplus of 17 parameters); density q(x) = prod_d F_d'(x_d), sampling
+ * x_d = F_d^{-1}(z_d). Smooth and acting on each axis alone, it keeps the structure that
+ * quasi-Monte Carlo exploits. Same calls as the coupling flow (map, sample, gradient,
+ * train, fit, work items); parameters: kb_flow_num_params = dim * 49 floats, [dim][16 width
+ * logits, 16 height logits, 17 derivative parameters]; created as the identity map. */
+#define KB_FLOW_COUPLING 0
+#define KB_FLOW_SPLINE 1
+int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_flow **out);
+/* Parameters of the flow: KB_FLOW_PARAMS (coupling) or dim * 49 (spline). */
+int kb_flow_num_params(const kb_flow *flow);
 int kb_flow_destroy(kb_flow *flow);
 int kb_flow_dim(const kb_flow *flow);
 int kb_flow_get_params(kb_flow *flow, float *params);

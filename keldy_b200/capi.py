@@ -43,6 +43,7 @@ EXPORTS = [
     "kb_model_set_rational",
     "kb_warper_table_from_samples", "kb_warper_projection_create", "kb_warper_projection_axis",
     "kb_warper_projection_from_integrand", "kb_device_allocations", "kb_integrate_kernel_single_omega",
+    "kb_flow_create_kind", "kb_flow_num_params",
 ]
 FLOW_LAYERS, FLOW_WIDTH, FLOW_MAX_DIM = 6, 128, 8
 FLOW_PARAMS = FLOW_LAYERS * 3 * FLOW_WIDTH * FLOW_WIDTH
@@ -172,6 +173,8 @@ def load():
     L.kb_context_get_launch.argtypes = [_VP, C.c_int, _I, _I]
     _F = C.POINTER(C.c_float)
     L.kb_flow_create.argtypes = [_VP, C.c_int, C.c_uint64, C.POINTER(_VP)]
+    L.kb_flow_create_kind.argtypes = [_VP, C.c_int, C.c_int, C.c_uint64, C.POINTER(_VP)]
+    L.kb_flow_num_params.argtypes = [_VP]
     L.kb_flow_destroy.argtypes = [_VP]
     L.kb_flow_dim.argtypes = [_VP]
     L.kb_flow_get_params.argtypes = [_VP, _F]
@@ -438,8 +441,9 @@ class Context:
         return Model(self, time_max, lesser, greater, alpha, lesser_down, greater_down, blocks)
 
     # --- learned flow ------------------------------------------------------
-    def flow(self, dim, seed=0):
-        return Flow(self, dim, seed)
+    def flow(self, dim, seed=0, kind=0):
+        """A learned warper (kind FLOW_COUPLING or FLOW_SPLINE)."""
+        return Flow(self, dim, seed, kind)
 
 
 class Sobol:
@@ -776,18 +780,27 @@ def train_cfg(epochs=20, batch=16384, lr=2e-3, lr_final=1e-4, beta1=0.9, beta2=0
                         int(seed))
 
 
-class Flow:
-    """Learned coupling-flow warper of dimension `dim` (2..8) on the device: a first
-    stage before the warper chain, trained on |integrand| samples of the plain method
-    (kb_flow_* in include/keldy_b200.h)."""
+FLOW_COUPLING, FLOW_SPLINE = 0, 1
 
-    def __init__(self, ctx, dim, seed=0):
+
+class Flow:
+    """Learned warper of dimension `dim` on the device, a first stage before the warper
+    chain trained on |integrand| samples of the plain method (kb_flow_* in
+    include/keldy_b200.h): kind FLOW_COUPLING (coupling layers with tensor-core MLP
+    conditioners, dim 2..8) or FLOW_SPLINE (separable rational-quadratic splines, dim 1..8)."""
+
+    def __init__(self, ctx, dim, seed=0, kind=FLOW_COUPLING):
         self.ctx = ctx
         self.dim = dim
+        self.kind = kind
         h = _VP()
-        check(ctx.L.kb_flow_create(ctx.h, dim, int(seed), C.byref(h)))
+        check(ctx.L.kb_flow_create_kind(ctx.h, dim, int(kind), int(seed), C.byref(h)))
         self.h = h
+        self.n_params = int(ctx.L.kb_flow_num_params(h))
         ctx._deps.add(self)
+
+    def _pshape(self):
+        return (FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH) if self.kind == FLOW_COUPLING else (self.dim, 49)
 
     def close(self):
         if self.h:
@@ -801,14 +814,14 @@ class Flow:
             pass
 
     def params(self):
-        """float32 [layer][matrix W1, W2, W3][out][in]."""
-        p = np.empty((FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH), dtype=np.float32)
+        """float32 [layer][matrix W1, W2, W3][out][in] (coupling) or [dim][49] (spline)."""
+        p = np.empty(self._pshape(), dtype=np.float32)
         check(self.ctx.L.kb_flow_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
         return p
 
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
-        assert p.size == FLOW_PARAMS
+        assert p.size == self.n_params
         check(self.ctx.L.kb_flow_set_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
 
     def map(self, x, direction):
@@ -838,7 +851,7 @@ class Flow:
         """(loss, grad [layer][matrix][out][in]) of sum w (-log q(x)) / len(x)."""
         x = np.ascontiguousarray(np.atleast_2d(x), dtype=np.float64)
         w = np.ascontiguousarray(w, dtype=np.float64)
-        g = np.empty((FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH), dtype=np.float32)
+        g = np.empty(self._pshape(), dtype=np.float32)
         loss = C.c_double()
         check(self.ctx.L.kb_flow_gradient(self.h, x.shape[0], _dp(x), _dp(w), g.ctypes.data_as(C.POINTER(C.c_float)),
                                           C.byref(loss)))

@@ -739,6 +739,9 @@ cudaError_t launch_flow_map(const FlowDev &f, int direction, long long count, co
                             uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out, double *out2,
                             int *err, int grid, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
+  if (f.kind == FLOW_KIND_SPLINE)
+    return launch_spline_map(f.spline, f.dim, direction, count, in, rng, k_first, k_first_dev, use_sobol, out, out2,
+                             4 * grid, st);
   const long long tiles = (count + NT - 1) / NT;
   if (grid > tiles) grid = (int)tiles;
   const size_t smem = flow_map_smem_bytes();

@@ -52,6 +52,60 @@ int train_grid(const kb_flow *f, long long count) {
   return (int)std::min<long long>(tiles, f->ctx->sm_count);
 }
 
+// CTAs of the spline flow's gradient kernel (256 threads each, grid-stride over the batch).
+int spline_grid(const kb_flow *f, long long count) {
+  return (int)std::max<long long>(1, std::min<long long>((count + 255) / 256, 2LL * f->ctx->sm_count));
+}
+
+// kb_flow_train for the spline flow (the caller holds the context's lock): per step the
+// batch's derivative partials, then the chained gradient and the Adam step, cosine-decayed
+// learning rate as for the coupling flow.
+int spline_train(kb_flow *f, int64_t count, const std::vector<float> &hx, const std::vector<float> &hw,
+                 const kb_flow_train_cfg *cfg, int64_t batch, int64_t per_epoch, int64_t steps, double *loss_hist,
+                 int *n_steps) {
+  kb_context *ctx = f->ctx;
+  cudaStream_t st = ctx->stream;
+  const int N = f->dim;
+  const int sg = spline_grid(f, batch);
+  DevBuf dx, dw, di, dpart, dlp, dhist;
+  KB_CUDA(dx.alloc(hx.size() * sizeof(float), st));
+  KB_CUDA(dw.alloc(hw.size() * sizeof(float), st));
+  KB_CUDA(di.alloc((size_t)count * sizeof(int), st));
+  KB_CUDA(dpart.alloc((size_t)sg * N * spline_grad_per_dim() * sizeof(double), st));
+  KB_CUDA(dlp.alloc((size_t)sg * sizeof(double), st));
+  KB_CUDA(dhist.alloc((size_t)steps * sizeof(double), st));
+  KB_CUDA(cudaMemcpyAsync(dx.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  KB_CUDA(cudaMemcpyAsync(dw.p, hw.data(), hw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  std::vector<int> perm((size_t)count);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::mt19937_64 shuffler(cfg->seed);
+  const double pi = 3.14159265358979323846;
+  int64_t s = 0;
+  for (int ep = 0; ep < cfg->epochs; ++ep) {
+    std::shuffle(perm.begin(), perm.end(), shuffler);
+    KB_CUDA(cudaStreamSynchronize(st)); // the previous epoch's steps read the old order
+    KB_CUDA(cudaMemcpyAsync(di.p, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    for (int64_t b = 0; b < per_epoch; ++b, ++s) {
+      KB_CUDA(launch_spline_grad(f->master, N, batch, dx.as<float>(), dw.as<float>(), di.as<int>() + b * batch,
+                                 1.0f / (float)batch, dpart.as<double>(), dlp.as<double>(), sg, st));
+      const int64_t t = ++f->adam_step;
+      const double lr = cfg->lr_final + 0.5 * (cfg->lr - cfg->lr_final) * (1.0 + std::cos(pi * (double)s / (double)steps));
+      const float bc1 = (float)(1.0 - std::pow((double)cfg->beta1, (double)t));
+      const float bc2 = (float)(1.0 - std::pow((double)cfg->beta2, (double)t));
+      KB_CUDA(launch_spline_adam(f->master, f->adam_m, f->adam_v, N, dpart.as<double>(), sg, dlp.as<double>(),
+                                 dhist.as<double>() + s, nullptr, (float)lr, cfg->beta1, cfg->beta2, cfg->eps, bc1, bc2,
+                                 st));
+    }
+  }
+  std::vector<double> hist((size_t)steps);
+  KB_CUDA(cudaMemcpyAsync(hist.data(), dhist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  KB_CUDA(cudaStreamSynchronize(st));
+  if (loss_hist)
+    for (int64_t i = 0; i < steps; ++i) loss_hist[i] = hist[(size_t)i];
+  if (n_steps) *n_steps = (int)steps;
+  return KB_OK;
+}
+
 } // namespace
 
 extern "C" {
@@ -100,6 +154,50 @@ int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out) {
   return KB_OK;
 }
 
+int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_flow **out) {
+  if (kind == KB_FLOW_COUPLING) return kb_flow_create(ctx, dim, seed, out);
+  KB_CHECK(ctx && out, "kb_flow_create_kind: null argument");
+  KB_CHECK(kind == KB_FLOW_SPLINE, "flow kind must be KB_FLOW_COUPLING or KB_FLOW_SPLINE");
+  KB_CHECK(dim >= 1 && dim <= FLOW_MAX_DIM, "flow dimension must be in [1, 8]");
+  // identity map: equal bins, knot derivatives 1 (softplus(c) = 1 - SPL_MIN_DERIV)
+  std::vector<float> init((size_t)FLOW_NPARAM, 0.0f);
+  const float c0 = (float)std::log(std::expm1(1.0 - SPL_MIN_DERIV));
+  for (int d = 0; d < dim; ++d)
+    for (int k = 0; k <= SPL_BINS; ++k) init[(size_t)d * SPL_PER_DIM + 2 * SPL_BINS + k] = c0;
+  (void)seed;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  KB_CUDA(cudaSetDevice(ctx->device));
+  auto *f = new kb_flow;
+  f->ctx = ctx;
+  f->device = ctx->device;
+  f->dim = dim;
+  f->layout.kind = FLOW_KIND_SPLINE;
+  f->layout.dim = dim;
+  const size_t nb = (size_t)FLOW_NPARAM * sizeof(float);
+  cudaError_t e = device_malloc(&f->master, nb);
+  if (e == cudaSuccess) e = device_malloc(&f->adam_m, nb);
+  if (e == cudaSuccess) e = device_malloc(&f->adam_v, nb);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(f->master, init.data(), nb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_m, 0, nb, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_v, 0, nb, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFree(f->master);
+    cudaFree(f->adam_m);
+    cudaFree(f->adam_v);
+    delete f;
+    return fail(KB_E_CUDA, std::string("kb_flow_create_kind: ") + cudaGetErrorString(e));
+  }
+  f->layout.spline = f->master;
+  *out = f;
+  return KB_OK;
+}
+
+int kb_flow_num_params(const kb_flow *f) {
+  if (!f) return 0;
+  return f->layout.kind == FLOW_KIND_SPLINE ? f->dim * SPL_PER_DIM : FLOW_NPARAM;
+}
+
 int kb_flow_destroy(kb_flow *f) {
   if (!f) return KB_OK;
   cudaSetDevice(f->device);
@@ -115,6 +213,14 @@ int kb_flow_dim(const kb_flow *f) { return f ? f->dim : 0; }
 
 int kb_flow_get_params(kb_flow *f, float *params) {
   KB_CHECK(f && params, "kb_flow_get_params: null argument");
+  if (f->layout.kind == FLOW_KIND_SPLINE) {
+    std::lock_guard<std::mutex> lk(f->ctx->mu);
+    KB_CUDA(cudaSetDevice(f->device));
+    KB_CUDA(cudaMemcpyAsync(params, f->master, (size_t)kb_flow_num_params(f) * sizeof(float), cudaMemcpyDeviceToHost,
+                            f->ctx->stream));
+    KB_CUDA(cudaStreamSynchronize(f->ctx->stream));
+    return KB_OK;
+  }
   std::vector<float> inr((size_t)FLOW_NPARAM);
   std::lock_guard<std::mutex> lk(f->ctx->mu);
   KB_CUDA(cudaSetDevice(f->device));
@@ -127,8 +233,20 @@ int kb_flow_get_params(kb_flow *f, float *params) {
 // Resets the Adam moments: new weights start a new optimisation.
 int kb_flow_set_params(kb_flow *f, const float *params) {
   KB_CHECK(f && params, "kb_flow_set_params: null argument");
-  for (int i = 0; i < FLOW_NPARAM; ++i)
+  for (int i = 0; i < kb_flow_num_params(f); ++i)
     if (!std::isfinite(params[i])) return fail(KB_E_INVALID, "flow parameters must be finite");
+  if (f->layout.kind == FLOW_KIND_SPLINE) {
+    std::lock_guard<std::mutex> lk(f->ctx->mu);
+    KB_CUDA(cudaSetDevice(f->device));
+    cudaStream_t st = f->ctx->stream;
+    const size_t nb = (size_t)kb_flow_num_params(f) * sizeof(float);
+    KB_CUDA(cudaMemcpyAsync(f->master, params, nb, cudaMemcpyHostToDevice, st));
+    KB_CUDA(cudaMemsetAsync(f->adam_m, 0, nb, st));
+    KB_CUDA(cudaMemsetAsync(f->adam_v, 0, nb, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    f->adam_step = 0;
+    return KB_OK;
+  }
   std::vector<float> inr((size_t)FLOW_NPARAM);
   api_to_internal(params, inr.data());
   std::lock_guard<std::mutex> lk(f->ctx->mu);
@@ -213,6 +331,30 @@ int kb_flow_gradient(kb_flow *f, int64_t count, const double *x, const double *w
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
+  if (f->layout.kind == FLOW_KIND_SPLINE) {
+    const int sg = spline_grid(f, count);
+    DevBuf dx, dw, di, dpart, dlp, dloss, dgrad;
+    KB_CUDA(dx.alloc(hx.size() * sizeof(float), st));
+    KB_CUDA(dw.alloc(hw.size() * sizeof(float), st));
+    KB_CUDA(di.alloc(idx.size() * sizeof(int), st));
+    KB_CUDA(dpart.alloc((size_t)sg * N * spline_grad_per_dim() * sizeof(double), st));
+    KB_CUDA(dlp.alloc((size_t)sg * sizeof(double), st));
+    KB_CUDA(dloss.alloc(sizeof(double), st));
+    KB_CUDA(dgrad.alloc((size_t)kb_flow_num_params(f) * sizeof(float), st));
+    KB_CUDA(cudaMemcpyAsync(dx.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    KB_CUDA(cudaMemcpyAsync(dw.p, hw.data(), hw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+    KB_CUDA(cudaMemcpyAsync(di.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    KB_CUDA(launch_spline_grad(f->master, N, count, dx.as<float>(), dw.as<float>(), di.as<int>(), 1.0f / (float)count,
+                               dpart.as<double>(), dlp.as<double>(), sg, st));
+    KB_CUDA(launch_spline_adam(f->master, f->adam_m, f->adam_v, N, dpart.as<double>(), sg, dlp.as<double>(),
+                               dloss.as<double>(), dgrad.as<float>(), 0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, st));
+    double lsum = 0.0;
+    KB_CUDA(cudaMemcpyAsync(grad, dgrad.p, (size_t)kb_flow_num_params(f) * sizeof(float), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaMemcpyAsync(&lsum, dloss.p, sizeof(double), cudaMemcpyDeviceToHost, st));
+    KB_CUDA(cudaStreamSynchronize(st));
+    if (loss) *loss = lsum;
+    return KB_OK;
+  }
   const int grid = train_grid(f, count);
   DevBuf dx, dw, di, dpart, dloss, dxs, dgrad;
   KB_CUDA(dx.alloc(hx.size() * sizeof(float), st));
@@ -274,6 +416,8 @@ int kb_flow_train(kb_flow *f, int64_t count, const double *x, const double *w, c
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
+  if (f->layout.kind == FLOW_KIND_SPLINE) return spline_train(f, count, hx, hw, cfg, batch, per_epoch, steps, loss_hist,
+                                                               n_steps);
   const int grid = train_grid(f, batch);
   DevBuf dx, dw, di, dpart, dlp, dxs, dhist;
   KB_CUDA(dx.alloc(hx.size() * sizeof(float), st));

@@ -36,7 +36,20 @@ __host__ __device__ inline int flow_img_index(int r, int k) {
   return (r >> 3) * 1024 + (k >> 3) * 64 + (r & 7) * 8 + (k & 7);
 }
 
+// The separable spline flow (flow_spline.cu): per dimension a rational-quadratic spline CDF
+// of SPL_BINS bins, SPL_PER_DIM parameters (width logits, height logits, knot-derivative
+// pre-activations); bins at least SPL_MIN_BIN wide and high, knot derivatives at least
+// SPL_MIN_DERIV.
+constexpr int FLOW_KIND_COUPLING = 0;
+constexpr int FLOW_KIND_SPLINE = 1;
+constexpr int SPL_BINS = 16;
+constexpr int SPL_PER_DIM = 3 * SPL_BINS + 1;
+constexpr double SPL_MIN_BIN = 1e-3;
+constexpr double SPL_MIN_DERIV = 1e-3;
+
 struct FlowDev {
+  int kind;            // FLOW_KIND_*
+  const float *spline; // FLOW_KIND_SPLINE: [dim][SPL_PER_DIM] parameters
   const uint16_t *img; // [FLOW_NMAT][FLOW_MAT] bf16 bit patterns, image layout
   int dim;
   int ntr[FLOW_LAYERS];              // number of transformed dims
@@ -70,5 +83,20 @@ cudaError_t launch_flow_adam(float *master, float *m, float *v, uint16_t *img, c
                              float bc1, float bc2, cudaStream_t st);
 // bf16 images from the fp32 master weights.
 cudaError_t launch_flow_pack(const float *master, uint16_t *img, cudaStream_t st);
+
+// Spline flow: the maps (as launch_flow_map), the per-CTA loss and derivative partials of a
+// batch ([grid][dim * spline_grad_per_dim()] and [grid], fp64), and the step that sums them
+// in CTA order, chains them to the parameters (grad_out, optional) and, with lr > 0, takes
+// the Adam step.
+cudaError_t launch_spline_map(const float *params, int dim, int direction, long long count, const double *in,
+                              SobolDev rng, uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out,
+                              double *out2, int grid, cudaStream_t st);
+int spline_grad_per_dim();
+cudaError_t launch_spline_grad(const float *params, int dim, long long count, const float *x, const float *w,
+                               const int *index, float inv_batch, double *partials, double *loss_part, int grid,
+                               cudaStream_t st);
+cudaError_t launch_spline_adam(float *params, float *m, float *v, int dim, const double *partials, int nparts,
+                               const double *loss_part, double *loss_out, float *grad_out, float lr, float beta1,
+                               float beta2, float eps, float bc1, float bc2, cudaStream_t st);
 
 } // namespace kb

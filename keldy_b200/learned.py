@@ -16,14 +16,16 @@ import numpy as np
 from . import capi, rqmc
 
 DEFAULT_TRAIN = dict(epochs=10, batch=8192, lr=2e-3, lr_final=1e-4)
+# the separable spline flow has ~50 parameters per dimension: larger steps, more epochs
+SPLINE_TRAIN = dict(epochs=20, batch=8192, lr=2e-2, lr_final=1e-3)
 
 
-def fit(ctx, model, A, B, chain, order, n_samples=1 << 18, seed=0, k_first=1, **cfg):
-    """Creates and trains a flow of dimension `order` on n_samples plain-method points.
-    Returns (flow, seconds, final loss)."""
-    c = dict(DEFAULT_TRAIN, **cfg)
+def fit(ctx, model, A, B, chain, order, n_samples=1 << 18, seed=0, k_first=1, kind=capi.FLOW_COUPLING, **cfg):
+    """Creates and trains a flow (kind FLOW_COUPLING or FLOW_SPLINE) of dimension `order` on
+    n_samples plain-method points. Returns (flow, seconds, final loss)."""
+    c = dict(SPLINE_TRAIN if kind == capi.FLOW_SPLINE else DEFAULT_TRAIN, **cfg)
     c.setdefault("seed", seed)
-    flow = ctx.flow(order, seed=seed)
+    flow = ctx.flow(order, seed=seed, kind=kind)
     ctx.synchronize()
     t0 = time.perf_counter()
     loss = flow.fit(model, A, B, chain, ctx.sobol(order), n_samples, k_first=k_first, **c)
