@@ -327,27 +327,57 @@ __device__ void pipe_finish(Pipe &P, uint32_t ncols, int *err) {
 }
 
 // ------------------------------------------------------------ sampling / density map
+// Two CTAs per SM, each with one activation buffer and two weight slots: while one CTA runs
+// its epilogues (ReLU, the CDF of the logits) on the CUDA cores, the other's products run on
+// the tensor core. The CTA's products are numbered q = 0, 1, ... over its tiles (18 per
+// tile: three per layer); product q reads weight slot q & 1, which is refilled with the
+// matrix of product q + 2 as soon as product q completes. Each epilogue writes its output
+// over the activation buffer the product just read (the product has completed).
 template <int DIR>
-__global__ void __launch_bounds__(NT, 1)
+__global__ void __launch_bounds__(NT, 2)
     flow_map_kernel(FlowDev f, long long count, const double *in, SobolDev rng, uint32_t k_first,
                     const uint32_t *k_first_dev, int use_sobol, double *out, double *out2, int *err) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char *base = aligned_smem(smem_raw);
-  unsigned char *act = base + 3 * MAT_BYTES;
-  SmemHead *head;
+  unsigned char *act = base + 2 * MAT_BYTES;
+  SmemHead *head = reinterpret_cast<SmemHead *>(base + 3 * MAT_BYTES);
   Pipe P;
-  pipe_init(P, base, 2, head, f.img, 128);
+  P.sW = su32(base);
+  P.sA = P.sW + 2 * MAT_BYTES;
+  P.mbar = su32(&head->bars[0]);
+  for (int j = 0; j < 3; ++j) {
+    P.wbar[j] = su32(&head->bars[1 + j]);
+    P.wphase[j] = 0;
+    P.pending[j] = 0;
+  }
+  P.mphase = 0;
+  P.img = f.img;
+  if (threadIdx.x == 0) {
+    mbar_init(P.mbar, 1);
+    for (int j = 0; j < 2; ++j) mbar_init(P.wbar[j], 1);
+    mbar_init_fence();
+  }
+  if (threadIdx.x < 32) tmem_alloc(su32(&head->tmem_slot), 128);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  P.tmem = head->tmem_slot;
   const int t = threadIdx.x, warp = t >> 5;
   const uint32_t trow = P.tmem + ((uint32_t)(warp * 32) << 16);
   const long long ntiles = (count + NT - 1) / NT;
+  const long long my_tiles = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const long long nq = my_tiles * 3 * FLOW_LAYERS;
   const int N = f.dim;
   if (k_first_dev) k_first = *k_first_dev;
   auto layer_at = [](int i) { return DIR == 0 ? i : FLOW_LAYERS - 1 - i; };
-  if (t == 0 && blockIdx.x < ntiles)
-    for (int j = 0; j < 3; ++j) load_weight(P, j, 3 * layer_at(0) + j);
+  // weight matrix read by product q
+  auto mat_of = [&](long long q) { return 3 * layer_at((int)((q / 3) % FLOW_LAYERS)) + (int)(q % 3); };
+  if (t == 0)
+    for (int j = 0; j < 2 && j < nq; ++j) load_weight(P, j, mat_of(j));
+  long long q = 0;
   bool ok = true;
+  Mma none = {};
   for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const bool more = tile + gridDim.x < ntiles;
     const long long p = tile * NT + t;
     const bool valid = p < count;
     double x[FLOW_MAX_DIM];
@@ -360,12 +390,19 @@ __global__ void __launch_bounds__(NT, 1)
     double acc = DIR == 0 ? 0.0 : 1.0;
     for (int li = 0; li < FLOW_LAYERS && ok; ++li) {
       const int l = layer_at(li);
-      const int next = li + 1 < FLOW_LAYERS ? layer_at(li + 1) : (more ? layer_at(0) : -1);
       float xf[FLOW_MAX_DIM];
 #pragma unroll
       for (int d = 0; d < FLOW_MAX_DIM; ++d) xf[d] = (float)x[d];
       encode_row(f, l, xf, act, t);
-      ok = conditioner(P, act, 0, next, trow);
+      // the layer's three products: features -> h1 -> h2 -> logits, all in one buffer
+      for (int j = 0; j < 3 && ok; ++j, ++q) {
+        const int slot = (int)(q & 1);
+        Mma m = {P.tmem, act_addr(P, 0), w_addr(P, slot), 0, 0, 0};
+        ok = mma_step(P, slot, m, none, 1);
+        if (!ok) break;
+        if (t == 0 && q + 2 < nq) load_weight(P, slot, mat_of(q + 2));
+        if (j < 2) epi_relu(trow, act, t);
+      }
       if (!ok) break;
 #pragma unroll
       for (int s = 0; s < FLOW_SLOTS; ++s) {
@@ -721,7 +758,7 @@ void flow_layout(int dim, FlowDev &f) {
   }
 }
 
-size_t flow_map_smem_bytes() { return 5 * (size_t)MAT_BYTES + sizeof(SmemHead) + 1024; }
+size_t flow_map_smem_bytes() { return 3 * (size_t)MAT_BYTES + sizeof(SmemHead) + 1024; }
 size_t flow_train_smem_bytes() { return 6 * (size_t)MAT_BYTES + sizeof(SmemHead) + 1024; }
 
 cudaError_t flow_configure() {
@@ -742,6 +779,7 @@ cudaError_t launch_flow_map(const FlowDev &f, int direction, long long count, co
   if (f.kind == FLOW_KIND_SPLINE)
     return launch_spline_map(f.spline, f.dim, direction, count, in, rng, k_first, k_first_dev, use_sobol, out, out2,
                              4 * grid, st);
+  grid *= 2; // two resident CTAs per SM (grid is given as the SM count)
   const long long tiles = (count + NT - 1) / NT;
   if (grid > tiles) grid = (int)tiles;
   const size_t smem = flow_map_smem_bytes();

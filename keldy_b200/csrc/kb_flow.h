@@ -64,7 +64,8 @@ cudaError_t flow_configure();
 
 // direction 0: x -> z with log q(x) in out2; direction 1: z -> x with dx/dz in out2.
 // Inputs from `in` ([count][dim]) or, with use_sobol, Sobol points k_first.. of rng
-// (k_first read from k_first_dev when that is not null: graph-captured launches).
+// (k_first read from k_first_dev when that is not null: graph-captured launches). grid:
+// the SM count (the coupling flow runs two CTAs per SM).
 cudaError_t launch_flow_map(const FlowDev &f, int direction, long long count, const double *in, SobolDev rng,
                             uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out, double *out2,
                             int *err, int grid, cudaStream_t st);
