@@ -87,7 +87,7 @@ int spline_train(kb_flow *f, int64_t count, const std::vector<float> &hx, const 
     KB_CUDA(cudaMemcpyAsync(di.p, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     for (int64_t b = 0; b < per_epoch; ++b, ++s) {
       KB_CUDA(launch_spline_grad(f->master, N, batch, dx.as<float>(), dw.as<float>(), di.as<int>() + b * batch,
-                                 1.0f / (float)batch, dpart.as<double>(), dlp.as<double>(), sg, st));
+                                 1.0 / (double)batch, dpart.as<double>(), dlp.as<double>(), sg, st));
       const int64_t t = ++f->adam_step;
       const double lr = cfg->lr_final + 0.5 * (cfg->lr - cfg->lr_final) * (1.0 + std::cos(pi * (double)s / (double)steps));
       const float bc1 = (float)(1.0 - std::pow((double)cfg->beta1, (double)t));
@@ -344,7 +344,7 @@ int kb_flow_gradient(kb_flow *f, int64_t count, const double *x, const double *w
     KB_CUDA(cudaMemcpyAsync(dx.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     KB_CUDA(cudaMemcpyAsync(dw.p, hw.data(), hw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     KB_CUDA(cudaMemcpyAsync(di.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    KB_CUDA(launch_spline_grad(f->master, N, count, dx.as<float>(), dw.as<float>(), di.as<int>(), 1.0f / (float)count,
+    KB_CUDA(launch_spline_grad(f->master, N, count, dx.as<float>(), dw.as<float>(), di.as<int>(), 1.0 / (double)count,
                                dpart.as<double>(), dlp.as<double>(), sg, st));
     KB_CUDA(launch_spline_adam(f->master, f->adam_m, f->adam_v, N, dpart.as<double>(), sg, dlp.as<double>(),
                                dloss.as<double>(), dgrad.as<float>(), 0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, st));

@@ -123,7 +123,7 @@ __global__ void spline_map_kernel(const float *params, int dim, long long count,
 // (w_j, x_j, h_j, delta_k); wn_i = w[index[i]] * inv_batch. partials [grid][dim * G_PER_DIM],
 // loss_part [grid]. Samples in fp32 as the coupling flow's training takes them.
 __global__ void spline_grad_kernel(const float *params, int dim, long long count, const float *x, const float *w,
-                                   const int *index, float inv_batch, double *partials, double *loss_part) {
+                                   const int *index, double inv_batch, double *partials, double *loss_part) {
   __shared__ Knots K[FLOW_MAX_DIM];
   __shared__ double G[FLOW_MAX_DIM * G_PER_DIM];
   __shared__ double sloss;
@@ -135,7 +135,7 @@ __global__ void spline_grad_kernel(const float *params, int dim, long long count
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < count;
        p += (long long)gridDim.x * blockDim.x) {
     const long long src = index[p];
-    const double wn = (double)w[src] * (double)inv_batch;
+    const double wn = (double)w[src] * inv_batch;
     if (wn == 0.0) continue;
     for (int d = 0; d < dim; ++d) {
       const Knots &k = K[d];
@@ -250,7 +250,7 @@ cudaError_t launch_spline_map(const float *params, int dim, int direction, long 
 int spline_grad_per_dim() { return G_PER_DIM; }
 
 cudaError_t launch_spline_grad(const float *params, int dim, long long count, const float *x, const float *w,
-                               const int *index, float inv_batch, double *partials, double *loss_part, int grid,
+                               const int *index, double inv_batch, double *partials, double *loss_part, int grid,
                                cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   spline_grad_kernel<<<grid, 256, 0, st>>>(params, dim, count, x, w, index, inv_batch, partials, loss_part);

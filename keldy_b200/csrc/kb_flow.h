@@ -94,7 +94,7 @@ cudaError_t launch_spline_map(const float *params, int dim, int direction, long 
                               double *out2, int grid, cudaStream_t st);
 int spline_grad_per_dim();
 cudaError_t launch_spline_grad(const float *params, int dim, long long count, const float *x, const float *w,
-                               const int *index, float inv_batch, double *partials, double *loss_part, int grid,
+                               const int *index, double inv_batch, double *partials, double *loss_part, int grid,
                                cudaStream_t st);
 cudaError_t launch_spline_adam(float *params, float *m, float *v, int dim, const double *partials, int nparts,
                                const double *loss_part, double *loss_out, float *grad_out, float lr, float beta1,

@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 @pytest.mark.parametrize("L", [3, 2001, 10001])
 def test_transform_vs_oracle(ctx, L):
     """Random frequency values with 1/w^2 tails: the GPU table equals numpy's FFT of the same
-    sum within 1e-12 of the table's largest value; the mirror block is -conj(g(-t))."""
+    sum within 1e-11 of the table's largest value (the direct sum of L terms and the FFT
+    round differently, ~sqrt(L) ulps); the mirror block is -conj(g(-t))."""
     rng = np.random.default_rng(L)
     w = g0_tables.adjoint_frequencies(7.0, L)
     gl = (rng.normal(size=L) + 1j * rng.normal(size=L)) / (1.0 + w * w)
@@ -23,8 +24,8 @@ def test_transform_vs_oracle(ctx, L):
     m.set_fft(1, 0, gl, gg, capi.FT_MIRROR)
     dl, dg = m.table(0, 1, 0)
     wl, wg = g0_fft_oracle.transform(gl, 7.0), g0_fft_oracle.transform(gg, 7.0)
-    assert np.abs(dl - wl).max() <= 1e-12 * np.abs(wl).max()
-    assert np.abs(dg - wg).max() <= 1e-12 * np.abs(wg).max()
+    assert np.abs(dl - wl).max() <= 1e-11 * np.abs(wl).max()
+    assert np.abs(dg - wg).max() <= 1e-11 * np.abs(wg).max()
     l01, _ = m.table(0, 0, 1)
     np.testing.assert_array_equal(l01, -np.conj(dl[::-1]))
 
@@ -140,7 +141,9 @@ def test_lorentzian_contour_tables(ctx):
     closed form equals the CPU restatement (oracle/g0_rational_oracle.py, pinned to direct
     quadrature in test_g0_fft_oracle.py) on the dot and dot-lead blocks at every mesh point to
     1e-10 of the table maximum, agrees with keldy's default fft tables of the same model
-    within the fft's discretisation (1e-3 at dw = 0.157), satisfies the sum rule
+    within the fft's discretisation (2e-4 with the fft on a five times wider window, the same
+    time step: the fft's table is periodic in t with the window's length, so near the edges
+    of a window as short as the decay of g it aliases), satisfies the sum rule
     g^<(0) - g^>(0) = i, and the (0, 1) block mirrors the (1, 0) block."""
     from oracle import g0_rational_oracle
     p = io.model_param_t(bath_type="lorentzian", ft_method="contour", Gamma=1.0, eps_d=0.3, bias_V=0.5, beta=20.0,
@@ -158,9 +161,10 @@ def test_lorentzian_contour_tables(ctx):
     c = len(t) // 2
     assert abs(l00[c] - g00[c] - 1j) < 1e-12
     np.testing.assert_array_equal(l01, -np.conj(l10[::-1]))
-    gf = io.G0Model(dict(p, ft_method="fft"), True)
-    assert np.abs(gf.get_table(0, 0, 0)[0] - l00).max() < 1e-3
-    assert np.abs(gf.get_table(0, 1, 0)[0] - l10).max() < 1e-3
+    gf = io.G0Model(dict(p, ft_method="fft", time_max=100.0, nr_time_points_gf=4001), True)
+    sl = slice(1600, 2401)  # t in [-20, 20] on the wider mesh (same step 0.05)
+    assert np.abs(gf.get_table(0, 0, 0)[0][sl] - l00).max() < 2e-4
+    assert np.abs(gf.get_table(0, 1, 0)[0][sl] - l10).max() < 2e-4
 
 
 def test_rational_builder_errors(ctx):
