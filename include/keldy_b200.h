@@ -379,13 +379,13 @@ int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_ind
  * KB_NOALLOC_MAX_ITEMS work items and KB_NOALLOC_MAX_CHUNKS scheduling chunks per call
  * (8,388,608 points with the default 128-point chunks; KB_E_INVALID beyond). The chunk
  * size and CTAs per SM are the context's launch shape (kb_context_set_launch), as in
- * kb_integrate; the tree grid is also capped at the per-CTA slots the array holds (348,
- * more than the 296 resident CTAs of a B200). All calls share the array: calls that overlap on
+ * kb_integrate; the tree grid is also capped at the per-CTA slots the array holds (more
+ * than the 592 resident CTAs of a B200). All calls share the array: calls that overlap on
  * the GPU race. The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress); make it before any stream capture. */
 #define KB_NOALLOC_MAX_ITEMS 64
 #define KB_NOALLOC_MAX_CHUNKS 65536
-#define KB_NOALLOC_SCRATCH_BYTES (32u << 20)
+#define KB_NOALLOC_SCRATCH_BYTES (40u << 20)
 int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc);
 
 /* Number of device allocations (cudaMalloc and stream-ordered pool allocations) the

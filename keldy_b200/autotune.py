@@ -13,12 +13,14 @@ import os
 from . import capi
 
 CHUNKS = (32, 64, 128)
-CTAS = (1, 2)
+CTAS = (2, 4)
 
 
 def _points(order):
-    return {1: 1 << 18, 2: 1 << 18, 3: 1 << 17, 4: 1 << 17, 5: 1 << 16, 6: 1 << 16, 7: 1 << 15, 8: 1 << 15,
-            9: 1 << 14, 10: 1 << 13, 11: 1 << 12, 12: 1 << 11}.get(order, 1 << 10)
+    """Points of a tuning run: enough for several 128-point chunks per resident CTA (a B200
+    holds 592) up to order 8, so that a small run does not favour small chunks; fewer at
+    the costly high orders."""
+    return {9: 1 << 18, 10: 1 << 17, 11: 1 << 16, 12: 1 << 15}.get(order, 1 << 19 if order <= 8 else 1 << 14)
 
 
 def cache_path(ctx):

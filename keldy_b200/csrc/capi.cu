@@ -74,7 +74,7 @@ int kb_context_create(int device, kb_context **out) {
     return fail(KB_E_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
   }
   // Persistent tree kernel: as many CTAs as fit on the device at once.
-  int per_sm = 2;
+  int per_sm = 4;
   ctx->tree_grid = ctx->sm_count * per_sm;
   *out = ctx;
   return KB_OK;
@@ -1716,7 +1716,7 @@ int kb_context_set_launch(kb_context *ctx, int order, int chunk_points, int ctas
   KB_CHECK(ctx, "null context");
   KB_CHECK(order == -1 || (order >= 0 && order <= MAX_ORDER), "order must be -1 or in [0, 16]");
   KB_CHECK(chunk_points >= 1 && chunk_points <= CHUNK_POINTS, "chunk_points must be in [1, 128]");
-  KB_CHECK(ctas_per_sm >= 0 && ctas_per_sm <= 2, "ctas_per_sm must be 0 (keep), 1 or 2");
+  KB_CHECK(ctas_per_sm >= 0 && ctas_per_sm <= 4, "ctas_per_sm must be 0 (keep) or 1..4");
   std::lock_guard<std::mutex> lk(ctx->mu);
   for (int n = 0; n <= MAX_ORDER; ++n)
     if (order == -1 || order == n) ctx->chunk_points[n] = chunk_points;
@@ -1784,7 +1784,7 @@ constexpr size_t NOALLOC_PTS_OFF =
 constexpr size_t NOALLOC_PTS_SLOTS = (KB_NOALLOC_SCRATCH_BYTES - NOALLOC_PTS_OFF) / (PTS_SLOT * sizeof(double));
 // one set-up slot per resident tree CTA of a 148-SM B200 at the most CTAs per SM the
 // launch shape allows; a device with more SMs runs the tree with a grid capped at the slots
-constexpr size_t NOALLOC_B200_TREE_CTAS = 148 * 2;
+constexpr size_t NOALLOC_B200_TREE_CTAS = 148 * 4;
 static_assert(NOALLOC_PTS_SLOTS >= NOALLOC_B200_TREE_CTAS, "scratch too small for one set-up slot per resident CTA");
 
 static __device__ __align__(256) unsigned char kb_noalloc_scratch[KB_NOALLOC_SCRATCH_BYTES];

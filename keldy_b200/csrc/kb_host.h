@@ -92,7 +92,7 @@ struct kb_context {
   int tree_grid = 0;
   int *d_err = nullptr; // error flags written by kernels
   int chunk_points[kb::MAX_ORDER + 1]; // scheduling chunk of each order (autotuned; default 128)
-  int ctas_per_sm = 2;                 // resident tree CTAs per SM
+  int ctas_per_sm = 4;                 // resident tree CTAs per SM
   bool timing = false;
   cudaEvent_t ev[4] = {};
   double last_ms[3] = {0, 0, 0};

@@ -29,7 +29,10 @@ constexpr int CHUNK_POINTS = 128; // points per scheduling chunk (<= 128: two 64
 // when its value is added, 2 bin when only counted, -1 when dropped) and its f*J (re,
 // im)), then G_STAGE complex entries of staged G matrices (a G-batch, tree_gbatch).
 constexpr int PTS_ROWS = CHUNK_POINTS * (MAX_ORDER + 5);
-constexpr int G_STAGE = 4096;
+constexpr int G_STAGE = 2048;
+// Frontier entries at the start of a buffer that the tree's fused bottom uses for its
+// per-point sums (CTA_THREADS double2 and CTA_THREADS / 2 double2 of doubles).
+constexpr int BOTTOM_SCRATCH = CTA_THREADS + CTA_THREADS / 2;
 constexpr int PTS_SLOT = PTS_ROWS + 2 * G_STAGE;
 static_assert(PTS_ROWS % 2 == 0 && PTS_SLOT % 2 == 0, "staged G on 16-byte boundaries");
 
@@ -44,6 +47,12 @@ __host__ __device__ inline int tree_gbatch(int N) {
   if (G_STAGE / (M * M) < g) g = G_STAGE / (M * M);
   g -= g % P;
   return g > 0 ? g : P;
+}
+
+// Orders whose G-batch is a single sub-batch (1..4) gain nothing from staging G in global
+// memory: the tree kernel builds their G directly in shared memory.
+__host__ __device__ inline bool tree_direct(int N) {
+  return N <= TREE_MAX_SUB && tree_gbatch(N) <= tree_points_per_chunk(N);
 }
 
 struct Launch {
@@ -122,7 +131,7 @@ __host__ __device__ inline int tree_root_buffer(int N) {
     if (use[t & 1] < nodes * m * m) use[t & 1] = nodes * m * m;
   }
   for (int b = 0; b < 2; ++b)
-    if (use[b] + root <= FRONTIER && root + 384 <= FRONTIER) return b;
+    if (use[b] + root <= FRONTIER && root + BOTTOM_SCRATCH <= FRONTIER) return b;
   return -1;
 }
 

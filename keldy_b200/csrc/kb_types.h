@@ -8,8 +8,8 @@ namespace kb {
 
 constexpr int MAX_ORDER = 16;      // 2^16 Keldysh configurations per point
 constexpr int SOBOL_COLS = 31;     // columns of the generating matrices (log_max_points <= 31)
-constexpr int CTA_THREADS = 128;   // threads per CTA of the tree kernel
-constexpr int TREE_MAX_SUB = 9;    // largest order solved breadth-first in one pass
+constexpr int CTA_THREADS = 128;   // threads per CTA of the tree kernel (four CTAs per SM)
+constexpr int TREE_MAX_SUB = 8;    // largest order solved breadth-first in one pass
 
 // g0 tables of one model on the device: per mesh point {lesser.re, lesser.im,
 // greater.re, greater.im} (32 bytes), one array per (spin, orbital a, orbital b); null
@@ -129,25 +129,27 @@ struct FallbackDev {
   int64_t index; // point offset within the item
 };
 
-// Points per CTA chunk of the tree kernel for each order (shared-memory budget of two
-// 51.2 KB frontier buffers; see tree_smem_bytes()).
+// Points per sub-batch of the tree kernel for each order: the widest breadth-first level
+// fits a frontier buffer, and the fused bottom's nodes (9x9: eight threads each, 7x7: four)
+// fit the CTA's 128 threads (16 nodes of 9x9 for orders 5..8, up to 32 of 7x7 for 3 and 4).
 __host__ __device__ inline int tree_points_per_chunk(int n) {
   switch (n) {
   case 0: return 128;
   case 1: return 128;
-  case 2: return 128;
-  case 3: return 64;
-  case 4: return 32;
-  case 5: return 16;
-  case 6: return 8;
-  case 7: return 4;
-  case 8: return 2;
+  case 2: return 32;
+  case 3: return 16;
+  case 4: return 8;
+  case 5: return 8;
+  case 6: return 4;
+  case 7: return 2;
+  case 8: return 1;
   default: return 1;
   }
 }
 
 // Complex entries per frontier buffer: enough for the widest breadth-first level of
-// every order (P * max_k 2^k (2(R-k)+1)^2 = 3200 for every P, R pair above).
-constexpr int FRONTIER = 3200;
+// every order (P * max_k 2^k (2(R-k)+1)^2 <= 1296 for every P, R pair above: 16 nodes of
+// 9x9 at orders 5..8), so that four CTAs (two buffers each) fit an SM's shared memory.
+constexpr int FRONTIER = 1296;
 
 } // namespace kb

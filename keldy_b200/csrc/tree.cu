@@ -13,9 +13,11 @@
 // subtree. At a leaf, det(s2_a) is the product of the pivots along the path (spin
 // symmetric models) and the remaining 1x1 Schur complement of the external corner is
 // det(s1_a)/det(s2_a). Cost O(2^n) complex FMAs per point instead of O(2^n n^3).
-// The top levels run breadth-first in shared memory (one 51.2 KB frontier buffer per
-// level, ping-pong), the last two levels per thread in registers. Orders above 9 walk
-// their first n-9 levels one root-to-subtree path at a time.
+// The top levels run breadth-first in shared memory (two 20.7 KB frontier buffers,
+// ping-pong), the last three (two at orders 3 and 4) per thread in registers. Orders above
+// 8 walk their first n-8 levels one root-to-subtree path at a time. Per G-batch of points
+// every table lookup is issued at once and G staged in global memory; each sub-batch's G
+// is copied into shared memory asynchronously while the previous sub-batch's bottom runs.
 //
 // Direct kernel: keldy's own algorithm, one partial-pivot LU pair per configuration
 // (pivot = first maximum of |re|+|im|, as LAPACK's zgetf2). It serves models whose
@@ -35,9 +37,9 @@ constexpr int NT = CTA_THREADS;
 // first of the set-up slot's three rows of per-point bin data (after the coordinates,
 // the Jacobians and the flags)
 constexpr int BIN_CODE_ROW = MAX_ORDER + 2;
-// Threads of a tree-kernel CTA: four per 7x7 node of the last breadth-first level (64
-// nodes per sub-batch at every order).
-constexpr int TREE_THREADS = 2 * CTA_THREADS;
+// Threads of a tree-kernel CTA: eight per 9x9 node (16 nodes per sub-batch at orders 5..8),
+// four per 7x7 node (up to 32 at orders 3 and 4).
+constexpr int TREE_THREADS = CTA_THREADS;
 
 struct TreeShared {
   double2 buf[2][FRONTIER];
@@ -631,7 +633,7 @@ __device__ __forceinline__ void tree_bottom9(const double2 *S, double2 D, int b,
 // (BOTTOM_SCRATCH entries), read until the caller's next barrier.
 template <int NODES>
 __device__ void bottom_sum(double2 v, double sc, int lg, int np, double2 *fval, double *fscale, double2 *scratch) {
-  static_assert(TREE_THREADS == 256 && NODES >= 32, "slots of whole warps");
+  static_assert(NODES >= 16 && NODES * (TREE_THREADS / NODES) == TREE_THREADS, "descendant slots of the CTA");
   const int tid = threadIdx.x, lane = tid & 31;
   const int g = lg < 5 ? (1 << lg) : 32;
   for (int off = 1; off < g; off <<= 1) {
@@ -713,18 +715,18 @@ __device__ int tree_sub(TreeShared &S, int N, int np, int rb, const double2 *roo
   double sc = 0.0;
   bool guard = false;
   int p = 0;
-  if (m == 7) { // four threads per 7x7 node: grandchild tid >> 6 of node tid & 63, so that a
+  if (m == 7) { // four threads per 7x7 node: grandchild tid >> 5 of node tid & 31, so that a
                 // warp's lanes read consecutive nodes (49-entry stride: no bank conflicts)
-    const int node = tid & 63, q = tid >> 6;
+    const int node = tid & 31, q = tid >> 5;
     if (node < nodes) {
       p = node >> lg;
       const int parity = __popc(node & ((1 << lg) - 1)) + parity0;
       tree_bottom7q(src + node * 49, S.D[cur][node], q >> 1, q & 1, parity, floor_, want_scale, v, sc, guard);
     }
     if (guard) flag[p] |= 2;
-    bottom_sum<64>(v, sc, lg, np, fval, fscale, S.buf[cur ^ 1]);
-  } else if (m == 9) { // eight threads per 9x9 node: great-grandchild tid >> 5 of node tid & 31
-    const int node = tid & 31, q = tid >> 5;
+    bottom_sum<32>(v, sc, lg, np, fval, fscale, S.buf[cur ^ 1]);
+  } else if (m == 9) { // eight threads per 9x9 node: great-grandchild tid >> 4 of node tid & 15
+    const int node = tid & 15, q = tid >> 4;
     if (node < nodes) {
       p = node >> lg;
       const int parity = __popc(node & ((1 << lg) - 1)) + parity0;
@@ -732,7 +734,7 @@ __device__ int tree_sub(TreeShared &S, int N, int np, int rb, const double2 *roo
                    guard);
     }
     if (guard) flag[p] |= 2;
-    bottom_sum<32>(v, sc, lg, np, fval, fscale, S.buf[cur ^ 1]);
+    bottom_sum<16>(v, sc, lg, np, fval, fscale, S.buf[cur ^ 1]);
   } else { // orders 1 and 2: the root itself, one thread per point
     if (tid < nodes) {
       p = tid;
@@ -747,9 +749,6 @@ __device__ int tree_sub(TreeShared &S, int N, int np, int rb, const double2 *roo
   return cur;
 }
 
-// Frontier entries at the start of a buffer that the fused bottom's per-point sums use.
-constexpr int BOTTOM_SCRATCH = TREE_THREADS + TREE_THREADS / 2;
-
 // Where a sub-batch's roots go when they are copied while the previous sub-batch's bottom
 // runs: past the bottom's scratch (orders 3 and up) of the buffer the bottom does not read.
 // -1: they do not fit beside it (order 3); those sub-batches copy theirs after a barrier.
@@ -762,7 +761,7 @@ __device__ __forceinline__ int tree_prefetch_offset(int N, int P) {
 // added to S.fval[p] (S.fscale[p]) with bit 1 of S.flag[p] set where a pivot fell below
 // the guard. S.D and the frontier buffers are free on entry; the caller's barrier follows.
 __device__ void tree_gbatch_points(TreeShared &S, const ItemDev &it, int N, int gb, const double2 *gst,
-                                   bool want_scale, int *bad) {
+                                   bool want_scale, bool direct, int *bad) {
   const int tid = threadIdx.x;
   const int M = 2 * N + 1, MM = M * M;
   const double floor_ = it.model.pivot_floor;
@@ -810,10 +809,10 @@ __device__ void tree_gbatch_points(TreeShared &S, const ItemDev &it, int N, int 
   int rb = 0, roff = 0;
   for (int sb = 0; sb < gb; sb += P) {
     const int np = min(P, gb - sb);
-    if (sb == 0 || pf < 0) { // copy this sub-batch's roots now
+    if (sb == 0 || pf < 0) { // copy this sub-batch's roots now (direct: built there already)
       rb = 0;
       roff = 0;
-      copy_roots(S.buf[0], gst + (size_t)sb * MM, np * MM);
+      if (!direct) copy_roots(S.buf[0], gst + (size_t)sb * MM, np * MM);
       if (tid < np) S.D[0][tid] = c2(1.0, 0.0);
       cp_async_wait_all();
       __syncthreads();
@@ -853,7 +852,7 @@ __device__ __forceinline__ void clear_bins(const Launch &L, int c) {
 // sub-batches, each sub-batch's G copied into shared memory asynchronously while the
 // previous sub-batch's bottom runs; then the batch's values in point order.
 template <bool EVAL, bool ANY_CUBIC>
-__global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
+__global__ void __launch_bounds__(TREE_THREADS, 4) tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   TreeShared &S = *reinterpret_cast<TreeShared *>(smem_raw);
   __shared__ int s_chunk;
@@ -898,11 +897,15 @@ __global__ void __launch_bounds__(TREE_THREADS, 2) tree_kernel(Launch L) {
         S.fscale[tid] = 0.0;
       }
       __syncthreads();
+      const bool direct = tree_direct(N);
       if (N > 0) {
-        build_G_any<ANY_CUBIC, 4>(it, N, gb, S.u, S.flag, gst, it.f.A.spin, &s_bad);
+        if (direct) // the batch is one sub-batch: G straight into the frontier buffer
+          build_G_any<ANY_CUBIC, 2>(it, N, gb, S.u, S.flag, S.buf[0], it.f.A.spin, &s_bad);
+        else
+          build_G_any<ANY_CUBIC, 4>(it, N, gb, S.u, S.flag, gst, it.f.A.spin, &s_bad);
         __syncthreads();
       }
-      tree_gbatch_points(S, it, N, gb, gst, want_scale, &s_bad);
+      tree_gbatch_points(S, it, N, gb, gst, want_scale, direct, &s_bad);
       if (EVAL) {
         if (tid < gb) {
           const long long o = cfirst + g0 + tid;

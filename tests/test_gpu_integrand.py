@@ -208,7 +208,7 @@ def test_cubic_interpolation_high_orders_vs_oracle(ctx, oracle, golden):
 
 @pytest.mark.parametrize("n", [13, 14, 15, 16])
 def test_integrand_maximum_orders_vs_oracle(ctx, oracle, golden, n):
-    """The largest orders (up to the library's 16): the tree walks its first n - 9 levels one
+    """The largest orders (up to the library's 16): the tree walks its first n - 8 levels one
     path at a time; one point each against the oracle's 2^n LU pairs."""
     le, gr = golden["table_beta20_lesser"], golden["table_beta20_greater"]
     gm = ctx.model(10.0, le, gr, 0.3)

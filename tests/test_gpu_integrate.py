@@ -48,7 +48,7 @@ def test_integrate_higher_orders_vs_oracle(ctx, oracle, golden):
 
 
 def test_kept_g_across_path_passes(ctx, oracle, golden):
-    """Orders 10-13 walk their first n - 9 levels in 2^(n-9) passes from one G per point,
+    """Orders 10-13 walk their first n - 8 levels in 2^(n-8) passes from one G per point,
     built once and kept at the end of a shared-memory frontier buffer. Their sums equal
     the oracle's, and bit for bit those of the no-alloc entry point (same kernel, its
     scratch in the library's static array)."""
