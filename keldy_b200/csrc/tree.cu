@@ -1458,9 +1458,13 @@ __device__ double2 kernel_point(KernelShared &K, const ItemDev &it, int N, int *
 // times; the per-warp partial sums of the leaves' reduction live in the frontier buffer
 // that the last level leaves free.
 constexpr int KM_MAX_PASS = 64;
+// Complex entries per frontier buffer of the kernel-method tree: its widest level (64 nodes
+// of 10 x 5 at order 8, one point per pass) is larger than the direct tree's.
+constexpr int KM_FRONTIER = 3200;
+
 struct KMTreeShared {
   union {
-    double2 buf[2][FRONTIER];
+    double2 buf[2][KM_FRONTIER];
     KernelShared K; // the pivoted-LU path of a guarded point (after the tree pass)
   };
   double2 D[2][KM_MAX_PASS];
@@ -1494,7 +1498,7 @@ __host__ __device__ inline int km_root_buffer(int N) {
     if (use[(j + 1) & 1] < sz) use[(j + 1) & 1] = sz;
   }
   const int b = use[0] <= use[1] ? 0 : 1;
-  return (use[b] + root <= FRONTIER && root + 160 <= FRONTIER) ? b : -1;
+  return (use[b] + root <= KM_FRONTIER && root + 160 <= KM_FRONTIER) ? b : -1;
 }
 
 // One elimination level: vertex j of every node (rows 2n - j, columns 2(n - j) + 1,
@@ -1663,7 +1667,7 @@ __device__ void km_tree_points(KMTreeShared &K, const ItemDev &it, int np, int *
   const int M = 2 * N + 1;
   // G built once for all passes (one point per pass) when it fits at a buffer's end
   const int rb = km_root_buffer(N);
-  double2 *root = rb >= 0 ? K.buf[rb] + (FRONTIER - M * M) : K.buf[0];
+  double2 *root = rb >= 0 ? K.buf[rb] + (KM_FRONTIER - M * M) : K.buf[0];
   for (int sub = 0; sub < (1 << K0); ++sub) {
     if (rb < 0 || sub == 0) build_G_any<true>(it, N, np, K.u, K.flag, root, spin, bad);
     __syncthreads();
