@@ -385,7 +385,7 @@ int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_ind
  * (cudaGetSymbolAddress); make it before any stream capture. */
 #define KB_NOALLOC_MAX_ITEMS 64
 #define KB_NOALLOC_MAX_CHUNKS 65536
-#define KB_NOALLOC_SCRATCH_BYTES (40u << 20)
+#define KB_NOALLOC_SCRATCH_BYTES (56u << 20)
 int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_work, kb_accum *acc);
 
 /* Number of device allocations (cudaMalloc and stream-ordered pool allocations) the

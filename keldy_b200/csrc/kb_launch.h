@@ -29,7 +29,7 @@ constexpr int CHUNK_POINTS = 128; // points per scheduling chunk (<= 128: two 64
 // when its value is added, 2 bin when only counted, -1 when dropped) and its f*J (re,
 // im)), then G_STAGE complex entries of staged G matrices (a G-batch, tree_gbatch).
 constexpr int PTS_ROWS = CHUNK_POINTS * (MAX_ORDER + 5);
-constexpr int G_STAGE = 2048;
+constexpr int G_STAGE = 4096;
 // Frontier entries at the start of a buffer that the tree's fused bottom uses for its
 // per-point sums (CTA_THREADS double2 and CTA_THREADS / 2 double2 of doubles).
 constexpr int BOTTOM_SCRATCH = CTA_THREADS + CTA_THREADS / 2;
