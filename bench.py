@@ -340,7 +340,7 @@ def measure_semicircle_build(ctx):
             "gpu_ms": gpu_s * 1e3, "host_numpy_s": host_s}
 
 
-def measure_sweep(ctx):
+def measure_sweep(ctx, learned_every=True):
     """256 models (V in [0,2] x eps_d in [-1,1] x beta in {10,50,200}, Gamma = 1), each with
     its own 20,001-point g0 table built on the GPU in one launch; model i integrates order
     2 + i % 9 (uneven costs) with 2^18 Sobol points; all 256 items in one graph launch."""
@@ -363,13 +363,54 @@ def measure_sweep(ctx):
     ms = ctx.last_timing()[0]
     plan.close()
     ref = sum(reference_flops(it["order"]) << 18 for it in items)
+    learned_sweep = measure_sweep_learned(ctx, models, items, chain) if learned_every else None
     for m in models:
         m.close()
-    return {"workload": "256 flat-band models (V in [0,2] x eps_d in [-1,1] x beta in {10,50,200}), own "
-                        "20,001-point g0 table each (GPU-built in one launch), orders 2..10 by model, "
-                        "2^18 Sobol points per (model, order), one graph launch",
-            "ms": ms, "evals_per_s": len(items) * (1 << 18) / (ms * 1e-3),
-            "reference_equivalent_tflops": ref / (ms * 1e-3) / 1e12, "g0_build_ms": build_s * 1e3}
+    out = {"workload": "256 flat-band models (V in [0,2] x eps_d in [-1,1] x beta in {10,50,200}), own "
+                       "20,001-point g0 table each (GPU-built in one launch), orders 2..10 by model, "
+                       "2^18 Sobol points per (model, order), one graph launch",
+           "ms": ms, "evals_per_s": len(items) * (1 << 18) / (ms * 1e-3),
+           "reference_equivalent_tflops": ref / (ms * 1e-3) / 1e12, "g0_build_ms": build_s * 1e3}
+    if learned_sweep is not None:
+        out["learned_where_trained"] = learned_sweep
+    return out
+
+
+def measure_sweep_learned(ctx, models, items, chain, every=16):
+    """The sweep with learned warpers where trained, the plain chain otherwise: a separable
+    spline flow is trained for every `every`-th model whose order has flows (up to 8; 2^16
+    plain-method samples), kept
+    when an RQMC pilot (16 shifts x 2^14 points) shows its standard error below the plain
+    chain's, and the 256 items run again as one graph launch with those flows applied in
+    line by the integrand kernel."""
+    from keldy_b200 import capi, learned
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    flows, kept = {}, []
+    for i in range(0, len(items), every):
+        it = items[i]
+        if it["order"] > 8:
+            continue
+        fl, _, _ = learned.fit(ctx, models[i], it["A"], it["B"], chain, it["order"], 1 << 16, seed=i,
+                               kind=capi.FLOW_SPLINE)
+        sel, c = learned.select(ctx, models[i], it["A"], it["B"], chain, it["order"], fl)
+        flows[i] = fl
+        if sel is not None:
+            kept.append((i, it["order"], c["stderr_ratio"]))
+    train_s = time.perf_counter() - t0
+    keep = {i for i, _, _ in kept}
+    litems = [dict(it, flow=flows[i]) if i in keep else it for i, it in enumerate(items)]
+    plan = capi.Plan(ctx, litems)
+    plan.run()
+    plan.run()
+    ms = ctx.last_timing()[0]
+    plan.close()
+    for fl in flows.values():
+        fl.close()
+    return {"trained": len(flows), "kept": len(kept),
+            "kept_models": [{"model": i, "order": n, "pilot_stderr_ratio_plain_over_learned": r} for i, n, r in kept],
+            "train_and_select_s": train_s, "ms": ms, "evals_per_s": len(items) * (1 << 18) / (ms * 1e-3),
+            "flows": "separable spline flows, mapped in line in the integrand kernel"}
 
 
 def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8), ladders=8):

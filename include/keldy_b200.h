@@ -441,7 +441,10 @@ int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out);
  * x_d = F_d^{-1}(z_d). Smooth and acting on each axis alone, it keeps the structure that
  * quasi-Monte Carlo exploits. Same calls as the coupling flow (map, sample, gradient,
  * train, fit, work items); parameters: kb_flow_num_params = dim * 49 floats, [dim][16 width
- * logits, 16 height logits, 17 derivative parameters]; created as the identity map. */
+ * logits, 16 height logits, 17 derivative parameters]; created as the identity map. In
+ * kb_integrate and plans its map runs in line in the integrand kernel's point set-up (its
+ * knots made from the current parameters at every call or replay): no mapped-point buffer
+ * and no extra pass, results equal to mapping by kb_flow_sample first. */
 #define KB_FLOW_COUPLING 0
 #define KB_FLOW_SPLINE 1
 int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_flow **out);

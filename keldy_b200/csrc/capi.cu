@@ -1149,6 +1149,7 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
   it.k_first = w.k_first;
   it.n_points = w.n_points;
   it.chunk_points = ctx->chunk_points[w.order];
+  if (w.flow && w.flow->layout.kind == FLOW_KIND_SPLINE) it.spline_knots = w.flow->knots; // mapped in line
   if (algo == KB_ALGO_TREE && !it.spin_symmetric)
     return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
   tree = ((algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric)) ? 1 : 0;
@@ -1156,6 +1157,24 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
 }
 
 int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc, const TimeBins *tb);
+
+// A flow whose points come from its own map kernel before the integration pass (the
+// coupling flow); spline flows are applied in line by the integrand kernels.
+bool mapped_flow(const kb_work &w) { return w.flow && w.flow->layout.kind != FLOW_KIND_SPLINE; }
+
+// The knots of every distinct spline flow among the work items, made from its current
+// parameters on stream st (ahead of the kernels that read them).
+int spline_knots_for(const kb_work *work, int n_work, cudaStream_t st, int *launches) {
+  std::vector<const kb_flow *> done;
+  for (int i = 0; i < n_work; ++i) {
+    const kb_flow *f = work[i].flow;
+    if (!f || f->layout.kind != FLOW_KIND_SPLINE || std::find(done.begin(), done.end(), f) != done.end()) continue;
+    done.push_back(f);
+    KB_CUDA(launch_spline_knots(f->master, f->dim, f->knots, st));
+    ++*launches;
+  }
+  return KB_OK;
+}
 } // namespace
 
 extern "C" {
@@ -1381,7 +1400,7 @@ int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, k
     int st = work_item(ctx, work[i], algo, items[(size_t)i], use_tree[(size_t)i]);
     if (st) return st;
     index[(size_t)i] = i;
-    any_flow = any_flow || (work[i].flow && work[i].n_points > 0);
+    any_flow = any_flow || (mapped_flow(work[i]) && work[i].n_points > 0);
   }
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
@@ -1389,6 +1408,10 @@ int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, k
   ctx->last_ms[0] = ctx->last_ms[1] = ctx->last_ms[2] = 0.0;
   ctx->last_launches = 0;
   KB_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), st));
+  {
+    int rc = spline_knots_for(work, n_work, st, &ctx->last_launches);
+    if (rc) return rc;
+  }
   if (!any_flow) {
     int rc = run_integrate(ctx, items, use_tree, index, acc, tb);
     if (rc) return rc;
@@ -1404,7 +1427,7 @@ int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, k
     std::vector<Piece> plain, flowed;
     for (int i = 0; i < n_work; ++i) {
       const ItemDev &it = items[(size_t)i];
-      if (!work[i].flow) {
+      if (!mapped_flow(work[i])) {
         plain.push_back({it, use_tree[(size_t)i], i, nullptr, 0});
         continue;
       }
@@ -1490,6 +1513,7 @@ struct kb_plan {
     double *buf = nullptr; // [n][order] points, then [n] Jacobians
   };
   std::vector<Fill> fills;
+  std::vector<const kb_flow *> splines; // spline flows of the items: knots made at every launch
   cudaGraphExec_t exec = nullptr;
   int device = 0;
 };
@@ -1535,7 +1559,10 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
   for (int i = 0; i < n_work; ++i) p->rng.push_back(work[i].rng);
   for (int i = 0; i < n_work; ++i) {
     const kb_work &w = work[i];
-    if (!w.flow || w.n_points == 0) continue;
+    if (w.flow && w.flow->layout.kind == FLOW_KIND_SPLINE &&
+        std::find(p->splines.begin(), p->splines.end(), w.flow) == p->splines.end())
+      p->splines.push_back(w.flow);
+    if (!mapped_flow(w) || w.n_points == 0) continue;
     kb_plan::Fill f;
     f.layout = w.flow->layout;
     f.rng = items[(size_t)i].rng;
@@ -1599,6 +1626,7 @@ int kb_plan_create(kb_context *ctx, const kb_work *work, int n_work, int algo, k
 
 // The launch sequence of one run (captured into the plan's graph).
 static int plan_enqueue(kb_context *ctx, kb_plan *p, cudaStream_t st) {
+  for (const kb_flow *f : p->splines) KB_CUDA(launch_spline_knots(f->master, f->dim, f->knots, st));
   for (const auto &f : p->fills) {
     const uint32_t *kf = &p->g[f.gi].d_items[f.pos].k_first;
     KB_CUDA(launch_flow_map(f.layout, 1, f.n, nullptr, f.rng, 0, kf, 1, f.buf, f.buf + (size_t)f.n * f.order, ctx->d_err,

@@ -177,6 +177,7 @@ int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_fl
   cudaError_t e = device_malloc(&f->master, nb);
   if (e == cudaSuccess) e = device_malloc(&f->adam_m, nb);
   if (e == cudaSuccess) e = device_malloc(&f->adam_v, nb);
+  if (e == cudaSuccess) e = device_malloc(&f->knots, (size_t)FLOW_MAX_DIM * SPL_KNOT_DOUBLES * sizeof(double));
   if (e == cudaSuccess) e = cudaMemcpyAsync(f->master, init.data(), nb, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_m, 0, nb, ctx->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(f->adam_v, 0, nb, ctx->stream);
@@ -185,10 +186,12 @@ int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_fl
     cudaFree(f->master);
     cudaFree(f->adam_m);
     cudaFree(f->adam_v);
+    cudaFree(f->knots);
     delete f;
     return fail(KB_E_CUDA, std::string("kb_flow_create_kind: ") + cudaGetErrorString(e));
   }
   f->layout.spline = f->master;
+  f->layout.knots = f->knots;
   *out = f;
   return KB_OK;
 }
@@ -205,6 +208,7 @@ int kb_flow_destroy(kb_flow *f) {
   cudaFree(f->adam_m);
   cudaFree(f->adam_v);
   cudaFree(f->img);
+  cudaFree(f->knots);
   delete f;
   return KB_OK;
 }

@@ -10,7 +10,7 @@
 // Parameters per dimension (fp32, the flow's master array): SPL_BINS width logits a,
 // SPL_BINS height logits b, SPL_BINS + 1 knot-derivative pre-activations c:
 //   w_j = mw + (1 - K mw) softmax(a)_j, x_0 = 0, x_{j+1} = x_j + w_j (x_K = 1),
-//   h_j = mh + (1 - K mh) softmax(b)_j, y likewise, delta_k = md + softplus(c_k).
+//   h_j = mh + (1 - K mh) softmax(b)_j, y likewise, delta_k = md + spline_softplus(c_k).
 // In bin j with xi = (x - x_j)/w_j, s = h_j/w_j:
 //   F(x) = y_j + h_j (s xi^2 + d0 xi (1 - xi)) / (s + (d1 + d0 - 2s) xi (1 - xi)),
 //   F'(x) = s^2 (d1 xi^2 + 2 s xi (1 - xi) + d0 (1 - xi)^2) / (s + (d1 + d0 - 2s) xi (1 - xi))^2,
@@ -25,58 +25,21 @@
 
 #include "kb_device.cuh"
 #include "kb_flow.h"
+#include "kb_spline.cuh"
 
 namespace kb {
 
 namespace {
 
-constexpr double MW = SPL_MIN_BIN, MH = SPL_MIN_BIN, MD = SPL_MIN_DERIV;
+constexpr double MW = SPL_MIN_BIN, MH = SPL_MIN_BIN;
 // per-dimension gradient accumulators: dL/dw_j, dL/dx_j (bin j's left knot), dL/dh_j, dL/ddelta_k
 constexpr int G_W = 0, G_X = SPL_BINS, G_H = 2 * SPL_BINS, G_D = 3 * SPL_BINS;
 constexpr int G_PER_DIM = 4 * SPL_BINS + 1;
 
-struct Knots {
-  double x[SPL_BINS + 1], y[SPL_BINS + 1], d[SPL_BINS + 1];
-};
-
-__device__ __forceinline__ double softplus(double v) { return v > 30.0 ? v : log1p(exp(v)); }
-
-// Knots of one dimension from its SPL_PER_DIM parameters.
-__device__ void make_knots(const float *p, Knots &k) {
-  double mxa = -1e300, mxb = -1e300;
-  for (int j = 0; j < SPL_BINS; ++j) {
-    mxa = fmax(mxa, (double)p[j]);
-    mxb = fmax(mxb, (double)p[SPL_BINS + j]);
-  }
-  double ea[SPL_BINS], eb[SPL_BINS], sa = 0.0, sb = 0.0;
-  for (int j = 0; j < SPL_BINS; ++j) {
-    ea[j] = exp((double)p[j] - mxa);
-    eb[j] = exp((double)p[SPL_BINS + j] - mxb);
-    sa += ea[j];
-    sb += eb[j];
-  }
-  k.x[0] = k.y[0] = 0.0;
-  for (int j = 0; j < SPL_BINS; ++j) {
-    k.x[j + 1] = k.x[j] + (MW + (1.0 - SPL_BINS * MW) * ea[j] / sa);
-    k.y[j + 1] = k.y[j] + (MH + (1.0 - SPL_BINS * MH) * eb[j] / sb);
-  }
-  k.x[SPL_BINS] = k.y[SPL_BINS] = 1.0;
-  for (int j = 0; j <= SPL_BINS; ++j) k.d[j] = MD + softplus((double)p[2 * SPL_BINS + j]);
-}
-
-__device__ __forceinline__ int find_bin(const double *knots, double v) {
-  int j = 0;
-#pragma unroll
-  for (int q = 1; q < SPL_BINS; ++q) j += (v >= knots[q]) ? 1 : 0;
-  return j;
-}
-
-// F'(x) of bin j at xi.
-__device__ __forceinline__ double rq_deriv(const Knots &k, int j, double xi) {
-  const double w = k.x[j + 1] - k.x[j], h = k.y[j + 1] - k.y[j], s = h / w;
-  const double d0 = k.d[j], d1 = k.d[j + 1], e = xi * (1.0 - xi);
-  const double den = s + (d1 + d0 - 2.0 * s) * e;
-  return s * s * (d1 * xi * xi + 2.0 * s * e + d0 * (1.0 - xi) * (1.0 - xi)) / (den * den);
+// Knots of every dimension (one thread per dimension), for the tree kernel's in-line map.
+__global__ void spline_knots_kernel(const float *params, int dim, SplineKnots *knots) {
+  const int d = threadIdx.x;
+  if (d < dim) spline_make_knots(params + d * SPL_PER_DIM, knots[d]);
 }
 
 // DIR 1: z -> x = F^{-1}(z), out2 = dx/dz; DIR 0: x -> z = F(x), out2 = log q(x).
@@ -84,34 +47,28 @@ template <int DIR>
 __global__ void spline_map_kernel(const float *params, int dim, long long count, const double *in, SobolDev rng,
                                   uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out,
                                   double *out2) {
-  __shared__ Knots K[FLOW_MAX_DIM];
-  if (threadIdx.x < dim) make_knots(params + threadIdx.x * SPL_PER_DIM, K[threadIdx.x]);
+  __shared__ SplineKnots K[FLOW_MAX_DIM];
+  if (threadIdx.x < dim) spline_make_knots(params + threadIdx.x * SPL_PER_DIM, K[threadIdx.x]);
   __syncthreads();
   if (k_first_dev) k_first = *k_first_dev;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < count;
        p += (long long)gridDim.x * blockDim.x) {
     double acc = DIR == 0 ? 0.0 : 1.0;
     for (int d = 0; d < dim; ++d) {
-      const Knots &k = K[d];
+      const SplineKnots &k = K[d];
       const double v = use_sobol ? sobol_coord(rng, k_first + (uint32_t)p, d) : in[p * dim + d];
       double r;
       if (DIR == 1) {
-        const int j = find_bin(k.y, v);
-        const double w = k.x[j + 1] - k.x[j], h = k.y[j + 1] - k.y[j], s = h / w;
-        const double d0 = k.d[j], d1 = k.d[j + 1], t = v - k.y[j], g = d1 + d0 - 2.0 * s;
-        const double qa = h * (s - d0) + t * g, qb = h * d0 - t * g, qc = -s * t;
-        const double disc = fmax(qb * qb - 4.0 * qa * qc, 0.0);
-        double xi = (2.0 * qc) / (-qb - sqrt(disc));
-        xi = fmin(fmax(xi, 0.0), 1.0);
-        r = fmin(fmax(k.x[j] + xi * w, 0.0), 1.0);
-        acc /= rq_deriv(k, j, xi);
+        double der;
+        r = spline_inverse(k, v, der);
+        acc /= der;
       } else {
-        const int j = find_bin(k.x, v);
+        const int j = spline_find_bin(k.x, v);
         const double w = k.x[j + 1] - k.x[j], h = k.y[j + 1] - k.y[j], s = h / w;
         const double xi = fmin(fmax((v - k.x[j]) / w, 0.0), 1.0), e = xi * (1.0 - xi);
         const double d0 = k.d[j], d1 = k.d[j + 1];
         r = k.y[j] + h * (s * xi * xi + d0 * e) / (s + (d1 + d0 - 2.0 * s) * e);
-        acc += log(rq_deriv(k, j, xi));
+        acc += log(spline_deriv(k, j, xi));
       }
       out[p * dim + d] = r;
     }
@@ -124,12 +81,12 @@ __global__ void spline_map_kernel(const float *params, int dim, long long count,
 // loss_part [grid]. Samples in fp32 as the coupling flow's training takes them.
 __global__ void spline_grad_kernel(const float *params, int dim, long long count, const float *x, const float *w,
                                    const int *index, double inv_batch, double *partials, double *loss_part) {
-  __shared__ Knots K[FLOW_MAX_DIM];
+  __shared__ SplineKnots K[FLOW_MAX_DIM];
   __shared__ double G[FLOW_MAX_DIM * G_PER_DIM];
   __shared__ double sloss;
   for (int i = threadIdx.x; i < dim * G_PER_DIM; i += blockDim.x) G[i] = 0.0;
   if (threadIdx.x == 0) sloss = 0.0;
-  if (threadIdx.x < dim) make_knots(params + threadIdx.x * SPL_PER_DIM, K[threadIdx.x]);
+  if (threadIdx.x < dim) spline_make_knots(params + threadIdx.x * SPL_PER_DIM, K[threadIdx.x]);
   __syncthreads();
   double lsum = 0.0;
   for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < count;
@@ -138,9 +95,9 @@ __global__ void spline_grad_kernel(const float *params, int dim, long long count
     const double wn = (double)w[src] * inv_batch;
     if (wn == 0.0) continue;
     for (int d = 0; d < dim; ++d) {
-      const Knots &k = K[d];
+      const SplineKnots &k = K[d];
       const double v = (double)x[src * dim + d];
-      const int j = find_bin(k.x, v);
+      const int j = spline_find_bin(k.x, v);
       const double wj = k.x[j + 1] - k.x[j], h = k.y[j + 1] - k.y[j], s = h / wj;
       const double xi = fmin(fmax((v - k.x[j]) / wj, 0.0), 1.0), e = xi * (1.0 - xi);
       const double d0 = k.d[j], d1 = k.d[j + 1];
@@ -244,6 +201,11 @@ cudaError_t launch_spline_map(const float *params, int dim, int direction, long 
     spline_map_kernel<0><<<g, 128, 0, st>>>(params, dim, count, in, rng, k_first, k_first_dev, use_sobol, out, out2);
   else
     spline_map_kernel<1><<<g, 128, 0, st>>>(params, dim, count, in, rng, k_first, k_first_dev, use_sobol, out, out2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spline_knots(const float *params, int dim, double *knots, cudaStream_t st) {
+  spline_knots_kernel<<<1, 32, 0, st>>>(params, dim, reinterpret_cast<SplineKnots *>(knots));
   return cudaGetLastError();
 }
 

@@ -46,10 +46,12 @@ constexpr int SPL_BINS = 16;
 constexpr int SPL_PER_DIM = 3 * SPL_BINS + 1;
 constexpr double SPL_MIN_BIN = 1e-3;
 constexpr double SPL_MIN_DERIV = 1e-3;
+constexpr int SPL_KNOT_DOUBLES = 3 * (SPL_BINS + 1); // x, y and derivative at each bin edge
 
 struct FlowDev {
   int kind;            // FLOW_KIND_*
   const float *spline; // FLOW_KIND_SPLINE: [dim][SPL_PER_DIM] parameters
+  double *knots;       // FLOW_KIND_SPLINE: [dim][SPL_KNOT_DOUBLES] knots made from them (launch_spline_knots)
   const uint16_t *img; // [FLOW_NMAT][FLOW_MAT] bf16 bit patterns, image layout
   int dim;
   int ntr[FLOW_LAYERS];              // number of transformed dims
@@ -92,6 +94,9 @@ cudaError_t launch_flow_pack(const float *master, uint16_t *img, cudaStream_t st
 cudaError_t launch_spline_map(const float *params, int dim, int direction, long long count, const double *in,
                               SobolDev rng, uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out,
                               double *out2, int grid, cudaStream_t st);
+// Knots of the spline flow's dimensions from its parameters, [dim][SPL_KNOT_DOUBLES]: what a
+// work item's in-line map reads (ItemDev::spline_knots).
+cudaError_t launch_spline_knots(const float *params, int dim, double *knots, cudaStream_t st);
 int spline_grad_per_dim();
 cudaError_t launch_spline_grad(const float *params, int dim, long long count, const float *x, const float *w,
                                const int *index, double inv_batch, double *partials, double *loss_part, int grid,

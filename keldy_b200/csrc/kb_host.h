@@ -162,5 +162,6 @@ struct kb_flow {
   float *adam_m = nullptr;
   float *adam_v = nullptr;
   uint16_t *img = nullptr; // [FLOW_NPARAM] bf16
+  double *knots = nullptr; // spline flows: [FLOW_MAX_DIM][SPL_KNOT_DOUBLES], made at each integration
   int64_t adam_step = 0;
 };

@@ -104,6 +104,9 @@ struct ItemDev {
   // Jacobian flow_jac[gp] instead of its Sobol point; null = plain Sobol points
   const double *flow_x;
   const double *flow_jac;
+  // learned separable spline flow applied in line (integrate mode): [order][3 * 17] knots
+  // (bin edges x, y and derivatives, kb_spline.cuh) of its dimensions; null = none
+  const double *spline_knots;
 };
 
 // One chunk of points of one item, processed by one CTA iteration.

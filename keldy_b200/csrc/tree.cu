@@ -28,6 +28,7 @@
 
 #include "kb_device.cuh"
 #include "kb_launch.h"
+#include "kb_spline.cuh"
 
 namespace kb {
 
@@ -66,6 +67,20 @@ __device__ __forceinline__ int find_item(const long long *off, int n_items, long
   return lo;
 }
 
+// The learned spline flow in line: the Sobol point x (stride `st`) to x_j = F_j^{-1}(x_j),
+// returning the flow's Jacobian prod_j 1 / F_j'(x_j), formed as the flow's own map kernel
+// forms it (same operations, same order).
+__device__ __forceinline__ double spline_flow_point(const double *knots, int N, double *x, int st) {
+  const SplineKnots *k = reinterpret_cast<const SplineKnots *>(knots);
+  double jac = 1.0;
+  for (int j = 0; j < N; ++j) {
+    double der;
+    x[j * st] = spline_inverse(k[j], x[j * st], der);
+    jac /= der;
+  }
+  return jac;
+}
+
 // Inputs of np points (thread p < np): vertex times into u[j*np+p], Jacobian and
 // domain flag. keep: drop points with a negative time (keep_u_hypercube).
 __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, long long gp0, double *u,
@@ -82,6 +97,7 @@ __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, l
     } else {
       uint32_t k = it.k_first + (uint32_t)gp;
       for (int j = 0; j < N; ++j) x[j * np] = sobol_coord(it.rng, k, j);
+      if (it.spline_knots) jac = spline_flow_point(it.spline_knots, N, x, np);
     }
     jac *= chain_reverse(it.chain, it.chain_len, 0, N, x, np);
   } else {
@@ -122,6 +138,7 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
     } else {
       const uint32_t k = it.k_first + (uint32_t)gp;
       for (int j = 0; j < N; ++j) x[j] = sobol_coord(it.rng, k, j);
+      if (it.spline_knots) jac = spline_flow_point(it.spline_knots, N, x, 1);
     }
     jac *= chain_reverse(it.chain, it.chain_len, 0, N, x, 1);
   } else {

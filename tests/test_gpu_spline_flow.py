@@ -104,3 +104,44 @@ def test_spline_flow_gain_and_unbiased(ctx):
     plan = capi.Plan(ctx, [item])
     assert plan.run()[0] == capi.integrate(ctx, [item])[0]
     plan.close()
+
+
+@pytest.mark.parametrize("n", [3, 8])
+def test_inline_map_equals_map_kernel(ctx, n):
+    """Work items with a spline flow are mapped in line by the integrand kernel (no mapped
+    point buffer): the sum equals f J over the points that the flow's own map kernel gives
+    for the same Sobol indices, and a parameter change takes effect at the next call and the
+    next plan replay."""
+    gm = _model(ctx)
+    fl = ctx.flow(n, kind=capi.FLOW_SPLINE)
+    npts, k0 = 3000, 5
+    for seed in (31, 32):
+        fl.set_params(_params(n, seed))
+        rng = ctx.sobol(n)
+        x, jac = fl.sample_sobol(rng, k0, npts)
+        f = gm.evaluate_warped(CHARGE[0], CHARGE[1], PLASMA_EXP, x)[0] * jac
+        item = dict(model=gm, rng=rng, chain=PLASMA_EXP, A=CHARGE[0], B=CHARGE[1], order=n, k_first=k0,
+                    n_points=npts, flow=fl)
+        s, npt, nd, nfb = capi.integrate(ctx, [item])[0]
+        assert npt == npts and nfb == 0
+        assert abs(s - f.sum()) <= 1e-12 * np.abs(f).sum(), (s, f.sum())
+        if seed == 31:
+            plan = capi.Plan(ctx, [item])
+            assert plan.run()[0] == (s, npt, nd, nfb)
+    assert plan.run()[0] == (s, npt, nd, nfb)  # replay after set_params: the new knots
+    plan.close()
+
+
+def test_mixed_batch_equals_separate(ctx):
+    """One kb_integrate call over a plain item, a spline-flow item and a coupling-flow item
+    gives each the sum of its own call."""
+    gm = _model(ctx)
+    sp = ctx.flow(4, kind=capi.FLOW_SPLINE)
+    sp.set_params(_params(4, 3))
+    cp = ctx.flow(5)
+    base = dict(model=gm, chain=PLASMA_EXP, A=CHARGE[0], B=CHARGE[1], n_points=5000)
+    items = [dict(base, rng=ctx.sobol(6), order=6), dict(base, rng=ctx.sobol(4), order=4, flow=sp),
+             dict(base, rng=ctx.sobol(5), order=5, flow=cp)]
+    together = capi.integrate(ctx, items)
+    for it, r in zip(items, together):
+        assert capi.integrate(ctx, [it])[0] == r
