@@ -412,7 +412,10 @@ int kb_plan_result(kb_context *ctx, kb_plan *plan, kb_accum *acc);
 int kb_plan_set_k_first(kb_context *ctx, kb_plan *plan, int item, uint32_t k_first);
 
 /* Launch shape of the tree kernel: points per scheduling chunk for `order` (1..128;
- * order -1 sets every order) and resident CTAs per SM (1 or 2; 0 keeps the value). */
+ * order -1 sets every order) and resident CTAs per SM (1 to 4; 0 keeps the value). A work
+ * item with fewer chunks than half the resident CTAs runs in chunks halved (down to 8
+ * points) until it has that many, so that it spreads over the GPU; the chunking depends on
+ * the item alone. */
 int kb_context_set_launch(kb_context *ctx, int order, int chunk_points, int ctas_per_sm);
 int kb_context_get_launch(kb_context *ctx, int order, int *chunk_points, int *ctas_per_sm);
 

@@ -1124,6 +1124,19 @@ int run_integrate(kb_context *ctx, const std::vector<ItemDev> &items, const std:
 constexpr int64_t FLOW_PIECE = 1 << 22;            // points per flow-mapped piece
 constexpr size_t FLOW_ROUND_BYTES = (size_t)1 << 30; // flow-mapped points held at once
 
+// Points per scheduling chunk of a work item of n points: the context's chunk size for its
+// order (autotuned or kb_context_set_launch), halved (down to 8) while the item would have
+// fewer chunks than half the resident tree CTAs, so that a small item is spread over the
+// GPU instead of a few CTAs walking long chunks one point after another (a batch of many
+// small items keeps larger chunks than one small item alone would need). It depends on
+// the item alone: a batch adds each item's points in the order of a call of its own.
+int item_chunk(const kb_context *ctx, int order, int64_t n) {
+  int c = ctx->chunk_points[order];
+  const int64_t want = (int64_t)ctx->sm_count * ctx->ctas_per_sm / 2;
+  while (c > 8 && (n + c - 1) / c < want) c >>= 1;
+  return c;
+}
+
 // Checks of a work item shared by kb_integrate and kb_plan_create; fills `it`.
 int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tree) {
   int st = check_integrand(w.m, &w.f, w.order);
@@ -1148,7 +1161,7 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
   it.rng = sobol_dev(w.rng);
   it.k_first = w.k_first;
   it.n_points = w.n_points;
-  it.chunk_points = ctx->chunk_points[w.order];
+  it.chunk_points = item_chunk(ctx, w.order, w.n_points);
   if (w.flow && w.flow->layout.kind == FLOW_KIND_SPLINE) it.spline_knots = w.flow->knots; // mapped in line
   if (algo == KB_ALGO_TREE && !it.spin_symmetric)
     return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
@@ -1267,8 +1280,12 @@ int integrate_kernel_impl(kb_context *ctx, const kb_work *work, int n_work, cons
     L.km_omega = *omega;
   }
   L.err = ctx->d_err;
+  const int kgrid = (int)std::min<long long>(nchunks, (long long)ctx->sm_count * KM_CTAS_PER_SM);
+  DevBuf dpts;
+  KB_CUDA(dpts.alloc((size_t)kgrid * KM_SLOT * sizeof(double), st));
+  L.pts = dpts.as<double>();
   if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[0], st));
-  KB_CUDA(launch_kernel_method(L, (int)std::min<long long>(nchunks, (long long)ctx->sm_count * 4), st));
+  KB_CUDA(launch_kernel_method(L, kgrid, st));
   if (ctx->timing) KB_CUDA(cudaEventRecord(ctx->ev[1], st));
   KB_CUDA(launch_reduce(L, dacc.as<kb_accum>(), st));
   if (nb)
@@ -1376,7 +1393,11 @@ int kb_integrand_kernel_eval(kb_context *ctx, const kb_model *m, const kb_gf_ind
   L.out_kvals = dout.as<double2>();
   L.out_dom = ddom.as<int>();
   L.err = ctx->d_err;
-  KB_CUDA(launch_kernel_method(L, (int)std::min<long long>(nchunks, (long long)ctx->sm_count * 4), s));
+  const int kgrid = (int)std::min<long long>(nchunks, (long long)ctx->sm_count * KM_CTAS_PER_SM);
+  DevBuf dpts;
+  KB_CUDA(dpts.alloc((size_t)kgrid * KM_SLOT * sizeof(double), s));
+  L.pts = dpts.as<double>();
+  KB_CUDA(launch_kernel_method(L, kgrid, s));
   int err = 0;
   KB_CUDA(cudaMemcpyAsync(out, dout.p, (size_t)count * 2 * order * sizeof(double2), cudaMemcpyDeviceToHost, s));
   if (in_domain) KB_CUDA(cudaMemcpyAsync(in_domain, ddom.p, (size_t)count * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1867,9 +1888,9 @@ extern "C" int kb_integrate_noalloc(kb_context *ctx, const kb_work *work, int n_
     it.k_first = w.k_first;
     it.n_points = w.n_points;
     group_of[i] = it.spin_symmetric ? 0 : 1;
-    // the same scheduling chunks as kb_integrate (the context's launch shape of the order),
-    // so that the sums are added in the same order
-    it.chunk_points = ctx->chunk_points[w.order];
+    // the same scheduling chunks as kb_integrate (the context's launch shape of the order,
+    // smaller for a small item), so that the sums are added in the same order
+    it.chunk_points = item_chunk(ctx, w.order, w.n_points);
     chunks_total += (w.n_points + it.chunk_points - 1) / it.chunk_points;
   }
   if (chunks_total > KB_NOALLOC_MAX_CHUNKS)

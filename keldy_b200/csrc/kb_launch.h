@@ -34,6 +34,10 @@ constexpr int G_STAGE = 4096;
 // per-point sums (CTA_THREADS double2 and CTA_THREADS / 2 double2 of doubles).
 constexpr int BOTTOM_SCRATCH = CTA_THREADS + CTA_THREADS / 2;
 constexpr int PTS_SLOT = PTS_ROWS + 2 * G_STAGE;
+// Per-CTA slot of the kernel-method tree: the chunk's set-up rows only.
+constexpr int KM_SLOT = PTS_ROWS;
+// Resident CTAs per SM of the kernel-method tree (256 threads, ~114 KB of shared memory).
+constexpr int KM_CTAS_PER_SM = 2;
 static_assert(PTS_ROWS % 2 == 0 && PTS_SLOT % 2 == 0, "staged G on 16-byte boundaries");
 
 // Points per G-batch of the tree kernel at order N: their (2N+1)^2 matrices G fit the
@@ -72,7 +76,8 @@ struct Launch {
   int *out_dom;
   double *out_scale;
   int *out_flag;        // tree: 1 = point needs the pivoted-LU kernel
-  // tree kernel: gridDim.x * PTS_SLOT doubles of set-up and staging scratch
+  // tree kernel: gridDim.x * PTS_SLOT doubles of set-up and staging scratch (kernel-method
+  // tree: gridDim.x * KM_SLOT)
   double *pts;
   // IN_SOBOL
   ChunkPartial *partials; // [n_chunks]

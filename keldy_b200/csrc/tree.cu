@@ -1755,7 +1755,7 @@ __device__ void km_tree_points_any(KMTreeShared &K, const ItemDev &it, int N, in
   }
 }
 
-__global__ void __launch_bounds__(KM_THREADS, 2) km_tree_kernel(Launch L) {
+__global__ void __launch_bounds__(KM_THREADS, KM_CTAS_PER_SM) km_tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   KMTreeShared &K = *reinterpret_cast<KMTreeShared *>(smem_raw);
   __shared__ int s_chunk;
@@ -1786,9 +1786,25 @@ __global__ void __launch_bounds__(KM_THREADS, 2) km_tree_kernel(Launch L) {
     double2 csum = c2(0.0, 0.0);
     unsigned long long cdom = 0;
     const int P = it.spin_symmetric ? km_points_per_pass(N) : 1;
+    // passes of at most 8 points (orders 5 and up): the chunk's points are set up at once
+    // (Sobol coordinates or given inputs, warper chain, domain flag: one thread per point)
+    // into the CTA's slot and each pass reads its own, instead of a pass's few threads
+    // walking the chain for its points while the others wait
+    const bool staged = P <= 8;
+    double *slot = L.pts + (size_t)blockIdx.x * KM_SLOT;
+    if (staged) {
+      if (tid < ccount) prepare_point(L, it, N, cfirst + tid, keep, slot, tid);
+      __syncthreads();
+    }
     for (int sb = 0; sb < ccount; sb += P) {
       const int np = min(P, ccount - sb);
-      load_points(L, it, N, np, cfirst + sb, K.u, K.jac, K.flag, keep);
+      if (!staged) {
+        load_points(L, it, N, np, cfirst + sb, K.u, K.jac, K.flag, keep);
+      } else if (tid < np) {
+        for (int j = 0; j < N; ++j) K.u[j * np + tid] = slot[j * CHUNK_POINTS + sb + tid];
+        K.jac[tid] = slot[MAX_ORDER * CHUNK_POINTS + sb + tid];
+        K.flag[tid] = (int)slot[(MAX_ORDER + 1) * CHUNK_POINTS + sb + tid];
+      }
       __syncthreads();
       if (it.spin_symmetric) {
         km_tree_points_any(K, it, N, np, &s_bad);
