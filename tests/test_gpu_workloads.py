@@ -98,7 +98,7 @@ def test_sweep_models_vs_oracle(ctx, oracle):
 GUARD_MODELS = [(1.0, 0.5, 1.0, 100.0), (1.0, -1.0, 0.0, 10.0), (1.0, 1.0, 2.0, 200.0), (1.0, -1.0, 2.0, 200.0)]
 
 
-@pytest.mark.parametrize("order,n_pts", [(10, 256), (12, 128)])
+@pytest.mark.parametrize("order,n_pts", [(10, 256), (12, 256)])
 def test_high_order_pivot_guard_vs_oracle(ctx, oracle, order, n_pts):
     """Point values at orders 10 and 12 on the biased dot (t = 50, 100,001 points) and on the
     sweep grid's corners (t = 20, 20,001 points). The tree pivots on the diagonal and hands
