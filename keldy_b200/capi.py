@@ -213,6 +213,9 @@ def _ip(a):
     return None if a is None else a.ctypes.data_as(_I)
 
 
+_WARPER_P = C.POINTER(Warper)
+
+
 def chain_array(chain):
     """chain: list of (kind, u_max, w[, power]) or (WARPER_TABLE, WarperTable) -> (ctypes array,
     length)."""
@@ -641,17 +644,29 @@ def semicircle_model(ctx, gamma, eps_d, bias_V, beta, half_bandwidth, time_max, 
 
 
 def _works(items):
+    """The kb_work array of `items` and the ctypes objects it points into (keep them alive
+    during the call). Items that share a chain list or external-point objects share one
+    converted copy: a call over many replicas of one integrand converts them once."""
     n = len(items)
     works = (Work * max(1, n))()
-    keep = []
+    keep, chains, fs = [], {}, {}
     for i, it in enumerate(items):
-        arr, L = chain_array(it["chain"])
-        keep.append(arr)
+        ch = it["chain"]
+        c = chains.get(id(ch))
+        if c is None:
+            arr, L = chain_array(ch)
+            keep.append(arr)
+            c = chains[id(ch)] = (C.cast(arr, _WARPER_P), L)
+        A = it["A"]
+        B = it.get("B", A)
+        cut = it.get("cutoff", 0.0)
+        f = fs.get((id(A), id(B), cut))
+        if f is None:
+            f = fs[(id(A), id(B), cut)] = Integrand(gf_index(A), gf_index(B), float(cut))
         flow = it.get("flow")
-        works[i] = Work(it["model"].h.value, it["rng"].h.value, C.cast(arr, C.POINTER(Warper)), L,
-                        Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
-                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]),
-                        flow.h.value if flow is not None else None)
+        works[i] = Work(it["model"].h.value, it["rng"].h.value, c[0], c[1], f, int(it["order"]),
+                        int(it.get("k_first", 1)), int(it["n_points"]), flow.h.value if flow is not None else None)
+    keep.append((chains, fs, items))
     return works, keep
 
 
@@ -760,19 +775,10 @@ def integrate(ctx, items, algo=ALGO_AUTO):
     """items: list of dicts {model, rng, chain, A, B, cutoff, order, k_first, n_points}.
     Returns a list of (sum f*J, n_points, n_in_domain, n_fallback)."""
     n = len(items)
-    works = (Work * n)()
-    keep = []
-    for i, it in enumerate(items):
-        arr, L = chain_array(it["chain"])
-        keep.append(arr)
-        flow = it.get("flow")
-        works[i] = Work(it["model"].h.value, it["rng"].h.value, C.cast(arr, C.POINTER(Warper)), L,
-                        Integrand(gf_index(it["A"]), gf_index(it["B"]), float(it.get("cutoff", 0.0))),
-                        int(it["order"]), int(it.get("k_first", 1)), int(it["n_points"]),
-                        flow.h.value if flow is not None else None)
-    acc = (Accum * n)()
+    works, keep = _works(items)
+    acc = (Accum * max(1, n))()
     check(ctx.L.kb_integrate(ctx.h, works, n, algo, acc))
-    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback) for a in acc]
+    return [(complex(a.sum_re, a.sum_im), a.n_points, a.n_in_domain, a.n_fallback) for a in acc[:n]]
 
 
 def train_cfg(epochs=20, batch=16384, lr=2e-3, lr_final=1e-4, beta1=0.9, beta2=0.999, eps=1e-8, seed=0):
