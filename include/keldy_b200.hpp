@@ -107,6 +107,7 @@ class sobol {
     seed(rng_state_seed);
   }
 
+  // one point per call (a device round trip); points(count) draws many in one call
   std::vector<double> operator()() { return points(1); }
 
   // next `count` points, row-major (an addition to keldy's interface)
@@ -762,8 +763,22 @@ class integrand_g_direct {
       throw std::runtime_error("An external point is out of g0 time window.");
   }
 
+  // One point per call, as keldy's: each call is a device round trip (tens of
+  // microseconds). A loop over many points should call eval_many instead.
   std::pair<result_t, int> operator()(std::vector<double> const &times, bool const keep_u_hypercube = true) const {
     return eval(times, keep_u_hypercube, false);
+  }
+  // count points of `order` vertex times each (row-major in `times`), one device call:
+  // values[p], in_domain[p] (an addition to keldy's interface).
+  void eval_many(int order, int64_t count, double const *times, std::vector<result_t> &values,
+                 std::vector<int> &in_domain, bool const keep_u_hypercube = true) const {
+    kb_integrand f = abi();
+    std::vector<double> out((size_t)(2 * count));
+    in_domain.assign((size_t)count, 0);
+    keldy_b200::check(kb_integrand_eval(keldy_b200::default_context(), g0.model.handle(), &f, order, count, times,
+                                        keep_u_hypercube, algo_, out.data(), in_domain.data(), nullptr));
+    values.resize((size_t)count);
+    for (int64_t p = 0; p < count; ++p) values[(size_t)p] = dcomplex(out[(size_t)(2 * p)], out[(size_t)(2 * p + 1)]);
   }
   std::pair<result_t, int> eval_no_det(std::vector<double> const &times, bool const keep_u_hypercube = true) const {
     return eval(times, keep_u_hypercube, true);
@@ -794,6 +809,7 @@ class integrator_g_direct {
     if (dimension <= 0) throw std::runtime_error("Dimension of the integration space must be > 0.");
   }
 
+  // One point per call, as keldy's (a device round trip); kb_evaluate_warped takes many.
   std::pair<dcomplex, double> evaluate_warped_integrand(std::vector<double> const &li_vec, int start_domain_nr,
                                                         bool keep_u_hypercube = true) const {
     kb_integrand f = integrand.abi();

@@ -308,15 +308,14 @@ PYBIND11_MODULE(_keldy, m) {
              bool keep) {
             if (times.ndim() != 2) throw std::runtime_error("times must be a [count, order] array");
             const int64_t count = times.shape(0);
-            const int n = (int)times.shape(1);
+            std::vector<dcomplex> vals;
+            std::vector<int> dom;
+            f.eval_many((int)times.shape(1), count, times.data(), vals, dom, keep);
             py::array_t<std::complex<double>> out(count);
-            py::array_t<int> dom(count);
-            kb_integrand a = f.abi();
-            keldy_b200::check(kb_integrand_eval(keldy_b200::default_context(), f.get_g0().model.handle(), &a, n, count,
-                                                times.data(), keep, f.algorithm(),
-                                                reinterpret_cast<double *>(out.mutable_data()), dom.mutable_data(),
-                                                nullptr));
-            return py::make_tuple(out, dom);
+            py::array_t<int> pdom(count);
+            std::copy(vals.begin(), vals.end(), out.mutable_data());
+            std::copy(dom.begin(), dom.end(), pdom.mutable_data());
+            return py::make_tuple(out, pdom);
           },
           py::arg("times"), py::arg("keep_u_hypercube") = true,
           "the integrand at many time vectors in one device launch: (values, in_domain)");
