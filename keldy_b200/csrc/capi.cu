@@ -378,8 +378,9 @@ int kb_model_destroy(kb_model *m) {
   cudaSetDevice(m->device); // cudaFree waits for the device's pending work
   for (int s = 0; s < 2; ++s)
     for (int a = 0; a < 2; ++a)
-      for (int b = 0; b < 2; ++b) cudaFree(m->tab[s][a][b]);
-  delete m;
+      for (int b = 0; b < 2; ++b)
+        if (!(m->slab && s == 0 && a == 0 && b == 0)) cudaFree(m->tab[s][a][b]);
+  delete m; // releases its share of a slab
   return KB_OK;
 }
 
@@ -499,11 +500,27 @@ int kb_models_set_flatband(int n, kb_model *const *models, const double *params)
   KB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   std::vector<double2 *> tabs((size_t)n);
-  for (int i = 0; i < n; ++i) {
-    kb_model *m = models[i];
-    if (!m->tab[0][0][0]) KB_CUDA(device_malloc(&m->tab[0][0][0], (size_t)npts * 2 * sizeof(double2)));
-    tabs[(size_t)i] = m->tab[0][0][0];
+  // models without a dot table get slices of one allocation (one cudaMalloc for the call,
+  // not one per model)
+  size_t fresh = 0;
+  for (int i = 0; i < n; ++i) fresh += models[i]->tab[0][0][0] ? 0 : 1;
+  if (fresh) {
+    const size_t per = (size_t)npts * 2;
+    double2 *block = nullptr;
+    KB_CUDA(device_malloc(&block, fresh * per * sizeof(double2)));
+    const int dev = ctx->device;
+    std::shared_ptr<void> slab(block, [dev](void *q) {
+      cudaSetDevice(dev);
+      cudaFree(q);
+    });
+    size_t k = 0;
+    for (int i = 0; i < n; ++i)
+      if (!models[i]->tab[0][0][0]) {
+        models[i]->tab[0][0][0] = block + (k++) * per;
+        models[i]->slab = slab;
+      }
   }
+  for (int i = 0; i < n; ++i) tabs[(size_t)i] = models[i]->tab[0][0][0];
   DevBuf dpar, dtab, dx, dw, dmax;
   KB_CUDA(dpar.alloc((size_t)n * 4 * sizeof(double), st));
   KB_CUDA(dtab.alloc((size_t)n * sizeof(double2 *), st));
@@ -516,7 +533,7 @@ int kb_models_set_flatband(int n, kb_model *const *models, const double *params)
   KB_CUDA(cudaMemcpyAsync(dw.p, gw.data(), NODES * sizeof(double), cudaMemcpyHostToDevice, st));
   KB_CUDA(launch_flatband_tables(n, dpar.as<double>(), dtab.as<double2 *>(), npts, tmax, dx.as<double>(),
                                  dw.as<double>(), NODES, st));
-  for (int i = 0; i < n; ++i) KB_CUDA(launch_table_max(tabs[(size_t)i], npts, dmax.as<double>() + i, st));
+  KB_CUDA(launch_tables_max(dtab.as<double2 *>(), n, npts, dmax.as<double>(), st));
   std::vector<double> mx((size_t)n);
   KB_CUDA(cudaMemcpyAsync(mx.data(), dmax.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st));
   KB_CUDA(cudaStreamSynchronize(st));

@@ -7,6 +7,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -111,6 +112,9 @@ struct kb_model {
   uint64_t hash[2][2][2] = {}; // 0 = unknown (device upload)
   double tabmax = 0;
   int interp = 1; // 1 linear, 3 cubic
+  // tab[0][0][0] lies in a device block shared with the other models of one
+  // kb_models_set_flatband call (freed with its last owner) instead of its own allocation
+  std::shared_ptr<void> slab;
 };
 
 struct kb_sobol {

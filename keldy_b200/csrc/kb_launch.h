@@ -166,6 +166,8 @@ cudaError_t launch_g0_eval(ModelDev m, const kb_gf_index *a, const kb_gf_index *
 cudaError_t launch_no_det(ModelDev m, kb_integrand f, int order, long long count, const double *times, int keep,
                           double2 *out, int *dom, int *err, cudaStream_t st);
 cudaError_t launch_table_max(const double2 *tab, int npts, double *out, cudaStream_t st);
+// the same for n tables (device array of their pointers): out[i] for table i, one launch
+cudaError_t launch_tables_max(double2 *const *tabs, int n, int npts, double *out, cudaStream_t st);
 cudaError_t launch_fp64_peak(int iters, double *sink, int grid, int block, cudaStream_t st);
 // Flat-band dot g0 tables of n models ({Gamma, eps_d, V, beta} each) on the mesh of
 // npts points over [-tmax, tmax] (g0_build.cu); Gauss-Legendre rule on [-1, 1].

@@ -115,6 +115,21 @@ __global__ void table_max_kernel(const double2 *tab, int n2, double *out) {
   if (threadIdx.x == 0) *out = red[0];
 }
 
+// max |re| + |im| of table blockIdx.x of tabs[] into out[blockIdx.x].
+__global__ void tables_max_kernel(double2 *const *tabs, int n2, double *out) {
+  __shared__ double red[256];
+  const double2 *tab = tabs[blockIdx.x];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) m = fmax(m, cabs1(tab[i]));
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
 // Eight independent FMA chains per thread, `iters` steps each.
 __global__ void fp64_peak_kernel(int iters, double *sink) {
   double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
@@ -171,6 +186,12 @@ cudaError_t launch_no_det(ModelDev m, kb_integrand f, int order, long long count
 
 cudaError_t launch_table_max(const double2 *tab, int npts, double *out, cudaStream_t st) {
   table_max_kernel<<<1, 256, 0, st>>>(tab, 2 * npts, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tables_max(double2 *const *tabs, int n, int npts, double *out, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  tables_max_kernel<<<n, 256, 0, st>>>(tabs, 2 * npts, out);
   return cudaGetLastError();
 }
 

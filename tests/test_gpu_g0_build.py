@@ -26,6 +26,32 @@ def test_gpu_builder_equals_host_builder(ctx, time_max, npts):
         assert np.abs(dg - hg).max() <= 1e-11 * scale, (g, e, v, b, np.abs(dg - hg).max())
 
 
+def test_batch_tables_outlive_their_neighbours(ctx):
+    """The models of one kb_models_set_flatband call share one device allocation: closing
+    some of them leaves the others' tables intact, with their maxima set (the batched
+    maximum kernel), and a table uploaded later replaces a slice in place."""
+    models = capi.flatband_models(ctx, CASES, 10.0, 2001)
+    for i in (0, 3, 5):
+        models[i].close()
+    for i in (1, 2, 4, 6, 7):
+        g, e, v, b = CASES[i]
+        _, hl, hg = g0_tables.flatband(g, e, v, b, 10.0, 2001)
+        dl, dg = models[i].table()
+        scale = max(np.abs(hl).max(), np.abs(hg).max())
+        assert np.abs(dl - hl).max() <= 1e-11 * scale and np.abs(dg - hg).max() <= 1e-11 * scale
+    _, hl, hg = g0_tables.flatband(1.0, 0.1, 0.2, 30.0, 10.0, 2001)
+    models[2].set_table(0, 0, 0, hl, hg)
+    dl, dg = models[2].table()
+    np.testing.assert_array_equal(dl, hl)
+    np.testing.assert_array_equal(dg, hg)
+    chain = [(capi.WARPER_PLASMA_UV, 10.0, 0.0), (capi.WARPER_EXPONENTIAL, 10.0, 1.0)]
+    r = capi.integrate(ctx, [dict(model=models[7], rng=ctx.sobol(3), chain=chain, A=(10.0, 0, 0), B=(10.0, 0, 1),
+                                  order=3, n_points=4096)])[0]
+    assert r[1] == 4096 and np.isfinite(r[0])
+    for i in (1, 2, 4, 6, 7):
+        models[i].close()
+
+
 def test_gpu_builder_known_answers(ctx, keldy_tests):
     # keldy's model_flatband_test.cpp:154-220 values (tol as in keldy)
     for case in keldy_tests["flatband_kat"]:
