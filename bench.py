@@ -36,8 +36,8 @@ GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
 # order 8) from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
 # the hash of the kernel's sources (tree_source_hash) at the time of the capture. A build
 # whose sources hash differently reports no traffic figure until it is captured again.
-TREE_DRAM_CAPTURES = {}
-TREE_SOURCES = ("tree.cu", "kb_device.cuh", "kb_types.h", "kb_launch.h")
+TREE_DRAM_CAPTURES = {"9275079184e39f0e": 2217984 + 161223936}
+TREE_SOURCES = ("tree.cu", "kb_device.cuh", "kb_types.h", "kb_launch.h", "kb_spline.cuh", "kb_flow.h")
 E2E_REPEATS = 5
 
 
@@ -605,8 +605,9 @@ def run_ours(args, rank, world, local_rank):
         src_hash = tree_source_hash()
         traffic = TREE_DRAM_CAPTURES.get(src_hash) if (order == 8 and N == 1 << 20) else None
         traffic_source = (f"dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-point order-8 tree_kernel launch "
-                          f"(ncu) of the kernel sources with hash {src_hash}: the g0 table, generator and set-up data; "
-                          f"the 17,440 B per evaluation of table gathers are served by L2/L1"
+                          f"(ncu) of the kernel sources with hash {src_hash}: the g0 table and set-up data read once, "
+                          f"and the staged G matrices that L2 writes back (~154 B per evaluation of the 4.6 KB "
+                          f"staged); the table gathers are served by L2/L1"
                           if traffic is not None else
                           f"no ncu capture of the kernel sources with hash {src_hash} at this workload")
         line = {
