@@ -414,8 +414,8 @@ def measure_sweep_learned(ctx, models, items, chain, every=16):
 
 
 def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8), ladders=8):
-    """Learned flows (coupling layers, and the separable spline flow) vs the plain chain per
-    order: training time, per-point variance gain,
+    """Learned flows (coupling layers, the separable spline flow and the autoregressive
+    spline flow) vs the plain chain per order: training time, per-point variance gain,
     RQMC standard errors at a fixed 2^24-evaluation budget (16 shifts x 2^20 points) and
     wall time to a 1e-3 (and, at order 6, 1e-4) relative standard error: `ladders`
     independent ladders of 16 shifts each (disjoint shift seeds), points per shift on a
@@ -433,8 +433,10 @@ def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8), ladders=8):
     for n in orders:
         flow, fit_s, loss = learned.fit(ctx, model, A, B, chain, n, 1 << 18, seed=n)
         sflow, sfit_s, sloss = learned.fit(ctx, model, A, B, chain, n, 1 << 18, seed=n, kind=capi.FLOW_SPLINE)
+        rflow, rfit_s, rloss = learned.fit(ctx, model, A, B, chain, n, 1 << 18, seed=n, kind=capi.FLOW_AR_SPLINE)
         budget = learned.compare(ctx, model, A, B, chain, n, flow, 1 << 20, 16)
         sbudget = learned.compare(ctx, model, A, B, chain, n, sflow, 1 << 20, 16)
+        rbudget = learned.compare(ctx, model, A, B, chain, n, rflow, 1 << 20, 16)
         ctx.synchronize()
         t0 = time.perf_counter()
         table = capi.WarperTable.from_projection(ctx, model, A, B, chain, n, 100, 1 << 14, 0.05)
@@ -446,13 +448,16 @@ def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8), ladders=8):
         ttr = {}
         for tgt in targets:
             tp, tl, ta = ladder(chain, n, tgt), ladder(chain, n, tgt, flow), ladder(achain, n, tgt)
-            ts = ladder(chain, n, tgt, sflow)
-            ttr[f"{tgt:g}"] = {"plain": tp, "learned": tl, "learned_spline": ts, "adaptive_plain": ta,
+            ts, tr = ladder(chain, n, tgt, sflow), ladder(chain, n, tgt, rflow)
+            ttr[f"{tgt:g}"] = {"plain": tp, "learned": tl, "learned_spline": ts, "learned_ar_spline": tr,
+                              "adaptive_plain": ta,
                               "speedup_learned_over_plain": tp["seconds_median"] / tl["seconds_median"],
                               "speedup_spline_over_plain": tp["seconds_median"] / ts["seconds_median"],
+                              "speedup_ar_spline_over_plain": tp["seconds_median"] / tr["seconds_median"],
                               "speedup_adaptive_over_plain": tp["seconds_median"] / ta["seconds_median"],
                               "learned_incl_training_s": tl["seconds_median"] + fit_s,
-                              "spline_incl_training_s": ts["seconds_median"] + sfit_s}
+                              "spline_incl_training_s": ts["seconds_median"] + sfit_s,
+                              "ar_spline_incl_training_s": tr["seconds_median"] + rfit_s}
         adaptive = {"build_s": build_s, "budget_2e24_stderr": ea, "budget_2e24_rel": ea / abs(ma),
                     "stderr_ratio_plain_over_adaptive": budget["plain"]["stderr"] / ea,
                     "diff_in_combined_sigma": abs(ma - mp) / math.hypot(ea, budget["plain"]["stderr"])}
@@ -472,9 +477,15 @@ def measure_learned(ctx, model, A, B, chain, orders=(4, 5, 6, 7, 8), ladders=8):
                                "budget_2e24_stderr": sbudget["learned"]["stderr"],
                                "stderr_ratio_plain_over_spline": sbudget["stderr_ratio"],
                                "diff_in_combined_sigma": sbudget["diff_sigma"]},
+            "learned_ar_spline": {"fit_s": rfit_s, "fit_loss": rloss,
+                                  "per_point_variance_gain": learned.variance_gain(ctx, model, A, B, chain, rflow),
+                                  "budget_2e24_stderr": rbudget["learned"]["stderr"],
+                                  "stderr_ratio_plain_over_ar_spline": rbudget["stderr_ratio"],
+                                  "diff_in_combined_sigma": rbudget["diff_sigma"]},
         }
         flow.close()
         sflow.close()
+        rflow.close()
     return out
 
 

@@ -450,8 +450,18 @@ int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out);
  * and no extra pass, results equal to mapping by kb_flow_sample first. */
 #define KB_FLOW_COUPLING 0
 #define KB_FLOW_SPLINE 1
+/* No counterpart in keldy: the third learned first stage, an autoregressive
+ * (Knothe-Rosenblatt) spline flow. Dimension d goes through the spline CDF above with its
+ * 49 parameters theta_d = A_d phi_d, phi_d = [1, P1(x_k), P2(x_k), P3(x_k) for k < d]
+ * (Legendre polynomials on [0, 1] of the dimensions before it), so each vertex time's
+ * density is conditioned smoothly on the earlier ones. Parameters: kb_flow_num_params =
+ * 49 * (dim + 3 dim (dim - 1) / 2) floats, A_0, A_1, ... each [49][1 + 3 d] row-major;
+ * created as the identity map; with only the constant column set it is the separable flow
+ * of those parameters. Mapped in line like the separable flow. */
+#define KB_FLOW_AR_SPLINE 2
 int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_flow **out);
-/* Parameters of the flow: KB_FLOW_PARAMS (coupling) or dim * 49 (spline). */
+/* Parameters of the flow: KB_FLOW_PARAMS (coupling), dim * 49 (spline) or
+ * 49 * (dim + 3 dim (dim - 1) / 2) (autoregressive spline). */
 int kb_flow_num_params(const kb_flow *flow);
 int kb_flow_destroy(kb_flow *flow);
 int kb_flow_dim(const kb_flow *flow);

@@ -20,8 +20,8 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(PKG, "libkeldy_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC] + ARCH
-CUDA_SOURCES = ["tree.cu", "misc_kernels.cu", "flow.cu", "flow_spline.cu", "g0_build.cu", "capi.cu", "flow_capi.cu", "table_capi.cu", "host_sobol.cpp"]
-HEADERS = ["kb_types.h", "kb_device.cuh", "kb_launch.h", "kb_flow.h", "kb_host.h", "sobol_joe_kuo.h"]
+CUDA_SOURCES = ["tree.cu", "misc_kernels.cu", "flow.cu", "flow_spline.cu", "flow_arspline.cu", "g0_build.cu", "capi.cu", "flow_capi.cu", "table_capi.cu", "host_sobol.cpp"]
+HEADERS = ["kb_types.h", "kb_device.cuh", "kb_launch.h", "kb_flow.h", "kb_host.h", "kb_spline.cuh", "sobol_joe_kuo.h"]
 
 
 def _nvcc():

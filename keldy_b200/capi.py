@@ -786,14 +786,16 @@ def train_cfg(epochs=20, batch=16384, lr=2e-3, lr_final=1e-4, beta1=0.9, beta2=0
                         int(seed))
 
 
-FLOW_COUPLING, FLOW_SPLINE = 0, 1
+FLOW_COUPLING, FLOW_SPLINE, FLOW_AR_SPLINE = 0, 1, 2
 
 
 class Flow:
     """Learned warper of dimension `dim` on the device, a first stage before the warper
     chain trained on |integrand| samples of the plain method (kb_flow_* in
     include/keldy_b200.h): kind FLOW_COUPLING (coupling layers with tensor-core MLP
-    conditioners, dim 2..8) or FLOW_SPLINE (separable rational-quadratic splines, dim 1..8)."""
+    conditioners, dim 2..8), FLOW_SPLINE (separable rational-quadratic splines, dim 1..8)
+    or FLOW_AR_SPLINE (autoregressive splines whose parameters are linear in Legendre
+    features of the earlier dimensions, dim 1..8)."""
 
     def __init__(self, ctx, dim, seed=0, kind=FLOW_COUPLING):
         self.ctx = ctx
@@ -806,7 +808,9 @@ class Flow:
         ctx._deps.add(self)
 
     def _pshape(self):
-        return (FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH) if self.kind == FLOW_COUPLING else (self.dim, 49)
+        if self.kind == FLOW_COUPLING:
+            return (FLOW_LAYERS, 3, FLOW_WIDTH, FLOW_WIDTH)
+        return (self.dim, 49) if self.kind == FLOW_SPLINE else (self.n_params,)
 
     def close(self):
         if self.h:
@@ -820,7 +824,8 @@ class Flow:
             pass
 
     def params(self):
-        """float32 [layer][matrix W1, W2, W3][out][in] (coupling) or [dim][49] (spline)."""
+        """float32 [layer][matrix W1, W2, W3][out][in] (coupling), [dim][49] (spline) or the
+        flat [A_0, A_1, ...] (autoregressive spline)."""
         p = np.empty(self._pshape(), dtype=np.float32)
         check(self.ctx.L.kb_flow_get_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float))))
         return p

@@ -1180,6 +1180,7 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
   it.n_points = w.n_points;
   it.chunk_points = item_chunk(ctx, w.order, w.n_points);
   if (w.flow && w.flow->layout.kind == FLOW_KIND_SPLINE) it.spline_knots = w.flow->knots; // mapped in line
+  if (w.flow && w.flow->layout.kind == FLOW_KIND_AR_SPLINE) it.ar_spline = w.flow->master; // mapped in line
   if (algo == KB_ALGO_TREE && !it.spin_symmetric)
     return fail(KB_E_INVALID, "the tree algorithm needs equal spin-up and spin-down g0 tables");
   tree = ((algo == KB_ALGO_TREE) || (algo == KB_ALGO_AUTO && it.spin_symmetric)) ? 1 : 0;
@@ -1189,8 +1190,8 @@ int work_item(kb_context *ctx, const kb_work &w, int algo, ItemDev &it, int &tre
 int integrate_impl(kb_context *ctx, const kb_work *work, int n_work, int algo, kb_accum *acc, const TimeBins *tb);
 
 // A flow whose points come from its own map kernel before the integration pass (the
-// coupling flow); spline flows are applied in line by the integrand kernels.
-bool mapped_flow(const kb_work &w) { return w.flow && w.flow->layout.kind != FLOW_KIND_SPLINE; }
+// coupling flow); the spline flows are applied in line by the integrand kernels.
+bool mapped_flow(const kb_work &w) { return w.flow && w.flow->layout.kind == FLOW_KIND_COUPLING; }
 
 // The knots of every distinct spline flow among the work items, made from its current
 // parameters on stream st (ahead of the kernels that read them).

@@ -768,8 +768,10 @@ cudaError_t flow_configure() {
   e = cudaFuncSetAttribute(flow_map_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)flow_map_smem_bytes());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(flow_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)flow_train_smem_bytes());
+  e = cudaFuncSetAttribute(flow_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)flow_train_smem_bytes());
+  if (e != cudaSuccess) return e;
+  return ar_configure();
 }
 
 cudaError_t launch_flow_map(const FlowDev &f, int direction, long long count, const double *in, SobolDev rng,
@@ -779,6 +781,9 @@ cudaError_t launch_flow_map(const FlowDev &f, int direction, long long count, co
   if (f.kind == FLOW_KIND_SPLINE)
     return launch_spline_map(f.spline, f.dim, direction, count, in, rng, k_first, k_first_dev, use_sobol, out, out2,
                              4 * grid, st);
+  if (f.kind == FLOW_KIND_AR_SPLINE)
+    return launch_ar_map(f.spline, f.dim, direction, count, in, rng, k_first, k_first_dev, use_sobol, out, out2,
+                         4 * grid, st);
   grid *= 2; // two resident CTAs per SM (grid is given as the SM count)
   const long long tiles = (count + NT - 1) / NT;
   if (grid > tiles) grid = (int)tiles;

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "kb_host.h"
+#include "kb_spline.cuh"
 
 using namespace kb;
 
@@ -57,8 +58,34 @@ int spline_grid(const kb_flow *f, long long count) {
   return (int)std::max<long long>(1, std::min<long long>((count + 255) / 256, 2LL * f->ctx->sm_count));
 }
 
-// kb_flow_train for the spline flow (the caller holds the context's lock): per step the
-// batch's derivative partials, then the chained gradient and the Adam step, cosine-decayed
+// The flows whose parameters are a plain fp32 vector trained by their own gradient and Adam
+// kernels (the separable and the autoregressive spline flows), and those kernels by kind.
+bool param_flow(const kb_flow *f) { return f->layout.kind != FLOW_KIND_COUPLING; }
+int param_grid(const kb_flow *f, long long count) {
+  return f->layout.kind == FLOW_KIND_AR_SPLINE ? ar_grad_grid(count, f->ctx->sm_count) : spline_grid(f, count);
+}
+size_t param_partial(const kb_flow *f) {
+  return f->layout.kind == FLOW_KIND_AR_SPLINE ? (size_t)ar_num_params(f->dim)
+                                                : (size_t)f->dim * spline_grad_per_dim();
+}
+cudaError_t param_grad(const kb_flow *f, long long count, const float *x, const float *w, const int *index,
+                       double inv_batch, double *partials, double *loss_part, int grid, cudaStream_t st) {
+  if (f->layout.kind == FLOW_KIND_AR_SPLINE)
+    return launch_ar_grad(f->master, f->dim, count, x, w, index, inv_batch, partials, loss_part, grid, st);
+  return launch_spline_grad(f->master, f->dim, count, x, w, index, inv_batch, partials, loss_part, grid, st);
+}
+cudaError_t param_adam(kb_flow *f, const double *partials, int nparts, const double *loss_part, double *loss_out,
+                       float *grad_out, float lr, float beta1, float beta2, float eps, float bc1, float bc2,
+                       cudaStream_t st) {
+  if (f->layout.kind == FLOW_KIND_AR_SPLINE)
+    return launch_ar_adam(f->master, f->adam_m, f->adam_v, f->dim, partials, nparts, loss_part, loss_out, grad_out,
+                          lr, beta1, beta2, eps, bc1, bc2, st);
+  return launch_spline_adam(f->master, f->adam_m, f->adam_v, f->dim, partials, nparts, loss_part, loss_out, grad_out,
+                            lr, beta1, beta2, eps, bc1, bc2, st);
+}
+
+// kb_flow_train for the spline flows (the caller holds the context's lock): per step the
+// batch's derivative partials, then the gradient and the Adam step, cosine-decayed
 // learning rate as for the coupling flow.
 int spline_train(kb_flow *f, int64_t count, const std::vector<float> &hx, const std::vector<float> &hw,
                  const kb_flow_train_cfg *cfg, int64_t batch, int64_t per_epoch, int64_t steps, double *loss_hist,
@@ -66,12 +93,13 @@ int spline_train(kb_flow *f, int64_t count, const std::vector<float> &hx, const 
   kb_context *ctx = f->ctx;
   cudaStream_t st = ctx->stream;
   const int N = f->dim;
-  const int sg = spline_grid(f, batch);
+  const int sg = param_grid(f, batch);
+  (void)N;
   DevBuf dx, dw, di, dpart, dlp, dhist;
   KB_CUDA(dx.alloc(hx.size() * sizeof(float), st));
   KB_CUDA(dw.alloc(hw.size() * sizeof(float), st));
   KB_CUDA(di.alloc((size_t)count * sizeof(int), st));
-  KB_CUDA(dpart.alloc((size_t)sg * N * spline_grad_per_dim() * sizeof(double), st));
+  KB_CUDA(dpart.alloc((size_t)sg * param_partial(f) * sizeof(double), st));
   KB_CUDA(dlp.alloc((size_t)sg * sizeof(double), st));
   KB_CUDA(dhist.alloc((size_t)steps * sizeof(double), st));
   KB_CUDA(cudaMemcpyAsync(dx.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
@@ -86,15 +114,14 @@ int spline_train(kb_flow *f, int64_t count, const std::vector<float> &hx, const 
     KB_CUDA(cudaStreamSynchronize(st)); // the previous epoch's steps read the old order
     KB_CUDA(cudaMemcpyAsync(di.p, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     for (int64_t b = 0; b < per_epoch; ++b, ++s) {
-      KB_CUDA(launch_spline_grad(f->master, N, batch, dx.as<float>(), dw.as<float>(), di.as<int>() + b * batch,
-                                 1.0 / (double)batch, dpart.as<double>(), dlp.as<double>(), sg, st));
+      KB_CUDA(param_grad(f, batch, dx.as<float>(), dw.as<float>(), di.as<int>() + b * batch, 1.0 / (double)batch,
+                         dpart.as<double>(), dlp.as<double>(), sg, st));
       const int64_t t = ++f->adam_step;
       const double lr = cfg->lr_final + 0.5 * (cfg->lr - cfg->lr_final) * (1.0 + std::cos(pi * (double)s / (double)steps));
       const float bc1 = (float)(1.0 - std::pow((double)cfg->beta1, (double)t));
       const float bc2 = (float)(1.0 - std::pow((double)cfg->beta2, (double)t));
-      KB_CUDA(launch_spline_adam(f->master, f->adam_m, f->adam_v, N, dpart.as<double>(), sg, dlp.as<double>(),
-                                 dhist.as<double>() + s, nullptr, (float)lr, cfg->beta1, cfg->beta2, cfg->eps, bc1, bc2,
-                                 st));
+      KB_CUDA(param_adam(f, dpart.as<double>(), sg, dlp.as<double>(), dhist.as<double>() + s, nullptr, (float)lr,
+                         cfg->beta1, cfg->beta2, cfg->eps, bc1, bc2, st));
     }
   }
   std::vector<double> hist((size_t)steps);
@@ -157,13 +184,21 @@ int kb_flow_create(kb_context *ctx, int dim, uint64_t seed, kb_flow **out) {
 int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_flow **out) {
   if (kind == KB_FLOW_COUPLING) return kb_flow_create(ctx, dim, seed, out);
   KB_CHECK(ctx && out, "kb_flow_create_kind: null argument");
-  KB_CHECK(kind == KB_FLOW_SPLINE, "flow kind must be KB_FLOW_COUPLING or KB_FLOW_SPLINE");
+  KB_CHECK(kind == KB_FLOW_SPLINE || kind == KB_FLOW_AR_SPLINE,
+           "flow kind must be KB_FLOW_COUPLING, KB_FLOW_SPLINE or KB_FLOW_AR_SPLINE");
   KB_CHECK(dim >= 1 && dim <= FLOW_MAX_DIM, "flow dimension must be in [1, 8]");
-  // identity map: equal bins, knot derivatives 1 (softplus(c) = 1 - SPL_MIN_DERIV)
+  // identity map: equal bins, knot derivatives 1 (softplus(c) = 1 - SPL_MIN_DERIV); the
+  // autoregressive flow holds them in each dimension's constant feature, the other
+  // features' weights zero
   std::vector<float> init((size_t)FLOW_NPARAM, 0.0f);
   const float c0 = (float)std::log(std::expm1(1.0 - SPL_MIN_DERIV));
   for (int d = 0; d < dim; ++d)
-    for (int k = 0; k <= SPL_BINS; ++k) init[(size_t)d * SPL_PER_DIM + 2 * SPL_BINS + k] = c0;
+    for (int k = 0; k <= SPL_BINS; ++k) {
+      if (kind == KB_FLOW_SPLINE)
+        init[(size_t)d * SPL_PER_DIM + 2 * SPL_BINS + k] = c0;
+      else
+        init[(size_t)ar_offset(d) + (size_t)(2 * SPL_BINS + k) * ar_features(d)] = c0;
+    }
   (void)seed;
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
@@ -171,7 +206,7 @@ int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_fl
   f->ctx = ctx;
   f->device = ctx->device;
   f->dim = dim;
-  f->layout.kind = FLOW_KIND_SPLINE;
+  f->layout.kind = kind == KB_FLOW_SPLINE ? FLOW_KIND_SPLINE : FLOW_KIND_AR_SPLINE;
   f->layout.dim = dim;
   const size_t nb = (size_t)FLOW_NPARAM * sizeof(float);
   cudaError_t e = device_malloc(&f->master, nb);
@@ -198,6 +233,7 @@ int kb_flow_create_kind(kb_context *ctx, int dim, int kind, uint64_t seed, kb_fl
 
 int kb_flow_num_params(const kb_flow *f) {
   if (!f) return 0;
+  if (f->layout.kind == FLOW_KIND_AR_SPLINE) return ar_num_params(f->dim);
   return f->layout.kind == FLOW_KIND_SPLINE ? f->dim * SPL_PER_DIM : FLOW_NPARAM;
 }
 
@@ -217,7 +253,7 @@ int kb_flow_dim(const kb_flow *f) { return f ? f->dim : 0; }
 
 int kb_flow_get_params(kb_flow *f, float *params) {
   KB_CHECK(f && params, "kb_flow_get_params: null argument");
-  if (f->layout.kind == FLOW_KIND_SPLINE) {
+  if (param_flow(f)) {
     std::lock_guard<std::mutex> lk(f->ctx->mu);
     KB_CUDA(cudaSetDevice(f->device));
     KB_CUDA(cudaMemcpyAsync(params, f->master, (size_t)kb_flow_num_params(f) * sizeof(float), cudaMemcpyDeviceToHost,
@@ -239,7 +275,7 @@ int kb_flow_set_params(kb_flow *f, const float *params) {
   KB_CHECK(f && params, "kb_flow_set_params: null argument");
   for (int i = 0; i < kb_flow_num_params(f); ++i)
     if (!std::isfinite(params[i])) return fail(KB_E_INVALID, "flow parameters must be finite");
-  if (f->layout.kind == FLOW_KIND_SPLINE) {
+  if (param_flow(f)) {
     std::lock_guard<std::mutex> lk(f->ctx->mu);
     KB_CUDA(cudaSetDevice(f->device));
     cudaStream_t st = f->ctx->stream;
@@ -335,23 +371,23 @@ int kb_flow_gradient(kb_flow *f, int64_t count, const double *x, const double *w
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  if (f->layout.kind == FLOW_KIND_SPLINE) {
-    const int sg = spline_grid(f, count);
+  if (param_flow(f)) {
+    const int sg = param_grid(f, count);
     DevBuf dx, dw, di, dpart, dlp, dloss, dgrad;
     KB_CUDA(dx.alloc(hx.size() * sizeof(float), st));
     KB_CUDA(dw.alloc(hw.size() * sizeof(float), st));
     KB_CUDA(di.alloc(idx.size() * sizeof(int), st));
-    KB_CUDA(dpart.alloc((size_t)sg * N * spline_grad_per_dim() * sizeof(double), st));
+    KB_CUDA(dpart.alloc((size_t)sg * param_partial(f) * sizeof(double), st));
     KB_CUDA(dlp.alloc((size_t)sg * sizeof(double), st));
     KB_CUDA(dloss.alloc(sizeof(double), st));
     KB_CUDA(dgrad.alloc((size_t)kb_flow_num_params(f) * sizeof(float), st));
     KB_CUDA(cudaMemcpyAsync(dx.p, hx.data(), hx.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     KB_CUDA(cudaMemcpyAsync(dw.p, hw.data(), hw.size() * sizeof(float), cudaMemcpyHostToDevice, st));
     KB_CUDA(cudaMemcpyAsync(di.p, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-    KB_CUDA(launch_spline_grad(f->master, N, count, dx.as<float>(), dw.as<float>(), di.as<int>(), 1.0 / (double)count,
-                               dpart.as<double>(), dlp.as<double>(), sg, st));
-    KB_CUDA(launch_spline_adam(f->master, f->adam_m, f->adam_v, N, dpart.as<double>(), sg, dlp.as<double>(),
-                               dloss.as<double>(), dgrad.as<float>(), 0.0f, 0.0f, 0.0f, 1.0f, 1.0f, 1.0f, st));
+    KB_CUDA(param_grad(f, count, dx.as<float>(), dw.as<float>(), di.as<int>(), 1.0 / (double)count,
+                       dpart.as<double>(), dlp.as<double>(), sg, st));
+    KB_CUDA(param_adam(f, dpart.as<double>(), sg, dlp.as<double>(), dloss.as<double>(), dgrad.as<float>(), 0.0f, 0.0f,
+                       0.0f, 1.0f, 1.0f, 1.0f, st));
     double lsum = 0.0;
     KB_CUDA(cudaMemcpyAsync(grad, dgrad.p, (size_t)kb_flow_num_params(f) * sizeof(float), cudaMemcpyDeviceToHost, st));
     KB_CUDA(cudaMemcpyAsync(&lsum, dloss.p, sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -420,7 +456,7 @@ int kb_flow_train(kb_flow *f, int64_t count, const double *x, const double *w, c
   std::lock_guard<std::mutex> lk(ctx->mu);
   KB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
-  if (f->layout.kind == FLOW_KIND_SPLINE) return spline_train(f, count, hx, hw, cfg, batch, per_epoch, steps, loss_hist,
+  if (param_flow(f)) return spline_train(f, count, hx, hw, cfg, batch, per_epoch, steps, loss_hist,
                                                                n_steps);
   const int grid = train_grid(f, batch);
   DevBuf dx, dw, di, dpart, dlp, dxs, dhist;

@@ -42,6 +42,7 @@ __host__ __device__ inline int flow_img_index(int r, int k) {
 // SPL_MIN_DERIV.
 constexpr int FLOW_KIND_COUPLING = 0;
 constexpr int FLOW_KIND_SPLINE = 1;
+constexpr int FLOW_KIND_AR_SPLINE = 2; // autoregressive spline flow (flow_arspline.cu)
 constexpr int SPL_BINS = 16;
 constexpr int SPL_PER_DIM = 3 * SPL_BINS + 1;
 constexpr double SPL_MIN_BIN = 1e-3;
@@ -94,6 +95,23 @@ cudaError_t launch_flow_pack(const float *master, uint16_t *img, cudaStream_t st
 cudaError_t launch_spline_map(const float *params, int dim, int direction, long long count, const double *in,
                               SobolDev rng, uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out,
                               double *out2, int grid, cudaStream_t st);
+// The autoregressive spline flow (flow_arspline.cu; parameters: kb_spline.cuh's layout,
+// ar_num_params(dim) floats): its maps, the per-CTA partial derivatives of the weighted
+// negative log-likelihood over a batch ([grid][ar_num_params(dim)] and [grid], fp64; grid
+// from ar_grad_grid), and the step that sums them in CTA order and takes the Adam step.
+cudaError_t ar_configure();
+size_t ar_grad_smem_bytes(int dim);
+int ar_grad_grid(long long count, int sm_count);
+cudaError_t launch_ar_map(const float *params, int dim, int direction, long long count, const double *in,
+                          SobolDev rng, uint32_t k_first, const uint32_t *k_first_dev, int use_sobol, double *out,
+                          double *out2, int grid, cudaStream_t st);
+cudaError_t launch_ar_grad(const float *params, int dim, long long count, const float *x, const float *w,
+                           const int *index, double inv_batch, double *partials, double *loss_part, int grid,
+                           cudaStream_t st);
+cudaError_t launch_ar_adam(float *params, float *m, float *v, int dim, const double *partials, int nparts,
+                           const double *loss_part, double *loss_out, float *grad_out, float lr, float beta1,
+                           float beta2, float eps, float bc1, float bc2, cudaStream_t st);
+
 // Knots of the spline flow's dimensions from its parameters, [dim][SPL_KNOT_DOUBLES]: what a
 // work item's in-line map reads (ItemDev::spline_knots).
 cudaError_t launch_spline_knots(const float *params, int dim, double *knots, cudaStream_t st);

@@ -20,8 +20,10 @@ static_assert(sizeof(SplineKnots) == SPL_KNOT_DOUBLES * sizeof(double), "knots l
 __device__ __forceinline__ double spline_softplus(double v) { return v > 30.0 ? v : log1p(exp(v)); }
 
 // Knots of one dimension from its SPL_PER_DIM parameters (width logits, height logits,
-// knot-derivative pre-activations).
-__device__ inline void spline_make_knots(const float *p, SplineKnots &k) {
+// knot-derivative pre-activations): the flow's fp32 parameters, or the autoregressive
+// flow's fp64 conditioner output.
+template <typename T>
+__device__ inline void spline_make_knots(const T *p, SplineKnots &k) {
   constexpr double MW = SPL_MIN_BIN, MH = SPL_MIN_BIN, MD = SPL_MIN_DERIV;
   double mxa = -1e300, mxb = -1e300;
   for (int j = 0; j < SPL_BINS; ++j) {
@@ -72,6 +74,52 @@ __device__ __forceinline__ double spline_inverse(const SplineKnots &k, double v,
   xi = fmin(fmax(xi, 0.0), 1.0);
   deriv = spline_deriv(k, j, xi);
   return fmin(fmax(k.x[j] + xi * w, 0.0), 1.0);
+}
+
+// ---- the autoregressive (Knothe-Rosenblatt) spline flow: dimension d's SPL_PER_DIM
+// parameters are theta_d = A_d phi_d, phi_d = [1, P1(x_k), P2(x_k), P3(x_k) for k < d]
+// (Legendre polynomials on [0, 1]); A_d is [SPL_PER_DIM][ar_features(d)] row-major and the
+// flow's parameters hold A_0, A_1, ... in order.
+constexpr int AR_NFEAT = 3;
+constexpr int AR_MAX_FEAT = 1 + AR_NFEAT * (FLOW_MAX_DIM - 1);
+__host__ __device__ inline int ar_features(int d) { return 1 + AR_NFEAT * d; }
+__host__ __device__ inline int ar_offset(int d) { return SPL_PER_DIM * (d + AR_NFEAT * d * (d - 1) / 2); }
+__host__ __device__ inline int ar_num_params(int dim) { return ar_offset(dim); }
+
+// Appends coordinate x_k's features to phi (phi[1 + 3k .. 3 + 3k]).
+__device__ __forceinline__ void ar_append_features(double *phi, int k, double xk) {
+  const double u = 2.0 * xk - 1.0;
+  phi[1 + AR_NFEAT * k] = u;
+  phi[2 + AR_NFEAT * k] = 1.5 * u * u - 0.5;
+  phi[3 + AR_NFEAT * k] = (2.5 * u * u - 1.5) * u;
+}
+
+// theta = A phi, A [SPL_PER_DIM][F] (fp32), sums over the features in order.
+__device__ __forceinline__ void ar_theta(const float *A, const double *phi, int F, double *theta) {
+  for (int q = 0; q < SPL_PER_DIM; ++q) {
+    double s = 0.0;
+    for (int f = 0; f < F; ++f) s = fma((double)A[q * F + f], phi[f], s);
+    theta[q] = s;
+  }
+}
+
+// Sampling direction of the autoregressive flow on one point: x (stride st) holds the
+// Sobol coordinates z on entry and x = F^{-1}(z) on return, dimension by dimension (each
+// conditioned on the ones before); returns dx/dz = prod_d 1 / F_d'(x_d).
+static __device__ __noinline__ double ar_spline_point(const float *params, int N, double *x, int st) {
+  double phi[AR_MAX_FEAT], theta[SPL_PER_DIM];
+  SplineKnots k;
+  phi[0] = 1.0;
+  double jac = 1.0;
+  for (int d = 0; d < N; ++d) {
+    if (d > 0) ar_append_features(phi, d - 1, x[(d - 1) * st]);
+    ar_theta(params + ar_offset(d), phi, ar_features(d), theta);
+    spline_make_knots(theta, k);
+    double der;
+    x[d * st] = spline_inverse(k, x[d * st], der);
+    jac /= der;
+  }
+  return jac;
 }
 
 } // namespace kb

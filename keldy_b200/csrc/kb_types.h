@@ -107,6 +107,9 @@ struct ItemDev {
   // learned separable spline flow applied in line (integrate mode): [order][3 * 17] knots
   // (bin edges x, y and derivatives, kb_spline.cuh) of its dimensions; null = none
   const double *spline_knots;
+  // learned autoregressive spline flow applied in line: its fp32 parameters (the
+  // conditioners A_d, kb_spline.cuh); null = none
+  const float *ar_spline;
 };
 
 // One chunk of points of one item, processed by one CTA iteration.

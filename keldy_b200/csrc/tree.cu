@@ -98,6 +98,7 @@ __device__ void load_points(const Launch &L, const ItemDev &it, int N, int np, l
       uint32_t k = it.k_first + (uint32_t)gp;
       for (int j = 0; j < N; ++j) x[j * np] = sobol_coord(it.rng, k, j);
       if (it.spline_knots) jac = spline_flow_point(it.spline_knots, N, x, np);
+      if (it.ar_spline) jac = ar_spline_point(it.ar_spline, N, x, np);
     }
     jac *= chain_reverse(it.chain, it.chain_len, 0, N, x, np);
   } else {
@@ -139,6 +140,7 @@ __device__ void prepare_point(const Launch &L, const ItemDev &it, int N, long lo
       const uint32_t k = it.k_first + (uint32_t)gp;
       for (int j = 0; j < N; ++j) x[j] = sobol_coord(it.rng, k, j);
       if (it.spline_knots) jac = spline_flow_point(it.spline_knots, N, x, 1);
+      if (it.ar_spline) jac = ar_spline_point(it.ar_spline, N, x, 1);
     }
     jac *= chain_reverse(it.chain, it.chain_len, 0, N, x, 1);
   } else {

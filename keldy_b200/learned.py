@@ -18,19 +18,43 @@ from . import capi, rqmc
 DEFAULT_TRAIN = dict(epochs=10, batch=8192, lr=2e-3, lr_final=1e-4)
 # the separable spline flow has ~50 parameters per dimension: larger steps, more epochs
 SPLINE_TRAIN = dict(epochs=20, batch=8192, lr=2e-2, lr_final=1e-3)
+# the autoregressive spline flow after its separable warm start: a smaller first step
+AR_TRAIN = dict(epochs=20, batch=8192, lr=5e-3, lr_final=2e-4)
 
 
 def fit(ctx, model, A, B, chain, order, n_samples=1 << 18, seed=0, k_first=1, kind=capi.FLOW_COUPLING, **cfg):
-    """Creates and trains a flow (kind FLOW_COUPLING or FLOW_SPLINE) of dimension `order` on
-    n_samples plain-method points. Returns (flow, seconds, final loss)."""
-    c = dict(SPLINE_TRAIN if kind == capi.FLOW_SPLINE else DEFAULT_TRAIN, **cfg)
+    """Creates and trains a flow (kind FLOW_COUPLING, FLOW_SPLINE or FLOW_AR_SPLINE) of
+    dimension `order` on n_samples plain-method points. The autoregressive spline flow is
+    warm-started from a separable spline flow trained first (its parameters in the constant
+    feature), then trained as a whole. Returns (flow, seconds, final loss)."""
+    c = dict(DEFAULT_TRAIN if kind == capi.FLOW_COUPLING else SPLINE_TRAIN, **cfg)
     c.setdefault("seed", seed)
     flow = ctx.flow(order, seed=seed, kind=kind)
     ctx.synchronize()
     t0 = time.perf_counter()
+    if kind == capi.FLOW_AR_SPLINE:
+        sep = ctx.flow(order, seed=seed, kind=capi.FLOW_SPLINE)
+        sep.fit(model, A, B, chain, ctx.sobol(order), n_samples, k_first=k_first, **c)
+        flow.set_params(ar_from_separable(sep.params()))
+        sep.close()
+        c = dict(c, **AR_TRAIN)
+        c.update(cfg)
     loss = flow.fit(model, A, B, chain, ctx.sobol(order), n_samples, k_first=k_first, **c)
     ctx.synchronize()
     return flow, time.perf_counter() - t0, loss
+
+
+def ar_from_separable(sep):
+    """Parameters of the autoregressive spline flow equal to a separable spline flow's
+    (sep [dim][49]): each dimension's in its constant feature, the other weights zero."""
+    sep = np.atleast_2d(np.asarray(sep, dtype=np.float32))
+    dim = sep.shape[0]
+    out = []
+    for d in range(dim):
+        a = np.zeros((49, 1 + 3 * d), dtype=np.float32)
+        a[:, 0] = sep[d]
+        out.append(a.ravel())
+    return np.concatenate(out)
 
 
 def variance_gain(ctx, model, A, B, chain, flow, n_points=1 << 15, seed_shift=977):
