@@ -366,12 +366,32 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
 
 // Two breadth-first levels at once: node `par` (m x m) into its four grandchildren
 // 4 par + 2 b + bp (pivot on row b, then on row bp of that child), (m-4) x (m-4) each,
-// every entry formed exactly as two tree_level2 steps form it. Each item (grandchild row
-// i of a parent, a column segment, all four grandchildren) forms the pivots and child
-// entries it needs itself, so the pair takes one barrier and never stores the children.
+// every entry formed exactly as two tree_level2 steps form it. A pre-pass forms each
+// parent's pivot quantities once (one thread per (parent, b, b'), into pv); then each item
+// (grandchild row i of a parent, a column segment, all four grandchildren) forms the child
+// entries it needs itself, so the pair takes two barriers and never stores the children.
+// (Items that formed the pivot quantities themselves, six reciprocals each, with one
+// barrier per pair, were 4-13 % slower at orders 6-10.)
 __device__ void tree_level4(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int nodes,
-                            int lg_npp, int m, double floor_) {
+                            int lg_npp, int m, double floor_, double2 *pv) {
   const int mg = m - 4, mm = m * m, mgg = mg * mg;
+  // the pivot quantities of every (parent, b, b') once, before the rows (pv: 12 entries
+  // per parent): the first pivot's reciprocal, child row b''s factor and the second
+  // pivot's reciprocal; the guard flags and the grandchildren's prefix determinants
+  for (int c = threadIdx.x; c < nodes * 4; c += blockDim.x) {
+    const int par = c >> 2, b = (c >> 1) & 1, bp = c & 1;
+    const double2 *S = cur + par * mm;
+    const double2 piv = S[b * (m + 1)];
+    const double2 ibv = crcp(piv);
+    const double2 Lpv = cmul(S[(2 + bp) * m + b], ibv); // child row bp's factor
+    const double2 cpv = cfms(S[(2 + bp) * m + 2 + bp], Lpv, S[b * m + 2 + bp]);
+    pv[c * 3 + 0] = ibv;
+    pv[c * 3 + 1] = Lpv;
+    pv[c * 3 + 2] = crcp(cpv);
+    if (!(cabs1(piv) >= floor_) || !(cabs1(cpv) >= floor_)) flag[par >> lg_npp] |= 2;
+    Dn[c] = cmul(cmul(Dc[par], piv), cpv);
+  }
+  __syncthreads();
   const unsigned rows = (unsigned)(nodes * mg);
   const unsigned magic = 0xFFFFFFFFu / (unsigned)mg + 1u; // r / mg == umulhi(r, magic) for r < 2^20, mg <= 31
   int lgseg = 0;
@@ -387,21 +407,14 @@ __device__ void tree_level4(const double2 *cur, double2 *nxt, const double2 *Dc,
     double2 ib[2], Lp[2][2], icp[2][2], Lr[2], Lg[2][2];
 #pragma unroll
     for (int b = 0; b < 2; ++b) {
-      ib[b] = crcp(S[b * (m + 1)]);
+      ib[b] = pv[(par * 4 + 2 * b) * 3];
       Lr[b] = cmul(S[(i + 4) * m + b], ib[b]);
 #pragma unroll
       for (int bp = 0; bp < 2; ++bp) {
-        Lp[b][bp] = cmul(S[(2 + bp) * m + b], ib[b]); // child row bp's factor
-        const double2 cpv = cfms(S[(2 + bp) * m + 2 + bp], Lp[b][bp], S[b * m + 2 + bp]);
-        icp[b][bp] = crcp(cpv);
+        Lp[b][bp] = pv[(par * 4 + 2 * b + bp) * 3 + 1];
+        icp[b][bp] = pv[(par * 4 + 2 * b + bp) * 3 + 2];
         const double2 cib = cfms(S[(i + 4) * m + 2 + bp], Lr[b], S[b * m + 2 + bp]); // child row i+2, column bp
         Lg[b][bp] = cmul(cib, icp[b][bp]);
-        if (i == 0 && j0 == 0) {
-          const int g = 4 * par + 2 * b + bp;
-          const double2 piv = S[b * (m + 1)];
-          if (!(cabs1(piv) >= floor_) || !(cabs1(cpv) >= floor_)) flag[par >> lg_npp] |= 2;
-          Dn[g] = cmul(cmul(Dc[par], piv), cpv);
-        }
       }
     }
     const double2 *sr = S + (i + 4) * m + 4, *s0 = S + 4, *s1 = S + m + 4, *s2 = S + 2 * m + 4, *s3 = S + 3 * m + 4;
@@ -714,7 +727,7 @@ __device__ int tree_sub(TreeShared &S, int N, int np, int rb, const double2 *roo
   int m = 2 * N + 1, cur = rb, nodes = np, lg = 0;
   const double2 *src = root;
   for (int k = 0; k + 1 < LB; k += 2) { // pairs of levels, then a last single one
-    tree_level4(src, S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], flag, nodes, lg, m, floor_);
+    tree_level4(src, S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], flag, nodes, lg, m, floor_, S.tmp);
     nodes *= 4;
     lg += 2;
     m -= 4;
