@@ -617,8 +617,8 @@ def run_ours(args, rank, world, local_rank):
         traffic = TREE_DRAM_CAPTURES.get(src_hash) if (order == 8 and N == 1 << 20) else None
         traffic_source = (f"dram__bytes_read.sum + dram__bytes_write.sum of one 2^20-point order-8 tree_kernel launch "
                           f"(ncu) of the kernel sources with hash {src_hash}: the g0 table and set-up data read once, "
-                          f"and the staged G matrices that L2 writes back (~154 B per evaluation of the 4.6 KB "
-                          f"staged); the table gathers are served by L2/L1"
+                          f"and the part of the staged G matrices (4.6 KB per evaluation) that L2 writes back; the "
+                          f"table gathers are served by L2/L1"
                           if traffic is not None else
                           f"no ncu capture of the kernel sources with hash {src_hash} at this workload")
         line = {
