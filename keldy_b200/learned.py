@@ -1,10 +1,13 @@
-"""The learned warper workflow: a coupling flow per perturbation order, trained on the
-GPU on |integrand| samples of the plain method, judged against the plain warper chain.
+"""The learned warper workflow: a flow per perturbation order, trained on the GPU on
+|integrand| samples of the plain method, judged against the plain warper chain.
 
-The flow (kb_flow_*, keldy_b200/csrc/flow.cu) is a first stage before keldy's warper
-chain (warpers.hpp:72-85); the plain chain alone is the method without it. Both are
-estimated with randomised QMC (R random digital shifts of the Sobol sequence,
-qrng.hpp:77-109), so their standard errors and their agreement are measured the same way.
+Three flow designs (kb_flow_*): coupling layers with tensor-core MLP conditioners
+(csrc/flow.cu), a separable rational-quadratic spline per dimension (csrc/flow_spline.cu;
+the one that pays under quasi-Monte Carlo) and its autoregressive extension
+(csrc/flow_arspline.cu). The flow is a first stage before keldy's warper chain
+(warpers.hpp:72-85); the plain chain alone is the method without it. Both are estimated
+with randomised QMC (R random digital shifts of the Sobol sequence, qrng.hpp:77-109), so
+their standard errors and their agreement are measured the same way.
 """
 from __future__ import annotations
 
