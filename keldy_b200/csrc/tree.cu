@@ -1544,7 +1544,10 @@ __host__ __device__ inline int km_root_buffer(int N) {
 // 2(n - j) - 1). bsel < 0: both children (child 2 par + b pivots on copy b); otherwise
 // the single child on copy bsel. inv and Dn get the children's pivot reciprocals and
 // prefix determinants. (Each item forming its own reciprocals instead, without the
-// barrier after them, was 2-5 % slower at orders 6-8.)
+// barrier after them, was 2-5 % slower at orders 6-8; levels fused in pairs as in the
+// direct tree, with a pivot pre-pass and the children never stored, were 6-16 % slower at
+// orders 5-8: the kept rows make each grandchild entry cost 2.5 complex FMAs there
+// against 1.5 in two single levels.)
 __device__ void km_level(const double2 *cur, int cs, double2 *nxt, const double2 *Dc, double2 *Dn, double2 *inv,
                          int *flag, int nodes, int lg_npp, int j, int n, int bsel, double floor_) {
   const int R = 2 * n - j, C = 2 * (n - j) + 1;
