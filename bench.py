@@ -34,20 +34,30 @@ if ROOT not in sys.path:
 GAMMA, EPS_D, BIAS, BETA, T_MAX, NPTS = 1.0, 0.0, 0.0, 50.0, 20.0, 40001
 # DRAM bytes (read + write) of one tree_kernel launch of this workload (2^20 points,
 # order 8) from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
-# the hash of the kernel's sources (tree_source_hash) at the time of the capture. A build
+# the hash of the kernel's code (tree_source_hash, comments stripped) at the time of the capture. A build
 # whose sources hash differently reports no traffic figure until it is captured again.
-TREE_DRAM_CAPTURES = {"c7803a48e9775d6f": 2231296 + 157266944}
+TREE_DRAM_CAPTURES = {"c7e203613128e12e": 2231296 + 157266944}
 TREE_SOURCES = ("tree.cu", "kb_device.cuh", "kb_types.h", "kb_launch.h", "kb_spline.cuh", "kb_flow.h")
 E2E_REPEATS = 5
 
 
+def _code_only(text):
+    """C++ source without its comments and with runs of white space collapsed (these sources
+    hold no string literal with a comment marker), so that a comment edit keeps the hash."""
+    import re
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    text = re.sub(r"//[^\n]*", " ", text)
+    return " ".join(text.split())
+
+
 def tree_source_hash():
-    """First 16 hex digits of the SHA-256 of the tree kernel's source files."""
+    """First 16 hex digits of the SHA-256 of the tree kernel's source files, comments
+    stripped."""
     import hashlib
     h = hashlib.sha256()
     for f in TREE_SOURCES:
-        with open(os.path.join(ROOT, "keldy_b200", "csrc", f), "rb") as fh:
-            h.update(fh.read())
+        with open(os.path.join(ROOT, "keldy_b200", "csrc", f), encoding="utf-8") as fh:
+            h.update(_code_only(fh.read()).encode())
     return h.hexdigest()[:16]
 
 
