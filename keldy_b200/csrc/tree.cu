@@ -899,6 +899,7 @@ __global__ void __launch_bounds__(TREE_THREADS, 4) tree_kernel(Launch L) {
   // hold no registers through the tree
   __shared__ ChunkPartial s_part;
   __shared__ unsigned s_drop;
+  __shared__ unsigned s_bal[3][TREE_THREADS / 32]; // per warp: in-domain, guarded and dropped points of a batch
   const int tid = threadIdx.x;
   if (tid == 0) s_bad = 0;
   for (;;) {
@@ -959,49 +960,79 @@ __global__ void __launch_bounds__(TREE_THREADS, 4) tree_kernel(Launch L) {
           if (L.out_scale) L.out_scale[o] = dom ? S.fscale[tid] * fabs(j) : 0.0;
           if (L.out_flag) L.out_flag[o] = (dom && (fl & 2)) ? 1 : 0;
         }
-      } else if (tid == 0) {
-        double2 csum = c2(s_part.sum_re, s_part.sum_im);
-        unsigned long long cdom = s_part.n_in_domain, cfb = s_part.n_fallback;
-        unsigned long long mask0 = s_part.fb_mask[0], mask1 = s_part.fb_mask[1];
-        unsigned cdrop = s_drop;
-        for (int p = 0; p < gb; ++p) {
-          int fl = S.flag[p];
-          const double2 fv = S.fval[p];
+      } else {
+        // the batch's point values, one thread per point; then each warp's sum in a fixed
+        // shuffle order, and thread 0 adds the warps in order (deterministic)
+        const int lane = tid & 31, w = tid >> 5;
+        bool dom = false, fb = false, drop = false;
+        double2 fj = c2(0.0, 0.0);
+        if (tid < gb) {
+          int fl = S.flag[tid];
+          const double2 fv = S.fval[tid];
           if (!isfinite(fv.x) || !isfinite(fv.y)) fl |= 2;
-          const int q = g0 + p;
+          const int q = g0 + tid;
           int bin = -2;
           if (L.nbins) { // the code prepare_point stored: 2 bin, or -1 when dropped
             const double code = slot[BIN_CODE_ROW * CHUNK_POINTS + q];
             bin = code < 0.0 ? -1 : (int)code >> 1;
-            if (bin < 0) cdrop++;
+            drop = bin < 0;
           }
-          if (fl & 1) continue;
-          cdom++;
-          if (fl & 2) {
-            if (q < 64)
-              mask0 |= 1ull << q;
-            else
-              mask1 |= 1ull << (q - 64);
-            cfb++;
-            continue;
-          }
-          const double2 f = apply_cutoff(fv, it.f.cutoff);
-          const double j = S.jac[p];
-          csum.x += f.x * j;
-          csum.y += f.y * j;
-          if (bin >= 0) {
-            slot[BIN_CODE_ROW * CHUNK_POINTS + q] = (double)(2 * bin + 1);
-            slot[(BIN_CODE_ROW + 1) * CHUNK_POINTS + q] = f.x * j;
-            slot[(BIN_CODE_ROW + 2) * CHUNK_POINTS + q] = f.y * j;
+          if (!(fl & 1)) {
+            dom = true;
+            fb = (fl & 2) != 0;
+            if (!fb) {
+              const double2 f = apply_cutoff(fv, it.f.cutoff);
+              const double j = S.jac[tid];
+              fj = c2(f.x * j, f.y * j);
+              if (bin >= 0) {
+                slot[BIN_CODE_ROW * CHUNK_POINTS + q] = (double)(2 * bin + 1);
+                slot[(BIN_CODE_ROW + 1) * CHUNK_POINTS + q] = fj.x;
+                slot[(BIN_CODE_ROW + 2) * CHUNK_POINTS + q] = fj.y;
+              }
+            }
           }
         }
-        s_part.sum_re = csum.x;
-        s_part.sum_im = csum.y;
-        s_part.n_in_domain = cdom;
-        s_part.n_fallback = cfb;
-        s_part.fb_mask[0] = mask0;
-        s_part.fb_mask[1] = mask1;
-        s_drop = cdrop;
+        for (int off = 16; off > 0; off >>= 1) {
+          fj.x += __shfl_xor_sync(0xffffffffu, fj.x, off);
+          fj.y += __shfl_xor_sync(0xffffffffu, fj.y, off);
+        }
+        const unsigned bdom = __ballot_sync(0xffffffffu, dom), bfb = __ballot_sync(0xffffffffu, fb);
+        const unsigned bdrop = __ballot_sync(0xffffffffu, drop);
+        if (lane == 0) {
+          S.wsum[w] = fj;
+          s_bal[0][w] = bdom;
+          s_bal[1][w] = bfb;
+          s_bal[2][w] = bdrop;
+        }
+        __syncthreads();
+        if (tid == 0) {
+          double2 csum = c2(s_part.sum_re, s_part.sum_im);
+          unsigned long long cdom = s_part.n_in_domain, cfb = s_part.n_fallback;
+          unsigned long long mask0 = s_part.fb_mask[0], mask1 = s_part.fb_mask[1];
+          unsigned cdrop = s_drop;
+          for (int k = 0; k < TREE_THREADS / 32; ++k) {
+            csum = cadd(csum, S.wsum[k]);
+            cdom += __popc(s_bal[0][k]);
+            cfb += __popc(s_bal[1][k]);
+            cdrop += __popc(s_bal[2][k]);
+            // guarded points' chunk bits: point q = g0 + 32 k + lane
+            const unsigned long long m = s_bal[1][k];
+            const int b0 = g0 + 32 * k;
+            if (m && b0 < 64) {
+              mask0 |= m << b0;
+              if (b0 > 32) mask1 |= m >> (64 - b0);
+            } else if (m) {
+              mask1 |= m << (b0 - 64);
+            }
+          }
+          s_part.sum_re = csum.x;
+          s_part.sum_im = csum.y;
+          s_part.n_in_domain = cdom;
+          s_part.n_fallback = cfb;
+          s_part.fb_mask[0] = mask0;
+          s_part.fb_mask[1] = mask1;
+          s_drop = cdrop;
+        }
       }
       __syncthreads();
     }
