@@ -1811,6 +1811,54 @@ __device__ void km_tree_points_any(KMTreeShared &K, const ItemDev &it, int N, in
   }
 }
 
+// A pass's point values (one per thread, f, in the domain or not, with its dropped bin
+// terms) into the chunk's sums: each warp's by a fixed xor-shuffle pattern, then thread 0
+// adds the warps in order (deterministic). Every thread calls it; the caller's barrier
+// follows before the next pass.
+__device__ __noinline__ void km_pass_sum(double2 f, bool dom, unsigned long long drop, double2 &csum,
+                                         unsigned long long &cdom, unsigned *dropped) {
+  __shared__ double2 wsum[KM_THREADS / 32];
+  __shared__ unsigned wdom[KM_THREADS / 32];
+  __shared__ unsigned long long wdrop[KM_THREADS / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int off = 16; off > 0; off >>= 1) {
+    f.x += __shfl_xor_sync(0xffffffffu, f.x, off);
+    f.y += __shfl_xor_sync(0xffffffffu, f.y, off);
+    drop += __shfl_xor_sync(0xffffffffu, drop, off);
+  }
+  const unsigned bdom = __ballot_sync(0xffffffffu, dom);
+  if (lane == 0) {
+    wsum[w] = f;
+    wdom[w] = bdom;
+    wdrop[w] = drop;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned long long d = 0;
+    for (int k = 0; k < KM_THREADS / 32; ++k) {
+      csum = cadd(csum, wsum[k]);
+      cdom += __popc(wdom[k]);
+      d += wdrop[k];
+    }
+    if (dropped) *dropped += (unsigned)d;
+  }
+}
+
+// integrand_g_kernel_single_omega (wick_kernel_single_omega.cpp:126-135): point p's terms
+// weighted by e^{i omega t} of their vertex, in vertex order, times its Jacobian.
+__device__ __forceinline__ double2 km_fourier_value(const KMTreeShared &K, const Launch &L, int p, int np, int N) {
+  const int n2 = 2 * N;
+  double2 f = c2(0.0, 0.0);
+  for (int i = 0; i < N; ++i) {
+    double sn, cs;
+    sincos(L.km_omega * K.u[i * np + p], &sn, &cs);
+    const double2 sv = cadd(K.S[p * n2 + 2 * i], K.S[p * n2 + 2 * i + 1]);
+    f = cadd(f, cmul(sv, c2(cs, sn)));
+  }
+  const double j = K.jac[p];
+  return c2(f.x * j, f.y * j);
+}
+
 __global__ void __launch_bounds__(KM_THREADS, KM_CTAS_PER_SM) km_tree_kernel(Launch L) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   KMTreeShared &K = *reinterpret_cast<KMTreeShared *>(smem_raw);
@@ -1870,7 +1918,10 @@ __global__ void __launch_bounds__(KM_THREADS, KM_CTAS_PER_SM) km_tree_kernel(Lau
         __syncthreads();
       }
       // guarded points (and the spin-asymmetric ones): keldy's pivoted-LU path, one by one
-      for (int p = 0; p < np; ++p) {
+      bool g = false; // any guarded point (every warp finds the same answer, no barrier)
+      for (int p = tid & 31; p < np; p += 32) g = g || (K.flag[p] & 3) == 2;
+      const bool any_guarded = __any_sync(0xffffffffu, g);
+      for (int p = 0; any_guarded && p < np; ++p) {
         if ((K.flag[p] & 3) != 2) continue;
         double ut[KM_MAX_ORDER];
         for (int j = 0; j < N; ++j) ut[j] = K.u[j * np + p];
@@ -1897,19 +1948,17 @@ __global__ void __launch_bounds__(KM_THREADS, KM_CTAS_PER_SM) km_tree_kernel(Lau
       } else if (L.km_fourier) {
         // integrand_g_kernel_single_omega (wick_kernel_single_omega.cpp:126-135): the
         // point's terms weighted by e^{i omega t} of their vertex, in point and vertex order
-        if (tid == 0) {
+        // passes of more than two points: one thread per point, then km_pass_sum; one or
+        // two points: thread 0 in point order (no extra barrier)
+        if (P > 2) {
+          const bool dom = tid < np && !(K.flag[tid] & 1);
+          const double2 f = dom ? km_fourier_value(K, L, tid, np, N) : c2(0.0, 0.0);
+          km_pass_sum(f, dom, 0ull, csum, cdom, nullptr);
+        } else if (tid == 0) {
           for (int p = 0; p < np; ++p) {
             if (K.flag[p] & 1) continue;
             cdom++;
-            const double j = K.jac[p];
-            double2 f = c2(0.0, 0.0);
-            for (int i = 0; i < N; ++i) {
-              double sn, cs;
-              sincos(L.km_omega * K.u[i * np + p], &sn, &cs);
-              const double2 sv = cadd(K.S[p * n2 + 2 * i], K.S[p * n2 + 2 * i + 1]);
-              f = cadd(f, cmul(sv, c2(cs, sn)));
-            }
-            csum = c2(csum.x + f.x * j, csum.y + f.y * j);
+            csum = cadd(csum, km_fourier_value(K, L, p, np, N));
           }
         }
       } else {
@@ -1941,7 +1990,22 @@ __global__ void __launch_bounds__(KM_THREADS, KM_CTAS_PER_SM) km_tree_kernel(Lau
             L.bin_counts[(size_t)c * nb + bk] += cnt;
           }
         }
-        if (tid == 0) {
+        if (P > 2) { // as above: one thread per point, then km_pass_sum
+          double2 f = c2(0.0, 0.0);
+          unsigned long long drop = 0;
+          const bool dom = tid < np && !(K.flag[tid] & 1);
+          if (dom) {
+            const double j = K.jac[tid];
+            for (int i = 0; i < N; ++i) {
+              if (K.bidx[tid * N + i] < 0) drop += 2 * half;
+              for (int k = 0; k < 2; ++k) {
+                const double2 sv = K.S[tid * n2 + 2 * i + k];
+                f = c2(f.x + sv.x * j, f.y + sv.y * j);
+              }
+            }
+          }
+          km_pass_sum(f, dom, drop, csum, cdom, L.bin_dropped + c);
+        } else if (tid == 0) {
           for (int p = 0; p < np; ++p) {
             if (K.flag[p] & 1) continue;
             cdom++;
