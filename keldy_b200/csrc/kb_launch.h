@@ -46,9 +46,12 @@ static_assert(PTS_ROWS % 2 == 0 && PTS_SLOT % 2 == 0, "staged G on 16-byte bound
 __host__ __device__ inline int tree_gbatch(int N) {
   const int P = tree_points_per_chunk(N);
   const int M = 2 * N + 1;
+  // orders above TREE_MAX_SUB keep up to four subtree roots (17 x 17) and their prefix
+  // determinants after the batch's G matrices
+  const int R = 2 * TREE_MAX_SUB + 1, reserve = N > TREE_MAX_SUB ? 4 * R * R + 4 : 0;
   int g = CHUNK_POINTS;
   if (N > 0 && 256 / N < g) g = 256 / N;
-  if (G_STAGE / (M * M) < g) g = G_STAGE / (M * M);
+  if ((G_STAGE - reserve) / (M * M) < g) g = (G_STAGE - reserve) / (M * M);
   g -= g % P;
   return g > 0 ? g : P;
 }
@@ -107,37 +110,6 @@ inline int items_any_cubic(const ItemDev *items, size_t n) {
   for (size_t i = 0; i < n; ++i)
     if (items[i].model.interp == 3) return 1;
   return 0;
-}
-
-// Orders above TREE_MAX_SUB solve one point per sub-batch in 2^K0 passes (K0 = N -
-// TREE_MAX_SUB path steps, then the breadth-first levels down to 9x9 nodes), all starting
-// from the same G. That G stays at the end of one frontier buffer across the passes when
-// no step of a pass writes that buffer far enough to reach it (step t writes buffer t & 1
-// from its start) and it clears the bottom's scratch at the start of the free buffer.
-// Returns the buffer (0 or 1), or -1 when G has to be copied from the kernel's staging
-// area again for every pass (no order up to MAX_ORDER needs that).
-__host__ __device__ inline int tree_root_buffer(int N) {
-  if (N <= TREE_MAX_SUB) return -1;
-  // the kernel's schedule: K0 path steps, then the levels in pairs (tree_level4) and a
-  // last single one, each write into the other buffer
-  const int K0 = N - TREE_MAX_SUB, LB = TREE_MAX_SUB - 4, root = (2 * N + 1) * (2 * N + 1);
-  int use[2] = {0, 0};
-  int m = 2 * N + 1, nodes = 1, t = 0;
-  for (int k = 0; k < K0; ++k) {
-    m -= 2;
-    ++t;
-    if (use[t & 1] < m * m) use[t & 1] = m * m;
-  }
-  for (int k = 0; k < LB; k += (k + 1 < LB) ? 2 : 1) {
-    const int step = (k + 1 < LB) ? 2 : 1;
-    m -= 2 * step;
-    nodes <<= step;
-    ++t;
-    if (use[t & 1] < nodes * m * m) use[t & 1] = nodes * m * m;
-  }
-  for (int b = 0; b < 2; ++b)
-    if (use[b] + root <= FRONTIER && root + BOTTOM_SCRATCH <= FRONTIER) return b;
-  return -1;
 }
 
 size_t tree_smem_bytes();

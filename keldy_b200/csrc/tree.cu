@@ -798,7 +798,7 @@ __device__ __forceinline__ int tree_prefetch_offset(int N, int P) {
 // The G-batch's points (gb, staged G at gst: point p at p M^2): the integrand of each,
 // added to S.fval[p] (S.fscale[p]) with bit 1 of S.flag[p] set where a pivot fell below
 // the guard. S.D and the frontier buffers are free on entry; the caller's barrier follows.
-__device__ void tree_gbatch_points(TreeShared &S, const ItemDev &it, int N, int gb, const double2 *gst,
+__device__ void tree_gbatch_points(TreeShared &S, const ItemDev &it, int N, int gb, double2 *gst,
                                    bool want_scale, bool direct, int *bad) {
   const int tid = threadIdx.x;
   const int M = 2 * N + 1, MM = M * M;
@@ -815,29 +815,59 @@ __device__ void tree_gbatch_points(TreeShared &S, const ItemDev &it, int N, int 
     return;
   }
   if (N > TREE_MAX_SUB) {
-    // one point at a time in 2^K0 passes, each walking K0 levels along one root-to-subtree
-    // path, then the breadth-first levels of its subtree; the point's G is copied once and
-    // kept at the end of a frontier buffer when the passes leave it there (tree_root_buffer)
+    // one point at a time: the K0 = N - 8 levels above the order-8 subtrees. The last one
+    // (order 9) or two of them run breadth-first (tree_level2 / tree_level4 on one node) into
+    // the staging area after the batch's G matrices, 2^Kb subtree roots of 17 x 17 and their
+    // prefix determinants; the Kp levels before them are walked one root-to-node path at a
+    // time (2^Kp passes, the point's G copied again for each). Against walking all K0 levels
+    // by paths: orders 10 / 12 -4 / -20 %, order 9 +7 % (its one breadth-first level computes
+    // what its two paths did, through the staging area; the code that kept paths for order 9
+    // compiled into a kernel 13 % slower at order 10). Each subtree root is copied into shared memory
+    // asynchronously while the previous subtree's bottom runs. Subtrees are summed in the
+    // order of their path bits, first level first, as walking all K0 levels by paths would.
     const int K0 = N - TREE_MAX_SUB;
-    const int rb = tree_root_buffer(N);
-    double2 *root = rb >= 0 ? S.buf[rb] + (FRONTIER - MM) : S.buf[0];
+    const int Kb = K0 >= 2 ? 2 : 1, Kp = K0 - Kb, NS = 1 << Kb;
+    constexpr int R = 2 * TREE_MAX_SUB + 1, RR = R * R;
+    double2 *gsub = gst + (size_t)gb * MM;
+    double2 *gD = gsub + (size_t)NS * RR;
+    const int pf = tree_prefetch_offset(TREE_MAX_SUB, 1);
     for (int p = 0; p < gb; ++p) {
-      for (int sub = 0; sub < (1 << K0); ++sub) {
-        if (rb < 0 || sub == 0) copy_roots(root, gst + (size_t)p * MM, MM);
+      for (int sub = 0; sub < (1 << Kp); ++sub) {
+        copy_roots(S.buf[0], gst + (size_t)p * MM, MM);
         if (tid == 0) S.D[0][0] = c2(1.0, 0.0);
         cp_async_wait_all();
         __syncthreads();
         int m = M, cur = 0;
-        for (int k = 0; k < K0; ++k) {
-          const int b = (sub >> (K0 - 1 - k)) & 1;
-          tree_path_step(k == 0 ? root : S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag + p, m, b,
-                         floor_);
+        for (int k = 0; k < Kp; ++k) {
+          const int b = (sub >> (Kp - 1 - k)) & 1;
+          tree_path_step(S.buf[cur], S.buf[cur ^ 1], S.D[cur], S.D[cur ^ 1], S.flag + p, m, b, floor_);
           m -= 2;
           cur ^= 1;
         }
-        tree_sub(S, TREE_MAX_SUB, 1, cur, S.buf[cur], S.flag + p, S.fval + p, S.fscale + p, floor_, want_scale,
-                 __popc(sub), nullptr, 0, 0);
-        __syncthreads();
+        if (Kb == 2)
+          tree_level4(S.buf[cur], gsub, S.D[cur], gD, S.flag + p, 1, 0, m, floor_, S.tmp);
+        else
+          tree_level2(S.buf[cur], gsub, S.D[cur], gD, S.tmp, S.flag + p, 1, 0, m, floor_);
+        int rb = 0, roff = 0;
+        for (int g = 0; g < NS; ++g) {
+          if (g == 0) {
+            copy_roots(S.buf[0], gsub, RR);
+            if (tid == 0) S.D[0][0] = gD[0];
+            cp_async_wait_all();
+            __syncthreads();
+          }
+          const bool prefetch = pf >= 0 && g + 1 < NS;
+          const int bot = tree_sub(S, TREE_MAX_SUB, 1, rb, S.buf[rb] + roff, S.flag + p, S.fval + p, S.fscale + p,
+                                   floor_, want_scale, __popc(sub) + __popc(g), gsub + (size_t)(g + 1) * RR,
+                                   prefetch ? RR : 0, pf);
+          if (prefetch) {
+            rb = bot ^ 1;
+            roff = pf;
+            if (tid == 0) S.D[rb][0] = gD[g + 1];
+            cp_async_wait_all();
+          }
+          __syncthreads();
+        }
       }
     }
     return;
