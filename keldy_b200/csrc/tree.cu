@@ -1622,10 +1622,13 @@ __device__ void km_level(const double2 *cur, int cs, double2 *nxt, const double2
     Dn[c] = cmul(Dc[par], piv);
   }
   __syncthreads();
-  // rows split into column segments of at least 4 columns while the CTA has idle threads
+  // rows split into column segments while the CTA has idle threads: of at least 4 columns,
+  // down to single columns when a pass holds at most 4 points (orders 6 and up, whose top
+  // levels have few rows: order 8 7 % faster, orders 9 / 10 6 / 5 %; orders 4-5 2 % slower)
   const int rows = nodes * R1;
+  const int minc = (nodes >> lg_npp) <= 4 ? 1 : 4;
   int lgseg = 0;
-  while ((rows << (lgseg + 1)) <= (int)blockDim.x && (C1 >> (lgseg + 1)) >= 4) ++lgseg;
+  while ((rows << (lgseg + 1)) <= (int)blockDim.x && (C1 >> (lgseg + 1)) >= minc) ++lgseg;
   const int seglen = (C1 + (1 << lgseg) - 1) >> lgseg;
   for (int t = threadIdx.x; t < (rows << lgseg); t += blockDim.x) {
     const int r = t >> lgseg;
