@@ -371,7 +371,11 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
 // (grandchild row i of a parent, a column segment, all four grandchildren) forms the child
 // entries it needs itself, so the pair takes two barriers and never stores the children.
 // (Items that formed the pivot quantities themselves, six reciprocals each, with one
-// barrier per pair, were 4-13 % slower at orders 6-10.)
+// barrier per pair, were 4-13 % slower at orders 6-10. A pre-pass that also formed the
+// grandchildren's pivot rows, so that an item of one row and one first pivot b does three
+// complex products per column instead of ten for both b, was 4 % slower at order 8 and
+// 6-10 % at orders 9-10 with the same sums: the items then load four entries per three
+// products instead of five per ten.)
 __device__ void tree_level4(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int nodes,
                             int lg_npp, int m, double floor_, double2 *pv) {
   const int mg = m - 4, mm = m * m, mgg = mg * mg;
