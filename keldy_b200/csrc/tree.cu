@@ -368,14 +368,15 @@ __device__ void tree_level2(const double2 *cur, double2 *nxt, const double2 *Dc,
 // 4 par + 2 b + bp (pivot on row b, then on row bp of that child), (m-4) x (m-4) each,
 // every entry formed exactly as two tree_level2 steps form it. A pre-pass forms each
 // parent's pivot quantities once (one thread per (parent, b, b'), into pv); then each item
-// (grandchild row i of a parent, a column segment, all four grandchildren) forms the child
-// entries it needs itself, so the pair takes two barriers and never stores the children.
-// (Items that formed the pivot quantities themselves, six reciprocals each, with one
-// barrier per pair, were 4-13 % slower at orders 6-10. A pre-pass that also formed the
-// grandchildren's pivot rows, so that an item of one row and one first pivot b does three
-// complex products per column instead of ten for both b, was 4 % slower at order 8 and
-// 6-10 % at orders 9-10 with the same sums: the items then load four entries per three
-// products instead of five per ten.)
+// (grandchild row i of a parent, one first pivot b, a column segment) forms the entries of
+// child b it needs itself and writes row i of grandchildren (b, 0) and (b, 1), so the pair
+// takes two barriers and never stores the children. (Items of both first pivots, twice the
+// work per item and half the items, were 6 % slower at order 8 and 3-5 % at orders 6, 7,
+// 9 and 10: the first pair of a one-point sub-batch had 26 busy threads of 128. Items
+// that formed the pivot quantities themselves, six reciprocals each, with one barrier per
+// pair, were slower again, 4-13 % at orders 6-10. A pre-pass that also formed the
+// grandchildren's pivot rows, three complex products per column and item instead of five,
+// was slower as well: four loads per three products, less work in flight per thread.)
 __device__ void tree_level4(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int nodes,
                             int lg_npp, int m, double floor_, double2 *pv) {
   const int mg = m - 4, mm = m * m, mgg = mg * mg;
@@ -398,53 +399,43 @@ __device__ void tree_level4(const double2 *cur, double2 *nxt, const double2 *Dc,
   __syncthreads();
   const unsigned rows = (unsigned)(nodes * mg);
   const unsigned magic = 0xFFFFFFFFu / (unsigned)mg + 1u; // r / mg == umulhi(r, magic) for r < 2^20, mg <= 31
-  int lgseg = 0;
   // column segments of at least two columns while the CTA has idle threads; four for a
   // single node (a one-point sub-batch's first pair, orders 8 and up), where fewer, longer
-  // segments repeat each row's own quantities (Lr, the child-row entries, Lg) less often:
-  // 2.5-3 % faster there than two, while two stay faster when several nodes share the
-  // pair (1.5 % at order 7)
+  // segments repeat each item's own quantities (Lr, the child-row entries, Lg) less often
   const int minc = nodes == 1 ? 4 : 2;
-  while ((rows << (lgseg + 1)) <= blockDim.x && (mg >> (lgseg + 1)) >= minc) ++lgseg;
+  int lgseg = 0;
+  while (((2 * rows) << (lgseg + 1)) <= blockDim.x && (mg >> (lgseg + 1)) >= minc) ++lgseg;
   const int seglen = (mg + (1 << lgseg) - 1) >> lgseg;
-  const unsigned items = rows << lgseg;
+  const unsigned items = (2 * rows) << lgseg;
   for (unsigned t = threadIdx.x; t < items; t += blockDim.x) {
-    const unsigned r = t >> lgseg;
+    const unsigned rb2 = t >> lgseg;
     const int j0 = (int)(t & ((1u << lgseg) - 1)) * seglen, j1 = min(mg, j0 + seglen);
+    const int b = (int)(rb2 & 1u);
+    const unsigned r = rb2 >> 1;
     const unsigned par = __umulhi(r, magic);
     const int i = (int)(r - par * (unsigned)mg);
     const double2 *S = cur + par * mm;
-    double2 ib[2], Lp[2][2], icp[2][2], Lr[2], Lg[2][2];
-#pragma unroll
-    for (int b = 0; b < 2; ++b) {
-      ib[b] = pv[(par * 4 + 2 * b) * 3];
-      Lr[b] = cmul(S[(i + 4) * m + b], ib[b]);
-#pragma unroll
-      for (int bp = 0; bp < 2; ++bp) {
-        Lp[b][bp] = pv[(par * 4 + 2 * b + bp) * 3 + 1];
-        icp[b][bp] = pv[(par * 4 + 2 * b + bp) * 3 + 2];
-        const double2 cib = cfms(S[(i + 4) * m + 2 + bp], Lr[b], S[b * m + 2 + bp]); // child row i+2, column bp
-        Lg[b][bp] = cmul(cib, icp[b][bp]);
-      }
-    }
-    const double2 *sr = S + (i + 4) * m + 4, *s0 = S + 4, *s1 = S + m + 4, *s2 = S + 2 * m + 4, *s3 = S + 3 * m + 4;
-    double2 *o = nxt + (4 * par) * mgg + i * mg;
-#pragma unroll 2
+    const double2 ib = pv[(par * 4 + 2 * b) * 3];
+    const double2 Lr = cmul(S[(i + 4) * m + b], ib);
+    const double2 Lp0 = pv[(par * 4 + 2 * b) * 3 + 1], Lp1 = pv[(par * 4 + 2 * b + 1) * 3 + 1];
+    const double2 Lg0 = cmul(cfms(S[(i + 4) * m + 2], Lr, S[b * m + 2]), pv[(par * 4 + 2 * b) * 3 + 2]);
+    const double2 Lg1 = cmul(cfms(S[(i + 4) * m + 3], Lr, S[b * m + 3]), pv[(par * 4 + 2 * b + 1) * 3 + 2]);
+    const double2 *sr = S + (i + 4) * m + 4, *sb = S + b * m + 4, *s2 = S + 2 * m + 4, *s3 = S + 3 * m + 4;
+    double2 *o = nxt + (4 * par + 2 * b) * mgg + i * mg;
+    // (unrolled by 2 the kernel spilled five times as many bytes and ran 3-16 % slower)
+#pragma unroll 3
     for (int j = j0; j < j1; ++j) {
-      const double2 v = sr[j], a0 = s0[j], a1 = s1[j], a2 = s2[j], a3 = s3[j];
-#pragma unroll
-      for (int b = 0; b < 2; ++b) {
-        const double2 pb = b ? a1 : a0;
-        const double2 cij = cfms(v, Lr[b], pb);            // child b, row i+2
-        const double2 c0 = cfms(a2, Lp[b][0], pb);         // child b, row 0 (pivot row of bp = 0)
-        const double2 c1 = cfms(a3, Lp[b][1], pb);         // child b, row 1
-        o[(2 * b) * mgg + j] = cfms(cij, Lg[b][0], c0);
-        o[(2 * b + 1) * mgg + j] = cfms(cij, Lg[b][1], c1);
-      }
+      const double2 v = sr[j], pb = sb[j], a2 = s2[j], a3 = s3[j];
+      const double2 cij = cfms(v, Lr, pb);  // child b, row i + 2
+      const double2 c0 = cfms(a2, Lp0, pb); // child b, row 0 (pivot row of b' = 0)
+      const double2 c1 = cfms(a3, Lp1, pb); // child b, row 1
+      o[j] = cfms(cij, Lg0, c0);
+      o[mgg + j] = cfms(cij, Lg1, c1);
     }
   }
   __syncthreads();
 }
+
 
 // One step down a fixed path (single point): pivot on row b, drop rows 0 and 1.
 __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *Dc, double2 *Dn, int *flag, int m,
