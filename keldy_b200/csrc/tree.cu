@@ -178,6 +178,10 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
   const double2 *trow = m.tab[spin][A.orbital][0];
   const double2 *tcol = m.tab[spin][0][B.orbital];
   const int total = np * per;
+  // r / per and q / (N - 1) as a multiply-high by 2^32 / d rounded up (exact for the
+  // quotients here: r < 2^16, d <= 289); mn1 wraps to 0 for N - 1 = 1 (q / 1 = q)
+  const unsigned mper = 0xFFFFFFFFu / (unsigned)per + 1u;
+  const unsigned mn1 = N > 1 ? 0xFFFFFFFFu / (unsigned)(N - 1) + 1u : 0u;
   for (int base = threadIdx.x; base < total; base += GK * blockDim.x) {
     int kind[GK], pi[GK], qi[GK], ix[GK];
     double wt[GK], dt[GK];
@@ -193,7 +197,7 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
       pi[k] = 0;
       qi[k] = 0;
       if (r >= total) continue;
-      const int p = r / per, q = r - p * per;
+      const int p = (int)__umulhi((unsigned)r, mper), q = r - p * per;
       pi[k] = p;
       qi[k] = q;
       const double *x = u + p;
@@ -202,7 +206,7 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
         continue;
       }
       if (q < npair) {
-        const int i = q / (N - 1), r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
+        const int i = mn1 ? (int)__umulhi((unsigned)q, mn1) : q, r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
         kind[k] = 1;
         dt[k] = x[i * np] - x[j * np];
         tb[k] = t00;
@@ -243,7 +247,7 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
       const int q = qi[k];
       const double *x = u + pi[k];
       if (kind[k] == 1) {
-        const int i = q / (N - 1), r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
+        const int i = mn1 ? (int)__umulhi((unsigned)q, mn1) : q, r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
         double2 *g = G + (2 * i) * M + 2 * j;
         const double d = dt[k];
         const bool later = (d != 0.0) ? (d > 0.0) : (i > j);
@@ -276,7 +280,7 @@ __device__ void build_G(const ItemDev &it, int N, int np, const double *u, const
       } else { // out of domain: identity blocks, zero externals
         const double2 z = c2(0.0, 0.0), one = c2(1.0, 0.0);
         if (q < npair) {
-          const int i = q / (N - 1), r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
+          const int i = mn1 ? (int)__umulhi((unsigned)q, mn1) : q, r2 = q - i * (N - 1), j = r2 + (r2 >= i ? 1 : 0);
           double2 *g = G + (2 * i) * M + 2 * j;
           g[0] = g[1] = g[M] = g[M + 1] = z;
         } else if (q < npair + N) {
