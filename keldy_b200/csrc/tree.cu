@@ -452,8 +452,9 @@ __device__ void tree_path_step(const double2 *cur, double2 *nxt, const double2 *
     if (!(cabs1(piv) >= floor_)) flag[0] |= 2;
     Dn[0] = cmul(Dc[0], piv);
   }
+  const unsigned magic = 0xFFFFFFFFu / (unsigned)mc + 1u; // r / mc == umulhi(r, magic) for r < 2^20, mc >= 2
   for (int r = threadIdx.x; r < mc * mc; r += blockDim.x) {
-    int i = r / mc, j = r - i * mc;
+    const int i = (int)__umulhi((unsigned)r, magic), j = r - i * mc;
     double2 Lf = cmul(cur[(i + 2) * m + b], inv);
     nxt[r] = cfms(cur[(i + 2) * m + j + 2], Lf, cur[b * m + j + 2]);
   }
@@ -1614,7 +1615,7 @@ __device__ void km_level(const double2 *cur, int cs, double2 *nxt, const double2
   const int R1 = R - 1, C1 = C - 2;
   const int nch = bsel < 0 ? 2 : 1;
   for (int c = threadIdx.x; c < nodes * nch; c += blockDim.x) {
-    const int par = c / nch, b = bsel < 0 ? (c & 1) : bsel;
+    const int par = bsel < 0 ? c >> 1 : c, b = bsel < 0 ? (c & 1) : bsel;
     const double2 piv = cur[par * cs + (j + b) * C + b];
     if (!(cabs1(piv) >= floor_)) flag[par >> lg_npp] |= 2;
     inv[c] = crcp(piv);
@@ -1629,10 +1630,11 @@ __device__ void km_level(const double2 *cur, int cs, double2 *nxt, const double2
   int lgseg = 0;
   while ((rows << (lgseg + 1)) <= (int)blockDim.x && (C1 >> (lgseg + 1)) >= minc) ++lgseg;
   const int seglen = (C1 + (1 << lgseg) - 1) >> lgseg;
+  const unsigned magic = 0xFFFFFFFFu / (unsigned)R1 + 1u; // r / R1 == umulhi(r, magic) for r < 2^20, R1 >= 3
   for (int t = threadIdx.x; t < (rows << lgseg); t += blockDim.x) {
     const int r = t >> lgseg;
     const int q0 = (t & ((1 << lgseg) - 1)) * seglen, q1 = min(C1, q0 + seglen);
-    const int par = r / R1, ri = r - par * R1;
+    const int par = (int)__umulhi((unsigned)r, magic), ri = r - par * R1;
     const double2 *S = cur + par * cs;
     for (int k = 0; k < nch; ++k) {
       const int b = bsel < 0 ? k : bsel;
